@@ -1,0 +1,186 @@
+/* pvb200.h — C ABI of the B200-native point-vortex backend (libpvb200.so).
+ *
+ * The library evaluates the direct O(N^2) Biot–Savart velocity of point vortices in the
+ * three geometries of jplaurie/PointVortex (infinite plane with core radius, Weiss–McWilliams
+ * periodic square box, disk with circle-theorem images) on an NVIDIA B200 (sm_100a), and runs
+ * the reference's RK4 and DOPRI5 steps with the state resident in GPU memory.
+ *
+ * Every entry point replaces one member of the reference's link-time backend interface
+ * (src/backend.h:9-16) or of its VelocityKernel class (src/compute.h:18-36); the comment above
+ * each one names it. Plain pointers and sizes only; all arrays are structure-of-arrays
+ * doubles (src/vortex.h:15-51). Unless stated otherwise pointers are HOST pointers.
+ *
+ * Errors: every function returns a pv_status. The codes map one to one onto the exception
+ * types the reference throws (std::invalid_argument, std::out_of_range, std::runtime_error,
+ * std::logic_error); pv_last_error() returns the message, which follows the reference's text.
+ *
+ * Threading: a context belongs to one host thread at a time. Work is ordered on the
+ * context's own CUDA stream; functions that return results to the host synchronise it.
+ */
+#ifndef PVB200_H
+#define PVB200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define PVB200_ABI_VERSION 1
+
+typedef enum pv_status {
+    PV_OK = 0,
+    PV_ERROR_INVALID_ARGUMENT = 1, /* std::invalid_argument */
+    PV_ERROR_OUT_OF_RANGE = 2,     /* std::out_of_range */
+    PV_ERROR_RUNTIME = 3,          /* std::runtime_error (non-finite, coincident, DOPRI5 failure) */
+    PV_ERROR_LOGIC = 4,            /* std::logic_error (hook used out of order) */
+    PV_ERROR_CUDA = 5              /* CUDA runtime failure; the message names the call */
+} pv_status;
+
+typedef enum pv_geometry {
+    PV_GEOMETRY_INFINITE = 0, /* boundaryCondition infinite (src/params.h:56) */
+    PV_GEOMETRY_PERIODIC = 1, /* boundaryCondition periodic */
+    PV_GEOMETRY_DISK = 2      /* boundaryCondition disk */
+} pv_geometry;
+
+typedef enum pv_precision {
+    PV_PRECISION_FP64 = 0, /* plain FP64 pair sums (the reference's arithmetic) */
+    PV_PRECISION_FP32C = 1 /* FP32 bulk pair sums, compensated, FP64 where cancellation needs it */
+} pv_precision;
+
+/* The SimParams fields (src/params.h:37-78) that the velocity path reads. */
+typedef struct pv_params {
+    int geometry;          /* pv_geometry */
+    double core_radius;    /* coreRadius (infinite plane only) */
+    double box_length_x;   /* boxLengthX (periodic) */
+    double box_length_y;   /* boxLengthY (periodic; must equal boxLengthX) */
+    int image_layers;      /* periodicImageLayers, 0..64 */
+    double disk_radius;    /* diskRadius (disk) */
+    int precision;         /* pv_precision */
+} pv_params;
+
+/* StepResult, src/compute.h:11-16 */
+typedef struct pv_step_result {
+    double accepted_time_step;
+    double suggested_time_step;
+    double normalized_error;
+    unsigned rejected_steps;
+} pv_step_result;
+
+/* One close-dipole candidate of DipoleManager::process (src/dipole.cpp:49-78):
+ * second == population marks a disk wall-image candidate. */
+typedef struct pv_dipole_candidate {
+    uint64_t first;
+    uint64_t second;
+    double distance_squared;
+} pv_dipole_candidate;
+
+typedef struct pv_context pv_context;
+
+/* ---- lifecycle -------------------------------------------------------------------------- */
+
+/* makeBackendKernel (src/backend.h:16) with the kernel constructors' validation
+ * (src/compute.cpp:50-56, 165-173, 258-261). device: CUDA ordinal. */
+pv_status pv_context_create(const pv_params *params, int device, pv_context **out);
+/* ~VelocityKernel; frees every device buffer of the context. */
+void pv_context_destroy(pv_context *ctx);
+/* Message of the last failure on ctx, or of the calling thread's last pv_context_create
+ * failure when ctx is NULL. Valid until the next call on the same context/thread. */
+const char *pv_last_error(const pv_context *ctx);
+/* backendName (src/backend.h:13). */
+const char *pv_backend_name(void);
+/* backendRuntimeDetails (src/backend.h:14): "key value" lines, NUL-terminated in buf. */
+pv_status pv_runtime_details(int device, char *buf, size_t len);
+
+/* ---- host-array evaluation ---------------------------------------------------------------- */
+
+/* VelocityKernel::evaluateRange (src/compute.h:26-28; src/compute.cpp:88, 203, 286):
+ * velocities of targets [begin, end) due to all n sources, written to u[0..end-begin) and
+ * v[0..end-begin). Does not touch the context's device-resident state. */
+pv_status pv_evaluate_range(pv_context *ctx, const double *x, const double *y,
+                            const double *circulation, size_t n, size_t begin, size_t end,
+                            double *u, double *v);
+/* VelocityKernel::evaluate (src/compute.cpp:57-69): full range plus the finiteness check. */
+pv_status pv_evaluate(pv_context *ctx, const double *x, const double *y,
+                      const double *circulation, size_t n, double *u, double *v);
+/* VelocityKernel::hamiltonian (src/compute.h:29): computed on the GPU. */
+pv_status pv_hamiltonian(pv_context *ctx, const double *x, const double *y,
+                         const double *circulation, size_t n, double *hamiltonian);
+/* computeInvariants(vortices, kernel) (src/compute.cpp:157-163):
+ * out[0..4] = circulation, linear impulse x, linear impulse y, angular impulse, Hamiltonian. */
+pv_status pv_invariants(pv_context *ctx, const double *x, const double *y,
+                        const double *circulation, size_t n, double out[5]);
+
+/* ---- device-resident state (the VelocityKernel device-stepping hooks) --------------------- */
+
+/* uploadDeviceState (src/compute.h:31). Validates like the reference (finite data; periodic
+ * zero total circulation; disk positions inside). Invalidates the DOPRI5 FSAL derivative. */
+pv_status pv_upload_state(pv_context *ctx, const double *x, const double *y,
+                          const double *circulation, size_t n);
+/* downloadDeviceState (src/compute.h:32): n must equal the uploaded population. */
+pv_status pv_download_state(pv_context *ctx, double *x, double *y, size_t n);
+/* evaluateDeviceState (src/compute.h:33): velocities of the device state. */
+pv_status pv_evaluate_state(pv_context *ctx, double *u, double *v, size_t n);
+/* deviceRk4Step (src/compute.h:34); semantics of RungeKuttaIntegrator::rk4Step
+ * (src/timestep.cpp:31-61). The state is unchanged when the step fails. */
+pv_status pv_rk4_step(pv_context *ctx, double dt);
+/* deviceDopri5Step (src/compute.h:35); semantics of RungeKuttaIntegrator::dopri5Step
+ * (src/timestep.cpp:62-120): FSAL, max-norm error, step-size control and rejections all run
+ * on the GPU; one host synchronisation per attempt. */
+pv_status pv_dopri5_step(pv_context *ctx, double dt, double absolute_tolerance,
+                         double relative_tolerance, double minimum_time_step,
+                         double maximum_time_step, pv_step_result *result);
+/* invalidateDeviceDerivative (src/compute.h:36). */
+pv_status pv_invalidate_derivative(pv_context *ctx);
+/* computeInvariants of the device state (src/compute.cpp:157-163), out as pv_invariants. */
+pv_status pv_state_invariants(pv_context *ctx, double out[5]);
+/* The candidate scan of DipoleManager::process (src/dipole.cpp:49-78) on the device state:
+ * opposite-sign pairs closer than threshold (minimum image in the periodic box) and, in a disk,
+ * wall-image candidates. Writes min(count, capacity) candidates in no particular order;
+ * *count is the full number. count == 0 means process() would return 0 without touching its
+ * random generator (src/dipole.cpp:101-102), so a driver may skip the download. */
+pv_status pv_dipole_scan(pv_context *ctx, double threshold, pv_dipole_candidate *out,
+                         size_t capacity, size_t *count);
+/* Population of the device state. */
+pv_status pv_state_size(const pv_context *ctx, size_t *n);
+/* Velocity evaluations made so far by the stepping hooks (the reference's CountingKernel,
+ * tests/tests.cpp:281-296, counts the same events). */
+pv_status pv_evaluation_count(const pv_context *ctx, uint64_t *count);
+
+/* ---- multi-step device loops (no reference counterpart: the reference's driver calls one
+ *      step at a time, src/main.cpp:292-308) ------------------------------------------------- */
+
+/* `steps` RK4 steps of size dt, enqueued back to back with one synchronisation at the end. */
+pv_status pv_rk4_advance(pv_context *ctx, double dt, uint64_t steps);
+
+/* ---- diagnostics (no reference counterpart) --------------------------------------------- */
+
+/* Kernel kinds counted by pv_get_kernel_stats. */
+#define PV_KERNEL_VELOCITY 0   /* tiled pair-sum kernel */
+#define PV_KERNEL_STAGE 1      /* chunk reduction + stage position / combine / error + control */
+#define PV_KERNEL_ACCEPT 2     /* state update of an accepted step */
+#define PV_KERNEL_INVARIANTS 3 /* moments, Hamiltonian tiles, final sum */
+#define PV_KERNEL_DIPOLE 4     /* close-dipole candidate scan */
+#define PV_KERNEL_KINDS 5
+
+typedef struct pv_kernel_stats {
+    uint64_t launches[PV_KERNEL_KINDS];       /* kernels launched by this context */
+    uint64_t timed_launches[PV_KERNEL_KINDS]; /* launches bracketed by CUDA events */
+    double milliseconds[PV_KERNEL_KINDS];     /* summed event time of the timed launches */
+} pv_kernel_stats;
+
+/* Bracket every launch of the context with CUDA events recorded on its own stream. */
+pv_status pv_set_profiling(pv_context *ctx, int enabled);
+/* Synchronises the context stream and returns the counters accumulated since the last reset. */
+pv_status pv_get_kernel_stats(pv_context *ctx, pv_kernel_stats *out);
+pv_status pv_reset_kernel_stats(pv_context *ctx);
+
+/* Arithmetic peak of `device` at its current clocks, measured with independent FMA chains on
+ * every SM: kind 0 = FP64 FMA, 1 = FP32 FMA. *flops_per_second = 2 x FMAs / elapsed time. */
+pv_status pv_probe_peak(int device, int kind, double *flops_per_second);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

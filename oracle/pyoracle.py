@@ -1,0 +1,277 @@
+"""ctypes access to the CPU checkers.
+
+TEST INFRASTRUCTURE ONLY. Imported by tests/, ``__graft_entry__.smoke()`` and the CPU-baseline
+leg of ``bench.py``; the product package never imports it.
+
+Two checkers share one interface:
+
+* ``Oracle("port")``      -- oracle/liboracle_pv.so, the C restatement (pv_oracle.c);
+* ``Oracle("reference")`` -- oracle/_ref/libpvref.so, the unmodified reference compiled from its
+  own sources (oracle/Makefile, target ``ref``) behind ref_shim.cpp.
+
+Both raise the Python analogue of the reference's exception type: ValueError for
+std::invalid_argument, IndexError for std::out_of_range, RuntimeError for std::runtime_error.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+from dataclasses import dataclass
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+PORT_LIB = os.path.join(HERE, "liboracle_pv.so")
+REF_LIB = os.path.join(HERE, "_ref", "libpvref.so")
+REF_CUDA_LIB = os.path.join(HERE, "_ref", "libpvref_cuda.so")
+REF_DIR = os.path.join(HERE, "_ref")
+
+GEOMETRIES = {"infinite": 0, "periodic": 1, "disk": 2}
+
+
+class _Params(ctypes.Structure):
+    _fields_ = [
+        ("geometry", ctypes.c_int),
+        ("core_radius", ctypes.c_double),
+        ("box_length_x", ctypes.c_double),
+        ("box_length_y", ctypes.c_double),
+        ("image_layers", ctypes.c_int),
+        ("disk_radius", ctypes.c_double),
+        ("absolute_tolerance", ctypes.c_double),
+        ("relative_tolerance", ctypes.c_double),
+        ("minimum_time_step", ctypes.c_double),
+        ("maximum_time_step", ctypes.c_double),
+        ("dipole_removal", ctypes.c_int),
+        ("dipole_removal_distance", ctypes.c_double),
+        ("dipole_reinjection", ctypes.c_int),
+        ("random_seed", ctypes.c_uint64),
+    ]
+
+
+class _Candidate(ctypes.Structure):
+    _fields_ = [("first", ctypes.c_size_t), ("second", ctypes.c_size_t),
+                ("distance_squared", ctypes.c_double)]
+
+
+@dataclass
+class Geometry:
+    """Parameters of one simulation (the fields of the reference's SimParams that the hot path
+    reads; defaults follow src/params.h:37-78)."""
+
+    boundary: str = "infinite"
+    core_radius: float = 0.0
+    box_length_x: float = 2.0
+    box_length_y: float = 2.0
+    image_layers: int = 8
+    disk_radius: float = 1.0
+    absolute_tolerance: float = 1e-10
+    relative_tolerance: float = 1e-8
+    minimum_time_step: float = 1e-12
+    maximum_time_step: float = 0.1
+    dipole_removal: bool = False
+    dipole_removal_distance: float = 0.01
+    dipole_reinjection: int = 0
+    random_seed: int = 1234567
+
+    def c(self) -> _Params:
+        return _Params(GEOMETRIES[self.boundary], self.core_radius, self.box_length_x,
+                       self.box_length_y, self.image_layers, self.disk_radius,
+                       self.absolute_tolerance, self.relative_tolerance, self.minimum_time_step,
+                       self.maximum_time_step, int(self.dipole_removal),
+                       self.dipole_removal_distance, self.dipole_reinjection, self.random_seed)
+
+
+_EXC = {1: ValueError, 2: IndexError, 3: RuntimeError, 4: NotImplementedError, 9: RuntimeError}
+_D = ctypes.POINTER(ctypes.c_double)
+
+
+def _p(a: np.ndarray):
+    return a.ctypes.data_as(_D)
+
+
+def build(reference: bool = False) -> None:
+    """Compile the checker(s) with oracle/Makefile (the reference only where its sources are)."""
+    subprocess.run(["make", "-s", "-C", HERE], check=True)
+    if reference:
+        subprocess.run(["make", "-s", "-C", HERE, "ref"], check=True)
+
+
+class Oracle:
+    """One CPU checker. ``kind`` is "port" (the C restatement) or "reference"."""
+
+    def __init__(self, kind: str = "port"):
+        self.kind = kind
+        path = PORT_LIB if kind == "port" else REF_LIB
+        if not os.path.exists(path):
+            raise FileNotFoundError(f"{path} is missing; run make -C oracle{' ref' if kind != 'port' else ''}")
+        lib = ctypes.CDLL(path)
+        self.lib = lib
+        pre = "pvo_" if kind == "port" else "pvref_"
+        self._pre = pre
+        getattr(lib, pre + "last_error").restype = ctypes.c_char_p
+        sz = ctypes.c_size_t
+        P = ctypes.POINTER(_Params)
+        getattr(lib, pre + "evaluate_range").argtypes = [P, _D, _D, _D, sz, sz, sz, _D, _D]
+        getattr(lib, pre + "hamiltonian").argtypes = [P, _D, _D, _D, sz, _D]
+        getattr(lib, pre + "invariants").argtypes = [P, _D, _D, _D, sz, _D]
+        getattr(lib, pre + "stepper_create").argtypes = [P, sz]
+        getattr(lib, pre + "stepper_create").restype = ctypes.c_void_p
+        getattr(lib, pre + "stepper_destroy").argtypes = [ctypes.c_void_p]
+        getattr(lib, pre + "stepper_invalidate").argtypes = [ctypes.c_void_p]
+        if kind == "port":
+            lib.pvo_evaluate.argtypes = [P, _D, _D, _D, sz, _D, _D]
+            lib.pvo_rk4_step.argtypes = [ctypes.c_void_p, _D, _D, _D, sz, ctypes.c_double]
+            lib.pvo_dopri5_step.argtypes = [ctypes.c_void_p, _D, _D, _D, sz, ctypes.c_double, _D]
+            lib.pvo_stepper_evaluations.argtypes = [ctypes.c_void_p]
+            lib.pvo_stepper_evaluations.restype = sz
+            lib.pvo_dipole_scan.argtypes = [P, _D, _D, _D, sz, ctypes.POINTER(_Candidate), sz,
+                                            ctypes.POINTER(sz)]
+        else:
+            lib.pvref_rk4_steps.argtypes = [ctypes.c_void_p, _D, _D, _D, sz, ctypes.c_double, sz]
+            lib.pvref_dopri5_step.argtypes = [ctypes.c_void_p, _D, _D, _D, sz, ctypes.c_double, _D]
+            lib.pvref_dipole_process.argtypes = [P, _D, _D, _D, ctypes.POINTER(sz), sz,
+                                                 ctypes.POINTER(sz)]
+            lib.pvref_max_threads.restype = ctypes.c_int
+            lib.pvref_set_threads.argtypes = [ctypes.c_int]
+
+    def _check(self, rc: int) -> None:
+        if rc:
+            msg = getattr(self.lib, self._pre + "last_error")().decode()
+            raise _EXC.get(rc, RuntimeError)(msg)
+
+    @staticmethod
+    def _arrays(x, y, g):
+        x = np.ascontiguousarray(x, dtype=np.float64)
+        y = np.ascontiguousarray(y, dtype=np.float64)
+        g = np.ascontiguousarray(g, dtype=np.float64)
+        if not (x.shape == y.shape == g.shape):
+            raise ValueError("vortex arrays have different lengths")
+        return x, y, g
+
+    def evaluate(self, geo: Geometry, x, y, g):
+        """VelocityKernel::evaluate (src/compute.cpp:60-69): full range + finiteness check."""
+        x, y, g = self._arrays(x, y, g)
+        n = x.size
+        u = np.empty(n)
+        v = np.empty(n)
+        par = geo.c()
+        if self.kind == "port":
+            self._check(self.lib.pvo_evaluate(ctypes.byref(par), _p(x), _p(y), _p(g), n, _p(u), _p(v)))
+        else:
+            self._check(self.lib.pvref_evaluate_range(ctypes.byref(par), _p(x), _p(y), _p(g), n, 0, n,
+                                                      _p(u), _p(v)))
+        return u, v
+
+    def evaluate_range(self, geo: Geometry, x, y, g, begin: int, end: int):
+        """VelocityKernel::evaluateRange (src/compute.h:26-28); returns u, v for [begin, end)."""
+        x, y, g = self._arrays(x, y, g)
+        k = max(end - begin, 0)
+        u = np.empty(max(k, 1))
+        v = np.empty(max(k, 1))
+        par = geo.c()
+        self._check(getattr(self.lib, self._pre + "evaluate_range")(ctypes.byref(par), _p(x), _p(y), _p(g),
+                                                           x.size, begin, end, _p(u), _p(v)))
+        return u[:k], v[:k]
+
+    def hamiltonian(self, geo: Geometry, x, y, g) -> float:
+        x, y, g = self._arrays(x, y, g)
+        out = np.zeros(1)
+        par = geo.c()
+        self._check(getattr(self.lib, self._pre + "hamiltonian")(ctypes.byref(par), _p(x), _p(y), _p(g),
+                                                        x.size, _p(out)))
+        return float(out[0])
+
+    def invariants(self, geo: Geometry, x, y, g) -> np.ndarray:
+        """computeInvariants: [circulation, Ix, Iy, angular impulse, Hamiltonian]."""
+        x, y, g = self._arrays(x, y, g)
+        out = np.zeros(5)
+        par = geo.c()
+        self._check(getattr(self.lib, self._pre + "invariants")(ctypes.byref(par), _p(x), _p(y), _p(g),
+                                                       x.size, _p(out)))
+        return out
+
+    def stepper(self, geo: Geometry, n: int) -> "Stepper":
+        return Stepper(self, geo, n)
+
+    def dipole_scan(self, geo: Geometry, x, y, g):
+        """Candidate list of DipoleManager::process (src/dipole.cpp:49-78), in scan order, as an
+        (k, 3) array of (first, second, distance^2); second == n marks a disk wall image."""
+        if self.kind != "port":
+            raise NotImplementedError("the reference exposes the scan only inside process()")
+        x, y, g = self._arrays(x, y, g)
+        par = geo.c()
+        count = ctypes.c_size_t(0)
+        cap = 1024
+        while True:
+            buf = (_Candidate * cap)()
+            self._check(self.lib.pvo_dipole_scan(ctypes.byref(par), _p(x), _p(y), _p(g), x.size,
+                                                 buf, cap, ctypes.byref(count)))
+            if count.value <= cap:
+                break
+            cap = count.value
+        return [(buf[i].first, buf[i].second, buf[i].distance_squared) for i in range(count.value)]
+
+    def dipole_process(self, geo: Geometry, x, y, g):
+        """DipoleManager::process on a fresh manager; returns (events, x, y, g) (reference only)."""
+        if self.kind == "port":
+            raise NotImplementedError("selection and reinjection are host logic of the reference")
+        x, y, g = (np.array(a, dtype=np.float64) for a in (x, y, g))
+        n = ctypes.c_size_t(x.size)
+        cap = x.size
+        xx, yy, gg = (np.resize(a, max(cap, 1)).copy() for a in (x, y, g))
+        events = ctypes.c_size_t(0)
+        par = geo.c()
+        self._check(self.lib.pvref_dipole_process(ctypes.byref(par), _p(xx), _p(yy), _p(gg),
+                                                  ctypes.byref(n), cap, ctypes.byref(events)))
+        k = n.value
+        return events.value, xx[:k].copy(), yy[:k].copy(), gg[:k].copy()
+
+    def set_threads(self, n: int) -> None:
+        if self.kind != "port":
+            self.lib.pvref_set_threads(n)
+
+    def max_threads(self) -> int:
+        return self.lib.pvref_max_threads() if self.kind != "port" else 1
+
+
+class Stepper:
+    """RungeKuttaIntegrator (src/timestep.h:18-34) of one checker; keeps the FSAL derivative."""
+
+    def __init__(self, oracle: Oracle, geo: Geometry, n: int):
+        self.o = oracle
+        self.geo = geo
+        self._par = geo.c()
+        self.h = getattr(oracle.lib, oracle._pre + "stepper_create")(ctypes.byref(self._par), n)
+        if not self.h:
+            oracle._check(1)
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            getattr(self.o.lib, self.o._pre + "stepper_destroy")(self.h)
+            self.h = None
+
+    def invalidate(self) -> None:
+        getattr(self.o.lib, self.o._pre + "stepper_invalidate")(self.h)
+
+    def rk4_step(self, x, y, g, dt: float):
+        x, y, g = (np.array(a, dtype=np.float64) for a in (x, y, g))
+        if self.o.kind == "port":
+            self.o._check(self.o.lib.pvo_rk4_step(self.h, _p(x), _p(y), _p(g), x.size, dt))
+        else:
+            self.o._check(self.o.lib.pvref_rk4_steps(self.h, _p(x), _p(y), _p(g), x.size, dt, 1))
+        return x, y
+
+    def dopri5_step(self, x, y, g, dt: float):
+        """Returns (x, y, [accepted dt, suggested dt, error, rejected])."""
+        x, y, g = (np.array(a, dtype=np.float64) for a in (x, y, g))
+        out = np.zeros(4)
+        fn = self.o.lib.pvo_dopri5_step if self.o.kind == "port" else self.o.lib.pvref_dopri5_step
+        self.o._check(fn(self.h, _p(x), _p(y), _p(g), x.size, dt, _p(out)))
+        return x, y, out
+
+    @property
+    def evaluations(self) -> int:
+        if self.o.kind != "port":
+            raise NotImplementedError
+        return int(self.o.lib.pvo_stepper_evaluations(self.h))

@@ -1,0 +1,32 @@
+"""pointvortex_b200 — B200-native direct O(N^2) point-vortex velocity and RK4/DOPRI5 stepping.
+
+The compute path is libpvb200.so (hand-written sm_100a CUDA behind the C ABI of
+include/pvb200.h); this package is its host-side mirror of the reference's VelocityKernel
+interface. Importing it without the built library raises ImportError.
+"""
+from .kernel import (  # noqa: F401
+    CudaError,
+    DiskKernel,
+    DipoleCandidate,
+    InfinitePlaneKernel,
+    Invariants,
+    LogicError,
+    PeriodicBoxKernel,
+    StepResult,
+    VelocityField,
+    VelocityKernel,
+    VortexSystem,
+    backendName,
+    backendRuntimeDetails,
+    computeInvariants,
+    makeBackendKernel,
+    probePeak,
+)
+from ._lib import LIB_PATH  # noqa: F401
+
+__all__ = [
+    "CudaError", "DiskKernel", "DipoleCandidate", "InfinitePlaneKernel", "Invariants",
+    "LogicError", "PeriodicBoxKernel", "StepResult", "VelocityField", "VelocityKernel",
+    "VortexSystem", "backendName", "backendRuntimeDetails", "computeInvariants",
+    "makeBackendKernel", "probePeak", "LIB_PATH",
+]

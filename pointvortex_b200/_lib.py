@@ -1,0 +1,117 @@
+"""ctypes binding of libpvb200.so (the C ABI declared in include/pvb200.h).
+
+The shared library is built in-tree by ``python pointvortex_b200/build.py``. Importing this module
+without it raises ImportError: there is no CPU fallback.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libpvb200.so")
+
+PV_OK = 0
+PV_ERROR_INVALID_ARGUMENT = 1
+PV_ERROR_OUT_OF_RANGE = 2
+PV_ERROR_RUNTIME = 3
+PV_ERROR_LOGIC = 4
+PV_ERROR_CUDA = 5
+
+GEOMETRY_INFINITE = 0
+GEOMETRY_PERIODIC = 1
+GEOMETRY_DISK = 2
+PRECISION_FP64 = 0
+PRECISION_FP32C = 1
+
+
+class PvParams(ctypes.Structure):
+    _fields_ = [
+        ("geometry", ctypes.c_int),
+        ("core_radius", ctypes.c_double),
+        ("box_length_x", ctypes.c_double),
+        ("box_length_y", ctypes.c_double),
+        ("image_layers", ctypes.c_int),
+        ("disk_radius", ctypes.c_double),
+        ("precision", ctypes.c_int),
+    ]
+
+
+class PvStepResult(ctypes.Structure):
+    _fields_ = [
+        ("accepted_time_step", ctypes.c_double),
+        ("suggested_time_step", ctypes.c_double),
+        ("normalized_error", ctypes.c_double),
+        ("rejected_steps", ctypes.c_uint),
+    ]
+
+
+class PvDipoleCandidate(ctypes.Structure):
+    _fields_ = [
+        ("first", ctypes.c_uint64),
+        ("second", ctypes.c_uint64),
+        ("distance_squared", ctypes.c_double),
+    ]
+
+
+KERNEL_KINDS = ("velocity", "stage", "accept", "invariants", "dipole")
+
+
+class PvKernelStats(ctypes.Structure):
+    _fields_ = [
+        ("launches", ctypes.c_uint64 * 5),
+        ("timed_launches", ctypes.c_uint64 * 5),
+        ("milliseconds", ctypes.c_double * 5),
+    ]
+
+
+_D = ctypes.POINTER(ctypes.c_double)
+_SZ = ctypes.c_size_t
+_CTX = ctypes.c_void_p
+_ST = ctypes.c_int
+
+# name -> (restype, argtypes): every function of include/pvb200.h
+SIGNATURES = {
+    "pv_context_create": (_ST, [ctypes.POINTER(PvParams), ctypes.c_int, ctypes.POINTER(_CTX)]),
+    "pv_context_destroy": (None, [_CTX]),
+    "pv_last_error": (ctypes.c_char_p, [_CTX]),
+    "pv_backend_name": (ctypes.c_char_p, []),
+    "pv_runtime_details": (_ST, [ctypes.c_int, ctypes.c_char_p, _SZ]),
+    "pv_evaluate_range": (_ST, [_CTX, _D, _D, _D, _SZ, _SZ, _SZ, _D, _D]),
+    "pv_evaluate": (_ST, [_CTX, _D, _D, _D, _SZ, _D, _D]),
+    "pv_hamiltonian": (_ST, [_CTX, _D, _D, _D, _SZ, _D]),
+    "pv_invariants": (_ST, [_CTX, _D, _D, _D, _SZ, _D]),
+    "pv_upload_state": (_ST, [_CTX, _D, _D, _D, _SZ]),
+    "pv_download_state": (_ST, [_CTX, _D, _D, _SZ]),
+    "pv_evaluate_state": (_ST, [_CTX, _D, _D, _SZ]),
+    "pv_rk4_step": (_ST, [_CTX, ctypes.c_double]),
+    "pv_dopri5_step": (_ST, [_CTX, ctypes.c_double, ctypes.c_double, ctypes.c_double,
+                             ctypes.c_double, ctypes.c_double, ctypes.POINTER(PvStepResult)]),
+    "pv_invalidate_derivative": (_ST, [_CTX]),
+    "pv_state_invariants": (_ST, [_CTX, _D]),
+    "pv_dipole_scan": (_ST, [_CTX, ctypes.c_double, ctypes.POINTER(PvDipoleCandidate), _SZ,
+                             ctypes.POINTER(_SZ)]),
+    "pv_state_size": (_ST, [_CTX, ctypes.POINTER(_SZ)]),
+    "pv_evaluation_count": (_ST, [_CTX, ctypes.POINTER(ctypes.c_uint64)]),
+    "pv_rk4_advance": (_ST, [_CTX, ctypes.c_double, ctypes.c_uint64]),
+    "pv_probe_peak": (_ST, [ctypes.c_int, ctypes.c_int, _D]),
+    "pv_set_profiling": (_ST, [_CTX, ctypes.c_int]),
+    "pv_get_kernel_stats": (_ST, [_CTX, ctypes.POINTER(PvKernelStats)]),
+    "pv_reset_kernel_stats": (_ST, [_CTX]),
+}
+
+
+def load(path: str = LIB_PATH) -> ctypes.CDLL:
+    if not os.path.exists(path):
+        raise ImportError(
+            f"{path} is missing: build the CUDA library with `python pointvortex_b200/build.py` "
+            "(there is no CPU fallback)")
+    lib = ctypes.CDLL(path)
+    for name, (res, args) in SIGNATURES.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    return lib
+
+
+lib = load()

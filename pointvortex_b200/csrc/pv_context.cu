@@ -1,0 +1,1056 @@
+// pv_context.cu — host side of libpvb200: contexts, device buffers, the step flows and the C ABI
+// declared in include/pvb200.h.
+//
+// A context is the B200 counterpart of one VelocityKernel object of the reference
+// (src/compute.h:18-36) plus the device-stepping state the reference CUDA backend keeps in mutable
+// members (src/backend_cuda.cu:519-532). All device work of a context is ordered on its own
+// stream; results are read back at synchronisation points only (one per RK4 step / DOPRI5 attempt
+// / query), unlike the reference backend, which synchronises after every evaluation.
+#include "pvb200.h"
+#include "pv_internal.h"
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <string>
+#include <vector>
+
+using namespace pvb;
+
+namespace {
+
+thread_local std::string g_create_error;
+
+// Butcher rows of the Dormand–Prince pair, src/timestep.h:8-15, and the weights b5, b4 of
+// src/timestep.cpp:69-73, as the reference's constant expressions evaluate them.
+constexpr double kDopri[7][7] = {
+    {0},
+    {1.0 / 5.0},
+    {3.0 / 40.0, 9.0 / 40.0},
+    {44.0 / 45.0, -56.0 / 15.0, 32.0 / 9.0},
+    {19372.0 / 6561.0, -25360.0 / 2187.0, 64448.0 / 6561.0, -212.0 / 729.0},
+    {9017.0 / 3168.0, -355.0 / 33.0, 46732.0 / 5247.0, 49.0 / 176.0, -5103.0 / 18656.0},
+    {35.0 / 384.0, 0.0, 500.0 / 1113.0, 125.0 / 192.0, -2187.0 / 6784.0, 11.0 / 84.0}};
+constexpr double kB5[7] = {35.0 / 384.0,     0.0,         500.0 / 1113.0, 125.0 / 192.0,
+                           -2187.0 / 6784.0, 11.0 / 84.0, 0.0};
+constexpr double kB4[7] = {5179.0 / 57600.0, 0.0,          7571.0 / 16695.0,   393.0 / 640.0,
+                           -92097.0 / 339200.0, 187.0 / 2100.0, 1.0 / 40.0};
+
+// A growable device allocation.
+struct DeviceArray {
+    double *p = nullptr;
+    size_t cap = 0;
+    cudaError_t ensure(size_t n) {
+        if (n <= cap && p)
+            return cudaSuccess;
+        if (p)
+            cudaFree(p);
+        p = nullptr;
+        cap = 0;
+        const size_t want = std::max<size_t>(n, 64);
+        cudaError_t e = cudaMalloc(&p, want * sizeof(double));
+        if (e == cudaSuccess)
+            cap = want;
+        return e;
+    }
+    void release() {
+        if (p)
+            cudaFree(p);
+        p = nullptr;
+        cap = 0;
+    }
+};
+
+size_t padded(size_t n) { return (n + 255) & ~static_cast<size_t>(255); }
+
+bool finite_arrays(const double *x, const double *y, const double *g, size_t n) {
+    for (size_t i = 0; i < n; ++i)
+        if (!std::isfinite(x[i]) || !std::isfinite(y[i]) || !std::isfinite(g[i]))
+            return false;
+    return true;
+}
+
+} // namespace
+
+struct pv_context {
+    pv_params params{};
+    GeometryConsts gc{};
+    int device = 0;
+    int sm_count = 148;
+    cudaStream_t stream = nullptr;
+    std::string error;
+
+    // device-resident state
+    size_t n = 0;
+    bool state_valid = false;
+    bool fsal_valid = false;
+    uint64_t evaluations = 0;
+    EvalPlan plan{};
+    DeviceArray x, y, gamma, gs;     // state and scaled circulations
+    DeviceArray p0x, p0y, p1x, p1y;  // stage positions (ping-pong)
+    DeviceArray kx[7], ky[7];        // stage velocities
+    DeviceArray pu, pv;              // chunk partials
+    DeviceArray inv_scratch, inv_out;
+    DeviceArray cand;                // dipole candidates (3 doubles-worth each)
+    DeviceControl *ctl = nullptr;    // device control block
+    DeviceControl *ctl_host = nullptr; // pinned mirror
+    double *pinned = nullptr;        // pinned staging for small results (16 doubles)
+
+    // host-array evaluation (kept apart from the device state)
+    DeviceArray ex, ey, eg, egs, eu, ev, epu, epv;
+
+    // launch accounting and optional per-launch CUDA-event timing (pv_set_profiling)
+    bool profiling = false;
+    uint64_t launches[PV_KERNEL_KINDS] = {};
+    uint64_t timed[PV_KERNEL_KINDS] = {};
+    double milliseconds[PV_KERNEL_KINDS] = {};
+    struct Timer {
+        cudaEvent_t start, stop;
+        int kind;
+    };
+    std::vector<Timer> pending, pool;
+
+    ~pv_context() {
+        for (DeviceArray *a : {&x, &y, &gamma, &gs, &p0x, &p0y, &p1x, &p1y, &pu, &pv, &inv_scratch,
+                               &inv_out, &cand, &ex, &ey, &eg, &egs, &eu, &ev, &epu, &epv})
+            a->release();
+        for (int s = 0; s < 7; ++s) {
+            kx[s].release();
+            ky[s].release();
+        }
+        if (ctl)
+            cudaFree(ctl);
+        if (ctl_host)
+            cudaFreeHost(ctl_host);
+        if (pinned)
+            cudaFreeHost(pinned);
+        for (auto &t : pending)
+            pool.push_back(t);
+        for (auto &t : pool) {
+            cudaEventDestroy(t.start);
+            cudaEventDestroy(t.stop);
+        }
+        if (stream)
+            cudaStreamDestroy(stream);
+    }
+};
+
+namespace {
+
+// Keeps the caller's current device and restores it on exit.
+struct DeviceGuard {
+    int previous = -1;
+    bool ok = false;
+    explicit DeviceGuard(int device) {
+        if (cudaGetDevice(&previous) != cudaSuccess)
+            previous = -1;
+        ok = cudaSetDevice(device) == cudaSuccess;
+    }
+    ~DeviceGuard() {
+        if (previous >= 0)
+            cudaSetDevice(previous);
+    }
+};
+
+pv_status fail(pv_context *c, pv_status code, const std::string &message) {
+    c->error = message;
+    return code;
+}
+
+pv_status cuda_fail(pv_context *c, cudaError_t e, const char *what) {
+    return fail(c, PV_ERROR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+#define PV_CUDA(ctx, call)                                                                         \
+    do {                                                                                           \
+        cudaError_t e_ = (call);                                                                   \
+        if (e_ != cudaSuccess)                                                                     \
+            return cuda_fail((ctx), e_, #call);                                                    \
+    } while (0)
+
+// Runs `launch` (which enqueues `count` kernels of one kind on the context stream), counting the
+// launches and, when profiling is on, bracketing them with CUDA events on the same stream.
+template <class F> cudaError_t counted(pv_context *c, int kind, int count, F &&launch) {
+    c->launches[kind] += static_cast<uint64_t>(count);
+    if (!c->profiling)
+        return launch();
+    pv_context::Timer t{};
+    if (!c->pool.empty()) {
+        t = c->pool.back();
+        c->pool.pop_back();
+    } else {
+        cudaError_t e = cudaEventCreate(&t.start);
+        if (e == cudaSuccess)
+            e = cudaEventCreate(&t.stop);
+        if (e != cudaSuccess)
+            return e;
+    }
+    t.kind = kind;
+    cudaEventRecord(t.start, c->stream);
+    const cudaError_t e = launch();
+    cudaEventRecord(t.stop, c->stream);
+    c->pending.push_back(t);
+    return e;
+}
+
+// Folds the timings of completed launches into the totals (call after a stream synchronisation).
+void collect_timers(pv_context *c) {
+    for (auto &t : c->pending) {
+        float ms = 0.0f;
+        if (cudaEventElapsedTime(&ms, t.start, t.stop) == cudaSuccess) {
+            c->milliseconds[t.kind] += ms;
+            ++c->timed[t.kind];
+        }
+        c->pool.push_back(t);
+    }
+    c->pending.clear();
+}
+
+const char *coincident_message(int geometry, bool hamiltonian) {
+    if (geometry == GEO_PERIODIC)
+        return "coincident periodic vortices";
+    if (geometry == GEO_DISK)
+        return "coincident vortices in disk";
+    return hamiltonian ? "coincident vortices" : "coincident vortices in singular point-vortex kernel";
+}
+
+// Maps a device status word to the reference's exception type and message.
+pv_status status_error(pv_context *c, int status, bool hamiltonian = false) {
+    switch (status) {
+    case ST_OK:
+        return PV_OK;
+    case ST_NONFINITE_POSITION:
+        return fail(c, PV_ERROR_INVALID_ARGUMENT, "vortex data must be finite");
+    case ST_OUTSIDE_DISK:
+        return fail(c, PV_ERROR_INVALID_ARGUMENT, "vortex lies on or outside the disk");
+    case ST_COINCIDENT:
+        return fail(c, PV_ERROR_RUNTIME, coincident_message(c->params.geometry, hamiltonian));
+    case ST_NONFINITE_VELOCITY:
+        return fail(c, PV_ERROR_RUNTIME, "non-finite velocity; check scales and close encounters");
+    case ST_DOPRI_NONFINITE:
+        return fail(c, PV_ERROR_RUNTIME, "non-finite adaptive error estimate or invalid tolerance");
+    case ST_DOPRI_FAILED:
+        return fail(c, PV_ERROR_RUNTIME, "adaptive integrator could not satisfy tolerance");
+    case ST_NONFINITE_MOMENT:
+        return fail(c, PV_ERROR_RUNTIME, "non-finite vortex moment; check input scales");
+    case ST_NONFINITE_HAMILTONIAN:
+        return fail(c, PV_ERROR_RUNTIME, "non-finite Hamiltonian; check input scales");
+    case ST_OUTSIDE_DISK_H:
+        return fail(c, PV_ERROR_INVALID_ARGUMENT, "vortex outside disk");
+    case ST_TIMEOUT:
+        return fail(c, PV_ERROR_RUNTIME, "a bounded device wait timed out");
+    default:
+        return fail(c, PV_ERROR_RUNTIME, "device reported status " + std::to_string(status));
+    }
+}
+
+// Kernel constructors' validation (src/compute.cpp:50-56, 165-173, 258-261) and the derived
+// constants of the fast paths.
+pv_status make_consts(const pv_params &p, GeometryConsts &g, std::string &message) {
+    std::memset(&g, 0, sizeof(g));
+    g.geometry = p.geometry;
+    g.image_layers = p.image_layers;
+    if (p.precision != PV_PRECISION_FP64 && p.precision != PV_PRECISION_FP32C) {
+        message = "unsupported precision";
+        return PV_ERROR_INVALID_ARGUMENT;
+    }
+    if (p.geometry == PV_GEOMETRY_INFINITE) {
+        const double r = p.core_radius, r2 = r * r;
+        if (!(r >= 0.0) || !std::isfinite(r2) || (r > 0.0 && r2 == 0.0)) {
+            message = "core radius is negative or outside the supported numeric range";
+            return PV_ERROR_INVALID_ARGUMENT;
+        }
+        g.eps2 = r2;
+        return PV_OK;
+    }
+    if (p.geometry == PV_GEOMETRY_PERIODIC) {
+        const double lx = p.box_length_x, ly = p.box_length_y;
+        if (!(lx > 0.0) || !(ly > 0.0) || !std::isfinite(lx) || !std::isfinite(ly) ||
+            !std::isfinite(2.0 * kPi / lx) || p.image_layers < 0 || p.image_layers > 64) {
+            message = "invalid periodic-box parameters";
+            return PV_ERROR_INVALID_ARGUMENT;
+        }
+        if (std::fabs(lx - ly) > 1e-13 * std::max(lx, ly)) {
+            message = "Weiss-McWilliams kernel requires a square periodic box";
+            return PV_ERROR_INVALID_ARGUMENT;
+        }
+        g.lx = lx;
+        g.ly = ly;
+        g.inv_lx = 1.0 / lx;
+        g.inv_ly = 1.0 / ly;
+        g.half_lx = 0.5 * lx;
+        g.half_ly = 0.5 * ly;
+        g.wave = 2.0 * kPi / lx;
+        g.scale = 0.5 / lx;
+        g.m_pairs = std::min(p.image_layers, 5);
+        g.has6 = p.image_layers >= 6 ? 1 : 0;
+        for (int m = 0; m <= 5; ++m) {
+            const double a = 2.0 * kPi * m;
+            g.cosh_m[m] = std::cosh(a);
+            const double s = std::sinh(a);
+            g.sinh2_m[m] = s * s;
+        }
+        g.shift6 = 2.0 * kPi * static_cast<double>(6);
+        g.cosh6 = std::cosh(12.0 * kPi);
+        g.sinh6 = std::sinh(12.0 * kPi);
+        return PV_OK;
+    }
+    if (p.geometry == PV_GEOMETRY_DISK) {
+        const double r = p.disk_radius, r2 = r * r;
+        if (!(r > 0.0) || !std::isfinite(r2) || r2 == 0.0) {
+            message = "invalid disk parameters";
+            return PV_ERROR_INVALID_ARGUMENT;
+        }
+        g.radius = r;
+        g.radius2 = r2;
+        g.inv_radius = 1.0 / r;
+        g.inv_radius2 = 1.0 / r2;
+        return PV_OK;
+    }
+    message = "unsupported boundary condition";
+    return PV_ERROR_INVALID_ARGUMENT;
+}
+
+// Geometry validation of evaluateRange (src/compute.cpp:31-48, 211, 293).
+pv_status validate_geometry(pv_context *c, const double *x, const double *y, const double *g,
+                            size_t n) {
+    if (c->params.geometry == PV_GEOMETRY_PERIODIC) {
+        double total = 0.0, absolute_total = 0.0;
+        for (size_t i = 0; i < n; ++i) {
+            total += g[i];
+            absolute_total += std::fabs(g[i]);
+        }
+        if (std::fabs(total) > 1e-12 * std::max(1.0, absolute_total))
+            return fail(c, PV_ERROR_INVALID_ARGUMENT, "periodic box requires zero total circulation");
+    } else if (c->params.geometry == PV_GEOMETRY_DISK) {
+        for (size_t i = 0; i < n; ++i)
+            if (x[i] * x[i] + y[i] * y[i] >= c->gc.radius2)
+                return fail(c, PV_ERROR_INVALID_ARGUMENT, "vortex lies on or outside the disk");
+    }
+    return PV_OK;
+}
+
+pv_status reset_control(pv_context *c) {
+    std::memset(c->ctl_host, 0, sizeof(DeviceControl));
+    PV_CUDA(c, cudaMemcpyAsync(c->ctl, c->ctl_host, sizeof(DeviceControl), cudaMemcpyHostToDevice,
+                               c->stream));
+    return PV_OK;
+}
+
+pv_status read_control(pv_context *c) {
+    PV_CUDA(c, cudaMemcpyAsync(c->ctl_host, c->ctl, sizeof(DeviceControl), cudaMemcpyDeviceToHost,
+                               c->stream));
+    PV_CUDA(c, cudaStreamSynchronize(c->stream));
+    collect_timers(c);
+    return PV_OK;
+}
+
+std::vector<double> scaled(const GeometryConsts &g, const double *gamma, size_t n) {
+    std::vector<double> out(n);
+    for (size_t i = 0; i < n; ++i)
+        out[i] = scaled_circulation(g, gamma[i]);
+    return out;
+}
+
+// Velocity of the state positions (px, py) into k_s via partials + stage kernel.
+pv_status launch_eval(pv_context *c, const double *px, const double *py) {
+    EvalArgs a{};
+    a.tx = px;
+    a.ty = py;
+    a.sx = px;
+    a.sy = py;
+    a.sg = c->gs.p;
+    a.t_begin = 0;
+    a.t_end = c->n;
+    a.n_src = c->n;
+    a.pu = c->pu.p;
+    a.pv = c->pv.p;
+    a.stride = padded(c->n);
+    a.chunk = c->plan.chunk;
+    a.num_chunks = c->plan.num_chunks;
+    a.status = &c->ctl->status;
+    a.g = c->gc;
+    PV_CUDA(c, counted(c, PV_KERNEL_VELOCITY, 1, [&] { return launch_velocity(a, c->plan, c->stream); }));
+    ++c->evaluations;
+    return PV_OK;
+}
+
+StageArgs stage_base(pv_context *c) {
+    StageArgs s{};
+    s.n = c->n;
+    s.reduce = 1;
+    s.num_chunks = c->plan.num_chunks;
+    s.stride = padded(c->n);
+    s.pu = c->pu.p;
+    s.pv = c->pv.p;
+    for (int j = 0; j < 7; ++j) {
+        s.kx[j] = c->kx[j].p;
+        s.ky[j] = c->ky[j].p;
+    }
+    s.gamma = c->gamma.p;
+    s.n_src = c->n;
+    s.x0 = c->x.p;
+    s.y0 = c->y.p;
+    s.ctl = c->ctl;
+    s.g = c->gc;
+    return s;
+}
+
+pv_status ensure_state_capacity(pv_context *c, size_t n) {
+    const size_t np = padded(std::max<size_t>(n, 1));
+    for (DeviceArray *a : {&c->x, &c->y, &c->gamma, &c->gs, &c->p0x, &c->p0y, &c->p1x, &c->p1y})
+        PV_CUDA(c, a->ensure(np));
+    for (int s = 0; s < 7; ++s) {
+        PV_CUDA(c, c->kx[s].ensure(np));
+        PV_CUDA(c, c->ky[s].ensure(np));
+    }
+    c->plan = plan_evaluation(c->gc.geometry, n, n, c->sm_count);
+    const size_t partial = static_cast<size_t>(c->plan.num_chunks) * np;
+    PV_CUDA(c, c->pu.ensure(partial));
+    PV_CUDA(c, c->pv.ensure(partial));
+    return PV_OK;
+}
+
+pv_status require_state(pv_context *c) {
+    if (!c->state_valid)
+        return fail(c, PV_ERROR_LOGIC, "device state has not been uploaded");
+    return PV_OK;
+}
+
+// Host-array evaluation of targets [begin, end) (evaluateRange). nonfinite_is_error: the
+// VelocityKernel::evaluate finiteness check.
+pv_status evaluate_host(pv_context *c, const double *x, const double *y, const double *g, size_t n,
+                        size_t begin, size_t end, double *u, double *v, bool nonfinite_is_error) {
+    if (!finite_arrays(x, y, g, n))
+        return fail(c, PV_ERROR_INVALID_ARGUMENT, "vortex data must be finite");
+    if (begin > end || end > n)
+        return fail(c, PV_ERROR_OUT_OF_RANGE, "invalid target-vortex range");
+    pv_status st = validate_geometry(c, x, y, g, n);
+    if (st != PV_OK)
+        return st;
+    if (begin == end)
+        return PV_OK;
+    DeviceGuard guard(c->device);
+    const size_t np = padded(n);
+    const size_t nt = end - begin;
+    for (DeviceArray *a : {&c->ex, &c->ey, &c->eg, &c->egs})
+        PV_CUDA(c, a->ensure(np));
+    PV_CUDA(c, c->eu.ensure(padded(nt)));
+    PV_CUDA(c, c->ev.ensure(padded(nt)));
+    const EvalPlan plan = plan_evaluation(c->gc.geometry, nt, n, c->sm_count);
+    const size_t stride = padded(nt);
+    PV_CUDA(c, c->epu.ensure(static_cast<size_t>(plan.num_chunks) * stride));
+    PV_CUDA(c, c->epv.ensure(static_cast<size_t>(plan.num_chunks) * stride));
+    const std::vector<double> gs = scaled(c->gc, g, n);
+    const size_t bytes = n * sizeof(double);
+    PV_CUDA(c, cudaMemcpyAsync(c->ex.p, x, bytes, cudaMemcpyHostToDevice, c->stream));
+    PV_CUDA(c, cudaMemcpyAsync(c->ey.p, y, bytes, cudaMemcpyHostToDevice, c->stream));
+    PV_CUDA(c, cudaMemcpyAsync(c->eg.p, g, bytes, cudaMemcpyHostToDevice, c->stream));
+    PV_CUDA(c, cudaMemcpyAsync(c->egs.p, gs.data(), bytes, cudaMemcpyHostToDevice, c->stream));
+    if ((st = reset_control(c)) != PV_OK)
+        return st;
+    EvalArgs a{};
+    a.tx = c->ex.p;
+    a.ty = c->ey.p;
+    a.sx = c->ex.p;
+    a.sy = c->ey.p;
+    a.sg = c->egs.p;
+    a.t_begin = begin;
+    a.t_end = end;
+    a.n_src = n;
+    a.pu = c->epu.p;
+    a.pv = c->epv.p;
+    a.stride = stride;
+    a.chunk = plan.chunk;
+    a.num_chunks = plan.num_chunks;
+    a.status = &c->ctl->status;
+    a.g = c->gc;
+    PV_CUDA(c, counted(c, PV_KERNEL_VELOCITY, 1, [&] { return launch_velocity(a, plan, c->stream); }));
+    StageArgs s{};
+    s.n = nt;
+    s.mode = STAGE_REDUCE_ONLY;
+    s.reduce = 1;
+    s.num_chunks = plan.num_chunks;
+    s.stride = stride;
+    s.pu = c->epu.p;
+    s.pv = c->epv.p;
+    s.s = 0;
+    s.kx[0] = c->eu.p;
+    s.ky[0] = c->ev.p;
+    s.ex = c->ex.p;
+    s.ey = c->ey.p;
+    s.gamma = c->eg.p;
+    s.t_offset = begin;
+    s.n_src = n;
+    s.nonfinite_ok = nonfinite_is_error ? 0 : 1;
+    s.ctl = c->ctl;
+    s.g = c->gc;
+    PV_CUDA(c, counted(c, PV_KERNEL_STAGE, 1, [&] { return launch_stage(s, c->stream, c->sm_count); }));
+    PV_CUDA(c, cudaMemcpyAsync(u, c->eu.p, nt * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    PV_CUDA(c, cudaMemcpyAsync(v, c->ev.p, nt * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    if ((st = read_control(c)) != PV_OK)
+        return st;
+    return status_error(c, c->ctl_host->status);
+}
+
+pv_status invariants_of(pv_context *c, const double *x, const double *y, const double *g, size_t n,
+                        double out[5]) {
+    if (n == 0) {
+        for (int k = 0; k < 5; ++k)
+            out[k] = 0.0;
+        return PV_OK;
+    }
+    PV_CUDA(c, c->inv_scratch.ensure(invariants_scratch_doubles(n, c->sm_count)));
+    PV_CUDA(c, c->inv_out.ensure(8));
+    pv_status st = reset_control(c);
+    if (st != PV_OK)
+        return st;
+    PV_CUDA(c, counted(c, PV_KERNEL_INVARIANTS, 3, [&] {
+                return launch_invariants(x, y, g, n, c->gc, c->inv_scratch.p, c->inv_out.p,
+                                         &c->ctl->status, &c->ctl->status2, c->stream);
+            }));
+    PV_CUDA(c, cudaMemcpyAsync(c->pinned, c->inv_out.p, 5 * sizeof(double), cudaMemcpyDeviceToHost,
+                               c->stream));
+    if ((st = read_control(c)) != PV_OK)
+        return st;
+    if ((st = status_error(c, c->ctl_host->status)) != PV_OK)
+        return st;
+    if ((st = status_error(c, c->ctl_host->status2, true)) != PV_OK)
+        return st;
+    std::memcpy(out, c->pinned, 5 * sizeof(double));
+    return PV_OK;
+}
+
+} // namespace
+
+// =============================================================================================
+// C ABI
+// =============================================================================================
+extern "C" {
+
+pv_status pv_context_create(const pv_params *params, int device, pv_context **out) {
+    if (!out || !params) {
+        g_create_error = "null argument";
+        return PV_ERROR_INVALID_ARGUMENT;
+    }
+    *out = nullptr;
+    GeometryConsts gc;
+    std::string message;
+    pv_status st = make_consts(*params, gc, message);
+    if (st != PV_OK) {
+        g_create_error = message;
+        return st;
+    }
+    int count = 0;
+    cudaError_t e = cudaGetDeviceCount(&count);
+    if (e != cudaSuccess || device < 0 || device >= count) {
+        g_create_error = std::string("cudaGetDeviceCount: ") +
+                         (e != cudaSuccess ? cudaGetErrorString(e) : "device ordinal out of range");
+        return PV_ERROR_CUDA;
+    }
+    DeviceGuard guard(device);
+    auto *c = new pv_context();
+    c->params = *params;
+    c->gc = gc;
+    c->device = device;
+    const auto bail = [&](cudaError_t err, const char *what) {
+        g_create_error = std::string(what) + ": " + cudaGetErrorString(err);
+        delete c;
+        return PV_ERROR_CUDA;
+    };
+    if ((e = cudaDeviceGetAttribute(&c->sm_count, cudaDevAttrMultiProcessorCount, device)) != cudaSuccess)
+        return bail(e, "cudaDeviceGetAttribute");
+    if ((e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking)) != cudaSuccess)
+        return bail(e, "cudaStreamCreate");
+    if ((e = cudaMalloc(&c->ctl, sizeof(DeviceControl))) != cudaSuccess)
+        return bail(e, "cudaMalloc(control)");
+    if ((e = cudaMallocHost(&c->ctl_host, sizeof(DeviceControl))) != cudaSuccess)
+        return bail(e, "cudaMallocHost(control)");
+    if ((e = cudaMallocHost(&c->pinned, 16 * sizeof(double))) != cudaSuccess)
+        return bail(e, "cudaMallocHost(staging)");
+    std::memset(c->ctl_host, 0, sizeof(DeviceControl));
+    if ((e = cudaMemcpy(c->ctl, c->ctl_host, sizeof(DeviceControl), cudaMemcpyHostToDevice)) !=
+        cudaSuccess)
+        return bail(e, "cudaMemcpy(control)");
+    *out = c;
+    return PV_OK;
+}
+
+void pv_context_destroy(pv_context *ctx) {
+    if (!ctx)
+        return;
+    DeviceGuard guard(ctx->device);
+    if (ctx->stream)
+        cudaStreamSynchronize(ctx->stream);
+    delete ctx;
+}
+
+const char *pv_last_error(const pv_context *ctx) {
+    return ctx ? ctx->error.c_str() : g_create_error.c_str();
+}
+
+const char *pv_backend_name(void) { return "CUDA/B200"; }
+
+pv_status pv_runtime_details(int device, char *buf, size_t len) {
+    cudaDeviceProp prop{};
+    cudaError_t e = cudaGetDeviceProperties(&prop, device);
+    if (e != cudaSuccess) {
+        g_create_error = std::string("cudaGetDeviceProperties: ") + cudaGetErrorString(e);
+        return PV_ERROR_CUDA;
+    }
+    const std::string text = "cuda_device " + std::to_string(device) + "\ncuda_device_name \"" +
+                             prop.name + "\"\ncuda_compute_capability " +
+                             std::to_string(prop.major) + "." + std::to_string(prop.minor) +
+                             "\ncuda_multiprocessors " + std::to_string(prop.multiProcessorCount);
+    if (buf && len) {
+        const size_t k = std::min(len - 1, text.size());
+        std::memcpy(buf, text.data(), k);
+        buf[k] = '\0';
+    }
+    return PV_OK;
+}
+
+pv_status pv_evaluate_range(pv_context *ctx, const double *x, const double *y,
+                            const double *circulation, size_t n, size_t begin, size_t end,
+                            double *u, double *v) {
+    if (!ctx)
+        return PV_ERROR_INVALID_ARGUMENT;
+    return evaluate_host(ctx, x, y, circulation, n, begin, end, u, v, false);
+}
+
+pv_status pv_evaluate(pv_context *ctx, const double *x, const double *y, const double *circulation,
+                      size_t n, double *u, double *v) {
+    if (!ctx)
+        return PV_ERROR_INVALID_ARGUMENT;
+    return evaluate_host(ctx, x, y, circulation, n, 0, n, u, v, true);
+}
+
+pv_status pv_invariants(pv_context *ctx, const double *x, const double *y,
+                        const double *circulation, size_t n, double out[5]) {
+    if (!ctx)
+        return PV_ERROR_INVALID_ARGUMENT;
+    if (!finite_arrays(x, y, circulation, n))
+        return fail(ctx, PV_ERROR_INVALID_ARGUMENT, "vortex data must be finite");
+    DeviceGuard guard(ctx->device);
+    const size_t np = padded(n);
+    for (DeviceArray *a : {&ctx->ex, &ctx->ey, &ctx->eg})
+        PV_CUDA(ctx, a->ensure(np));
+    const size_t bytes = n * sizeof(double);
+    if (n) {
+        PV_CUDA(ctx, cudaMemcpyAsync(ctx->ex.p, x, bytes, cudaMemcpyHostToDevice, ctx->stream));
+        PV_CUDA(ctx, cudaMemcpyAsync(ctx->ey.p, y, bytes, cudaMemcpyHostToDevice, ctx->stream));
+        PV_CUDA(ctx, cudaMemcpyAsync(ctx->eg.p, circulation, bytes, cudaMemcpyHostToDevice,
+                                     ctx->stream));
+    }
+    return invariants_of(ctx, ctx->ex.p, ctx->ey.p, ctx->eg.p, n, out);
+}
+
+pv_status pv_hamiltonian(pv_context *ctx, const double *x, const double *y,
+                         const double *circulation, size_t n, double *hamiltonian) {
+    double out[5];
+    const pv_status st = pv_invariants(ctx, x, y, circulation, n, out);
+    if (st == PV_OK)
+        *hamiltonian = out[4];
+    return st;
+}
+
+pv_status pv_upload_state(pv_context *ctx, const double *x, const double *y,
+                          const double *circulation, size_t n) {
+    if (!ctx)
+        return PV_ERROR_INVALID_ARGUMENT;
+    if (!finite_arrays(x, y, circulation, n))
+        return fail(ctx, PV_ERROR_INVALID_ARGUMENT, "vortex data must be finite");
+    pv_status st = validate_geometry(ctx, x, y, circulation, n);
+    if (st != PV_OK)
+        return st;
+    DeviceGuard guard(ctx->device);
+    if ((st = ensure_state_capacity(ctx, n)) != PV_OK)
+        return st;
+    ctx->n = n;
+    ctx->fsal_valid = false;
+    ctx->state_valid = true;
+    if (n == 0)
+        return PV_OK;
+    const size_t bytes = n * sizeof(double);
+    const std::vector<double> gs = scaled(ctx->gc, circulation, n);
+    PV_CUDA(ctx, cudaMemcpyAsync(ctx->x.p, x, bytes, cudaMemcpyHostToDevice, ctx->stream));
+    PV_CUDA(ctx, cudaMemcpyAsync(ctx->y.p, y, bytes, cudaMemcpyHostToDevice, ctx->stream));
+    PV_CUDA(ctx, cudaMemcpyAsync(ctx->gamma.p, circulation, bytes, cudaMemcpyHostToDevice, ctx->stream));
+    PV_CUDA(ctx, cudaMemcpyAsync(ctx->gs.p, gs.data(), bytes, cudaMemcpyHostToDevice, ctx->stream));
+    PV_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    return PV_OK;
+}
+
+pv_status pv_download_state(pv_context *ctx, double *x, double *y, size_t n) {
+    if (!ctx)
+        return PV_ERROR_INVALID_ARGUMENT;
+    pv_status st = require_state(ctx);
+    if (st != PV_OK)
+        return st;
+    if (n != ctx->n)
+        return fail(ctx, PV_ERROR_RUNTIME, "host and device vortex populations differ");
+    if (n == 0)
+        return PV_OK;
+    DeviceGuard guard(ctx->device);
+    PV_CUDA(ctx, cudaMemcpyAsync(x, ctx->x.p, n * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    PV_CUDA(ctx, cudaMemcpyAsync(y, ctx->y.p, n * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    PV_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    return PV_OK;
+}
+
+pv_status pv_evaluate_state(pv_context *ctx, double *u, double *v, size_t n) {
+    if (!ctx)
+        return PV_ERROR_INVALID_ARGUMENT;
+    pv_status st = require_state(ctx);
+    if (st != PV_OK)
+        return st;
+    if (n != ctx->n)
+        return fail(ctx, PV_ERROR_RUNTIME, "host and device vortex populations differ");
+    if (n == 0)
+        return PV_OK;
+    DeviceGuard guard(ctx->device);
+    if ((st = reset_control(ctx)) != PV_OK)
+        return st;
+    if ((st = launch_eval(ctx, ctx->x.p, ctx->y.p)) != PV_OK)
+        return st;
+    --ctx->evaluations; // not a stepping evaluation
+    // Reduce into the last stage slot's partner buffer p1 (scratch), leaving stages untouched.
+    StageArgs s = stage_base(ctx);
+    s.mode = STAGE_REDUCE_ONLY;
+    s.s = 0;
+    s.kx[0] = ctx->p1x.p;
+    s.ky[0] = ctx->p1y.p;
+    s.ex = ctx->x.p;
+    s.ey = ctx->y.p;
+    PV_CUDA(ctx, counted(ctx, PV_KERNEL_STAGE, 1, [&] { return launch_stage(s, ctx->stream, ctx->sm_count); }));
+    PV_CUDA(ctx, cudaMemcpyAsync(u, ctx->p1x.p, n * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    PV_CUDA(ctx, cudaMemcpyAsync(v, ctx->p1y.p, n * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    if ((st = read_control(ctx)) != PV_OK)
+        return st;
+    return status_error(ctx, ctx->ctl_host->status);
+}
+
+namespace {
+// Enqueues one RK4 step (src/timestep.cpp:31-61) on the context stream.
+pv_status enqueue_rk4(pv_context *c, double dt) {
+    const double *px = c->x.p, *py = c->y.p;
+    double *pos_x[2] = {c->p0x.p, c->p1x.p};
+    double *pos_y[2] = {c->p0y.p, c->p1y.p};
+    static const double rows[3][3] = {{0.5}, {0.0, 0.5}, {0.0, 0.0, 1.0}};
+    pv_status st;
+    for (int s = 0; s < 4; ++s) {
+        if ((st = launch_eval(c, px, py)) != PV_OK)
+            return st;
+        StageArgs a = stage_base(c);
+        a.s = s;
+        a.ex = px;
+        a.ey = py;
+        a.dt = dt;
+        a.xt = pos_x[s & 1];
+        a.yt = pos_y[s & 1];
+        if (s < 3) {
+            a.mode = STAGE_POSITION;
+            a.ncoef = s + 1;
+            for (int j = 0; j <= s; ++j)
+                a.coef[j] = rows[s][j];
+        } else {
+            a.mode = STAGE_RK4_COMBINE;
+        }
+        PV_CUDA(c, counted(c, PV_KERNEL_STAGE, 1, [&] { return launch_stage(a, c->stream, c->sm_count); }));
+        px = a.xt;
+        py = a.yt;
+    }
+    PV_CUDA(c, counted(c, PV_KERNEL_ACCEPT, 1, [&] {
+                return launch_accept(c->x.p, c->y.p, px, py, nullptr, nullptr, nullptr, nullptr, c->n,
+                                     0, c->ctl, c->stream);
+            }));
+    return PV_OK;
+}
+} // namespace
+
+pv_status pv_rk4_step(pv_context *ctx, double dt) {
+    if (!ctx)
+        return PV_ERROR_INVALID_ARGUMENT;
+    if (!std::isfinite(dt) || !(dt > 0.0))
+        return fail(ctx, PV_ERROR_INVALID_ARGUMENT, "timestep must be finite and positive");
+    pv_status st = require_state(ctx);
+    if (st != PV_OK)
+        return st;
+    ctx->fsal_valid = false;
+    if (ctx->n == 0)
+        return PV_OK;
+    DeviceGuard guard(ctx->device);
+    if ((st = reset_control(ctx)) != PV_OK)
+        return st;
+    if ((st = enqueue_rk4(ctx, dt)) != PV_OK)
+        return st;
+    if ((st = read_control(ctx)) != PV_OK)
+        return st;
+    return status_error(ctx, ctx->ctl_host->status);
+}
+
+pv_status pv_rk4_advance(pv_context *ctx, double dt, uint64_t steps) {
+    if (!ctx)
+        return PV_ERROR_INVALID_ARGUMENT;
+    if (!std::isfinite(dt) || !(dt > 0.0))
+        return fail(ctx, PV_ERROR_INVALID_ARGUMENT, "timestep must be finite and positive");
+    pv_status st = require_state(ctx);
+    if (st != PV_OK)
+        return st;
+    ctx->fsal_valid = false;
+    if (ctx->n == 0 || steps == 0)
+        return PV_OK;
+    DeviceGuard guard(ctx->device);
+    if ((st = reset_control(ctx)) != PV_OK)
+        return st;
+    for (uint64_t k = 0; k < steps; ++k)
+        if ((st = enqueue_rk4(ctx, dt)) != PV_OK)
+            return st;
+    if ((st = read_control(ctx)) != PV_OK)
+        return st;
+    return status_error(ctx, ctx->ctl_host->status);
+}
+
+pv_status pv_dopri5_step(pv_context *ctx, double dt, double absolute_tolerance,
+                         double relative_tolerance, double minimum_time_step,
+                         double maximum_time_step, pv_step_result *result) {
+    if (!ctx || !result)
+        return PV_ERROR_INVALID_ARGUMENT;
+    if (!std::isfinite(dt) || !(dt > 0.0))
+        return fail(ctx, PV_ERROR_INVALID_ARGUMENT, "timestep must be finite and positive");
+    pv_status st = require_state(ctx);
+    if (st != PV_OK)
+        return st;
+    if (ctx->n == 0) {
+        // Empty population: the reference's error is 0, so the step is accepted with factor 5.
+        ctx->evaluations += ctx->fsal_valid ? 6 : 7;
+        ctx->fsal_valid = true;
+        const double s = dt * 5.0;
+        result->accepted_time_step = dt;
+        result->suggested_time_step =
+            s < minimum_time_step ? minimum_time_step : (maximum_time_step < s ? maximum_time_step : s);
+        result->normalized_error = 0.0;
+        result->rejected_steps = 0;
+        return PV_OK;
+    }
+    DeviceGuard guard(ctx->device);
+    std::memset(ctx->ctl_host, 0, sizeof(DeviceControl));
+    ctx->ctl_host->dt = dt;
+    ctx->ctl_host->absolute_tolerance = absolute_tolerance;
+    ctx->ctl_host->relative_tolerance = relative_tolerance;
+    ctx->ctl_host->minimum_time_step = minimum_time_step;
+    ctx->ctl_host->maximum_time_step = maximum_time_step;
+    PV_CUDA(ctx, cudaMemcpyAsync(ctx->ctl, ctx->ctl_host, sizeof(DeviceControl),
+                                 cudaMemcpyHostToDevice, ctx->stream));
+    double *pos_x[2] = {ctx->p0x.p, ctx->p1x.p};
+    double *pos_y[2] = {ctx->p0y.p, ctx->p1y.p};
+    double w[7];
+    for (int j = 0; j < 7; ++j)
+        w[j] = kB5[j] - kB4[j];
+    bool need_k0 = !ctx->fsal_valid;
+    for (int attempt = 0; attempt < 40; ++attempt) {
+        const double *px = ctx->x.p, *py = ctx->y.p;
+        if (need_k0 && (st = launch_eval(ctx, px, py)) != PV_OK)
+            return st;
+        for (int s = 0; s < 7; ++s) {
+            if (s > 0 && (st = launch_eval(ctx, px, py)) != PV_OK)
+                return st;
+            StageArgs a = stage_base(ctx);
+            a.s = s;
+            a.reduce = (s > 0 || need_k0) ? 1 : 0;
+            a.ex = px;
+            a.ey = py;
+            a.dt_from_control = 1;
+            if (s < 6) {
+                a.mode = STAGE_POSITION;
+                a.ncoef = s + 1;
+                for (int j = 0; j <= s; ++j)
+                    a.coef[j] = kDopri[s + 1][j];
+                a.xt = pos_x[s & 1];
+                a.yt = pos_y[s & 1];
+            } else {
+                a.mode = STAGE_DOPRI_ERROR;
+                a.xt = const_cast<double *>(px); // y5, the position k6 was evaluated at
+                a.yt = const_cast<double *>(py);
+                for (int j = 0; j < 7; ++j)
+                    a.w[j] = w[j];
+            }
+            PV_CUDA(ctx, counted(ctx, PV_KERNEL_STAGE, 1, [&] { return launch_stage(a, ctx->stream, ctx->sm_count); }));
+            if (s < 6) {
+                px = a.xt;
+                py = a.yt;
+            }
+        }
+        need_k0 = false;
+        PV_CUDA(ctx, counted(ctx, PV_KERNEL_ACCEPT, 1, [&] {
+                    return launch_accept(ctx->x.p, ctx->y.p, px, py, ctx->kx[0].p, ctx->ky[0].p,
+                                         ctx->kx[6].p, ctx->ky[6].p, ctx->n, 1, ctx->ctl, ctx->stream);
+                }));
+        if ((st = read_control(ctx)) != PV_OK)
+            return st;
+        if (ctx->ctl_host->status != 0) {
+            ctx->fsal_valid = false;
+            return status_error(ctx, ctx->ctl_host->status);
+        }
+        if (ctx->ctl_host->accepted) {
+            ctx->fsal_valid = true;
+            result->accepted_time_step = ctx->ctl_host->result[0];
+            result->suggested_time_step = ctx->ctl_host->result[1];
+            result->normalized_error = ctx->ctl_host->result[2];
+            result->rejected_steps = static_cast<unsigned>(ctx->ctl_host->result[3]);
+            return PV_OK;
+        }
+    }
+    return fail(ctx, PV_ERROR_RUNTIME, "adaptive integrator could not satisfy tolerance");
+}
+
+pv_status pv_invalidate_derivative(pv_context *ctx) {
+    if (!ctx)
+        return PV_ERROR_INVALID_ARGUMENT;
+    ctx->fsal_valid = false;
+    return PV_OK;
+}
+
+pv_status pv_state_invariants(pv_context *ctx, double out[5]) {
+    if (!ctx)
+        return PV_ERROR_INVALID_ARGUMENT;
+    pv_status st = require_state(ctx);
+    if (st != PV_OK)
+        return st;
+    DeviceGuard guard(ctx->device);
+    return invariants_of(ctx, ctx->x.p, ctx->y.p, ctx->gamma.p, ctx->n, out);
+}
+
+pv_status pv_dipole_scan(pv_context *ctx, double threshold, pv_dipole_candidate *out,
+                         size_t capacity, size_t *count) {
+    if (!ctx || !count)
+        return PV_ERROR_INVALID_ARGUMENT;
+    if (!std::isfinite(threshold) || !(threshold > 0.0))
+        return fail(ctx, PV_ERROR_INVALID_ARGUMENT, "dipoleRemovalDistance must be positive");
+    pv_status st = require_state(ctx);
+    if (st != PV_OK)
+        return st;
+    *count = 0;
+    if (ctx->n == 0)
+        return PV_OK;
+    DeviceGuard guard(ctx->device);
+    static_assert(sizeof(DipoleCandidateDev) == 3 * sizeof(double), "candidate layout");
+    static_assert(sizeof(pv_dipole_candidate) == sizeof(DipoleCandidateDev), "candidate layout");
+    const size_t cap = std::max<size_t>(capacity, 1);
+    PV_CUDA(ctx, ctx->cand.ensure(3 * cap));
+    auto *dev = reinterpret_cast<DipoleCandidateDev *>(ctx->cand.p);
+    auto *dev_count = reinterpret_cast<unsigned long long *>(&ctx->ctl->dipole_count);
+    PV_CUDA(ctx, counted(ctx, PV_KERNEL_DIPOLE, 1, [&] {
+                return launch_dipole_scan(ctx->x.p, ctx->y.p, ctx->gamma.p, ctx->n, ctx->gc,
+                                          threshold, dev, cap, dev_count, ctx->stream);
+            }));
+    if ((st = read_control(ctx)) != PV_OK)
+        return st;
+    const unsigned long long found = ctx->ctl_host->dipole_count;
+    *count = static_cast<size_t>(found);
+    const size_t k = std::min<size_t>(static_cast<size_t>(found), capacity);
+    if (k && out) {
+        PV_CUDA(ctx, cudaMemcpyAsync(out, dev, k * sizeof(pv_dipole_candidate),
+                                     cudaMemcpyDeviceToHost, ctx->stream));
+        PV_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    }
+    return PV_OK;
+}
+
+pv_status pv_state_size(const pv_context *ctx, size_t *n) {
+    if (!ctx || !n)
+        return PV_ERROR_INVALID_ARGUMENT;
+    *n = ctx->n;
+    return PV_OK;
+}
+
+pv_status pv_evaluation_count(const pv_context *ctx, uint64_t *count) {
+    if (!ctx || !count)
+        return PV_ERROR_INVALID_ARGUMENT;
+    *count = ctx->evaluations;
+    return PV_OK;
+}
+
+pv_status pv_set_profiling(pv_context *ctx, int enabled) {
+    if (!ctx)
+        return PV_ERROR_INVALID_ARGUMENT;
+    ctx->profiling = enabled != 0;
+    return PV_OK;
+}
+
+pv_status pv_get_kernel_stats(pv_context *ctx, pv_kernel_stats *out) {
+    if (!ctx || !out)
+        return PV_ERROR_INVALID_ARGUMENT;
+    DeviceGuard guard(ctx->device);
+    PV_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    collect_timers(ctx);
+    for (int k = 0; k < PV_KERNEL_KINDS; ++k) {
+        out->launches[k] = ctx->launches[k];
+        out->timed_launches[k] = ctx->timed[k];
+        out->milliseconds[k] = ctx->milliseconds[k];
+    }
+    return PV_OK;
+}
+
+pv_status pv_reset_kernel_stats(pv_context *ctx) {
+    if (!ctx)
+        return PV_ERROR_INVALID_ARGUMENT;
+    DeviceGuard guard(ctx->device);
+    PV_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    collect_timers(ctx);
+    for (int k = 0; k < PV_KERNEL_KINDS; ++k) {
+        ctx->launches[k] = 0;
+        ctx->timed[k] = 0;
+        ctx->milliseconds[k] = 0.0;
+    }
+    return PV_OK;
+}
+
+pv_status pv_probe_peak(int device, int kind, double *flops_per_second) {
+    if (!flops_per_second || (kind != 0 && kind != 1))
+        return PV_ERROR_INVALID_ARGUMENT;
+    int count = 0;
+    if (cudaGetDeviceCount(&count) != cudaSuccess || device < 0 || device >= count) {
+        g_create_error = "no such CUDA device";
+        return PV_ERROR_CUDA;
+    }
+    DeviceGuard guard(device);
+    int sms = 0;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+    double *sink = nullptr;
+    cudaEvent_t e0, e1;
+    if (cudaMalloc(&sink, sizeof(double)) != cudaSuccess)
+        return PV_ERROR_CUDA;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    const int blocks = sms * 8, threads = 256;
+    // Double the work until one launch runs for at least 100 ms (after two warm-up launches), and
+    // keep the iteration count and the time of that same launch.
+    int iterations = 1024, timed_iterations = 0;
+    float ms = 0.0f;
+    cudaError_t e = cudaSuccess;
+    for (int pass = 0; pass < 16 && e == cudaSuccess; ++pass) {
+        cudaEventRecord(e0);
+        e = launch_peak_probe(kind, blocks, threads, iterations, sink, nullptr);
+        cudaEventRecord(e1);
+        cudaEventSynchronize(e1);
+        cudaEventElapsedTime(&ms, e0, e1);
+        timed_iterations = iterations;
+        if (ms >= 100.0f && pass >= 2)
+            break;
+        if (ms < 100.0f && iterations < (1 << 22))
+            iterations *= 2;
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    cudaFree(sink);
+    if (e != cudaSuccess) {
+        g_create_error = std::string("peak probe: ") + cudaGetErrorString(e);
+        return PV_ERROR_CUDA;
+    }
+    const double fmas = static_cast<double>(blocks) * threads * timed_iterations * 8.0;
+    *flops_per_second = 2.0 * fmas / (ms * 1e-3);
+    return PV_OK;
+}
+
+} // extern "C"

@@ -1,0 +1,144 @@
+// pv_dipole.cu — close-dipole candidate scan on the GPU, plus the peak-throughput probes.
+//
+// The scan replaces the O(N^2/2) candidate loop of DipoleManager::process (src/dipole.cpp:49-78)
+// that the reference runs on the host after every accepted step, with a full download of the
+// state first (src/main.cpp:327-328). The selection, compaction and optional re-injection stay in
+// the reference's host code; a candidate count of zero means process() would return 0 before
+// touching its random generator (src/dipole.cpp:101-102), so the download can be skipped.
+//
+// Candidate test, bit for bit as the reference computes it (g++ on x86-64 does not contract):
+//   opposite signs (Gamma != 0, signbit differs);
+//   dx = remainder(x_i - x_j, Lx) in the periodic box (exactly rounded by definition), else x_i - x_j;
+//   d2 = dx*dx + dy*dy (two products, one sum, each rounded) < threshold*threshold;
+//   disk wall image: r2 = x*x + y*y > 0, image = (R*R - r2)/sqrt(r2), image*image < threshold^2.
+#include "pv_internal.h"
+
+namespace pvb {
+
+namespace {
+constexpr int kDT = 128;
+
+__device__ __forceinline__ void push(DipoleCandidateDev *out, size_t capacity,
+                                     unsigned long long *count, unsigned long long a,
+                                     unsigned long long b, double d2) {
+    const unsigned long long slot = atomicAdd(count, 1ull);
+    if (slot < capacity) {
+        out[slot].first = a;
+        out[slot].second = b;
+        out[slot].distance_squared = d2;
+    }
+}
+
+__global__ void __launch_bounds__(kDT)
+    dipole_scan_kernel(const double *x, const double *y, const double *g, size_t n,
+                       GeometryConsts gc, double thr2, DipoleCandidateDev *out, size_t capacity,
+                       unsigned long long *count) {
+    const int I = blockIdx.y, J = blockIdx.x;
+    if (J < I)
+        return;
+    __shared__ double sx[kDT], sy[kDT], sg[kDT];
+    const size_t j0 = static_cast<size_t>(J) * kDT;
+    const size_t jl = j0 + threadIdx.x;
+    sx[threadIdx.x] = jl < n ? x[jl] : 0.0;
+    sy[threadIdx.x] = jl < n ? y[jl] : 0.0;
+    sg[threadIdx.x] = jl < n ? g[jl] : 0.0;
+    __syncthreads();
+    const size_t i = static_cast<size_t>(I) * kDT + threadIdx.x;
+    if (i >= n)
+        return;
+    const double xi = x[i], yi = y[i], gi = g[i];
+    if (gi == 0.0)
+        return;
+    const bool periodic = gc.geometry == GEO_PERIODIC;
+    const int jcount = static_cast<int>(min(static_cast<size_t>(kDT), n - j0));
+    const int jstart = (I == J) ? static_cast<int>(threadIdx.x) + 1 : 0;
+    const bool neg_i = signbit(gi);
+    for (int jj = jstart; jj < jcount; ++jj) {
+        const double gj = sg[jj];
+        if (gj == 0.0 || neg_i == static_cast<bool>(signbit(gj)))
+            continue;
+        double dx = xi - sx[jj], dy = yi - sy[jj];
+        if (periodic) {
+            dx = exact_remainder(dx, gc.lx, gc.inv_lx, gc.half_lx);
+            dy = exact_remainder(dy, gc.ly, gc.inv_ly, gc.half_ly);
+        }
+        const double d2 = __dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy));
+        if (d2 < thr2)
+            push(out, capacity, count, i, j0 + jj, d2);
+    }
+    if (gc.geometry == GEO_DISK && I == J) {
+        const double r2 = __dadd_rn(__dmul_rn(xi, xi), __dmul_rn(yi, yi));
+        if (r2 > 0.0) {
+            const double image = __ddiv_rn(__dsub_rn(gc.radius2, r2), __dsqrt_rn(r2));
+            const double i2 = __dmul_rn(image, image);
+            if (i2 < thr2)
+                push(out, capacity, count, i, n, i2);
+        }
+    }
+}
+
+// Peak probes: independent FMA chains (8 per thread) on the FP64 or FP32 pipe, or chains of the
+// FP64 reciprocal approximation, to measure the arithmetic roofline of this GPU at load clocks.
+__global__ void probe_dfma(int iterations, double *sink) {
+    double a[8];
+#pragma unroll
+    for (int k = 0; k < 8; ++k)
+        a[k] = 1.0 + 1e-9 * (threadIdx.x + k);
+    const double b = 0.999999999, c = 1e-12;
+    for (int it = 0; it < iterations; ++it) {
+#pragma unroll
+        for (int k = 0; k < 8; ++k)
+            a[k] = fma(a[k], b, c);
+    }
+    double s = 0.0;
+#pragma unroll
+    for (int k = 0; k < 8; ++k)
+        s += a[k];
+    if (s == 12345.678)
+        sink[0] = s;
+}
+
+__global__ void probe_ffma(int iterations, double *sink) {
+    float a[8];
+#pragma unroll
+    for (int k = 0; k < 8; ++k)
+        a[k] = 1.0f + 1e-6f * (threadIdx.x + k);
+    const float b = 0.9999999f, c = 1e-7f;
+    for (int it = 0; it < iterations; ++it) {
+#pragma unroll
+        for (int k = 0; k < 8; ++k)
+            a[k] = fmaf(a[k], b, c);
+    }
+    float s = 0.0f;
+#pragma unroll
+    for (int k = 0; k < 8; ++k)
+        s += a[k];
+    if (s == 12345.678f)
+        sink[0] = s;
+}
+} // namespace
+
+cudaError_t launch_dipole_scan(const double *x, const double *y, const double *gamma, size_t n,
+                               const GeometryConsts &g, double threshold,
+                               DipoleCandidateDev *out, size_t capacity,
+                               unsigned long long *count, cudaStream_t stream) {
+    cudaError_t e = cudaMemsetAsync(count, 0, sizeof(unsigned long long), stream);
+    if (e != cudaSuccess || n == 0)
+        return e;
+    const size_t nt = (n + kDT - 1) / kDT;
+    const dim3 grid(static_cast<unsigned>(nt), static_cast<unsigned>(nt));
+    dipole_scan_kernel<<<grid, kDT, 0, stream>>>(x, y, gamma, n, g, threshold * threshold, out,
+                                                 capacity, count);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_peak_probe(int kind, int blocks, int threads, int iterations, double *sink,
+                              cudaStream_t stream) {
+    if (kind == 0)
+        probe_dfma<<<blocks, threads, 0, stream>>>(iterations, sink);
+    else
+        probe_ffma<<<blocks, threads, 0, stream>>>(iterations, sink);
+    return cudaGetLastError();
+}
+
+} // namespace pvb

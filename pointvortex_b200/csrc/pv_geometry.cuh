@@ -1,0 +1,278 @@
+// pv_geometry.cuh — the three Biot–Savart pair interactions of PointVortex, FP64.
+//
+// Each geometry provides
+//   * a per-source record staged in shared memory (x, y, and a scaled circulation),
+//   * pair<CHECK>(): the fast form used by the tiled kernels, which adds one source's
+//     contribution to one target's (u, v); CHECK enables the self-pair test and is only
+//     instantiated for the diagonal tiles,
+//   * slow_target(): the reference form with IEEE divisions and the reference's singular-pair
+//     test, used to recompute a target whose fast-path sum came out non-finite. It returns the
+//     reference's verdict (coincident pair / non-finite / finite).
+#pragma once
+
+#include "pv_common.cuh"
+
+namespace pvb {
+
+constexpr double kPi = 3.141592653589793;            // std::numbers::pi
+constexpr double kInverseTwoPi = 0.5 / 3.141592653589793;
+
+enum GeometryId : int { GEO_INFINITE = 0, GEO_PERIODIC = 1, GEO_DISK = 2 };
+
+// Constants of one simulation, passed by value to every kernel (kernel parameter space).
+struct GeometryConsts {
+    int geometry;
+    int image_layers;
+    // infinite plane
+    double eps2;            // coreRadius^2
+    // periodic box (Weiss–McWilliams)
+    double lx, ly;          // box lengths (square within 1e-13)
+    double inv_lx, inv_ly;  // 1/L
+    double half_lx, half_ly;
+    double wave;            // 2 pi / Lx
+    double scale;           // 0.5 / Lx
+    int m_pairs;            // images m = +-1..m_pairs that are never dropped (min(M, 5))
+    int has6;               // images m = +-6 kept when within the |shift| <= 40 window (M >= 6)
+    double cosh_m[6];       // cosh(2 pi m), m = 0..5
+    double sinh2_m[6];      // sinh(2 pi m)^2
+    double shift6;          // (2 pi) * 6, rounded as the reference rounds it
+    double cosh6, sinh6;    // cosh(12 pi), sinh(12 pi)
+    // disk
+    double radius, radius2, inv_radius, inv_radius2;
+};
+
+// Scaled circulation stored per source, chosen so that each pair needs one multiply by it:
+// infinite plane and disk Gamma/(2 pi) (the reference's inverseTwoPi * Gamma), periodic box
+// Gamma * 0.5/L (the reference's scale * Gamma).
+__host__ __device__ __forceinline__ double scaled_circulation(const GeometryConsts &g, double gamma) {
+    if (g.geometry == GEO_PERIODIC)
+        return g.scale * gamma;
+    return kInverseTwoPi * gamma;
+}
+
+// ---------------------------------------------------------------------------------------------
+// Infinite plane, src/compute.cpp:88-133: u -= (G/2pi) dy/(r^2+eps^2), v += (G/2pi) dx/(r^2+eps^2).
+struct InfinitePair {
+    template <bool CHECK>
+    __device__ __forceinline__ static void pair(const GeometryConsts &g, double tx, double ty,
+                                                double sx, double sy, double sg, bool self,
+                                                double &u, double &v) {
+        const double dx = tx - sx;
+        const double dy = ty - sy;
+        const double r2 = fma(dx, dx, fma(dy, dy, g.eps2));
+        double c = sg * rcp_refined(r2);
+        if (CHECK && self)
+            c = 0.0;
+        u = fma(-c, dy, u);
+        v = fma(c, dx, v);
+    }
+};
+
+// Disk of radius R, src/compute.cpp:286-336, with the source record of the infinite plane
+// (x, y, G/(2 pi)). With p = z_i/R^2 and k = G/(2 pi):
+//   direct (j != i):  u -= k dy/r^2,  v += k dx/r^2                 (dx = x_i - x_j, ...)
+//   image (all j):    a = 1 - p.z_j, b = p_y x_j - p_x y_j,
+//                     u += (k/R^2) (b x_j - a y_j)/(a^2 + b^2),  v += (k/R^2) (a x_j + b y_j)/(a^2 + b^2)
+// which is the reference's circle-theorem image term written in unscaled source coordinates.
+struct DiskPair {
+    template <bool CHECK>
+    __device__ __forceinline__ static void pair(const GeometryConsts &g, double tx, double ty,
+                                                double sx, double sy, double sg, bool self,
+                                                double &u, double &v) {
+        const double dx = tx - sx;
+        const double dy = ty - sy;
+        const double r2 = fma(dx, dx, dy * dy);
+        double c = sg * rcp_refined(r2);
+        if (CHECK && self)
+            c = 0.0;
+        u = fma(-c, dy, u);
+        v = fma(c, dx, v);
+        const double px = tx * g.inv_radius2, py = ty * g.inv_radius2;
+        const double a = fma(-px, sx, fma(-py, sy, 1.0));
+        const double b = fma(py, sx, -px * sy);
+        const double ci = (sg * g.inv_radius2) * rcp_refined(fma(a, a, b * b));
+        u = fma(ci, fma(b, sx, -a * sy), u);
+        v = fma(ci, fma(a, sx, b * sy), v);
+    }
+};
+
+// Periodic square box, src/compute.cpp:203-256 (Weiss–McWilliams image sum, truncated at
+// |m| <= M with the reference's rule that an image whose |shift| exceeds 40 contributes 0).
+//
+// With x^ = (2 pi/L) remainder(dx, L), y^ likewise, the reference adds per source
+//   u -= k sin(y^) sum_m 1/D_u(m),  D_u(m) = 2 (sinh^2((x^ - 2 pi m)/2) + sin^2(y^/2)),
+//   v += k sin(x^) sum_m 1/D_v(m),  D_v(m) = 2 (sinh^2((y^ - 2 pi m)/2) + sin^2(x^/2)).
+// The same truncated series is evaluated here with one division per axis:
+//   * m = 0 keeps the cancellation-free form 2 (sinh^2(x^/2) + sin^2(y^/2));
+//   * m and -m (1 <= m <= 5, never dropped because |x^| <= pi) are combined exactly:
+//       D(m) = cosh(x^ - a) - cos y^,  a = 2 pi m,
+//       D(m) + D(-m) = 2 (cosh x^ cosh a - cos y^),
+//       D(m) D(-m)   = (cosh x^ - cos y^ cosh a)^2 + sinh^2 a sin^2 y^   (a sum of squares),
+//   * m = +-6 enter singly, each only when |x^ -+ 12 pi| <= 40 as in the reference;
+//   * |m| >= 7 always has |shift| > 40 and is dropped, as in the reference;
+//   * the m != 0 terms are accumulated as one fraction N/D (every D(m) >= cosh(pi) - 1 > 10, and
+//     the product over m stays below 1e113), so each axis costs one reciprocal.
+// sinh, cosh, sin, cos of x^/2 and y^/2 come from sinh_cosh_sin_cos (|x^/2| <= pi/2).
+struct PeriodicPair {
+    __device__ __forceinline__ static double axis_sum(const GeometryConsts &g, double hat,
+                                                      double cosh_hat, double sinh_hat,
+                                                      double cos_other, double sin2_other,
+                                                      double d0, double &den_out) {
+        double num = 0.0, den = 1.0;
+#pragma unroll
+        for (int m = 1; m <= 5; ++m) {
+            if (m <= g.m_pairs) {
+                const double pair_num = 2.0 * fma(cosh_hat, g.cosh_m[m], -cos_other);
+                const double p = fma(-cos_other, g.cosh_m[m], cosh_hat);
+                const double pair_den = fma(p, p, g.sinh2_m[m] * sin2_other);
+                num = fma(pair_num, den, num * pair_den);
+                den *= pair_den;
+            }
+        }
+        if (g.has6) {
+            // cosh(x^ -+ 12 pi) = cosh(12 pi) cosh x^ -+ sinh(12 pi) sinh x^; each single term is
+            // added as num/den + 1/dm = (num dm + den)/(den dm), or skipped (factor 1, addend 0).
+            const double base = fma(g.cosh6, cosh_hat, -cos_other);
+            const bool plus = fabs(hat - g.shift6) <= 40.0;
+            const bool minus = fabs(hat + g.shift6) <= 40.0;
+            const double dp = plus ? fma(-g.sinh6, sinh_hat, base) : 1.0;
+            num = fma(num, dp, plus ? den : 0.0);
+            den *= dp;
+            const double dn = minus ? fma(g.sinh6, sinh_hat, base) : 1.0;
+            num = fma(num, dn, minus ? den : 0.0);
+            den *= dn;
+        }
+        // sum_m 1/D(m) = 1/d0 + num/den = (den + d0 num) / (d0 den)
+        den_out = d0 * den;
+        return fma(d0, num, den);
+    }
+
+    template <bool CHECK>
+    __device__ __forceinline__ static void pair(const GeometryConsts &g, double tx, double ty,
+                                                double sx, double sy, double sg, bool self,
+                                                double &u, double &v) {
+        const double xh = g.wave * exact_remainder(tx - sx, g.lx, g.inv_lx, g.half_lx);
+        const double yh = g.wave * exact_remainder(ty - sy, g.ly, g.inv_ly, g.half_ly);
+        double shx, chx, snx, csx, shy, chy, sny, csy;
+        sinh_cosh_sin_cos(0.5 * xh, shx, chx, snx, csx);
+        sinh_cosh_sin_cos(0.5 * yh, shy, chy, sny, csy);
+        const double cosh_x = fma(2.0 * shx, shx, 1.0); // cosh x^ = 1 + 2 sinh^2(x^/2)
+        const double cosh_y = fma(2.0 * shy, shy, 1.0);
+        const double cos_x = fma(-2.0 * snx, snx, 1.0); // cos x^ = 1 - 2 sin^2(x^/2)
+        const double cos_y = fma(-2.0 * sny, sny, 1.0);
+        const double sin_x = 2.0 * snx * csx;           // sin x^
+        const double sin_y = 2.0 * sny * csy;
+        const double sinh_x = 2.0 * shx * chx;          // sinh x^
+        const double sinh_y = 2.0 * shy * chy;
+        double d0u = 2.0 * fma(shx, shx, sny * sny);
+        double d0v = 2.0 * fma(shy, shy, snx * snx);
+        if (CHECK && self) { // the self pair contributes exactly 0 in the reference (sin 0 = 0)
+            d0u = 1.0;
+            d0v = 1.0;
+        }
+        double den_u, den_v;
+        const double num_u = axis_sum(g, xh, cosh_x, sinh_x, cos_y, sin_y * sin_y, d0u, den_u);
+        const double num_v = axis_sum(g, yh, cosh_y, sinh_y, cos_x, sin_x * sin_x, d0v, den_v);
+        double cu = sg * sin_y * num_u;
+        double cv = sg * sin_x * num_v;
+        if (CHECK && self) {
+            cu = 0.0;
+            cv = 0.0;
+        }
+        u = fma(-cu, rcp_refined(den_u), u);
+        v = fma(cv, rcp_refined(den_v), v);
+    }
+};
+
+// ---------------------------------------------------------------------------------------------
+// Reference-form recomputation of one target (IEEE divisions, library sinh/sin/remainder,
+// the reference's singular-pair rule). Verdict: 0 finite, ST_COINCIDENT, ST_NONFINITE_VELOCITY.
+__device__ inline int slow_target(const GeometryConsts &g, const double *x, const double *y,
+                                  const double *gamma, size_t n, size_t t, double &u_out,
+                                  double &v_out) {
+    double u = 0.0, v = 0.0;
+    int singular = 0;
+    const double tx = x[t], ty = y[t];
+    if (g.geometry == GEO_INFINITE) {
+        for (size_t s = 0; s < n; ++s) {
+            if (s == t)
+                continue;
+            const double dx = tx - x[s], dy = ty - y[s];
+            const double den = __dadd_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)), g.eps2);
+            if (den == 0.0) {
+                singular = 1;
+                continue;
+            }
+            const double c = __dmul_rn(kInverseTwoPi, gamma[s]) / den;
+            u -= c * dy;
+            v += c * dx;
+        }
+    } else if (g.geometry == GEO_PERIODIC) {
+        const int layers = g.image_layers;
+        for (size_t s = 0; s < n; ++s) {
+            const double sdx = g.wave * remainder(tx - x[s], g.lx);
+            const double sdy = g.wave * remainder(ty - y[s], g.ly);
+            const double sine_x = sin(sdx), sine_y = sin(sdy);
+            const double shx = sin(0.5 * sdx), shy = sin(0.5 * sdy);
+            for (int m = -layers; m <= layers; ++m) {
+                if (s == t && m == 0)
+                    continue;
+                const double shift = __dmul_rn(2.0 * kPi, static_cast<double>(m));
+                const double ax = __dsub_rn(sdx, shift), ay = __dsub_rn(sdy, shift);
+                double du, dv;
+                if (fabs(ax) > 40.0) {
+                    du = __longlong_as_double(0x7ff0000000000000ll);
+                } else {
+                    const double h = sinh(0.5 * ax);
+                    du = 2.0 * __dadd_rn(__dmul_rn(h, h), __dmul_rn(shy, shy));
+                }
+                if (fabs(ay) > 40.0) {
+                    dv = __longlong_as_double(0x7ff0000000000000ll);
+                } else {
+                    const double h = sinh(0.5 * ay);
+                    dv = 2.0 * __dadd_rn(__dmul_rn(h, h), __dmul_rn(shx, shx));
+                }
+                if (du == 0.0 || dv == 0.0) {
+                    singular = 1;
+                    continue;
+                }
+                u -= __dmul_rn(__dmul_rn(g.scale, gamma[s]), sine_y) / du;
+                v += __dmul_rn(__dmul_rn(g.scale, gamma[s]), sine_x) / dv;
+            }
+        }
+    } else {
+        const double ir = g.inv_radius;
+        const double txs = tx * ir, tys = ty * ir;
+        for (size_t s = 0; s < n; ++s) {
+            if (s != t) {
+                const double dx = tx - x[s], dy = ty - y[s];
+                const double den = __dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy));
+                if (den == 0.0) {
+                    singular = 1;
+                    continue;
+                }
+                const double c = __dmul_rn(kInverseTwoPi, gamma[s]) / den;
+                u -= c * dy;
+                v += c * dx;
+            }
+            const double sx = x[s] * ir, sy = y[s] * ir;
+            const double a = 1.0 - __dadd_rn(__dmul_rn(txs, sx), __dmul_rn(tys, sy));
+            const double b = __dsub_rn(__dmul_rn(tys, sx), __dmul_rn(txs, sy));
+            const double den = __dadd_rn(__dmul_rn(a, a), __dmul_rn(b, b));
+            const double ix = __dsub_rn(__dmul_rn(-a, sx), __dmul_rn(b, sy));
+            const double iy = __dadd_rn(__dmul_rn(-a, sy), __dmul_rn(b, sx));
+            const double c = __dmul_rn(__dmul_rn(-kInverseTwoPi, gamma[s]), ir) / den;
+            u -= c * iy;
+            v += c * ix;
+        }
+    }
+    u_out = u;
+    v_out = v;
+    if (singular)
+        return ST_COINCIDENT;
+    if (!isfinite(u) || !isfinite(v))
+        return ST_NONFINITE_VELOCITY;
+    return 0;
+}
+
+} // namespace pvb

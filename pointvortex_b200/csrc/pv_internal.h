@@ -1,0 +1,107 @@
+// pv_internal.h — host-side declarations shared by the translation units of libpvb200.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stddef.h>
+#include <stdint.h>
+
+#include "pv_geometry.cuh"
+
+namespace pvb {
+
+// ---- velocity evaluation ---------------------------------------------------------------------
+// One launch evaluates targets [t_begin, t_end) against sources [0, n_src). The source range is
+// cut into `num_chunks` chunks; work item (target block, chunk) writes its partial sums to
+// pu/pv[chunk * stride + (t - t_begin)]. A reduction pass (stage kernel) sums the chunks in
+// fixed order, so results do not depend on scheduling.
+struct EvalArgs {
+    const double *tx, *ty;          // target positions (indexed by global vortex index)
+    const double *sx, *sy, *sg;     // source positions and scaled circulation
+    size_t t_begin, t_end;
+    size_t n_src;
+    double *pu, *pv;
+    size_t stride;
+    int chunk;                      // sources per chunk (even)
+    int num_chunks;
+    int *status;
+    GeometryConsts g;
+};
+
+struct EvalPlan {
+    int block;         // threads per CTA
+    int per_thread;    // targets held in registers per thread
+    int chunk;         // sources per work item
+    int num_chunks;
+    int target_blocks;
+    size_t items() const { return static_cast<size_t>(num_chunks) * target_blocks; }
+};
+
+EvalPlan plan_evaluation(int geometry, size_t n_targets, size_t n_sources, int sm_count,
+                         int per_thread_override = 0);
+cudaError_t launch_velocity(const EvalArgs &a, const EvalPlan &p, cudaStream_t stream);
+
+// ---- stage kernels (reduction, stage positions, RK4 combine, DOPRI5 error and control) ------
+enum StageMode : int {
+    STAGE_REDUCE_ONLY = 0,  // k = sum of partials
+    STAGE_POSITION = 1,     // ... then xt = x0 + dt * sum_j coef_j k_j, validated
+    STAGE_RK4_COMBINE = 2,  // ... then xt = x0 + dt * (k0 + 2 k1 + 2 k2 + k3) / 6, validated
+    STAGE_DOPRI_ERROR = 3,  // ... then scaled error, max-reduced, step control by the last block
+};
+
+struct StageArgs {
+    size_t n;
+    int mode;
+    int reduce;                     // 1: reduce partials into k_s; 0: k_s already final
+    int num_chunks;
+    size_t stride;
+    const double *pu, *pv;
+    int s;                          // index of the stage being produced (k_s)
+    double *kx[7], *ky[7];          // stage velocity fields
+    const double *ex, *ey;          // positions the stage was evaluated at (slow path)
+    const double *gamma;            // raw circulations (slow path)
+    size_t n_src;                   // population of ex/ey/gamma (slow path)
+    size_t t_offset;                // global index of element 0 (host-array target ranges)
+    int nonfinite_ok;               // evaluateRange: a finite-free result is returned, not an error
+    const double *x0, *y0;          // step-start state
+    double *xt, *yt;                // next stage position / combined state
+    double coef[7];                 // a_{s+1, j}
+    int ncoef;
+    double dt;                      // used when dt_from_control == 0
+    int dt_from_control;            // DOPRI5: read dt from the control block
+    double w[7];                    // DOPRI5: b5 - b4
+    DeviceControl *ctl;
+    GeometryConsts g;
+};
+
+cudaError_t launch_stage(const StageArgs &a, cudaStream_t stream, int sm_count);
+
+// Accept kernel: state <- xt (and, for DOPRI5, k0 <- k6 when the attempt was accepted).
+cudaError_t launch_accept(double *x, double *y, const double *xt, const double *yt, double *k0x,
+                          double *k0y, const double *k6x, const double *k6y, size_t n, int dopri,
+                          DeviceControl *ctl, cudaStream_t stream);
+
+// ---- invariants ------------------------------------------------------------------------------
+// Moments (circulation, Ix, Iy, angular impulse) and the Hamiltonian of n vortices. Block
+// partials go to `scratch` (>= invariants_scratch_doubles(n, sm) doubles); a final single-block
+// pass sums them in fixed order. out[0..4] (device) as computeInvariants. Moment errors go to
+// *status, Hamiltonian errors to *status_h.
+size_t invariants_scratch_doubles(size_t n, int sm_count);
+cudaError_t launch_invariants(const double *x, const double *y, const double *gamma, size_t n,
+                              const GeometryConsts &g, double *scratch, double *out, int *status,
+                              int *status_h, cudaStream_t stream);
+
+// ---- close-dipole candidate scan --------------------------------------------------------------
+struct DipoleCandidateDev {
+    unsigned long long first, second;
+    double distance_squared;
+};
+cudaError_t launch_dipole_scan(const double *x, const double *y, const double *gamma, size_t n,
+                               const GeometryConsts &g, double threshold,
+                               DipoleCandidateDev *out, size_t capacity,
+                               unsigned long long *count, cudaStream_t stream);
+
+// ---- diagnostics --------------------------------------------------------------------------------
+cudaError_t launch_peak_probe(int kind, int blocks, int threads, int iterations, double *sink,
+                              cudaStream_t stream);
+
+} // namespace pvb

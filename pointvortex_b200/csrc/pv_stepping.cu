@@ -1,0 +1,239 @@
+// pv_stepping.cu — the Runge–Kutta stage work between two velocity evaluations, on the GPU.
+//
+// Replaces RungeKuttaIntegrator::makeStage / rk4Step / dopri5Step (src/timestep.cpp:19-120)
+// and the reference CUDA backend's stage, combine, validation and error kernels with their
+// host round trips (src/backend_cuda.cu:115-200, 299-357, 387-450). One kernel per stage:
+//
+//   1. reduce the evaluation's chunk partials into k_s in fixed chunk order; a target whose sum is
+//      non-finite is recomputed in the reference form (IEEE divisions, the reference's singular
+//      test), which either yields the reference's finite value or its error;
+//   2. per mode: the next stage position y0 + dt * sum_j a_j k_j, or the RK4 combination, or the
+//      DOPRI5 scaled error (max-reduced with one atomicMax per block), each validated like the
+//      reference (finite positions; in a disk, inside the wall);
+//   3. DOPRI5: the last block to finish runs the step-size control of src/timestep.cpp:97-118 on
+//      the device (accept/reject, suggested step, rejection cap), so the state never leaves the GPU
+//      between attempts.
+//
+// All combination arithmetic uses explicitly rounded operations (__dmul_rn/__dadd_rn/__ddiv_rn)
+// in the reference's order, so that given the same stage velocities the new state is bit-identical
+// to the reference's (which x86-64 g++ computes without FMA contraction).
+#include "pv_internal.h"
+
+namespace pvb {
+
+namespace {
+__device__ __forceinline__ double max_ref(double a, double b) { return (a < b) ? b : a; }
+__device__ __forceinline__ double min_ref(double a, double b) { return (b < a) ? b : a; }
+__device__ __forceinline__ double clamp_ref(double v, double lo, double hi) {
+    return v < lo ? lo : (hi < v ? hi : v);
+}
+
+// Validation of a new position, src/vortex.h:7-14 and src/compute.cpp:41-48.
+__device__ __forceinline__ void validate_position(const StageArgs &a, double x, double y) {
+    if (!isfinite(x) || !isfinite(y))
+        set_status(&a.ctl->status, ST_NONFINITE_POSITION);
+    else if (a.g.geometry == GEO_DISK &&
+             __dadd_rn(__dmul_rn(x, x), __dmul_rn(y, y)) >= a.g.radius2)
+        set_status(&a.ctl->status, ST_OUTSIDE_DISK);
+}
+
+// DOPRI5 step-size control, src/timestep.cpp:95-118, run by one thread.
+__device__ void dopri_control(DeviceControl *ctl) {
+    const double error = __longlong_as_double(static_cast<long long>(ctl->err_bits));
+    const double dt = ctl->dt;
+    const double factor = error == 0.0 ? 5.0 : clamp_ref(0.9 * pow(error, -0.2), 0.2, 5.0);
+    const double suggested =
+        clamp_ref(__dmul_rn(dt, factor), ctl->minimum_time_step, ctl->maximum_time_step);
+    if (ctl->status == 0) {
+        if (error <= 1.0) {
+            ctl->accepted = 1;
+            ctl->result[0] = dt;
+            ctl->result[1] = suggested;
+            ctl->result[2] = error;
+            ctl->result[3] = static_cast<double>(ctl->rejected);
+        } else {
+            ctl->accepted = 0;
+            if (dt <= ctl->minimum_time_step || ++ctl->rejected > 32u)
+                set_status(&ctl->status, ST_DOPRI_FAILED);
+            else
+                ctl->dt = max_ref(ctl->minimum_time_step, min_ref(suggested, __dmul_rn(dt, 0.9)));
+        }
+    }
+    ctl->err_bits = 0ull;
+    ctl->blocks_done = 0u;
+}
+} // namespace
+
+template <int MODE>
+__global__ void __launch_bounds__(256) stage_kernel(const StageArgs a) {
+    __shared__ int s_status;
+    __shared__ double s_max[8];
+    const int tid = threadIdx.x;
+    if (tid == 0)
+        s_status = *reinterpret_cast<volatile int *>(&a.ctl->status);
+    __syncthreads();
+    if (s_status != 0)
+        return;
+
+    const double dt = a.dt_from_control ? a.ctl->dt : a.dt;
+    double local_max = 0.0;
+    for (size_t i = blockIdx.x * static_cast<size_t>(blockDim.x) + tid; i < a.n;
+         i += static_cast<size_t>(gridDim.x) * blockDim.x) {
+        double ku, kv;
+        if (a.reduce) {
+            ku = 0.0;
+            kv = 0.0;
+            for (int c = 0; c < a.num_chunks; ++c) {
+                ku += a.pu[static_cast<size_t>(c) * a.stride + i];
+                kv += a.pv[static_cast<size_t>(c) * a.stride + i];
+            }
+            if (!isfinite(ku) || !isfinite(kv)) {
+                const int verdict =
+                    slow_target(a.g, a.ex, a.ey, a.gamma, a.n_src, a.t_offset + i, ku, kv);
+                if (verdict == ST_COINCIDENT || (verdict && !a.nonfinite_ok))
+                    set_status(&a.ctl->status, verdict);
+            }
+            a.kx[a.s][i] = ku;
+            a.ky[a.s][i] = kv;
+        } else {
+            ku = a.kx[a.s][i];
+            kv = a.ky[a.s][i];
+        }
+        if (MODE == STAGE_POSITION) {
+            // makeStage, src/timestep.cpp:19-30 (zero coefficients add an exact zero: skipped)
+            double dx = 0.0, dy = 0.0;
+            for (int j = 0; j < a.ncoef; ++j) {
+                const double c = a.coef[j];
+                if (c == 0.0)
+                    continue;
+                const double kxj = j == a.s ? ku : a.kx[j][i];
+                const double kyj = j == a.s ? kv : a.ky[j][i];
+                dx = __dadd_rn(dx, __dmul_rn(c, kxj));
+                dy = __dadd_rn(dy, __dmul_rn(c, kyj));
+            }
+            const double nx = __dadd_rn(a.x0[i], __dmul_rn(dt, dx));
+            const double ny = __dadd_rn(a.y0[i], __dmul_rn(dt, dy));
+            a.xt[i] = nx;
+            a.yt[i] = ny;
+            validate_position(a, nx, ny);
+        } else if (MODE == STAGE_RK4_COMBINE) {
+            // src/timestep.cpp:52-57: x0 + dt * (k1 + 2 k2 + 2 k3 + k4) / 6
+            const double sx = __dadd_rn(__dadd_rn(__dadd_rn(a.kx[0][i], __dmul_rn(2.0, a.kx[1][i])),
+                                                  __dmul_rn(2.0, a.kx[2][i])),
+                                        ku);
+            const double sy = __dadd_rn(__dadd_rn(__dadd_rn(a.ky[0][i], __dmul_rn(2.0, a.ky[1][i])),
+                                                  __dmul_rn(2.0, a.ky[2][i])),
+                                        kv);
+            const double nx = __dadd_rn(a.x0[i], __ddiv_rn(__dmul_rn(dt, sx), 6.0));
+            const double ny = __dadd_rn(a.y0[i], __ddiv_rn(__dmul_rn(dt, sy), 6.0));
+            a.xt[i] = nx;
+            a.yt[i] = ny;
+            if (!isfinite(nx) || !isfinite(ny))
+                set_status(&a.ctl->status, ST_NONFINITE_POSITION);
+        } else if (MODE == STAGE_DOPRI_ERROR) {
+            // src/timestep.cpp:78-95: xt holds the fifth-order point y5 (stage 7's position).
+            double xe = 0.0, ye = 0.0;
+            for (int j = 0; j < 7; ++j) {
+                const double w = a.w[j];
+                if (w == 0.0)
+                    continue;
+                const double h = __dmul_rn(dt, w);
+                const double kxj = j == a.s ? ku : a.kx[j][i];
+                const double kyj = j == a.s ? kv : a.ky[j][i];
+                xe = __dadd_rn(xe, __dmul_rn(h, kxj));
+                ye = __dadd_rn(ye, __dmul_rn(h, kyj));
+            }
+            const double x5 = a.xt[i], y5 = a.yt[i];
+            const double xs = __dadd_rn(a.ctl->absolute_tolerance,
+                                        __dmul_rn(a.ctl->relative_tolerance,
+                                                  max_ref(fabs(a.x0[i]), fabs(x5))));
+            const double ys = __dadd_rn(a.ctl->absolute_tolerance,
+                                        __dmul_rn(a.ctl->relative_tolerance,
+                                                  max_ref(fabs(a.y0[i]), fabs(y5))));
+            if (!isfinite(xe) || !isfinite(ye) || !isfinite(xs) || !isfinite(ys) ||
+                !(xs > 0.0) || !(ys > 0.0)) {
+                set_status(&a.ctl->status, ST_DOPRI_NONFINITE);
+            } else {
+                local_max = max_ref(local_max, __ddiv_rn(fabs(xe), xs));
+                local_max = max_ref(local_max, __ddiv_rn(fabs(ye), ys));
+            }
+        }
+    }
+
+    if (MODE == STAGE_DOPRI_ERROR) {
+        // Block max (max is exact, so the order of the reduction cannot change the result).
+        for (int off = 16; off > 0; off >>= 1)
+            local_max = max_ref(local_max, __shfl_xor_sync(0xffffffffu, local_max, off));
+        if ((tid & 31) == 0)
+            s_max[tid >> 5] = local_max;
+        __syncthreads();
+        if (tid == 0) {
+            double m = 0.0;
+            for (int w = 0; w < static_cast<int>(blockDim.x >> 5); ++w)
+                m = max_ref(m, s_max[w]);
+            atomicMax(&a.ctl->err_bits, ordered_bits(m));
+            __threadfence();
+            const unsigned done = atomicAdd(&a.ctl->blocks_done, 1u);
+            if (done == gridDim.x - 1) {
+                __threadfence();
+                dopri_control(a.ctl);
+            }
+        }
+    }
+}
+
+__global__ void __launch_bounds__(256)
+    accept_kernel(double *x, double *y, const double *xt, const double *yt, double *k0x,
+                  double *k0y, const double *k6x, const double *k6y, size_t n, int dopri,
+                  const DeviceControl *ctl) {
+    if (ctl->status != 0 || (dopri && !ctl->accepted))
+        return;
+    for (size_t i = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; i < n;
+         i += static_cast<size_t>(gridDim.x) * blockDim.x) {
+        x[i] = xt[i];
+        y[i] = yt[i];
+        if (dopri) { // FSAL: k7 of the accepted step is k1 of the next (src/timestep.cpp:104-108)
+            k0x[i] = k6x[i];
+            k0y[i] = k6y[i];
+        }
+    }
+}
+
+namespace {
+unsigned grid_for(size_t n, int sm_count) {
+    const size_t blocks = (n + 255) / 256;
+    const size_t cap = static_cast<size_t>(sm_count > 0 ? sm_count : 148) * 8;
+    return static_cast<unsigned>(blocks < 1 ? 1 : (blocks < cap ? blocks : cap));
+}
+} // namespace
+
+cudaError_t launch_stage(const StageArgs &a, cudaStream_t stream, int sm_count) {
+    const unsigned grid = grid_for(a.n, sm_count);
+    switch (a.mode) {
+    case STAGE_REDUCE_ONLY:
+        stage_kernel<STAGE_REDUCE_ONLY><<<grid, 256, 0, stream>>>(a);
+        break;
+    case STAGE_POSITION:
+        stage_kernel<STAGE_POSITION><<<grid, 256, 0, stream>>>(a);
+        break;
+    case STAGE_RK4_COMBINE:
+        stage_kernel<STAGE_RK4_COMBINE><<<grid, 256, 0, stream>>>(a);
+        break;
+    case STAGE_DOPRI_ERROR:
+        stage_kernel<STAGE_DOPRI_ERROR><<<grid, 256, 0, stream>>>(a);
+        break;
+    default:
+        return cudaErrorInvalidValue;
+    }
+    return cudaGetLastError();
+}
+
+cudaError_t launch_accept(double *x, double *y, const double *xt, const double *yt, double *k0x,
+                          double *k0y, const double *k6x, const double *k6y, size_t n, int dopri,
+                          DeviceControl *ctl, cudaStream_t stream) {
+    accept_kernel<<<grid_for(n, 0), 256, 0, stream>>>(x, y, xt, yt, k0x, k0y, k6x, k6y, n, dopri,
+                                                       ctl);
+    return cudaGetLastError();
+}
+
+} // namespace pvb

@@ -1,0 +1,142 @@
+"""Generates the golden fixtures in this directory from the UNMODIFIED reference.
+
+Run in a tree where the reference sources are available (it builds oracle/_ref/ first):
+
+    python tests/golden/make_golden.py [--reference /path/to/PointVortex]
+
+Every number stored here comes from the reference's own code (src/compute.cpp, src/timestep.cpp,
+src/dipole.cpp of jplaurie/PointVortex), called through oracle/ref_shim.cpp. The initial
+conditions come from pointvortex_b200/ics.py and are stored beside the results, so the tests
+need neither the reference nor a random generator to use them.
+"""
+from __future__ import annotations
+
+import argparse
+import importlib.util
+import os
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, ROOT)
+
+from oracle.pyoracle import Geometry, Oracle  # noqa: E402
+
+_spec = importlib.util.spec_from_file_location("ics", os.path.join(ROOT, "pointvortex_b200", "ics.py"))
+ics = importlib.util.module_from_spec(_spec)
+_spec.loader.exec_module(ics)
+
+
+def save(name: str, **arrays) -> None:
+    path = os.path.join(HERE, name)
+    np.savez_compressed(path, **arrays)
+    print(f"{name}: {os.path.getsize(path) / 1024:.1f} KiB", flush=True)
+
+
+def small_case(ref: Oracle, geo: Geometry, x, y, g, tag: str) -> None:
+    u, v = ref.evaluate(geo, x, y, g)
+    inv = ref.invariants(geo, x, y, g)
+    st = ref.stepper(geo, x.size)
+    rk_x, rk_y = [x.copy()], [y.copy()]
+    for _ in range(3):
+        nx, ny = st.rk4_step(rk_x[-1], rk_y[-1], g, 1e-3)
+        rk_x.append(nx)
+        rk_y.append(ny)
+    dp = ref.stepper(geo, x.size)
+    dp_x, dp_y, dp_r = [x.copy()], [y.copy()], []
+    dt = 1e-3
+    for _ in range(3):
+        nx, ny, r = dp.dopri5_step(dp_x[-1], dp_y[-1], g, dt)
+        dp_x.append(nx)
+        dp_y.append(ny)
+        dp_r.append(r)
+        dt = r[1]
+    save(f"small_{tag}.npz", x=x, y=y, g=g, u=u, v=v, inv=inv, rk_x=np.array(rk_x),
+         rk_y=np.array(rk_y), dp_x=np.array(dp_x), dp_y=np.array(dp_y), dp_r=np.array(dp_r),
+         params=np.array([geo.core_radius, geo.box_length_x, geo.image_layers, geo.disk_radius,
+                          geo.absolute_tolerance, geo.relative_tolerance]))
+
+
+def main() -> int:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--reference", default="/root/reference")
+    args = ap.parse_args()
+    subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle"), "ref",
+                    f"REF={args.reference}"], check=True)
+    ref = Oracle("reference")
+    t0 = time.time()
+
+    # small cases, all three geometries (+ the core-radius plane)
+    for tag, geo, (x, y, g) in [
+        ("infinite", Geometry("infinite"), ics.infinite_plane(64, 11)),
+        ("infinite_core", Geometry("infinite", core_radius=0.05), ics.infinite_plane(64, 12)),
+        ("periodic", Geometry("periodic", box_length_x=2.0, box_length_y=2.0),
+         ics.periodic_box(64, 13, 2.0)),
+        ("periodic_m3", Geometry("periodic", box_length_x=2.0, box_length_y=2.0, image_layers=3),
+         ics.periodic_box(64, 14, 2.0)),
+        ("disk", Geometry("disk", disk_radius=1.0), ics.disk(64, 15, 1.0, 0.8, gaussian=False)),
+    ]:
+        small_case(ref, geo, x, y, g, tag)
+
+    # the three single-simulation workloads at full size (target samples where the reference
+    # CPU path is too slow for the full matrix)
+    x, y, g = ics.workload_state("infinite_rk4_n1024")
+    geo = Geometry("infinite")
+    u, v = ref.evaluate(geo, x, y, g)
+    inv = ref.invariants(geo, x, y, g)
+    st = ref.stepper(geo, x.size)
+    xs, ys = [x.copy()], [y.copy()]
+    for _ in range(5):
+        nx, ny = st.rk4_step(xs[-1], ys[-1], g, 1e-3)
+        xs.append(nx)
+        ys.append(ny)
+    save("workload_infinite_n1024.npz", x=x, y=y, g=g, u=u, v=v, inv=inv, rk_x=np.array(xs),
+         rk_y=np.array(ys))
+
+    x, y, g = ics.workload_state("periodic_dopri5_n4096")
+    geo = Geometry("periodic", box_length_x=2 * np.pi, box_length_y=2 * np.pi)
+    u, v = ref.evaluate_range(geo, x, y, g, 0, 256)
+    inv = ref.invariants(geo, x, y, g)
+    save("workload_periodic_n4096.npz", x=x, y=y, g=g, u=u, v=v, inv=inv, targets=np.array([0, 256]))
+
+    x, y, g = ics.workload_state("disk_rk4_n16384")
+    geo = Geometry("disk", disk_radius=1.0)
+    u, v = ref.evaluate_range(geo, x, y, g, 0, 256)
+    inv = ref.invariants(geo, x, y, g)
+    save("workload_disk_n16384.npz", x=x, y=y, g=g, u=u, v=v, inv=inv, targets=np.array([0, 256]))
+
+    # close-dipole removal (removal only): states with planted close opposite-sign pairs
+    rng = np.random.default_rng(16)
+    for tag, geo, (x, y, g) in [
+        ("periodic", Geometry("periodic", box_length_x=2.0, box_length_y=2.0,
+                              dipole_removal=True, dipole_removal_distance=0.05),
+         ics.periodic_box(200, 17, 2.0)),
+        ("disk", Geometry("disk", disk_radius=1.0, dipole_removal=True,
+                          dipole_removal_distance=0.05), ics.disk(200, 18, 1.0, 0.999, gaussian=False)),
+        ("infinite", Geometry("infinite", dipole_removal=True, dipole_removal_distance=0.05),
+         ics.infinite_plane(200, 19)),
+    ]:
+        x, y = x.copy(), y.copy()
+        # move a few positive vortices next to negative ones (and across the periodic seam)
+        pos = np.flatnonzero(g > 0)[:6]
+        neg = np.flatnonzero(g < 0)[:6]
+        for k, (a, b) in enumerate(zip(pos, neg)):
+            x[a] = x[b] + 0.01 * (k + 1) * 0.5
+            y[a] = y[b] - 0.004 * k
+        if tag == "periodic":
+            x[pos[5]], x[neg[5]] = 0.995, -0.997
+            y[pos[5]] = y[neg[5]]
+        events, sx, sy, sg = ref.dipole_process(geo, x, y, g)
+        save(f"dipole_{tag}.npz", x=x, y=y, g=g, events=np.array([events]), sx=sx, sy=sy, sg=sg,
+             threshold=np.array([geo.dipole_removal_distance]))
+    print(f"done in {time.time() - t0:.1f} s")
+    _ = rng
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

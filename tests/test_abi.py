@@ -1,0 +1,67 @@
+"""The C ABI library without a GPU: it loads, exports every function include/pvb200.h declares,
+and fails cleanly (a CUDA error status and message, no crash) when no device is present."""
+import ctypes
+import os
+import re
+
+import pytest
+
+from conftest import ROOT
+
+HEADER = os.path.join(ROOT, "include", "pvb200.h")
+
+
+def declared_functions():
+    text = open(HEADER).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(pv_[a-z0-9_]+)\s*\(", text)))
+
+
+def test_header_declares_the_boundary():
+    names = declared_functions()
+    for required in ["pv_context_create", "pv_context_destroy", "pv_last_error", "pv_evaluate",
+                     "pv_evaluate_range", "pv_hamiltonian", "pv_invariants", "pv_upload_state",
+                     "pv_download_state", "pv_evaluate_state", "pv_rk4_step", "pv_dopri5_step",
+                     "pv_invalidate_derivative", "pv_state_invariants", "pv_dipole_scan"]:
+        assert required in names
+
+
+def test_library_exports_every_declared_symbol():
+    from pointvortex_b200 import _lib
+    lib = ctypes.CDLL(_lib.LIB_PATH)
+    missing = [n for n in declared_functions() if not hasattr(lib, n)]
+    assert not missing, missing
+    assert set(declared_functions()) == set(_lib.SIGNATURES)
+
+
+def test_backend_name():
+    import pointvortex_b200 as pv
+    assert pv.backendName() == "CUDA/B200"
+
+
+def _has_gpu():
+    try:
+        import torch
+        return torch.cuda.is_available()
+    except Exception:
+        return False
+
+
+@pytest.mark.skipif(_has_gpu(), reason="checks the no-device failure path")
+def test_context_creation_without_device_is_a_clean_error():
+    import pointvortex_b200 as pv
+    with pytest.raises(pv.CudaError):
+        pv.InfinitePlaneKernel()
+
+
+def test_parameter_validation_precedes_device_access():
+    """The kernel constructors' checks (src/compute.cpp:50-56, 165-173, 258-261) run on the host
+    and raise ValueError even on a machine without a GPU."""
+    import pointvortex_b200 as pv
+    cases = [(lambda: pv.InfinitePlaneKernel(-1.0), "core radius is negative"),
+             (lambda: pv.PeriodicBoxKernel(2.0, 2.0, 65), "invalid periodic-box parameters"),
+             (lambda: pv.PeriodicBoxKernel(2.0, 2.5), "requires a square periodic box"),
+             (lambda: pv.DiskKernel(0.0), "invalid disk parameters")]
+    for make, message in cases:
+        with pytest.raises(ValueError, match=message):
+            make()
