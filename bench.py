@@ -1,0 +1,420 @@
+"""Benchmark of the B200 point-vortex path.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Workload (one GPU): the periodic-box case -- N = 4096 vortices, uniform in the 2 pi box, balanced
++-1 circulations, Weiss-McWilliams kernel with M = 8 image layers, adaptive DOPRI5 with
+rtol 1e-9 / atol 1e-12, close-dipole detection at separation 1e-3 (removal only) after every
+accepted step. One step = one accepted DOPRI5 step (with its rejections, 6 velocity evaluations
+per attempt thanks to FSAL) plus the dipole scan. The metric is pair-interactions per second,
+N(N-1) per velocity evaluation.
+
+With --gpus N (launched one process per GPU) every rank runs its own independent simulation
+(replicas: the path has no data exchange), and the value is the total over ranks.
+
+--impl reference times the reference's own CPU implementation (the unmodified PointVortex code
+compiled from its sources into oracle/_ref) on the same workload and metric, with all host
+threads, on a bounded sample of targets per step.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+N = 4096
+LENGTH = 2.0 * np.pi
+LAYERS = 8
+RTOL, ATOL, DTMIN, DTMAX, DT0 = 1e-9, 1e-12, 1e-12, 0.1, 1e-3
+DIPOLE_THRESHOLD = 1e-3
+SEED = 20240102
+WORKLOAD = "periodic_dopri5_n4096"
+L2_BYTES = 126 * 1024 * 1024
+METRIC = "pair-interactions/s"
+
+# Algorithmic FP64 operations per ordered pair of the periodic evaluation (FMA = 2, add/mul/
+# reciprocal/rint = 1), as the exp-factored truncated image series is evaluated: two exact
+# remainders and scalings (12), two shared sinh/cosh/sin/cos Taylor series (116), the derived
+# hyperbolic/circular values (20), the two m = 0 denominators (8), the m = +-1..5 image pairs and
+# the conditional m = +-6 terms accumulated as one fraction per axis (152), and the two
+# reciprocals and accumulations (24).
+FLOPS_PER_PAIR_PERIODIC = 332
+
+
+def rank_info():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+class ClockSampler:
+    """Samples SM clocks and throttle reasons with nvidia-smi while the timed region runs."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.rows = []
+        self._stop = threading.Event()
+        self._thread = None
+
+    def _run(self):
+        while not self._stop.is_set():
+            try:
+                out = subprocess.run(["nvidia-smi", "-i", str(self.device),
+                                      f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits"],
+                                     capture_output=True, text=True, timeout=5).stdout.strip()
+                if out:
+                    self.rows.append([c.strip() for c in out.split(",")])
+            except Exception:
+                pass
+            self._stop.wait(0.2)
+
+    def __enter__(self):
+        self._thread = threading.Thread(target=self._run, daemon=True)
+        self._thread.start()
+        return self
+
+    def __exit__(self, *exc):
+        self._stop.set()
+        if self._thread:
+            self._thread.join(timeout=10)
+
+    def summary(self):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"], "samples": 0}
+        sm = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in self.rows for k in range(4)
+                          if len(r) > 5 + k and r[5 + k].lower() == "active"})
+        return {"sm_mhz": float(np.median(sm)) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": reasons,
+                "samples": len(self.rows)}
+
+
+def flush_l2(buf):
+    buf.fill_(1.0)
+
+
+def dopri_step(k, dt, scan=True):
+    """One accepted DOPRI5 step + the close-dipole scan; returns (suggested dt, evaluations)."""
+    before = k.evaluationCount
+    r = k.deviceDopri5Step(dt, ATOL, RTOL, DTMIN, DTMAX)
+    if scan:
+        cands = k.dipoleScan(DIPOLE_THRESHOLD, capacity=64)
+        if cands:
+            remove_dipoles(k, cands)
+    return r.suggestedTimeStep, k.evaluationCount - before
+
+
+def remove_dipoles(k, cands):
+    """Closest-first disjoint removal (DipoleManager::process, src/dipole.cpp:79-127, removal
+    only) on the device candidates; then the state is re-uploaded (FSAL invalidated)."""
+    import pointvortex_b200 as pv
+    n = k.stateSize()
+    s = pv.VortexSystem(np.zeros(n), np.zeros(n), np.zeros(n))
+    s.circulation = k._circulation
+    k.downloadDeviceState(s)
+    chosen = np.zeros(n, bool)
+    for c in cands:
+        if chosen[c.first] or (c.second < n and chosen[c.second]):
+            continue
+        chosen[c.first] = True
+        if c.second < n:
+            chosen[c.second] = True
+    keep = ~chosen
+    new = pv.VortexSystem(s.x[keep], s.y[keep], s.circulation[keep])
+    k.uploadDeviceState(new)
+    k._circulation = new.circulation
+
+
+def run_ours(args):
+    import torch
+    import pointvortex_b200 as pv
+    from pointvortex_b200 import ics
+
+    rank, world, local = rank_info()
+    torch.cuda.set_device(local)
+    if world > 1:
+        import torch.distributed as dist
+        dist.init_process_group("nccl", device_id=torch.device("cuda", local),
+                                timeout=__import__("datetime").timedelta(seconds=120))
+    x, y, g = ics.periodic_box(N, SEED + rank, LENGTH)
+    k = pv.PeriodicBoxKernel(LENGTH, LENGTH, LAYERS, device=local)
+    k.uploadDeviceState(pv.VortexSystem(x, y, g))
+    k._circulation = g.copy()
+    flush = torch.empty(2 * L2_BYTES // 4, dtype=torch.float32, device=f"cuda:{local}")
+
+    # warm-up: the first steps also absorb the start-up rejections (dt 1e-3 -> ~1e-6)
+    dt = DT0
+    for _ in range(max(args.warmup, 3)):
+        dt, _ = dopri_step(k, dt)
+    torch.cuda.synchronize()
+
+    # timed region: CUDA events on the library's own stream bracket each step (kernels, copies
+    # and the gaps while the host reads the step-control word back); the library additionally
+    # brackets every launch with events so that the dominant kernel can be timed on its own
+    k.setProfiling(True)
+    k.resetKernelStats()
+    evals = 0
+    step_ms = []
+    lib_stream = torch.cuda.ExternalStream(k.cudaStream(), device=f"cuda:{local}")
+    events = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+              for _ in range(args.steps)]
+    if world > 1:
+        torch.distributed.barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clocks:
+        for s in range(args.steps):
+            flush_l2(flush)
+            torch.cuda.synchronize()
+            events[s][0].record(lib_stream)
+            dt, e = dopri_step(k, dt)
+            events[s][1].record(lib_stream)
+            evals += e
+        torch.cuda.synchronize()
+    step_ms = [a.elapsed_time(b) for a, b in events]
+    stats = k.kernelStats()
+    k.setProfiling(False)
+    total_ms = float(np.sum(step_ms))
+    if world > 1:
+        t = torch.tensor([total_ms], device=f"cuda:{local}", dtype=torch.float64)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        total_ms = float(t.item())
+        ev = torch.tensor([evals], device=f"cuda:{local}", dtype=torch.float64)
+        torch.distributed.all_reduce(ev)
+        evals_total = float(ev.item())
+    else:
+        evals_total = float(evals)
+    n_now = k.stateSize()
+    pairs = evals_total * n_now * (n_now - 1)
+    value = pairs / (total_ms * 1e-3)
+
+    # e2e: the same steps through the public API with host buffers -- every step uploads its
+    # input state from pinned host memory and downloads the new state and the step result.
+    e2e = measure_e2e(k, dt, max(10, args.steps // 4), local)
+
+    # roofline of the dominant kernel (the tiled periodic pair kernel), from its launch events
+    v_launch, v_timed, v_ms = stats["velocity"]
+    per_launch_ms = v_ms / max(v_timed, 1)
+    flops_per_launch = FLOPS_PER_PAIR_PERIODIC * n_now * (n_now - 1)
+    achieved = flops_per_launch / (per_launch_ms * 1e-3) / 1e12
+    peak = pv.probePeak("fp64", local) / 1e12
+    launches = sum(v[0] for v in stats.values())
+
+    result = None
+    if rank == 0:
+        result = {
+            "metric": METRIC,
+            "value": value,
+            "unit": "pair-interactions/s",
+            "n_gpus": world,
+            "steps": args.steps,
+            "warmup": args.warmup,
+            "ms_per_step": total_ms / args.steps,
+            "higher_is_better": True,
+            "scaling": "weak",
+            "vs_baseline": None,
+            "dtype": "f64",
+            "data": "synthetic (seeded uniform positions, balanced +-1 circulations)",
+            "config": {"workload": WORKLOAD, "geometry": "periodic", "n_vortices": N,
+                       "box_length": "2pi", "image_layers": LAYERS, "integrator": "dopri5",
+                       "rtol": RTOL, "atol": ATOL, "dipole_threshold": DIPOLE_THRESHOLD,
+                       "step": "one accepted DOPRI5 step + dipole scan",
+                       "evaluations_per_rank": evals, "parallelism": f"replicas x{world}",
+                       "l2": "256 MiB write between steps (outside the step timing)"},
+            "e2e": e2e,
+            "gpu_launches": int(launches),
+            "roofline": {"bound": "fp64", "achieved": achieved, "peak": peak,
+                         "unit": "TFLOP/s", "frac": achieved / peak, "traffic": None,
+                         "kernel": "velocity_kernel<PeriodicPair>",
+                         "flops_per_pair": FLOPS_PER_PAIR_PERIODIC,
+                         "ms_per_launch": per_launch_ms, "launches": v_timed,
+                         "peak_source": "measured FP64 FMA probe (pv_probe_peak) on this GPU"},
+            "kernel_ms": {kk: vv[2] for kk, vv in stats.items()},
+            "clocks": clocks.summary(),
+        }
+    return result, k
+
+
+def measure_e2e(k, dt, steps, device):
+    import pointvortex_b200 as pv
+    import torch
+    n = k.stateSize()
+    host = torch.empty((3, n), dtype=torch.float64).pin_memory().numpy()
+    s = pv.VortexSystem(np.zeros(n), np.zeros(n), k._circulation.copy())
+    k.downloadDeviceState(s)
+    host[0], host[1], host[2] = s.x, s.y, s.circulation
+    evals = 0
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        st = pv.VortexSystem(host[0], host[1], host[2])
+        k.uploadDeviceState(st)
+        before = k.evaluationCount
+        r = k.deviceDopri5Step(dt, ATOL, RTOL, DTMIN, DTMAX)
+        k.dipoleScan(DIPOLE_THRESHOLD, capacity=64)
+        k.downloadDeviceState(st)
+        host[0], host[1] = st.x, st.y
+        evals += k.evaluationCount - before
+        dt = r.suggestedTimeStep
+    sec = time.perf_counter() - t0
+    torch.cuda.synchronize(device)
+    return {"value": evals * n * (n - 1) / sec, "unit": "pair-interactions/s",
+            "h2d_bytes_per_step": 3 * 8 * n + 256, "d2h_bytes_per_step": 2 * 8 * n + 256 + 8,
+            "steps": steps, "note": "upload + DOPRI5 step + dipole scan + download per step; "
+            "the upload invalidates FSAL, so each step makes 7 evaluations"}
+
+
+def cpu_baseline(seconds: float = 10.0):
+    """The reference's CPU/OpenMP periodic kernel on a bounded sample of targets of the same
+    state, all host threads."""
+    from oracle.pyoracle import Geometry, Oracle
+    from pointvortex_b200 import ics
+    try:
+        ref = Oracle("reference")
+        kind = "reference"
+    except FileNotFoundError:
+        ref = Oracle("port")
+        kind = "port"
+    x, y, g = ics.periodic_box(N, SEED, LENGTH)
+    geo = Geometry("periodic", box_length_x=LENGTH, box_length_y=LENGTH, image_layers=LAYERS)
+    cores = ref.max_threads()
+    ref.set_threads(cores)
+    t0 = time.perf_counter()
+    ref.evaluate_range(geo, x, y, g, 0, 16)
+    t_probe = max(time.perf_counter() - t0, 1e-4)
+    targets = int(min(N, max(16, 16 * seconds / t_probe)))
+    t0 = time.perf_counter()
+    ref.evaluate_range(geo, x, y, g, 0, targets)
+    sec = time.perf_counter() - t0
+    return {"value": targets * (N - 1) / sec, "unit": "pair-interactions/s", "cores": cores,
+            "kind": kind, "sample": f"velocity of targets [0, {targets}) of the N={N} periodic "
+            f"state against all {N} sources, {sec:.1f} s"}
+
+
+def run_reference(args):
+    rank, world, _ = rank_info()
+    if rank != 0:
+        return None
+    from oracle.pyoracle import Geometry, Oracle
+    from pointvortex_b200 import ics
+    try:
+        ref = Oracle("reference")
+        kind = "reference"
+    except FileNotFoundError:
+        ref = Oracle("port")
+        kind = "port"
+    x, y, g = ics.periodic_box(N, SEED, LENGTH)
+    geo = Geometry("periodic", box_length_x=LENGTH, box_length_y=LENGTH, image_layers=LAYERS)
+    cores = ref.max_threads()
+    ref.set_threads(cores)
+    t0 = time.perf_counter()
+    ref.evaluate_range(geo, x, y, g, 0, 8)
+    per_target = max(time.perf_counter() - t0, 1e-5) / 8
+    budget = 150.0 / max(args.steps + args.warmup, 1)    # whole run within a few minutes
+    targets = int(min(N, max(1, budget / per_target)))
+    for _ in range(args.warmup):
+        ref.evaluate_range(geo, x, y, g, 0, targets)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        ref.evaluate_range(geo, x, y, g, 0, targets)
+    sec = time.perf_counter() - t0
+    value = args.steps * targets * (N - 1) / sec
+    sample = (f"each step: velocity of targets [0, {targets}) of the N={N} periodic state "
+              f"against all {N} sources (the reference's PeriodicBoxKernel::evaluateRange)")
+    return {"metric": METRIC, "value": value, "unit": "pair-interactions/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": sec * 1e3 / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded uniform positions, balanced +-1 circulations)",
+            "impl": "reference",
+            "config": {"workload": WORKLOAD, "geometry": "periodic", "n_vortices": N,
+                       "image_layers": LAYERS},
+            "cpu_baseline": {"value": value, "unit": "pair-interactions/s", "cores": cores,
+                             "kind": kind, "sample": sample},
+            "e2e": {"value": value, "unit": "pair-interactions/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+
+
+def run_kernel_case(spec: str, evals: int) -> dict:
+    """Velocity evaluations only (no stepping), for kernel timing and ncu captures:
+    spec = "geometry:N" with geometry infinite | periodic | disk."""
+    import torch
+    import pointvortex_b200 as pv
+    from pointvortex_b200 import ics
+    geo, n = spec.split(":")
+    n = int(n)
+    if geo == "infinite":
+        x, y, g = ics.infinite_plane(n, 1)
+        k = pv.InfinitePlaneKernel(0.0)
+        flops = 11
+    elif geo == "periodic":
+        x, y, g = ics.periodic_box(n, 2, LENGTH)
+        k = pv.PeriodicBoxKernel(LENGTH, LENGTH, LAYERS)
+        flops = FLOPS_PER_PAIR_PERIODIC
+    else:
+        x, y, g = ics.disk(n, 3, 1.0)
+        k = pv.DiskKernel(1.0)
+        flops = 33
+    k.uploadDeviceState(pv.VortexSystem(x, y, g))
+    for _ in range(2):
+        k.evaluateDeviceState()
+    k.setProfiling(True)
+    k.resetKernelStats()
+    for _ in range(evals):
+        k.evaluateDeviceState()
+    st = k.kernelStats()["velocity"]
+    ms = st[2] / max(st[1], 1)
+    pairs = n * (n - 1)
+    torch.cuda.synchronize()
+    return {"case": spec, "evaluations": evals, "ms_per_evaluation": ms,
+            "pairs_per_s": pairs / (ms * 1e-3), "formula_flops_per_pair": flops,
+            "tflops": flops * pairs / (ms * 1e-3) / 1e12}
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--kernel-case", default=None,
+                    help="geometry:N -- time velocity evaluations only (kernel timing / ncu)")
+    ap.add_argument("--evals", type=int, default=10)
+    args = ap.parse_args(argv)
+    rank, world, _ = rank_info()
+    if args.kernel_case:
+        print(json.dumps(run_kernel_case(args.kernel_case, args.evals)), flush=True)
+        return 0
+    if args.impl == "reference":
+        out = run_reference(args)
+        if out is not None:
+            print(json.dumps(out), flush=True)
+        return 0
+    result, k = run_ours(args)
+    if rank == 0:
+        if not args.no_cpu_baseline and world == 1:
+            result["cpu_baseline"] = cpu_baseline()
+        print(json.dumps(result), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

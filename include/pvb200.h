@@ -170,6 +170,9 @@ typedef struct pv_kernel_stats {
     double milliseconds[PV_KERNEL_KINDS];     /* summed event time of the timed launches */
 } pv_kernel_stats;
 
+/* The context's CUDA stream (a cudaStream_t) through *stream, so that a caller can order its own
+ * work or events after the context's kernels. */
+pv_status pv_context_stream(const pv_context *ctx, void **stream);
 /* Bracket every launch of the context with CUDA events recorded on its own stream. */
 pv_status pv_set_profiling(pv_context *ctx, int enabled);
 /* Synchronises the context stream and returns the counters accumulated since the last reset. */

@@ -95,6 +95,7 @@ SIGNATURES = {
     "pv_evaluation_count": (_ST, [_CTX, ctypes.POINTER(ctypes.c_uint64)]),
     "pv_rk4_advance": (_ST, [_CTX, ctypes.c_double, ctypes.c_uint64]),
     "pv_probe_peak": (_ST, [ctypes.c_int, ctypes.c_int, _D]),
+    "pv_context_stream": (_ST, [_CTX, ctypes.POINTER(ctypes.c_void_p)]),
     "pv_set_profiling": (_ST, [_CTX, ctypes.c_int]),
     "pv_get_kernel_stats": (_ST, [_CTX, ctypes.POINTER(PvKernelStats)]),
     "pv_reset_kernel_stats": (_ST, [_CTX]),

@@ -971,6 +971,13 @@ pv_status pv_evaluation_count(const pv_context *ctx, uint64_t *count) {
     return PV_OK;
 }
 
+pv_status pv_context_stream(const pv_context *ctx, void **stream) {
+    if (!ctx || !stream)
+        return PV_ERROR_INVALID_ARGUMENT;
+    *stream = static_cast<void *>(ctx->stream);
+    return PV_OK;
+}
+
 pv_status pv_set_profiling(pv_context *ctx, int enabled) {
     if (!ctx)
         return PV_ERROR_INVALID_ARGUMENT;

@@ -285,6 +285,12 @@ class VelocityKernel:
     def rk4Advance(self, dt: float, steps: int) -> None:
         self._check(lib.pv_rk4_advance(self._ctx, dt, steps))
 
+    def cudaStream(self) -> int:
+        """The context's cudaStream_t as an integer (e.g. for torch.cuda.ExternalStream)."""
+        s = ctypes.c_void_p()
+        self._check(lib.pv_context_stream(self._ctx, ctypes.byref(s)))
+        return int(s.value or 0)
+
     def setProfiling(self, enabled: bool) -> None:
         """Bracket every kernel launch with CUDA events on the context's stream."""
         self._check(lib.pv_set_profiling(self._ctx, int(bool(enabled))))
