@@ -28,7 +28,7 @@ def state(name, n, seed):
     if name == "periodic":
         return ics.periodic_box(n, seed, 2.0)
     if name == "disk":
-        return ics.disk(n, seed, 1.0, 0.8)
+        return ics.disk(n, seed, 1.0, 0.8, gaussian=False)
     return ics.infinite_plane(n, seed)
 
 
@@ -96,7 +96,7 @@ def test_dopri_sequence_against_oracle(port, name):
     ref = port.stepper(geo, x.size)
     gpu = GpuStepper(geo)
     rx, ry, gx, gy = x, y, x, y
-    dt = 5e-3
+    dt = 1e-3
     for _ in range(4):
         rx2, ry2, rr = ref.dopri5_step(rx, ry, g, dt)
         # teacher forcing: the GPU steps from the oracle's state; the upload only happens when the
