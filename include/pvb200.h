@@ -85,8 +85,8 @@ typedef struct pv_context pv_context;
 pv_status pv_context_create(const pv_params *params, int device, pv_context **out);
 /* ~VelocityKernel; frees every device buffer of the context. */
 void pv_context_destroy(pv_context *ctx);
-/* Message of the last failure on ctx, or of the calling thread's last pv_context_create
- * failure when ctx is NULL. Valid until the next call on the same context/thread. */
+/* Message of the last failure on ctx, or, when ctx is NULL, of the calling thread's last failed
+ * call that takes no context. Valid until the next call on the same context/thread. */
 const char *pv_last_error(const pv_context *ctx);
 /* backendName (src/backend.h:13). */
 const char *pv_backend_name(void);
@@ -153,6 +153,27 @@ pv_status pv_evaluation_count(const pv_context *ctx, uint64_t *count);
 
 /* `steps` RK4 steps of size dt, enqueued back to back with one synchronisation at the end. */
 pv_status pv_rk4_advance(pv_context *ctx, double dt, uint64_t steps);
+
+/* ---- allocation-free evaluation (no counterpart in the reference) ------------------------ */
+
+/* Largest population pv_evaluate_device_noalloc accepts. */
+#define PV_NOALLOC_MAX_VORTICES 349440
+
+/* VelocityKernel::evaluate semantics for n vortices whose arrays are already in GPU memory, for
+ * callers that cannot allocate device memory or let a library allocate it: hosts that own all GPU
+ * memory through their own pool, and time-stepping loops that cannot pay for the device-wide
+ * synchronisation of cudaMalloc/cudaFree. x, y, circulation (16-byte aligned) and u, v are DEVICE
+ * pointers of the current device; stream is a cudaStream_t (NULL: the legacy default stream).
+ * Creates no context and calls no allocator: its scratch (8 MiB: scaled circulations, chunk partial
+ * sums, status word) is one fixed device array inside the library, held by every GPU that loads
+ * the library until the process exits. n above PV_NOALLOC_MAX_VORTICES is rejected with
+ * PV_ERROR_INVALID_ARGUMENT. The call synchronises `stream`; the message of a failure is returned
+ * by pv_last_error(NULL). The first call on a device looks up the array's device address (do it
+ * before any stream capture). All calls on a device share the array, so calls whose GPU work
+ * overlaps in time race and must be ordered by the caller. FP64 only. */
+pv_status pv_evaluate_device_noalloc(const pv_params *params, const double *x, const double *y,
+                                     const double *circulation, size_t n, double *u, double *v,
+                                     void *stream);
 
 /* ---- diagnostics (no reference counterpart) --------------------------------------------- */
 

@@ -94,6 +94,9 @@ SIGNATURES = {
     "pv_state_size": (_ST, [_CTX, ctypes.POINTER(_SZ)]),
     "pv_evaluation_count": (_ST, [_CTX, ctypes.POINTER(ctypes.c_uint64)]),
     "pv_rk4_advance": (_ST, [_CTX, ctypes.c_double, ctypes.c_uint64]),
+    "pv_evaluate_device_noalloc": (_ST, [ctypes.POINTER(PvParams), ctypes.c_void_p, ctypes.c_void_p,
+                                         ctypes.c_void_p, _SZ, ctypes.c_void_p, ctypes.c_void_p,
+                                         ctypes.c_void_p]),
     "pv_probe_peak": (_ST, [ctypes.c_int, ctypes.c_int, _D]),
     "pv_context_stream": (_ST, [_CTX, ctypes.POINTER(ctypes.c_void_p)]),
     "pv_set_profiling": (_ST, [_CTX, ctypes.c_int]),

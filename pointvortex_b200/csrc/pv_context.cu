@@ -523,6 +523,13 @@ pv_status invariants_of(pv_context *c, const double *x, const double *y, const d
 
 } // namespace
 
+namespace pvb {
+int make_geometry_consts(const pv_params &p, GeometryConsts &g, std::string &message) {
+    return make_consts(p, g, message);
+}
+void set_thread_error(const std::string &message) { g_create_error = message; }
+} // namespace pvb
+
 // =============================================================================================
 // C ABI
 // =============================================================================================

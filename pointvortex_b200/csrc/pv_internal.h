@@ -5,6 +5,8 @@
 #include <stddef.h>
 #include <stdint.h>
 
+#include <string>
+
 #include "pv_geometry.cuh"
 
 namespace pvb {
@@ -99,6 +101,12 @@ cudaError_t launch_dipole_scan(const double *x, const double *y, const double *g
                                const GeometryConsts &g, double threshold,
                                DipoleCandidateDev *out, size_t capacity,
                                unsigned long long *count, cudaStream_t stream);
+
+// ---- shared host helpers (pv_context.cu) -------------------------------------------------------
+// Kernel-constructor validation and fast-path constants of a parameter set.
+int make_geometry_consts(const struct pv_params &p, GeometryConsts &g, std::string &message);
+// Sets the calling thread's message returned by pv_last_error(NULL).
+void set_thread_error(const std::string &message);
 
 // ---- diagnostics --------------------------------------------------------------------------------
 cudaError_t launch_peak_probe(int kind, int blocks, int threads, int iterations, double *sink,
