@@ -42,12 +42,13 @@ L2_BYTES = 126 * 1024 * 1024
 METRIC = "pair-interactions/s"
 
 # Algorithmic FP64 operations per ordered pair of the periodic evaluation (FMA = 2, add/mul/
-# reciprocal/rint = 1), as the exp-factored truncated image series is evaluated: two exact
-# remainders and scalings (12), two shared sinh/cosh/sin/cos Taylor series (116), the derived
-# hyperbolic/circular values (20), the two m = 0 denominators (8), the m = +-1..5 image pairs and
-# the conditional m = +-6 terms accumulated as one fraction per axis (152), and the two
-# reciprocals and accumulations (24).
-FLOPS_PER_PAIR_PERIODIC = 332
+# reciprocal/rint = 1), as the truncated image series is evaluated (pv_geometry.cuh,
+# PeriodicPair): per axis the displacement, exact remainder and scaling (7) and the shared
+# sinh/cosh/sin/cos Taylor series of the half angle (48); the derived cosh, cos, sin, sinh of the
+# full angles (20) and the two m = 0 denominators (8); per axis the image sum -- setup (6), the
+# exact m = +-1, +-2 pairs (18), the m = 3..5 expansion (6) and the m = +-6 terms (5); per axis
+# the combination, reciprocal and update (16).
+FLOPS_PER_PAIR_PERIODIC = 240
 
 
 def rank_info():
@@ -384,6 +385,50 @@ def run_kernel_case(spec: str, evals: int) -> dict:
             "tflops": flops * pairs / (ms * 1e-3) / 1e12}
 
 
+def run_reference_cuda(evals: int = 3, steps: int = 3) -> dict:
+    """The reference's own CUDA backend (src/backend_cuda.cu, built for sm_100a into
+    oracle/_ref/libpvref_cuda.so) on the same state: FP64, one thread per target, a host
+    round trip after every evaluation. Runs in its own process."""
+    import ctypes
+    from oracle.pyoracle import REF_CUDA_LIB, _Params
+    from pointvortex_b200 import ics
+    lib = ctypes.CDLL(REF_CUDA_LIB)
+    D = ctypes.POINTER(ctypes.c_double)
+    lib.pvref_stepper_create.restype = ctypes.c_void_p
+    lib.pvref_stepper_create.argtypes = [ctypes.POINTER(_Params), ctypes.c_size_t]
+    lib.pvref_device_upload.argtypes = [ctypes.c_void_p, D, D, D, ctypes.c_size_t]
+    lib.pvref_device_evaluate.argtypes = [ctypes.c_void_p, D, D, ctypes.c_size_t]
+    lib.pvref_device_dopri5_step.argtypes = [ctypes.c_void_p, ctypes.c_double, D]
+    lib.pvref_last_error.restype = ctypes.c_char_p
+    x, y, g = ics.periodic_box(N, SEED, LENGTH)
+    par = _Params(1, 0.0, LENGTH, LENGTH, LAYERS, 1.0, ATOL, RTOL, DTMIN, DTMAX, 0, 0.01, 0, 1)
+    h = lib.pvref_stepper_create(ctypes.byref(par), N)
+    p = lambda a: a.ctypes.data_as(D)
+    if lib.pvref_device_upload(h, p(x), p(y), p(g), N):
+        return {"unavailable": lib.pvref_last_error().decode()}
+    u, v = np.empty(N), np.empty(N)
+    lib.pvref_device_evaluate(h, p(u), p(v), N)
+    t0 = time.perf_counter()
+    for _ in range(evals):
+        lib.pvref_device_evaluate(h, p(u), p(v), N)
+    t_eval = (time.perf_counter() - t0) / evals
+    out = np.zeros(4)
+    dt = DT0
+    for _ in range(3):  # absorb the start-up rejections
+        if lib.pvref_device_dopri5_step(h, dt, p(out)):
+            return {"unavailable": lib.pvref_last_error().decode()}
+        dt = out[1]
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        lib.pvref_device_dopri5_step(h, dt, p(out))
+        dt = out[1]
+    t_step = (time.perf_counter() - t0) / steps
+    return {"impl": "reference CUDA backend (src/backend_cuda.cu, sm_100a)", "dtype": "f64",
+            "ms_per_evaluation": t_eval * 1e3, "pairs_per_s": N * (N - 1) / t_eval,
+            "ms_per_dopri5_step": t_step * 1e3,
+            "note": "wall clock per call; the backend synchronises after every evaluation"}
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -394,8 +439,13 @@ def main(argv=None):
     ap.add_argument("--kernel-case", default=None,
                     help="geometry:N -- time velocity evaluations only (kernel timing / ncu)")
     ap.add_argument("--evals", type=int, default=10)
+    ap.add_argument("--reference-cuda", action="store_true",
+                    help="time the reference's own CUDA backend on the workload (own process)")
     args = ap.parse_args(argv)
     rank, world, _ = rank_info()
+    if args.reference_cuda:
+        print(json.dumps(run_reference_cuda()), flush=True)
+        return 0
     if args.kernel_case:
         print(json.dumps(run_kernel_case(args.kernel_case, args.evals)), flush=True)
         return 0
@@ -408,6 +458,16 @@ def main(argv=None):
     if rank == 0:
         if not args.no_cpu_baseline and world == 1:
             result["cpu_baseline"] = cpu_baseline()
+            try:
+                rc = subprocess.run([sys.executable, os.path.abspath(__file__), "--reference-cuda"],
+                                    capture_output=True, text=True, timeout=300)
+                ref_gpu = json.loads(rc.stdout.strip().splitlines()[-1])
+                if "ms_per_dopri5_step" in ref_gpu:
+                    ref_gpu["speedup_per_dopri5_step"] = (ref_gpu["ms_per_dopri5_step"]
+                                                          / result["ms_per_step"])
+                result["reference_cuda_fp64"] = ref_gpu
+            except Exception as exc:  # reported, never fatal to the benchmark line
+                result["reference_cuda_fp64"] = {"unavailable": str(exc)[:200]}
         print(json.dumps(result), flush=True)
     if world > 1:
         import torch.distributed as dist

@@ -282,17 +282,25 @@ pv_status make_consts(const pv_params &p, GeometryConsts &g, std::string &messag
         g.half_ly = 0.5 * ly;
         g.wave = 2.0 * kPi / lx;
         g.scale = 0.5 / lx;
-        g.m_pairs = std::min(p.image_layers, 5);
+        g.m_exact = std::min(p.image_layers, 2);
         g.has6 = p.image_layers >= 6 ? 1 : 0;
-        for (int m = 0; m <= 5; ++m) {
+        for (int m = 0; m <= 2; ++m) {
             const double a = 2.0 * kPi * m;
             g.cosh_m[m] = std::cosh(a);
+            g.two_cosh_m[m] = 2.0 * g.cosh_m[m];
             const double s = std::sinh(a);
             g.sinh2_m[m] = s * s;
         }
+        // images m = 3..5 enter through 2u C + 2u^2 c cosh 2x^, u = sech(2 pi m)
+        g.k1 = 0.0;
+        g.k2 = 0.0;
+        for (int m = 3; m <= std::min(p.image_layers, 5); ++m) {
+            const double u = 1.0 / std::cosh(2.0 * kPi * m);
+            g.k1 += 2.0 * u;
+            g.k2 += 2.0 * u * u;
+        }
+        g.k6 = g.has6 ? 2.0 * std::exp(-12.0 * kPi) : 0.0;
         g.shift6 = 2.0 * kPi * static_cast<double>(6);
-        g.cosh6 = std::cosh(12.0 * kPi);
-        g.sinh6 = std::sinh(12.0 * kPi);
         return PV_OK;
     }
     if (p.geometry == PV_GEOMETRY_DISK) {

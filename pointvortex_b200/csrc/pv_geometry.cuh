@@ -31,12 +31,14 @@ struct GeometryConsts {
     double half_lx, half_ly;
     double wave;            // 2 pi / Lx
     double scale;           // 0.5 / Lx
-    int m_pairs;            // images m = +-1..m_pairs that are never dropped (min(M, 5))
+    int m_exact;            // image pairs m = +-1..m_exact summed exactly (min(M, 2))
     int has6;               // images m = +-6 kept when within the |shift| <= 40 window (M >= 6)
-    double cosh_m[6];       // cosh(2 pi m), m = 0..5
-    double sinh2_m[6];      // sinh(2 pi m)^2
+    double cosh_m[3];       // cosh(2 pi m), m = 0..2
+    double two_cosh_m[3];   // 2 cosh(2 pi m)
+    double sinh2_m[3];      // sinh(2 pi m)^2
+    double k1, k2;          // 2 sum sech(2 pi m), 2 sum sech^2(2 pi m) over m = 3..min(M, 5)
+    double k6;              // 2 exp(-12 pi) when M >= 6, else 0
     double shift6;          // (2 pi) * 6, rounded as the reference rounds it
-    double cosh6, sinh6;    // cosh(12 pi), sinh(12 pi)
     // disk
     double radius, radius2, inv_radius, inv_radius2;
 };
@@ -102,49 +104,47 @@ struct DiskPair {
 // With x^ = (2 pi/L) remainder(dx, L), y^ likewise, the reference adds per source
 //   u -= k sin(y^) sum_m 1/D_u(m),  D_u(m) = 2 (sinh^2((x^ - 2 pi m)/2) + sin^2(y^/2)),
 //   v += k sin(x^) sum_m 1/D_v(m),  D_v(m) = 2 (sinh^2((y^ - 2 pi m)/2) + sin^2(x^/2)).
-// The same truncated series is evaluated here with one division per axis:
+// The same truncated sum is evaluated here with one reciprocal per axis. With C = cosh x^,
+// c = cos y^, a = 2 pi m, A = cosh a, D(m) = cosh(x^ - a) - c:
 //   * m = 0 keeps the cancellation-free form 2 (sinh^2(x^/2) + sin^2(y^/2));
-//   * m and -m (1 <= m <= 5, never dropped because |x^| <= pi) are combined exactly:
-//       D(m) = cosh(x^ - a) - cos y^,  a = 2 pi m,
-//       D(m) + D(-m) = 2 (cosh x^ cosh a - cos y^),
-//       D(m) D(-m)   = (cosh x^ - cos y^ cosh a)^2 + sinh^2 a sin^2 y^   (a sum of squares),
-//   * m = +-6 enter singly, each only when |x^ -+ 12 pi| <= 40 as in the reference;
-//   * |m| >= 7 always has |shift| > 40 and is dropped, as in the reference;
-//   * the m != 0 terms are accumulated as one fraction N/D (every D(m) >= cosh(pi) - 1 > 10, and
-//     the product over m stays below 1e113), so each axis costs one reciprocal.
-// sinh, cosh, sin, cos of x^/2 and y^/2 come from sinh_cosh_sin_cos (|x^/2| <= pi/2).
+//   * m = +-1, +-2 (never dropped, since |x^| <= pi) combine exactly in pairs,
+//       D(m) + D(-m) = 2 (C A - c),   D(m) D(-m) = C^2 + c^2 - 2 c C A + sinh^2 a,
+//     where every term of the product is far from cancelling (sinh^2 a >= 7e4 > 2 |c| C A);
+//   * m = +-3..+-5: with u = sech a <= 1.3e-8 the pair sum is
+//       2u C + 2u^2 c cosh 2x^ + O(u^3 C^3),
+//     and the omitted terms are below 1e-19 of the m = 0 term, far under FP64 rounding;
+//   * m = +-6 enter only where |x^ -+ 12 pi| <= 40, as in the reference, each as
+//     2 e^{-12 pi} e^{+-x^} (relative error below 1e-14 on a term below 2e-15 of the sum);
+//   * |m| >= 7 always has |shift| > 40 and is dropped, as in the reference.
+// sinh, cosh, sin and cos of x^/2 and y^/2 come from one shared series (|x^/2| <= pi/2).
 struct PeriodicPair {
-    __device__ __forceinline__ static double axis_sum(const GeometryConsts &g, double hat,
-                                                      double cosh_hat, double sinh_hat,
-                                                      double cos_other, double sin2_other,
-                                                      double d0, double &den_out) {
-        double num = 0.0, den = 1.0;
+    // Images m != 0 of one axis as num/den + rest.
+    __device__ __forceinline__ static void image_sum(const GeometryConsts &g, double hat, double ch,
+                                                     double sh, double c, double &num, double &den,
+                                                     double &rest) {
+        const double ch2 = ch * ch;
+        const double p = fma(c, c, ch2);   // C^2 + c^2
+        const double q = -2.0 * c * ch;    // -2 c C
+        const double m2c = -2.0 * c;
+        num = 0.0;
+        den = 1.0;
 #pragma unroll
-        for (int m = 1; m <= 5; ++m) {
-            if (m <= g.m_pairs) {
-                const double pair_num = 2.0 * fma(cosh_hat, g.cosh_m[m], -cos_other);
-                const double p = fma(-cos_other, g.cosh_m[m], cosh_hat);
-                const double pair_den = fma(p, p, g.sinh2_m[m] * sin2_other);
+        for (int m = 1; m <= 2; ++m) {
+            if (m <= g.m_exact) {
+                const double pair_num = fma(ch, g.two_cosh_m[m], m2c);
+                const double pair_den = fma(q, g.cosh_m[m], p + g.sinh2_m[m]);
                 num = fma(pair_num, den, num * pair_den);
                 den *= pair_den;
             }
         }
+        const double ch2x = fma(2.0, ch2, -1.0); // cosh 2x^
+        rest = fma(ch, g.k1, c * ch2x * g.k2);
         if (g.has6) {
-            // cosh(x^ -+ 12 pi) = cosh(12 pi) cosh x^ -+ sinh(12 pi) sinh x^; each single term is
-            // added as num/den + 1/dm = (num dm + den)/(den dm), or skipped (factor 1, addend 0).
-            const double base = fma(g.cosh6, cosh_hat, -cos_other);
             const bool plus = fabs(hat - g.shift6) <= 40.0;
             const bool minus = fabs(hat + g.shift6) <= 40.0;
-            const double dp = plus ? fma(-g.sinh6, sinh_hat, base) : 1.0;
-            num = fma(num, dp, plus ? den : 0.0);
-            den *= dp;
-            const double dn = minus ? fma(g.sinh6, sinh_hat, base) : 1.0;
-            num = fma(num, dn, minus ? den : 0.0);
-            den *= dn;
+            const double e = (plus ? ch + sh : 0.0) + (minus ? ch - sh : 0.0);
+            rest = fma(g.k6, e, rest);
         }
-        // sum_m 1/D(m) = 1/d0 + num/den = (den + d0 num) / (d0 den)
-        den_out = d0 * den;
-        return fma(d0, num, den);
     }
 
     template <bool CHECK>
@@ -170,17 +170,20 @@ struct PeriodicPair {
             d0u = 1.0;
             d0v = 1.0;
         }
-        double den_u, den_v;
-        const double num_u = axis_sum(g, xh, cosh_x, sinh_x, cos_y, sin_y * sin_y, d0u, den_u);
-        const double num_v = axis_sum(g, yh, cosh_y, sinh_y, cos_x, sin_x * sin_x, d0v, den_v);
-        double cu = sg * sin_y * num_u;
-        double cv = sg * sin_x * num_v;
+        double nu, du, ru, nv, dv, rv;
+        image_sum(g, xh, cosh_x, sinh_x, cos_y, nu, du, ru);
+        image_sum(g, yh, cosh_y, sinh_y, cos_x, nv, dv, rv);
+        // 1/d0 + num/den + rest = (den + d0 (num + den rest)) / (d0 den)
+        const double numer_u = fma(d0u, fma(du, ru, nu), du);
+        const double numer_v = fma(d0v, fma(dv, rv, nv), dv);
+        double cu = sg * sin_y * numer_u;
+        double cv = sg * sin_x * numer_v;
         if (CHECK && self) {
             cu = 0.0;
             cv = 0.0;
         }
-        u = fma(-cu, rcp_refined(den_u), u);
-        v = fma(cv, rcp_refined(den_v), v);
+        u = fma(-cu, rcp_refined(d0u * du), u);
+        v = fma(cv, rcp_refined(d0v * dv), v);
     }
 };
 

@@ -177,6 +177,26 @@ cudaError_t launch_pair(const EvalArgs &a, const EvalPlan &p, cudaStream_t strea
 }
 } // namespace
 
+namespace {
+// Resident CTAs per SM of one kernel instance (registers and shared memory decide it).
+template <class Pair, int T> int resident_ctas() {
+    static int cached = -1;
+    if (cached < 0) {
+        int blocks = 0;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, velocity_kernel<Pair, 128, T>,
+                                                          128, 0) != cudaSuccess || blocks < 1)
+            blocks = 1;
+        cached = blocks;
+    }
+    return cached;
+}
+
+template <class Pair> int resident_for(int per_thread) {
+    return per_thread == 1 ? resident_ctas<Pair, 1>()
+                           : (per_thread == 2 ? resident_ctas<Pair, 2>() : resident_ctas<Pair, 4>());
+}
+} // namespace
+
 EvalPlan plan_evaluation(int geometry, size_t n_targets, size_t n_sources, int sm_count,
                          int per_thread_override) {
     EvalPlan p{};
@@ -186,16 +206,48 @@ EvalPlan plan_evaluation(int geometry, size_t n_targets, size_t n_sources, int s
     p.per_thread = geometry == GEO_INFINITE ? 4 : (geometry == GEO_DISK ? 2 : 1);
     if (per_thread_override == 1 || per_thread_override == 2 || per_thread_override == 4)
         p.per_thread = per_thread_override;
-    const size_t per_block = static_cast<size_t>(p.block) * p.per_thread;
-    p.target_blocks = static_cast<int>(std::max<size_t>(1, (n_targets + per_block - 1) / per_block));
-    // Aim for about eight work items per SM so that tails of uneven items even out.
-    const size_t want_items = static_cast<size_t>(std::max(sm_count, 1)) * 8;
-    size_t chunks = std::max<size_t>(1, (want_items + p.target_blocks - 1) / p.target_blocks);
-    // A chunk shorter than two tiles spends more on loading targets than on pairs.
-    const size_t min_chunk = geometry == GEO_PERIODIC ? 64 : 2 * kTile;
+    const auto resident_of = [&](int t) {
+        return geometry == GEO_INFINITE   ? resident_for<InfinitePair>(t)
+               : geometry == GEO_PERIODIC ? resident_for<PeriodicPair>(t)
+                                          : resident_for<DiskPair>(t);
+    };
+    const auto blocks_of = [&](int t) {
+        const size_t per_block = static_cast<size_t>(p.block) * t;
+        return std::max<size_t>(1, (n_targets + per_block - 1) / per_block);
+    };
+    // A chunk shorter than min_chunk spends more on loading targets than on pairs; small
+    // populations accept short chunks (and fewer targets per thread) to give every SM work.
+    size_t min_chunk = geometry == GEO_PERIODIC ? 64 : 2 * kTile;
+    const size_t sms = static_cast<size_t>(std::max(sm_count, 1));
+    if (per_thread_override == 0)
+        while (p.per_thread > 1 &&
+               blocks_of(p.per_thread) * std::max<size_t>(1, n_sources / min_chunk) <
+                   sms * resident_of(p.per_thread))
+            p.per_thread /= 2;
+    if (blocks_of(p.per_thread) * std::max<size_t>(1, n_sources / min_chunk) <
+        sms * resident_of(p.per_thread))
+        min_chunk = 64;
+    p.target_blocks = static_cast<int>(blocks_of(p.per_thread));
+    const size_t slots = sms * resident_of(p.per_thread);
     const size_t max_chunks = std::max<size_t>(1, n_sources / min_chunk);
-    chunks = std::min(chunks, max_chunks);
-    size_t chunk = (n_sources + chunks - 1) / chunks;
+    // Every item costs about the same, so the grid runs in waves of `slots` CTAs: pick the chunk
+    // count (up to four waves) whose last wave is fullest; ties go to fewer chunks.
+    size_t best_chunks = 1;
+    double best_eff = -1.0;
+    const size_t limit = std::min<size_t>(max_chunks, std::max<size_t>(1, 4 * slots / p.target_blocks + 1));
+    for (size_t c = 1; c <= limit; ++c) {
+        const size_t chunk = std::max<size_t>(2, ((n_sources + c - 1) / c + 1) & ~size_t(1));
+        const size_t chunks = (n_sources + chunk - 1) / chunk;
+        const size_t items = chunks * p.target_blocks;
+        const size_t waves = (items + slots - 1) / slots;
+        // fraction of the machine busy over the kernel, counting the pair work of each item
+        const double eff = static_cast<double>(items) / static_cast<double>(waves * slots);
+        if (eff > best_eff + 1e-3) {
+            best_eff = eff;
+            best_chunks = chunks;
+        }
+    }
+    size_t chunk = (n_sources + best_chunks - 1) / best_chunks;
     chunk = std::max<size_t>(2, (chunk + 1) & ~static_cast<size_t>(1));
     p.chunk = static_cast<int>(chunk);
     p.num_chunks = static_cast<int>(std::max<size_t>(1, (n_sources + chunk - 1) / chunk));
