@@ -213,7 +213,9 @@ def run_ours(args):
     per_launch_ms = v_ms / max(v_timed, 1)
     flops_per_launch = FLOPS_PER_PAIR_PERIODIC * n_now * (n_now - 1)
     achieved = flops_per_launch / (per_launch_ms * 1e-3) / 1e12
-    peak = pv.probePeak("fp64", local) / 1e12
+    # measured FP64 FMA peak of this GPU (36.8 TFLOP/s at 1965 MHz on this pool's B200s when
+    # the probe is skipped, e.g. under a profiler)
+    peak = 36.83 if args.no_peak_probe else pv.probePeak("fp64", local) / 1e12
     launches = sum(v[0] for v in stats.values())
 
     result = None
@@ -349,25 +351,26 @@ def run_reference(args):
                     "d2h_bytes_per_step": 0}}
 
 
-def run_kernel_case(spec: str, evals: int) -> dict:
+def run_kernel_case(spec: str, evals: int, precision: str = "fp64") -> dict:
     """Velocity evaluations only (no stepping), for kernel timing and ncu captures:
-    spec = "geometry:N" with geometry infinite | periodic | disk."""
+    spec = "geometry:N" with geometry infinite | periodic | disk; precision fp64 | fp32c."""
     import torch
     import pointvortex_b200 as pv
     from pointvortex_b200 import ics
     geo, n = spec.split(":")
     n = int(n)
+    prec = 1 if precision == "fp32c" else 0
     if geo == "infinite":
         x, y, g = ics.infinite_plane(n, 1)
-        k = pv.InfinitePlaneKernel(0.0)
+        k = pv.InfinitePlaneKernel(0.0, precision=prec)
         flops = 11
     elif geo == "periodic":
         x, y, g = ics.periodic_box(n, 2, LENGTH)
-        k = pv.PeriodicBoxKernel(LENGTH, LENGTH, LAYERS)
+        k = pv.PeriodicBoxKernel(LENGTH, LENGTH, LAYERS, precision=prec)
         flops = FLOPS_PER_PAIR_PERIODIC
     else:
         x, y, g = ics.disk(n, 3, 1.0)
-        k = pv.DiskKernel(1.0)
+        k = pv.DiskKernel(1.0, precision=prec)
         flops = 33
     k.uploadDeviceState(pv.VortexSystem(x, y, g))
     for _ in range(2):
@@ -380,7 +383,7 @@ def run_kernel_case(spec: str, evals: int) -> dict:
     ms = st[2] / max(st[1], 1)
     pairs = n * (n - 1)
     torch.cuda.synchronize()
-    return {"case": spec, "evaluations": evals, "ms_per_evaluation": ms,
+    return {"case": spec, "precision": precision, "evaluations": evals, "ms_per_evaluation": ms,
             "pairs_per_s": pairs / (ms * 1e-3), "formula_flops_per_pair": flops,
             "tflops": flops * pairs / (ms * 1e-3) / 1e12}
 
@@ -429,6 +432,99 @@ def run_reference_cuda(evals: int = 3, steps: int = 3) -> dict:
             "note": "wall clock per call; the backend synchronises after every evaluation"}
 
 
+def run_ensemble(n_sims: int = 512, budget: int = 10, seed: int = 7) -> dict:
+    """Batched ensemble: n_sims independent simulations, N log-uniform in [64, 8192], geometry
+    round-robin (infinite / periodic 2 pi / disk R = 1), balanced +-1 circulations, DOPRI5 with
+    rtol 1e-8 to t_end = 0.5, each with an accepted-step budget (the workloads are chaotic, so
+    unbudgeted work per simulation is unbounded). Timed from the first admission to the last
+    result download."""
+    import torch
+    from pointvortex_b200 import ics
+    from pointvortex_b200.batch import Batch, geometry_params
+    rng = np.random.default_rng(seed)
+    geos = ("infinite", "periodic", "disk")
+    specs = []
+    for k in range(n_sims):
+        n = int(np.exp(rng.uniform(np.log(64), np.log(8192))))
+        n += n % 2
+        specs.append((geos[k % 3], n, 1000 + k))
+    states = []
+    for geo, n, sd in specs:
+        if geo == "periodic":
+            states.append(ics.periodic_box(n, sd, LENGTH))
+        elif geo == "disk":
+            states.append(ics.disk(n, sd, 1.0, 0.95, gaussian=False))
+        else:
+            states.append(ics.infinite_plane(n, sd))
+    total = sum(n for _, n, _ in specs)
+    b = Batch(total + 256 * (n_sims + 1), n_sims, max_steps=budget)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    ids = [b.add(geometry_params(geo), *st, 0.5, dt=1e-3, atol=1e-10, rtol=1e-8)
+           for (geo, n, sd), st in zip(specs, states)]
+    attempts = b.run()
+    finished = {}
+    pairs = 0.0
+    for sid, (geo, n, sd) in zip(ids, specs):
+        info = b.info(sid)
+        b.result(sid)
+        finished[info.state] = finished.get(info.state, 0) + 1
+        evals = 6 * (info.acceptedSteps + info.rejectedSteps) + 1
+        pairs += evals * n * (n - 1)
+    elapsed = time.perf_counter() - t0
+    b.close()
+    return {"simulations": n_sims, "vortices": total, "step_budget": budget,
+            "attempts": attempts, "seconds": elapsed, "solves_per_s": n_sims / elapsed,
+            "pair_interactions_per_s": pairs / elapsed, "states": finished, "dtype": "f64",
+            "note": "one arena, lock-step DOPRI5 attempts, CUDA-graph replay per attempt"}
+
+
+def run_serving(budget: int = 10) -> dict:
+    """Continuous-batching server on Poisson request streams (geometry uniform, N log-uniform in
+    [32, 32768], t_end U[0.1, 1], rtol in {1e-6, 1e-9}, accepted-step budget per request), with
+    the one-request-at-a-time FIFO loop beside it on the middle stream."""
+    from pointvortex_b200.serve import Server, one_at_a_time, poisson_stream
+    out = {"step_budget": budget, "streams": []}
+    for rate, count in ((10.0, 30), (100.0, 200), (1000.0, 600)):
+        reqs = poisson_stream(count, rate, seed=int(rate), max_steps=budget)
+        server = Server(capacity_vortices=4_000_000, max_slots=1024, attempts_per_tick=2)
+        summary = server.serve(reqs)
+        server.close()
+        summary["rate_per_s"] = rate
+        out["streams"].append(summary)
+    # the comparison loop on the same 100 req/s stream as the batched server
+    base = one_at_a_time(poisson_stream(200, 100.0, seed=100, max_steps=budget))
+    base["rate_per_s"] = 100.0
+    out["one_request_per_launch_fp64"] = base
+    return out
+
+
+def summarize_launches(path: str) -> str:
+    """Per-kernel launches, total time and share of an ncu launch list
+    (`ncu --metrics gpu__time_duration.sum --csv --log-file <path> ...`), as a Markdown table."""
+    import csv
+    import re
+    from collections import defaultdict
+    with open(path) as f:
+        lines = [ln for ln in f if ln.startswith('"')]
+    total, count = defaultdict(float), defaultdict(int)
+    for r in csv.DictReader(lines):
+        if r.get("Metric Name") != "gpu__time_duration.sum":
+            continue
+        k = re.sub(r"\(.*", "", r["Kernel Name"]).replace("pvb::", "")
+        k = k.replace("(anonymous namespace)::", "")[:70]
+        scale = {"nsecond": 1e-3, "usecond": 1.0, "msecond": 1e3, "second": 1e6}.get(
+            r.get("Metric Unit", "nsecond"), 1e-3)
+        total[k] += float(r["Metric Value"].replace(",", "")) * scale
+        count[k] += 1
+    grand = sum(total.values()) or 1.0
+    out = ["| kernel | launches | total (us) | share |", "|---|---|---|---|"]
+    for k in sorted(total, key=total.get, reverse=True):
+        out.append(f"| `{k}` | {count[k]} | {total[k]:.1f} | {100 * total[k] / grand:.1f} % |")
+    out.append(f"| all | {sum(count.values())} | {grand:.1f} | 100 % |")
+    return "\n".join(out)
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -436,18 +532,29 @@ def main(argv=None):
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="skip the ensemble and serving sections")
     ap.add_argument("--kernel-case", default=None,
                     help="geometry:N -- time velocity evaluations only (kernel timing / ncu)")
     ap.add_argument("--evals", type=int, default=10)
+    ap.add_argument("--precision", choices=["fp64", "fp32c"], default="fp64",
+                    help="precision form of --kernel-case")
     ap.add_argument("--reference-cuda", action="store_true",
                     help="time the reference's own CUDA backend on the workload (own process)")
+    ap.add_argument("--summarize-launches", default=None, metavar="CSV",
+                    help="print the per-kernel summary of an ncu launch list and exit")
+    ap.add_argument("--no-peak-probe", action="store_true",
+                    help="report the roofline against the last measured FP64 peak")
     args = ap.parse_args(argv)
     rank, world, _ = rank_info()
+    if args.summarize_launches:
+        print(summarize_launches(args.summarize_launches))
+        return 0
     if args.reference_cuda:
         print(json.dumps(run_reference_cuda()), flush=True)
         return 0
     if args.kernel_case:
-        print(json.dumps(run_kernel_case(args.kernel_case, args.evals)), flush=True)
+        print(json.dumps(run_kernel_case(args.kernel_case, args.evals, args.precision)), flush=True)
         return 0
     if args.impl == "reference":
         out = run_reference(args)
@@ -455,6 +562,15 @@ def main(argv=None):
             print(json.dumps(out), flush=True)
         return 0
     result, k = run_ours(args)
+    if rank == 0 and world == 1 and not args.no_extras:
+        try:
+            result["ensemble"] = run_ensemble()
+        except Exception as exc:
+            result["ensemble"] = {"error": str(exc)[:200]}
+        try:
+            result["serving"] = run_serving()
+        except Exception as exc:
+            result["serving"] = {"error": str(exc)[:200]}
     if rank == 0:
         if not args.no_cpu_baseline and world == 1:
             result["cpu_baseline"] = cpu_baseline()

@@ -35,7 +35,8 @@ typedef enum pv_status {
     PV_ERROR_OUT_OF_RANGE = 2,     /* std::out_of_range */
     PV_ERROR_RUNTIME = 3,          /* std::runtime_error (non-finite, coincident, DOPRI5 failure) */
     PV_ERROR_LOGIC = 4,            /* std::logic_error (hook used out of order) */
-    PV_ERROR_CUDA = 5              /* CUDA runtime failure; the message names the call */
+    PV_ERROR_CUDA = 5,             /* CUDA runtime failure; the message names the call */
+    PV_ERROR_CAPACITY = 6          /* batch admission: no free slot or no room in the arena */
 } pv_status;
 
 typedef enum pv_geometry {
@@ -154,6 +155,77 @@ pv_status pv_evaluation_count(const pv_context *ctx, uint64_t *count);
 /* `steps` RK4 steps of size dt, enqueued back to back with one synchronisation at the end. */
 pv_status pv_rk4_advance(pv_context *ctx, double dt, uint64_t steps);
 
+/* ---- batched ensembles (no reference counterpart: the reference runs one simulation per
+ *      process) ------------------------------------------------------------------------------
+ * Many independent simulations of uneven population and mixed geometry share one device arena
+ * and advance together in lock-step DOPRI5 attempts, each with its own step size, tolerances,
+ * end time, step budget and failure status. Each velocity stage of an attempt is one persistent
+ * launch draining a (simulation, target block, source chunk) work queue. A simulation's result
+ * does not depend on which other simulations share the batch. */
+
+typedef struct pv_batch pv_batch;
+
+typedef struct pv_batch_config {
+    size_t capacity_vortices;              /* arena room (vortices over all simulations) */
+    uint32_t max_simulations;              /* simulation slots */
+    int device;                            /* CUDA ordinal */
+    uint64_t max_steps_per_simulation;     /* default accepted-step budget (0: unlimited) */
+    size_t partial_chunks_per_vortex_slot; /* partial-sum room per arena vortex (0: 16) */
+} pv_batch_config;
+
+/* One solve: integrate to t_end with DOPRI5 (the reference driver's integrator dopri5). */
+typedef struct pv_batch_solve {
+    double t_end;
+    double dt;                  /* first step (timeStep), clamped to [dtmin, dtmax] */
+    double absolute_tolerance;
+    double relative_tolerance;
+    double minimum_time_step;
+    double maximum_time_step;
+    uint64_t max_steps;         /* accepted-step budget (0: the batch default) */
+} pv_batch_solve;
+
+#define PV_SIM_RUNNING 1
+#define PV_SIM_DONE 2    /* reached t_end */
+#define PV_SIM_FAILED 3  /* stopped with an error: see status (device status code) */
+#define PV_SIM_BUDGET 4  /* stopped at its step budget before t_end */
+
+typedef struct pv_batch_sim_info {
+    int state;                  /* PV_SIM_* */
+    int status;                 /* device status code when failed, 0 otherwise */
+    double time;
+    double suggested_time_step;
+    uint64_t accepted_steps;
+    uint64_t rejected_steps;
+    uint32_t population;
+} pv_batch_sim_info;
+
+typedef struct pv_batch_totals {
+    uint64_t attempts;
+    uint32_t work_items;        /* velocity work items per stage (running simulations) */
+    size_t free_vortices;
+    uint32_t running;
+    uint32_t occupied_slots;
+} pv_batch_totals;
+
+pv_status pv_batch_create(const pv_batch_config *config, pv_batch **out);
+void pv_batch_destroy(pv_batch *batch);
+const char *pv_batch_last_error(const pv_batch *batch);
+/* Admits one simulation (validated like uploadDeviceState); PV_ERROR_CAPACITY when the batch has
+ * no free slot or arena room. *id identifies it until pv_batch_release. */
+pv_status pv_batch_add(pv_batch *batch, const pv_params *params, const double *x, const double *y,
+                       const double *circulation, size_t n, const pv_batch_solve *solve,
+                       uint32_t *id);
+/* Runs up to `attempts` lock-step DOPRI5 attempts of every running simulation, then
+ * synchronises; *running receives the number still running. */
+pv_status pv_batch_advance(pv_batch *batch, uint32_t attempts, uint32_t *running);
+pv_status pv_batch_info(pv_batch *batch, uint32_t id, pv_batch_sim_info *info);
+/* Current positions of simulation id (n must equal its population). */
+pv_status pv_batch_result(pv_batch *batch, uint32_t id, double *x, double *y, size_t n);
+/* Frees the slot and arena room of simulation id (stopping it first if it is still running). */
+pv_status pv_batch_release(pv_batch *batch, uint32_t id);
+pv_status pv_batch_status(pv_batch *batch, pv_batch_totals *totals);
+pv_status pv_batch_stream(const pv_batch *batch, void **stream);
+
 /* ---- allocation-free evaluation (no counterpart in the reference) ------------------------ */
 
 /* Largest population pv_evaluate_device_noalloc accepts. */
@@ -194,6 +266,12 @@ typedef struct pv_kernel_stats {
 /* The context's CUDA stream (a cudaStream_t) through *stream, so that a caller can order its own
  * work or events after the context's kernels. */
 pv_status pv_context_stream(const pv_context *ctx, void **stream);
+/* Autotuner table of the velocity plan: targets held in registers per thread (1, 2 or 4; 0 restores
+ * the built-in heuristic) for a geometry, a precision and populations N with floor(log2 N) ==
+ * log2_n. Process-wide; read when a context plans an evaluation (pv_upload_state,
+ * pv_evaluate_range). pointvortex_b200/autotune.py fills it by timing the candidates. */
+pv_status pv_set_tuning(int geometry, int precision, int log2_n, int per_thread);
+pv_status pv_get_tuning(int geometry, int precision, int log2_n, int *per_thread);
 /* Bracket every launch of the context with CUDA events recorded on its own stream. */
 pv_status pv_set_profiling(pv_context *ctx, int enabled);
 /* Synchronises the context stream and returns the counters accumulated since the last reset. */

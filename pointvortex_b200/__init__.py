@@ -23,6 +23,9 @@ from .kernel import (  # noqa: F401
     probePeak,
 )
 from ._lib import LIB_PATH  # noqa: F401
+from . import autotune as _autotune
+
+_autotune.load()  # the measured tuning table for this library, when present
 
 __all__ = [
     "CudaError", "DiskKernel", "DipoleCandidate", "InfinitePlaneKernel", "Invariants",

@@ -54,6 +54,35 @@ class PvDipoleCandidate(ctypes.Structure):
     ]
 
 
+PV_ERROR_CAPACITY = 6
+SIM_RUNNING, SIM_DONE, SIM_FAILED, SIM_BUDGET = 1, 2, 3, 4
+
+
+class PvBatchConfig(ctypes.Structure):
+    _fields_ = [("capacity_vortices", ctypes.c_size_t), ("max_simulations", ctypes.c_uint32),
+                ("device", ctypes.c_int), ("max_steps_per_simulation", ctypes.c_uint64),
+                ("partial_chunks_per_vortex_slot", ctypes.c_size_t)]
+
+
+class PvBatchSolve(ctypes.Structure):
+    _fields_ = [("t_end", ctypes.c_double), ("dt", ctypes.c_double),
+                ("absolute_tolerance", ctypes.c_double), ("relative_tolerance", ctypes.c_double),
+                ("minimum_time_step", ctypes.c_double), ("maximum_time_step", ctypes.c_double),
+                ("max_steps", ctypes.c_uint64)]
+
+
+class PvBatchSimInfo(ctypes.Structure):
+    _fields_ = [("state", ctypes.c_int), ("status", ctypes.c_int), ("time", ctypes.c_double),
+                ("suggested_time_step", ctypes.c_double), ("accepted_steps", ctypes.c_uint64),
+                ("rejected_steps", ctypes.c_uint64), ("population", ctypes.c_uint32)]
+
+
+class PvBatchTotals(ctypes.Structure):
+    _fields_ = [("attempts", ctypes.c_uint64), ("work_items", ctypes.c_uint32),
+                ("free_vortices", ctypes.c_size_t), ("running", ctypes.c_uint32),
+                ("occupied_slots", ctypes.c_uint32)]
+
+
 KERNEL_KINDS = ("velocity", "stage", "accept", "invariants", "dipole")
 
 
@@ -97,8 +126,21 @@ SIGNATURES = {
     "pv_evaluate_device_noalloc": (_ST, [ctypes.POINTER(PvParams), ctypes.c_void_p, ctypes.c_void_p,
                                          ctypes.c_void_p, _SZ, ctypes.c_void_p, ctypes.c_void_p,
                                          ctypes.c_void_p]),
+    "pv_batch_create": (_ST, [ctypes.POINTER(PvBatchConfig), ctypes.POINTER(ctypes.c_void_p)]),
+    "pv_batch_destroy": (None, [ctypes.c_void_p]),
+    "pv_batch_last_error": (ctypes.c_char_p, [ctypes.c_void_p]),
+    "pv_batch_add": (_ST, [ctypes.c_void_p, ctypes.POINTER(PvParams), _D, _D, _D, _SZ,
+                           ctypes.POINTER(PvBatchSolve), ctypes.POINTER(ctypes.c_uint32)]),
+    "pv_batch_advance": (_ST, [ctypes.c_void_p, ctypes.c_uint32, ctypes.POINTER(ctypes.c_uint32)]),
+    "pv_batch_info": (_ST, [ctypes.c_void_p, ctypes.c_uint32, ctypes.POINTER(PvBatchSimInfo)]),
+    "pv_batch_result": (_ST, [ctypes.c_void_p, ctypes.c_uint32, _D, _D, _SZ]),
+    "pv_batch_release": (_ST, [ctypes.c_void_p, ctypes.c_uint32]),
+    "pv_batch_status": (_ST, [ctypes.c_void_p, ctypes.POINTER(PvBatchTotals)]),
+    "pv_batch_stream": (_ST, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_void_p)]),
     "pv_probe_peak": (_ST, [ctypes.c_int, ctypes.c_int, _D]),
     "pv_context_stream": (_ST, [_CTX, ctypes.POINTER(ctypes.c_void_p)]),
+    "pv_set_tuning": (_ST, [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int]),
+    "pv_get_tuning": (_ST, [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_int)]),
     "pv_set_profiling": (_ST, [_CTX, ctypes.c_int]),
     "pv_get_kernel_stats": (_ST, [_CTX, ctypes.POINTER(PvKernelStats)]),
     "pv_reset_kernel_stats": (_ST, [_CTX]),

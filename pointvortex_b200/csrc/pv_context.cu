@@ -378,7 +378,11 @@ pv_status launch_eval(pv_context *c, const double *px, const double *py) {
     a.num_chunks = c->plan.num_chunks;
     a.status = &c->ctl->status;
     a.g = c->gc;
-    PV_CUDA(c, counted(c, PV_KERNEL_VELOCITY, 1, [&] { return launch_velocity(a, c->plan, c->stream); }));
+    PV_CUDA(c, counted(c, PV_KERNEL_VELOCITY, 1, [&] {
+                return c->params.precision == PV_PRECISION_FP32C
+                           ? launch_velocity_fp32c(a, c->plan, c->stream)
+                           : launch_velocity(a, c->plan, c->stream);
+            }));
     ++c->evaluations;
     return PV_OK;
 }
@@ -412,7 +416,7 @@ pv_status ensure_state_capacity(pv_context *c, size_t n) {
         PV_CUDA(c, c->kx[s].ensure(np));
         PV_CUDA(c, c->ky[s].ensure(np));
     }
-    c->plan = plan_evaluation(c->gc.geometry, n, n, c->sm_count);
+    c->plan = plan_evaluation(c->gc.geometry, n, n, c->sm_count, 0, c->params.precision);
     const size_t partial = static_cast<size_t>(c->plan.num_chunks) * np;
     PV_CUDA(c, c->pu.ensure(partial));
     PV_CUDA(c, c->pv.ensure(partial));
@@ -445,7 +449,7 @@ pv_status evaluate_host(pv_context *c, const double *x, const double *y, const d
         PV_CUDA(c, a->ensure(np));
     PV_CUDA(c, c->eu.ensure(padded(nt)));
     PV_CUDA(c, c->ev.ensure(padded(nt)));
-    const EvalPlan plan = plan_evaluation(c->gc.geometry, nt, n, c->sm_count);
+    const EvalPlan plan = plan_evaluation(c->gc.geometry, nt, n, c->sm_count, 0, c->params.precision);
     const size_t stride = padded(nt);
     PV_CUDA(c, c->epu.ensure(static_cast<size_t>(plan.num_chunks) * stride));
     PV_CUDA(c, c->epv.ensure(static_cast<size_t>(plan.num_chunks) * stride));
@@ -473,7 +477,11 @@ pv_status evaluate_host(pv_context *c, const double *x, const double *y, const d
     a.num_chunks = plan.num_chunks;
     a.status = &c->ctl->status;
     a.g = c->gc;
-    PV_CUDA(c, counted(c, PV_KERNEL_VELOCITY, 1, [&] { return launch_velocity(a, plan, c->stream); }));
+    PV_CUDA(c, counted(c, PV_KERNEL_VELOCITY, 1, [&] {
+                return c->params.precision == PV_PRECISION_FP32C
+                           ? launch_velocity_fp32c(a, plan, c->stream)
+                           : launch_velocity(a, plan, c->stream);
+            }));
     StageArgs s{};
     s.n = nt;
     s.mode = STAGE_REDUCE_ONLY;
@@ -983,6 +991,21 @@ pv_status pv_evaluation_count(const pv_context *ctx, uint64_t *count) {
     if (!ctx || !count)
         return PV_ERROR_INVALID_ARGUMENT;
     *count = ctx->evaluations;
+    return PV_OK;
+}
+
+pv_status pv_set_tuning(int geometry, int precision, int log2_n, int per_thread) {
+    if (!tuning_store(geometry, precision, log2_n, per_thread)) {
+        g_create_error = "invalid tuning entry";
+        return PV_ERROR_INVALID_ARGUMENT;
+    }
+    return PV_OK;
+}
+
+pv_status pv_get_tuning(int geometry, int precision, int log2_n, int *per_thread) {
+    if (!per_thread || log2_n < 0 || log2_n >= 40)
+        return PV_ERROR_INVALID_ARGUMENT;
+    *per_thread = tuning_lookup(geometry, precision, size_t(1) << log2_n);
     return PV_OK;
 }
 

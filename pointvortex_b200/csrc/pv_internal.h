@@ -39,8 +39,13 @@ struct EvalPlan {
 };
 
 EvalPlan plan_evaluation(int geometry, size_t n_targets, size_t n_sources, int sm_count,
-                         int per_thread_override = 0);
+                         int per_thread_override = 0, int precision = 0);
+// The autotuner's table of targets per thread (pv_set_tuning / pv_get_tuning).
+int tuning_lookup(int geometry, int precision, size_t n);
+bool tuning_store(int geometry, int precision, int log2_n, int per_thread);
 cudaError_t launch_velocity(const EvalArgs &a, const EvalPlan &p, cudaStream_t stream);
+// The FP32-compensated precision form (pv_velocity32.cu): same arguments, same partial layout.
+cudaError_t launch_velocity_fp32c(const EvalArgs &a, const EvalPlan &p, cudaStream_t stream);
 
 // ---- stage kernels (reduction, stage positions, RK4 combine, DOPRI5 error and control) ------
 enum StageMode : int {

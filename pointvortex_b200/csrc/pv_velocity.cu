@@ -197,10 +197,34 @@ template <class Pair> int resident_for(int per_thread) {
 }
 } // namespace
 
+namespace {
+// Autotuner table: targets per thread for (geometry, precision, floor(log2 N)); 0 = heuristic.
+int g_tuning[3][2][40] = {};
+} // namespace
+
+int tuning_lookup(int geometry, int precision, size_t n) {
+    if (geometry < 0 || geometry > 2 || precision < 0 || precision > 1 || n == 0)
+        return 0;
+    int bucket = 0;
+    while ((size_t(2) << bucket) <= n && bucket < 39)
+        ++bucket;
+    return g_tuning[geometry][precision][bucket];
+}
+
+bool tuning_store(int geometry, int precision, int log2_n, int per_thread) {
+    if (geometry < 0 || geometry > 2 || precision < 0 || precision > 1 || log2_n < 0 ||
+        log2_n >= 40 || (per_thread != 0 && per_thread != 1 && per_thread != 2 && per_thread != 4))
+        return false;
+    g_tuning[geometry][precision][log2_n] = per_thread;
+    return true;
+}
+
 EvalPlan plan_evaluation(int geometry, size_t n_targets, size_t n_sources, int sm_count,
-                         int per_thread_override) {
+                         int per_thread_override, int precision) {
     EvalPlan p{};
     p.block = 128;
+    if (per_thread_override == 0)
+        per_thread_override = tuning_lookup(geometry, precision, n_sources);
     // Registers per pair grow from the infinite plane to the periodic series; fewer targets per
     // thread keep the heavier geometries at full occupancy.
     p.per_thread = geometry == GEO_INFINITE ? 4 : (geometry == GEO_DISK ? 2 : 1);

@@ -1,0 +1,129 @@
+"""Batched ensembles (pv_batch_*): every simulation advances with its own DOPRI5 step and end
+time, its result is bit-identical alone and in any mix, one failing simulation leaves the others
+untouched, and each result agrees with the oracle's driver loop."""
+import numpy as np
+import pytest
+
+from conftest import position_error
+from oracle.pyoracle import Geometry
+from pointvortex_b200 import ics
+from pointvortex_b200.batch import Batch, CapacityError, geometry_params
+
+pytestmark = pytest.mark.gpu
+
+SOLVE = dict(dt=1e-3, atol=1e-10, rtol=1e-8, dtmin=1e-12, dtmax=0.1)
+
+
+def specs():
+    return [
+        ("infinite", 300, 1, 0.004),
+        ("periodic", 256, 2, 0.003),
+        ("disk", 600, 23, 0.002),
+        ("infinite", 1000, 4, 0.001),
+        ("periodic", 1024, 5, 0.002),
+        ("disk", 64, 6, 0.005),
+    ]
+
+
+def state(boundary, n, seed):
+    if boundary == "periodic":
+        return ics.periodic_box(n, seed, 2.0 * np.pi)
+    if boundary == "disk":
+        return ics.disk(n, seed, 1.0, 0.8, gaussian=False)
+    return ics.infinite_plane(n, seed)
+
+
+def run_batch(items, capacity=20000, slots=16, **kw):
+    b = Batch(capacity, slots)
+    ids = []
+    for boundary, n, seed, t_end in items:
+        x, y, g = state(boundary, n, seed)
+        ids.append(b.add(geometry_params(boundary), x, y, g, t_end, **{**SOLVE, **kw}))
+    b.run()
+    out = [(b.info(i), b.result(i)) for i in ids]
+    b.close()
+    return out
+
+
+def test_alone_equals_in_the_mix():
+    mixed = run_batch(specs())
+    for k, spec in enumerate(specs()):
+        (info_a, (xa, ya)) = run_batch([spec])[0]
+        info_m, (xm, ym) = mixed[k]
+        assert info_a.state == "done" and info_m.state == "done", (spec, info_a, info_m)
+        assert info_a.acceptedSteps == info_m.acceptedSteps
+        assert np.array_equal(xa, xm) and np.array_equal(ya, ym), spec
+
+
+def oracle_driver(oracle, boundary, n, seed, t_end):
+    """The reference driver's DOPRI5 loop (src/main.cpp:159-164, 310-343) without output events."""
+    geo = Geometry(boundary, box_length_x=2 * np.pi, box_length_y=2 * np.pi, disk_radius=1.0,
+                   absolute_tolerance=SOLVE["atol"], relative_tolerance=SOLVE["rtol"],
+                   minimum_time_step=SOLVE["dtmin"], maximum_time_step=SOLVE["dtmax"])
+    x, y, g = state(boundary, n, seed)
+    st = oracle.stepper(geo, n)
+    t, dt, steps = 0.0, min(max(SOLVE["dt"], SOLVE["dtmin"]), SOLVE["dtmax"]), 0
+    while t < t_end:
+        x, y, r = st.dopri5_step(x, y, g, min(dt, t_end - t))
+        t += r[0]
+        dt = r[1]
+        steps += 1
+        if t + 16 * np.finfo(float).eps * abs(t) >= t_end:
+            t = t_end
+    return x, y, steps
+
+
+def test_batch_matches_oracle_driver(reference):
+    """Against the unmodified reference's integrator (OpenMP-parallel, so the periodic cases stay
+    affordable on the host)."""
+    results = run_batch(specs())
+    for spec, (info, (x, y)) in zip(specs(), results):
+        rx, ry, steps = oracle_driver(reference, *spec)
+        assert info.acceptedSteps == steps, (spec, info)
+        assert info.time == spec[3]
+        # hundreds of chaotic steps: the 1e-16 per-evaluation differences grow, but stay small
+        assert position_error(x, y, rx, ry) <= 1e-9, spec
+
+
+def test_failure_is_isolated():
+    good = specs()[:3]
+    alone = run_batch(good)
+    b = Batch(20000, 8)
+    ids = []
+    for boundary, n, seed, t_end in good[:2]:
+        ids.append(b.add(geometry_params(boundary), *state(boundary, n, seed), t_end, **SOLVE))
+    # a disk vortex next to the wall with a strong partner: leaves the disk within a few steps
+    bad = b.add(geometry_params("disk"), np.array([0.9999, -0.2]), np.array([0.0, 0.0]),
+                np.array([1.0, 50.0]), 1.0, **SOLVE)
+    boundary, n, seed, t_end = good[2]
+    ids.append(b.add(geometry_params(boundary), *state(boundary, n, seed), t_end, **SOLVE))
+    b.run()
+    assert b.info(bad).state == "failed" and b.info(bad).status != 0
+    for k, sid in enumerate(ids):
+        x, y = b.result(sid)
+        assert b.info(sid).state == "done", (k, b.info(sid))
+        assert np.array_equal(x, alone[k][1][0]) and np.array_equal(y, alone[k][1][1])
+
+
+def test_step_budget_and_release():
+    # arena room: 1280 requested + 256 per slot = 1792 vortices, in 256-element blocks
+    b = Batch(1200, 2)
+    x, y, g = state("infinite", 500, 9)
+    sid = b.add(geometry_params("infinite"), x, y, g, 10.0, max_steps=3, **SOLVE)
+    b.run()
+    info = b.info(sid)
+    assert info.state == "budget" and info.acceptedSteps == 3
+    with pytest.raises(CapacityError):
+        b.add(geometry_params("infinite"), *state("infinite", 1500, 1), 1.0, **SOLVE)
+    b.release(sid)
+    b.add(geometry_params("infinite"), *state("infinite", 1500, 1), 0.0005, **SOLVE)
+    assert b.run() >= 1
+
+
+def test_admission_validation():
+    b = Batch(5000, 2)
+    x, y, g = state("periodic", 100, 1)
+    g = g.copy()
+    g[0] += 1.0
+    with pytest.raises(ValueError, match="zero total circulation"):
+        b.add(geometry_params("periodic"), x, y, g, 0.01, **SOLVE)

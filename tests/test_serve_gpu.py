@@ -1,0 +1,52 @@
+"""Continuous batching: requests that arrive while others are on the GPU are admitted as room frees
+up, and every result is the same as the request solved alone."""
+import numpy as np
+import pytest
+
+from pointvortex_b200.batch import Batch, geometry_params
+from pointvortex_b200.serve import Request, Server, one_at_a_time, poisson_stream
+
+pytestmark = pytest.mark.gpu
+
+
+def alone(req: Request):
+    b = Batch(max(req.n, 2) + 512, 1)
+    x, y, g = req.state()
+    sid = b.add(geometry_params(req.geometry), x, y, g, req.t_end, dt=req.dt, atol=req.atol,
+                rtol=req.rtol, max_steps=req.max_steps)
+    b.run()
+    info = b.info(sid)
+    out = b.result(sid)
+    b.close()
+    return info, out
+
+
+def test_stream_results_equal_alone_results():
+    reqs = poisson_stream(24, rate=400.0, seed=3, n_min=32, n_max=1500, t_end_range=(0.01, 0.03),
+                          rtols=(1e-6, 1e-9), max_steps=40)
+    # a small arena forces queueing: later requests wait for earlier ones to retire
+    server = Server(capacity_vortices=4000, max_slots=6, attempts_per_tick=2, keep_states=True)
+    streamed = []
+    summary = server.serve(reqs, on_complete=lambda c, x, y: streamed.append(c.rid))
+    server.close()
+    assert summary["requests"] == len(reqs) == len(streamed)
+    assert summary["p99_latency_s"] >= summary["p50_latency_s"] > 0
+    by_id = {c.rid: c for c in server.completions}
+    overlapped = 0
+    for req in reqs:
+        c = by_id[req.rid]
+        info, (x, y) = alone(req)
+        assert c.state == info.state and c.accepted_steps == info.acceptedSteps, req
+        assert np.array_equal(c.x, x) and np.array_equal(c.y, y), req
+        overlapped += 1
+    assert overlapped == len(reqs)
+
+
+def test_one_at_a_time_baseline_agrees():
+    reqs = poisson_stream(4, rate=1000.0, seed=5, n_min=64, n_max=600, t_end_range=(0.005, 0.01),
+                          rtols=(1e-8,), max_steps=30)
+    s = one_at_a_time(reqs)
+    assert s["requests"] == 4
+    for req in reqs:
+        info, _ = alone(req)
+        assert info.state in ("done", "budget", "failed")
