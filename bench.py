@@ -106,6 +106,20 @@ class ClockSampler:
                 "samples": len(self.rows)}
 
 
+def combine_ranks(total_ms: float, pairs: float, device: str = "cpu"):
+    """Whole-job figures of the replicas: the slowest rank's device time (max) and the pairs all
+    ranks evaluated (sum). Without a process group it returns its inputs."""
+    import torch
+    import torch.distributed as dist
+    if not (dist.is_available() and dist.is_initialized()) or dist.get_world_size() == 1:
+        return total_ms, pairs
+    t = torch.tensor([total_ms], device=device, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    p = torch.tensor([pairs], device=device, dtype=torch.float64)
+    dist.all_reduce(p)
+    return float(t.item()), float(p.item())
+
+
 def flush_l2(buf):
     buf.fill_(1.0)
 
@@ -171,7 +185,7 @@ def run_ours(args):
     k.setProfiling(True)
     k.resetKernelStats()
     evals = 0
-    step_ms = []
+    pairs = 0.0
     lib_stream = torch.cuda.ExternalStream(k.cudaStream(), device=f"cuda:{local}")
     events = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
               for _ in range(args.steps)]
@@ -182,26 +196,19 @@ def run_ours(args):
         for s in range(args.steps):
             flush_l2(flush)
             torch.cuda.synchronize()
+            n_step = k.stateSize()       # the evaluations of a step run before its removals
             events[s][0].record(lib_stream)
             dt, e = dopri_step(k, dt)
             events[s][1].record(lib_stream)
             evals += e
+            pairs += e * n_step * (n_step - 1)
         torch.cuda.synchronize()
     step_ms = [a.elapsed_time(b) for a, b in events]
     stats = k.kernelStats()
     k.setProfiling(False)
     total_ms = float(np.sum(step_ms))
-    if world > 1:
-        t = torch.tensor([total_ms], device=f"cuda:{local}", dtype=torch.float64)
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        total_ms = float(t.item())
-        ev = torch.tensor([evals], device=f"cuda:{local}", dtype=torch.float64)
-        torch.distributed.all_reduce(ev)
-        evals_total = float(ev.item())
-    else:
-        evals_total = float(evals)
-    n_now = k.stateSize()
-    pairs = evals_total * n_now * (n_now - 1)
+    pairs_local = pairs
+    total_ms, pairs = combine_ranks(total_ms, pairs, f"cuda:{local}")
     value = pairs / (total_ms * 1e-3)
 
     # e2e: the same steps through the public API with host buffers -- every step uploads its
@@ -211,8 +218,8 @@ def run_ours(args):
     # roofline of the dominant kernel (the tiled periodic pair kernel), from its launch events
     v_launch, v_timed, v_ms = stats["velocity"]
     per_launch_ms = v_ms / max(v_timed, 1)
-    flops_per_launch = FLOPS_PER_PAIR_PERIODIC * n_now * (n_now - 1)
-    achieved = flops_per_launch / (per_launch_ms * 1e-3) / 1e12
+    # every timed velocity launch is one evaluation of the step loop: its pairs over its time
+    achieved = FLOPS_PER_PAIR_PERIODIC * pairs_local / (v_ms * 1e-3) / 1e12
     # measured FP64 FMA peak of this GPU (36.8 TFLOP/s at 1965 MHz on this pool's B200s when
     # the probe is skipped, e.g. under a profiler)
     peak = 36.83 if args.no_peak_probe else pv.probePeak("fp64", local) / 1e12
@@ -528,7 +535,7 @@ def summarize_launches(path: str) -> str:
 def main(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--steps", type=int, default=1000)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
