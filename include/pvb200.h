@@ -143,6 +143,45 @@ pv_status pv_state_invariants(pv_context *ctx, double out[5]);
  * random generator (src/dipole.cpp:101-102), so a driver may skip the download. */
 pv_status pv_dipole_scan(pv_context *ctx, double threshold, pv_dipole_candidate *out,
                          size_t capacity, size_t *count);
+
+/* ---- dipole events on the device state (DipoleManager, src/dipole.h:19-40) ----------------- */
+
+/* SimParams::dipoleReinjection (src/params.h:10). */
+#define PV_REINJECT_NONE 0
+#define PV_REINJECT_INDEPENDENT 1
+#define PV_REINJECT_PAIRED 2
+
+typedef struct pv_dipole_config {
+    int removal;          /* SimParams::dipoleRemoval */
+    double distance;      /* SimParams::dipoleRemovalDistance */
+    int reinjection;      /* SimParams::dipoleReinjection, PV_REINJECT_* */
+    uint64_t random_seed; /* SimParams::randomSeed */
+} pv_dipole_config;
+
+/* DipoleManager::DipoleManager(params) (src/dipole.cpp:29-30): the event settings, zero counts
+ * and the reinjection generator seeded as the reference seeds it. The box length / disk radius
+ * are the context's. */
+pv_status pv_dipole_configure(pv_context *ctx, const pv_dipole_config *config);
+/* DipoleManager::process (src/dipole.cpp:42-127) applied to the device state in place: the
+ * candidate scan runs on the device, only the candidate list crosses to the host, where the
+ * closest-first disjoint selection and the reinjection draws are made; survivors are compacted
+ * in order on the device and reinjected vortices appended. The population, order, positions and
+ * generator state afterwards equal the reference's. *events = pairs processed (wall events
+ * count one). Any event invalidates the cached derivative. Errors as the reference throws them
+ * (a failed paired placement is PV_ERROR_RUNTIME; the state is then unspecified). */
+pv_status pv_dipole_process(pv_context *ctx, size_t *events);
+/* DipoleManager::state() (src/dipole.cpp:182-186): the removed/reinjected counts and the
+ * generator's text state (std::mt19937_64 stream format, as written into checkpoints).
+ * *length = bytes of the state text without a terminator; written only when capacity suffices
+ * (capacity > *length, NUL-terminated); PV_ERROR_CAPACITY otherwise. */
+pv_status pv_dipole_state(const pv_context *ctx, uint64_t *removed, uint64_t *reinjected,
+                          char *engine_state, size_t capacity, size_t *length);
+/* DipoleManager::DipoleManager(params, state) (src/dipole.cpp:32-40): restores counts and, when
+ * engine_state is non-empty, the generator ("invalid random-generator state in checkpoint"
+ * otherwise). pv_dipole_configure must have been called first. */
+pv_status pv_dipole_restore(pv_context *ctx, uint64_t removed, uint64_t reinjected,
+                            const char *engine_state);
+
 /* Population of the device state. */
 pv_status pv_state_size(const pv_context *ctx, size_t *n);
 /* Velocity evaluations made so far by the stepping hooks (the reference's CountingKernel,

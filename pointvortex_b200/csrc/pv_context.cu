@@ -12,6 +12,8 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <random>
+#include <sstream>
 #include <string>
 #include <vector>
 
@@ -99,6 +101,14 @@ struct pv_context {
     // host-array evaluation (kept apart from the device state)
     DeviceArray ex, ey, eg, egs, eu, ev, epu, epv;
 
+    // dipole events (DipoleManager, src/dipole.h:19-40)
+    pv_dipole_config dipole{};
+    bool dipole_configured = false;
+    std::mt19937_64 dipole_random;
+    uint64_t removed_pairs = 0, reinjected_pairs = 0;
+    std::vector<double> gamma_host;  // the device state's circulations (they change only here)
+    DeviceArray removed_index;
+
     // launch accounting and optional per-launch CUDA-event timing (pv_set_profiling)
     bool profiling = false;
     uint64_t launches[PV_KERNEL_KINDS] = {};
@@ -112,7 +122,8 @@ struct pv_context {
 
     ~pv_context() {
         for (DeviceArray *a : {&x, &y, &gamma, &gs, &p0x, &p0y, &p1x, &p1y, &pu, &pv, &inv_scratch,
-                               &inv_out, &cand, &ex, &ey, &eg, &egs, &eu, &ev, &epu, &epv})
+                               &inv_out, &cand, &ex, &ey, &eg, &egs, &eu, &ev, &epu, &epv,
+                               &removed_index})
             a->release();
         for (int s = 0; s < 7; ++s) {
             kx[s].release();
@@ -692,6 +703,7 @@ pv_status pv_upload_state(pv_context *ctx, const double *x, const double *y,
     ctx->n = n;
     ctx->fsal_valid = false;
     ctx->state_valid = true;
+    ctx->gamma_host.assign(circulation, circulation + n);
     if (n == 0)
         return PV_OK;
     const size_t bytes = n * sizeof(double);
@@ -977,6 +989,283 @@ pv_status pv_dipole_scan(pv_context *ctx, double threshold, pv_dipole_candidate 
                                      cudaMemcpyDeviceToHost, ctx->stream));
         PV_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
     }
+    return PV_OK;
+}
+
+namespace {
+
+// Every candidate of the device state (rescanning once with room for all of them).
+pv_status scan_all(pv_context *ctx, double threshold, std::vector<pv_dipole_candidate> &out) {
+    size_t cap = std::max<size_t>(ctx->cand.cap / 3, 256), count = 0;
+    out.resize(cap);
+    pv_status st = pv_dipole_scan(ctx, threshold, out.data(), cap, &count);
+    if (st == PV_OK && count > cap) {
+        if (count > (static_cast<size_t>(1) << 26))
+            return fail(ctx, PV_ERROR_CAPACITY, "more than 2^26 close-dipole candidates");
+        out.resize(count);
+        st = pv_dipole_scan(ctx, threshold, out.data(), count, &count);
+    }
+    out.resize(std::min(count, out.size()));
+    return st;
+}
+
+struct Position {
+    double x, y;
+};
+
+// The reinjection draws of src/dipole.cpp:129-180, in the reference's order and arithmetic.
+struct Reinjector {
+    pv_context *ctx;
+    std::uniform_real_distribution<double> unit{0.0, 1.0};
+
+    bool periodic() const { return ctx->params.geometry == PV_GEOMETRY_PERIODIC; }
+    double u() { return unit(ctx->dipole_random); }
+
+    Position random_position() {
+        const pv_params &p = ctx->params;
+        if (periodic()) {
+            const double px = (u() - 0.5) * p.box_length_x;
+            const double py = (u() - 0.5) * p.box_length_y;
+            return {px, py};
+        }
+        const double radius = p.disk_radius * std::sqrt(u());
+        const double angle = 2.0 * kPi * u();
+        return {radius * std::cos(angle), radius * std::sin(angle)};
+    }
+
+    // injectSingle: a wall event puts its one vortex back uniformly in the disk.
+    Position single() {
+        const double radius = ctx->params.disk_radius * std::sqrt(u());
+        const double angle = 2.0 * kPi * u();
+        return {radius * std::cos(angle), radius * std::sin(angle)};
+    }
+
+    // injectPair: two independent positions, or (paired) a first position and a second one at the
+    // mean spacing of the original population in a random direction.
+    bool pair(size_t population, Position &first, Position &second) {
+        const pv_params &p = ctx->params;
+        const double area = periodic() ? p.box_length_x * p.box_length_y
+                                       : kPi * p.disk_radius * p.disk_radius;
+        const double spacing = std::sqrt(area / static_cast<double>(population));
+        first = random_position();
+        second = random_position();
+        if (ctx->dipole.reinjection != PV_REINJECT_PAIRED)
+            return true;
+        for (size_t attempt = 0; attempt < 100000; ++attempt) {
+            first = random_position();
+            const double angle = 2.0 * kPi * u();
+            second = {first.x + spacing * std::cos(angle), first.y + spacing * std::sin(angle)};
+            if (periodic()) {
+                second.x = std::remainder(second.x, p.box_length_x);
+                second.y = std::remainder(second.y, p.box_length_y);
+                return true;
+            }
+            if (second.x * second.x + second.y * second.y < p.disk_radius * p.disk_radius)
+                return true;
+        }
+        return false;
+    }
+};
+
+} // namespace
+
+pv_status pv_dipole_configure(pv_context *ctx, const pv_dipole_config *config) {
+    if (!ctx || !config)
+        return PV_ERROR_INVALID_ARGUMENT;
+    // the dipole checks of SimParams::validate (src/read.cpp:55-99)
+    const double d = config->distance;
+    if (!std::isfinite(d))
+        return fail(ctx, PV_ERROR_INVALID_ARGUMENT, "simulation parameters must be finite");
+    if (!std::isfinite(d * d) || (d > 0.0 && d * d == 0.0))
+        return fail(ctx, PV_ERROR_INVALID_ARGUMENT,
+                    "radius or distance is outside the supported numeric range");
+    if (!(d > 0.0))
+        return fail(ctx, PV_ERROR_INVALID_ARGUMENT, "dipoleRemovalDistance must be positive");
+    if (config->reinjection < PV_REINJECT_NONE || config->reinjection > PV_REINJECT_PAIRED)
+        return fail(ctx, PV_ERROR_INVALID_ARGUMENT,
+                    "dipoleReinjection must be none, independent, or paired");
+    if (!config->removal && config->reinjection != PV_REINJECT_NONE)
+        return fail(ctx, PV_ERROR_INVALID_ARGUMENT, "dipoleReinjection requires dipoleRemoval true");
+    if (ctx->params.geometry == PV_GEOMETRY_INFINITE && config->reinjection != PV_REINJECT_NONE)
+        return fail(ctx, PV_ERROR_INVALID_ARGUMENT,
+                    "dipole reinjection is available only for periodic and disk geometries");
+    ctx->dipole = *config;
+    ctx->dipole_configured = true;
+    // DipoleManager seeds its engine with the run seed mixed by this constant
+    // (src/dipole.cpp:29-30); runs and checkpoints stay interchangeable only with the same seeding
+    ctx->dipole_random.seed(config->random_seed ^ 0xd1b54a32d192ed03ULL);
+    ctx->removed_pairs = ctx->reinjected_pairs = 0;
+    return PV_OK;
+}
+
+pv_status pv_dipole_process(pv_context *ctx, size_t *events) {
+    if (!ctx || !events)
+        return PV_ERROR_INVALID_ARGUMENT;
+    *events = 0;
+    if (!ctx->dipole_configured)
+        return fail(ctx, PV_ERROR_LOGIC, "dipole events have not been configured");
+    pv_status st = require_state(ctx);
+    if (st != PV_OK)
+        return st;
+    const size_t n = ctx->n;
+    if (!ctx->dipole.removal || n == 0)
+        return PV_OK;
+    std::vector<pv_dipole_candidate> cands;
+    if ((st = scan_all(ctx, ctx->dipole.distance, cands)) != PV_OK)
+        return st;
+    if (cands.empty())
+        return PV_OK;  // before any use of the generator, as the reference returns
+    // closest first; ties by (first, second) -- src/dipole.cpp:79-85
+    std::sort(cands.begin(), cands.end(), [](const pv_dipole_candidate &a,
+                                             const pv_dipole_candidate &b) {
+        if (a.distance_squared != b.distance_squared)
+            return a.distance_squared < b.distance_squared;
+        return a.first != b.first ? a.first < b.first : a.second < b.second;
+    });
+    // greedy disjoint selection (src/dipole.cpp:87-100)
+    struct Event {
+        double first_gamma, second_gamma;
+        bool wall;
+    };
+    std::vector<unsigned char> selected(n, 0);
+    std::vector<Event> chosen;
+    std::vector<unsigned long long> removed;
+    for (const pv_dipole_candidate &c : cands) {
+        if (selected[c.first] || (c.second < n && selected[c.second]))
+            continue;
+        selected[c.first] = 1;
+        removed.push_back(c.first);
+        if (c.second < n) {
+            selected[c.second] = 1;
+            removed.push_back(c.second);
+            chosen.push_back({ctx->gamma_host[c.first], ctx->gamma_host[c.second], false});
+        } else {
+            chosen.push_back({ctx->gamma_host[c.first], 0.0, true});
+        }
+    }
+    std::sort(removed.begin(), removed.end());
+    const size_t m = removed.size();
+    const size_t survivors = n - m;
+
+    DeviceGuard guard(ctx->device);
+    // compaction on the device: state -> stage-position scratch, then the buffers trade places
+    // (the cached derivative is invalidated below, so the scratch holds nothing live)
+    PV_CUDA(ctx, ctx->removed_index.ensure(m));
+    PV_CUDA(ctx, cudaMemcpyAsync(ctx->removed_index.p, removed.data(),
+                                 m * sizeof(unsigned long long), cudaMemcpyHostToDevice,
+                                 ctx->stream));
+    PV_CUDA(ctx, counted(ctx, PV_KERNEL_DIPOLE, 1, [&] {
+                return launch_compact_survivors(
+                    ctx->x.p, ctx->y.p, ctx->gamma.p, ctx->gs.p, n,
+                    reinterpret_cast<const unsigned long long *>(ctx->removed_index.p), m,
+                    ctx->p0x.p, ctx->p0y.p, ctx->p1x.p, ctx->p1y.p, ctx->stream);
+            }));
+    std::swap(ctx->x, ctx->p0x);
+    std::swap(ctx->y, ctx->p0y);
+    std::swap(ctx->gamma, ctx->p1x);
+    std::swap(ctx->gs, ctx->p1y);
+    std::vector<double> gamma_new;
+    gamma_new.reserve(n);
+    for (size_t i = 0; i < n; ++i)
+        if (!selected[i])
+            gamma_new.push_back(ctx->gamma_host[i]);
+    ctx->removed_pairs += chosen.size();
+    ctx->fsal_valid = false;
+    ctx->n = survivors;
+
+    // reinjection, appended after the survivors (src/dipole.cpp:116-124)
+    std::vector<double> ax, ay, ag;
+    if (ctx->dipole.reinjection != PV_REINJECT_NONE) {
+        Reinjector r{ctx};
+        for (const Event &e : chosen) {
+            if (e.wall) {
+                const Position q = r.single();
+                ax.push_back(q.x);
+                ay.push_back(q.y);
+                ag.push_back(e.first_gamma);
+                continue;
+            }
+            Position a{}, b{};
+            if (!r.pair(n, a, b)) {
+                ctx->gamma_host = gamma_new;
+                return fail(ctx, PV_ERROR_RUNTIME,
+                            "could not find a valid paired reinjection position");
+            }
+            ax.push_back(a.x);
+            ay.push_back(a.y);
+            ag.push_back(e.first_gamma);
+            ax.push_back(b.x);
+            ay.push_back(b.y);
+            ag.push_back(e.second_gamma);
+        }
+        ctx->reinjected_pairs += chosen.size();
+    }
+    const size_t added = ax.size();
+    if (added) {
+        const std::vector<double> ags = scaled(ctx->gc, ag.data(), added);
+        const size_t bytes = added * sizeof(double);
+        PV_CUDA(ctx, cudaMemcpyAsync(ctx->x.p + survivors, ax.data(), bytes, cudaMemcpyHostToDevice,
+                                     ctx->stream));
+        PV_CUDA(ctx, cudaMemcpyAsync(ctx->y.p + survivors, ay.data(), bytes, cudaMemcpyHostToDevice,
+                                     ctx->stream));
+        PV_CUDA(ctx, cudaMemcpyAsync(ctx->gamma.p + survivors, ag.data(), bytes,
+                                     cudaMemcpyHostToDevice, ctx->stream));
+        PV_CUDA(ctx, cudaMemcpyAsync(ctx->gs.p + survivors, ags.data(), bytes,
+                                     cudaMemcpyHostToDevice, ctx->stream));
+        gamma_new.insert(gamma_new.end(), ag.begin(), ag.end());
+    }
+    ctx->n = survivors + added;
+    ctx->gamma_host.swap(gamma_new);
+    PV_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    collect_timers(ctx);
+    if ((st = ensure_state_capacity(ctx, ctx->n)) != PV_OK)
+        return st;
+    *events = chosen.size();
+    // the checks the reference's driver meets when it re-uploads the new population
+    // (src/main.cpp:329-333 -> uploadDeviceState): zero net circulation in the periodic box and
+    // reinjected vortices strictly inside the disk
+    if (ctx->params.geometry == PV_GEOMETRY_PERIODIC &&
+        (st = validate_geometry(ctx, nullptr, nullptr, ctx->gamma_host.data(), ctx->n)) != PV_OK)
+        return st;
+    if (ctx->params.geometry == PV_GEOMETRY_DISK &&
+        (st = validate_geometry(ctx, ax.data(), ay.data(), ag.data(), added)) != PV_OK)
+        return st;
+    return PV_OK;
+}
+
+pv_status pv_dipole_state(const pv_context *ctx, uint64_t *removed, uint64_t *reinjected,
+                          char *engine_state, size_t capacity, size_t *length) {
+    if (!ctx || !length)
+        return PV_ERROR_INVALID_ARGUMENT;
+    if (removed)
+        *removed = ctx->removed_pairs;
+    if (reinjected)
+        *reinjected = ctx->reinjected_pairs;
+    std::ostringstream text;
+    text << ctx->dipole_random;
+    const std::string s = text.str();
+    *length = s.size();
+    if (!engine_state || capacity <= s.size())
+        return PV_ERROR_CAPACITY;
+    std::memcpy(engine_state, s.c_str(), s.size() + 1);
+    return PV_OK;
+}
+
+pv_status pv_dipole_restore(pv_context *ctx, uint64_t removed, uint64_t reinjected,
+                            const char *engine_state) {
+    if (!ctx)
+        return PV_ERROR_INVALID_ARGUMENT;
+    if (!ctx->dipole_configured)
+        return fail(ctx, PV_ERROR_LOGIC, "dipole events have not been configured");
+    if (engine_state && *engine_state) {
+        std::istringstream input(engine_state);
+        std::mt19937_64 engine;
+        if (!(input >> engine))
+            return fail(ctx, PV_ERROR_RUNTIME, "invalid random-generator state in checkpoint");
+        ctx->dipole_random = engine;
+    }
+    ctx->removed_pairs = removed;
+    ctx->reinjected_pairs = reinjected;
     return PV_OK;
 }
 

@@ -2,9 +2,11 @@
 //
 // The scan replaces the O(N^2/2) candidate loop of DipoleManager::process (src/dipole.cpp:49-78)
 // that the reference runs on the host after every accepted step, with a full download of the
-// state first (src/main.cpp:327-328). The selection, compaction and optional re-injection stay in
-// the reference's host code; a candidate count of zero means process() would return 0 before
-// touching its random generator (src/dipole.cpp:101-102), so the download can be skipped.
+// state first (src/main.cpp:327-328). A candidate count of zero means process() would return 0
+// before touching its random generator (src/dipole.cpp:101-102), so nothing else runs. Otherwise
+// only the candidates cross to the host (pv_dipole_process selects there) and the survivors are
+// compacted in place of the state by compact_survivors_kernel (src/dipole.cpp:104-113), so the
+// state itself never leaves the device.
 //
 // Candidate test, bit for bit as the reference computes it (g++ on x86-64 does not contract):
 //   opposite signs (Gamma != 0, signbit differs);
@@ -129,6 +131,48 @@ cudaError_t launch_dipole_scan(const double *x, const double *y, const double *g
     const dim3 grid(static_cast<unsigned>(nt), static_cast<unsigned>(nt));
     dipole_scan_kernel<<<grid, kDT, 0, stream>>>(x, y, gamma, n, g, threshold * threshold, out,
                                                  capacity, count);
+    return cudaGetLastError();
+}
+
+namespace {
+// Survivor i (not in the sorted removal list) moves to i - (removals below i): the order of
+// src/dipole.cpp:110-113. Reads the state arrays, writes the compacted copies.
+__global__ void __launch_bounds__(256)
+    compact_survivors_kernel(const double *__restrict__ x, const double *__restrict__ y,
+                             const double *__restrict__ g, const double *__restrict__ gs, size_t n,
+                             const unsigned long long *__restrict__ removed, size_t m,
+                             double *__restrict__ ox, double *__restrict__ oy,
+                             double *__restrict__ og, double *__restrict__ ogs) {
+    const size_t i = static_cast<size_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i >= n)
+        return;
+    size_t lo = 0, hi = m;
+    while (lo < hi) {
+        const size_t mid = (lo + hi) >> 1;
+        if (removed[mid] < i)
+            lo = mid + 1;
+        else
+            hi = mid;
+    }
+    if (lo < m && removed[lo] == i)
+        return;
+    const size_t o = i - lo;
+    ox[o] = x[i];
+    oy[o] = y[i];
+    og[o] = g[i];
+    ogs[o] = gs[i];
+}
+} // namespace
+
+cudaError_t launch_compact_survivors(const double *x, const double *y, const double *g,
+                                     const double *gs, size_t n, const unsigned long long *removed,
+                                     size_t m, double *ox, double *oy, double *og, double *ogs,
+                                     cudaStream_t stream) {
+    if (n == 0)
+        return cudaSuccess;
+    const unsigned blocks = static_cast<unsigned>((n + 255) / 256);
+    compact_survivors_kernel<<<blocks, 256, 0, stream>>>(x, y, g, gs, n, removed, m, ox, oy, og,
+                                                         ogs);
     return cudaGetLastError();
 }
 

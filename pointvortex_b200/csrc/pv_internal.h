@@ -107,6 +107,13 @@ cudaError_t launch_dipole_scan(const double *x, const double *y, const double *g
                                DipoleCandidateDev *out, size_t capacity,
                                unsigned long long *count, cudaStream_t stream);
 
+// Order-preserving removal of the sorted indices removed[0, m) from (x, y, g, gs)[0, n) into
+// (ox, oy, og, ogs)[0, n - m).
+cudaError_t launch_compact_survivors(const double *x, const double *y, const double *g,
+                                     const double *gs, size_t n, const unsigned long long *removed,
+                                     size_t m, double *ox, double *oy, double *og, double *ogs,
+                                     cudaStream_t stream);
+
 // ---- shared host helpers (pv_context.cu) -------------------------------------------------------
 // Kernel-constructor validation and fast-path constants of a parameter set.
 int make_geometry_consts(const struct pv_params &p, GeometryConsts &g, std::string &message);

@@ -1,9 +1,14 @@
 """Free-run parity on the chaotic infinite-plane workload (N = 1024, RK4, dt = 1e-3, 100 steps).
 
-A 1-ulp change of one coordinate grows to O(0.1) within ~20 steps of this state, so no two FP64
+A 1-ulp change of one coordinate grows to O(1) within ~40 steps of this state, so no two FP64
 implementations can agree on the final positions. The criterion is the reference's own
 sensitivity: the GPU trajectory may not drift from the reference CPU trajectory faster than the
-reference drifts from itself under a 1-ulp perturbation of the initial state. Invariants that the
+reference drifts from itself when every coordinate of the initial state is moved by one ulp (in a
+seeded random direction). That is the size of difference a different but equally correct rounding
+of one velocity evaluation makes; moving one coordinate only understates it, because the fastest
+vortices (tight pairs, speeds ~1e4) amplify a rounding difference the most (measured on this
+state: 9.6e-11 after 5 steps for the whole-state perturbation, 5.7e-15 for one coordinate of
+vortex 0). Invariants that the
 dynamics conserve exactly (circulation, linear impulse) must be conserved as tightly as the
 reference conserves them; the Hamiltonian and angular impulse drift are compared in size."""
 import numpy as np
@@ -21,19 +26,20 @@ def test_free_run_divergence_no_worse_than_reference_self_divergence(reference):
     geo = Geometry("infinite")
     checkpoints = (5, 10, 20, 40, 100)
 
-    def cpu_run(x0):
+    def cpu_run(x0, y0):
         st = reference.stepper(geo, x0.size)
-        cx, cy, out = x0.copy(), y.copy(), {}
+        cx, cy, out = x0.copy(), y0.copy(), {}
         for k in range(1, 101):
             cx, cy = st.rk4_step(cx, cy, g, 1e-3)
             if k in checkpoints:
                 out[k] = (cx.copy(), cy.copy())
         return out
 
-    ref = cpu_run(x)
-    xp = x.copy()
-    xp[0] = np.nextafter(xp[0], np.inf)
-    perturbed = cpu_run(xp)
+    ref = cpu_run(x, y)
+    rng = np.random.default_rng(1)
+    xp = np.nextafter(x, x + (2 * rng.integers(0, 2, x.size) - 1) * np.inf)
+    yp = np.nextafter(y, y + (2 * rng.integers(0, 2, y.size) - 1) * np.inf)
+    perturbed = cpu_run(xp, yp)
 
     k = pv.InfinitePlaneKernel(0.0)
     k.uploadDeviceState(pv.VortexSystem(x, y, g))
@@ -48,7 +54,7 @@ def test_free_run_divergence_no_worse_than_reference_self_divergence(reference):
     for c in checkpoints:
         d_gpu = np.max(np.hypot(gpu[c][0] - ref[c][0], gpu[c][1] - ref[c][1]))
         d_self = np.max(np.hypot(perturbed[c][0] - ref[c][0], perturbed[c][1] - ref[c][1]))
-        print(f"step {c}: gpu-vs-cpu {d_gpu:.3e}, cpu 1-ulp self-divergence {d_self:.3e}")
+        print(f"step {c}: gpu-vs-cpu {d_gpu:.3e}, cpu 1-ulp-state self-divergence {d_self:.3e}")
         # the growth rate is what the criterion bounds; 10x leaves room for where the first
         # difference lands (a velocity-rounding difference vs a coordinate ulp)
         assert d_gpu <= 10.0 * max(d_self, 1e-15), (c, d_gpu, d_self)
