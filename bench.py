@@ -124,36 +124,22 @@ def flush_l2(buf):
     buf.fill_(1.0)
 
 
-def dopri_step(k, dt, scan=True):
-    """One accepted DOPRI5 step + the close-dipole scan; returns (suggested dt, evaluations)."""
+def dopri_step(k, dt, dipoles=None):
+    """One accepted DOPRI5 step + the close-dipole events (removal only) on the device state;
+    returns (suggested dt, evaluations)."""
     before = k.evaluationCount
     r = k.deviceDopri5Step(dt, ATOL, RTOL, DTMIN, DTMAX)
-    if scan:
-        cands = k.dipoleScan(DIPOLE_THRESHOLD, capacity=64)
-        if cands:
-            remove_dipoles(k, cands)
+    if dipoles is not None:
+        dipoles.process()
     return r.suggestedTimeStep, k.evaluationCount - before
 
 
-def remove_dipoles(k, cands):
-    """Closest-first disjoint removal (DipoleManager::process, src/dipole.cpp:79-127, removal
-    only) on the device candidates; then the state is re-uploaded (FSAL invalidated)."""
+def dipole_manager(k, seed):
+    """DipoleManager of the workload (removal only, src/dipole.cpp:42-127) on the device state:
+    the scan runs on the GPU and, when it finds pairs, only the candidates reach the host."""
     import pointvortex_b200 as pv
-    n = k.stateSize()
-    s = pv.VortexSystem(np.zeros(n), np.zeros(n), np.zeros(n))
-    s.circulation = k._circulation
-    k.downloadDeviceState(s)
-    chosen = np.zeros(n, bool)
-    for c in cands:
-        if chosen[c.first] or (c.second < n and chosen[c.second]):
-            continue
-        chosen[c.first] = True
-        if c.second < n:
-            chosen[c.second] = True
-    keep = ~chosen
-    new = pv.VortexSystem(s.x[keep], s.y[keep], s.circulation[keep])
-    k.uploadDeviceState(new)
-    k._circulation = new.circulation
+    return pv.DeviceDipoleManager(k, removal=True, distance=DIPOLE_THRESHOLD, reinjection="none",
+                                  random_seed=seed)
 
 
 def run_ours(args):
@@ -170,13 +156,13 @@ def run_ours(args):
     x, y, g = ics.periodic_box(N, SEED + rank, LENGTH)
     k = pv.PeriodicBoxKernel(LENGTH, LENGTH, LAYERS, device=local)
     k.uploadDeviceState(pv.VortexSystem(x, y, g))
-    k._circulation = g.copy()
+    dipoles = dipole_manager(k, SEED + rank)
     flush = torch.empty(2 * L2_BYTES // 4, dtype=torch.float32, device=f"cuda:{local}")
 
     # warm-up: the first steps also absorb the start-up rejections (dt 1e-3 -> ~1e-6)
     dt = DT0
     for _ in range(max(args.warmup, 3)):
-        dt, _ = dopri_step(k, dt)
+        dt, _ = dopri_step(k, dt, dipoles)
     torch.cuda.synchronize()
 
     # timed region: CUDA events on the library's own stream bracket each step (kernels, copies
@@ -198,7 +184,7 @@ def run_ours(args):
             torch.cuda.synchronize()
             n_step = k.stateSize()       # the evaluations of a step run before its removals
             events[s][0].record(lib_stream)
-            dt, e = dopri_step(k, dt)
+            dt, e = dopri_step(k, dt, dipoles)
             events[s][1].record(lib_stream)
             evals += e
             pairs += e * n_step * (n_step - 1)
@@ -213,7 +199,7 @@ def run_ours(args):
 
     # e2e: the same steps through the public API with host buffers -- every step uploads its
     # input state from pinned host memory and downloads the new state and the step result.
-    e2e = measure_e2e(k, dt, max(10, args.steps // 4), local)
+    e2e = measure_e2e(k, dt, max(10, args.steps // 4), local, SEED + rank)
 
     # roofline of the dominant kernel (the tiled periodic pair kernel), from its launch events
     v_launch, v_timed, v_ms = stats["velocity"]
@@ -260,31 +246,43 @@ def run_ours(args):
     return result, k
 
 
-def measure_e2e(k, dt, steps, device):
+def measure_e2e(k, dt, steps, device, seed):
+    """The step through the public API with HOST buffers: every step uploads the state from
+    pinned host memory, takes the DOPRI5 step and the dipole events, and downloads the new state
+    (positions and circulations, since events may change the population)."""
     import pointvortex_b200 as pv
     import torch
-    n = k.stateSize()
+    s0 = k.downloadDeviceSystem()
+    n = s0.size()
     host = torch.empty((3, n), dtype=torch.float64).pin_memory().numpy()
-    s = pv.VortexSystem(np.zeros(n), np.zeros(n), k._circulation.copy())
-    k.downloadDeviceState(s)
-    host[0], host[1], host[2] = s.x, s.y, s.circulation
+    host[0], host[1], host[2] = s0.x, s0.y, s0.circulation
+    dipoles = dipole_manager(k, seed)
     evals = 0
+    pairs = 0.0
+    h2d = d2h = 0
     t0 = time.perf_counter()
     for _ in range(steps):
-        st = pv.VortexSystem(host[0], host[1], host[2])
+        st = pv.VortexSystem(host[0, :n], host[1, :n], host[2, :n])
         k.uploadDeviceState(st)
         before = k.evaluationCount
         r = k.deviceDopri5Step(dt, ATOL, RTOL, DTMIN, DTMAX)
-        k.dipoleScan(DIPOLE_THRESHOLD, capacity=64)
-        k.downloadDeviceState(st)
-        host[0], host[1] = st.x, st.y
-        evals += k.evaluationCount - before
+        dipoles.process()
+        e = k.evaluationCount - before
+        out = k.downloadDeviceSystem()
+        # x, y, circulation and the scaled circulations up; x, y, circulation down; the 256-byte
+        # control block up once per attempt and down after each attempt and after the scan
+        h2d += 32 * n + 256 * (1 + r.rejectedSteps)
+        d2h += 24 * out.size() + 256 * (2 + r.rejectedSteps)
+        pairs += e * n * (n - 1)
+        n = out.size()
+        host[0, :n], host[1, :n], host[2, :n] = out.x, out.y, out.circulation
+        evals += e
         dt = r.suggestedTimeStep
     sec = time.perf_counter() - t0
     torch.cuda.synchronize(device)
-    return {"value": evals * n * (n - 1) / sec, "unit": "pair-interactions/s",
-            "h2d_bytes_per_step": 3 * 8 * n + 256, "d2h_bytes_per_step": 2 * 8 * n + 256 + 8,
-            "steps": steps, "note": "upload + DOPRI5 step + dipole scan + download per step; "
+    return {"value": pairs / sec, "unit": "pair-interactions/s",
+            "h2d_bytes_per_step": h2d // steps, "d2h_bytes_per_step": d2h // steps,
+            "steps": steps, "note": "upload + DOPRI5 step + dipole events + download per step; "
             "the upload invalidates FSAL, so each step makes 7 evaluations"}
 
 

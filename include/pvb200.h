@@ -182,6 +182,11 @@ pv_status pv_dipole_state(const pv_context *ctx, uint64_t *removed, uint64_t *re
 pv_status pv_dipole_restore(pv_context *ctx, uint64_t removed, uint64_t reinjected,
                             const char *engine_state);
 
+/* Circulations of the device state (they change only through pv_upload_state and
+ * pv_dipole_process); n must equal the device population. No counterpart: the reference's
+ * driver keeps the population on the host and processes dipoles there. */
+pv_status pv_download_circulation(pv_context *ctx, double *circulation, size_t n);
+
 /* Population of the device state. */
 pv_status pv_state_size(const pv_context *ctx, size_t *n);
 /* Velocity evaluations made so far by the stepping hooks (the reference's CountingKernel,

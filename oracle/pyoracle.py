@@ -15,6 +15,7 @@ std::invalid_argument, IndexError for std::out_of_range, RuntimeError for std::r
 from __future__ import annotations
 
 import ctypes
+import math
 import os
 import subprocess
 from dataclasses import dataclass
@@ -132,6 +133,10 @@ class Oracle:
             lib.pvref_dopri5_step.argtypes = [ctypes.c_void_p, _D, _D, _D, sz, ctypes.c_double, _D]
             lib.pvref_dipole_process.argtypes = [P, _D, _D, _D, ctypes.POINTER(sz), sz,
                                                  ctypes.POINTER(sz)]
+            lib.pvref_dipole_process_state.argtypes = [
+                P, _D, _D, _D, ctypes.POINTER(sz), sz, ctypes.POINTER(sz),
+                ctypes.POINTER(ctypes.c_uint64), ctypes.POINTER(ctypes.c_uint64), ctypes.c_char_p,
+                ctypes.c_char_p, sz]
             lib.pvref_max_threads.restype = ctypes.c_int
             lib.pvref_set_threads.argtypes = [ctypes.c_int]
 
@@ -227,6 +232,30 @@ class Oracle:
         k = n.value
         return events.value, xx[:k].copy(), yy[:k].copy(), gg[:k].copy()
 
+    def dipole_events(self, geo: Geometry, x, y, g, state=None):
+        """One DipoleManager::process call (src/dipole.cpp:42-127) by a manager restored from
+        state = (removed, reinjected, engine text) (src/dipole.cpp:32-40; None: fresh seeding).
+        Returns (events, x, y, g, state after the call). The port restates the selection and the
+        reinjection draws in Python (DipolePort); the reference runs its own DipoleManager."""
+        if self.kind == "port":
+            return DipolePort(self, geo, state).process(x, y, g)
+        x, y, g = (np.array(a, dtype=np.float64) for a in (x, y, g))
+        cap = x.size + 2
+        xx, yy, gg = (np.resize(a, max(cap, 1)).copy() for a in (x, y, g))
+        n = ctypes.c_size_t(x.size)
+        events = ctypes.c_size_t(0)
+        removed = ctypes.c_uint64(state[0] if state else 0)
+        reinjected = ctypes.c_uint64(state[1] if state else 0)
+        out = ctypes.create_string_buffer(1 << 15)
+        par = geo.c()
+        self._check(self.lib.pvref_dipole_process_state(
+            ctypes.byref(par), _p(xx), _p(yy), _p(gg), ctypes.byref(n), cap, ctypes.byref(events),
+            ctypes.byref(removed), ctypes.byref(reinjected),
+            (state[2] if state else "").encode(), out, len(out)))
+        k = n.value
+        return (events.value, xx[:k].copy(), yy[:k].copy(), gg[:k].copy(),
+                (removed.value, reinjected.value, out.value.decode()))
+
     def set_threads(self, n: int) -> None:
         if self.kind != "port":
             self.lib.pvref_set_threads(n)
@@ -275,3 +304,151 @@ class Stepper:
         if self.o.kind != "port":
             raise NotImplementedError
         return int(self.o.lib.pvo_stepper_evaluations(self.h))
+
+
+# ---- DipoleManager restated (src/dipole.cpp:29-186) ---------------------------------------------
+
+class MT19937_64:
+    """std::mt19937_64: the 64-bit Mersenne Twister of Matsumoto and Nishimura with the
+    parameters the C++ standard fixes ([rand.predef]), and libstdc++'s text form of its state
+    (the 312 words, then the position, separated by spaces)."""
+
+    N, M = 312, 156
+    MATRIX = 0xB5026F5AA96619E9
+    UPPER, LOWER = 0xFFFFFFFF80000000, 0x7FFFFFFF
+    MASK = (1 << 64) - 1
+
+    def __init__(self, seed: int = 5489):
+        mt = [seed & self.MASK]
+        for i in range(1, self.N):
+            mt.append((6364136223846793005 * (mt[-1] ^ (mt[-1] >> 62)) + i) & self.MASK)
+        self.mt, self.p = mt, self.N
+
+    def _twist(self):
+        mt, n, m = self.mt, self.N, self.M
+        for i in range(n):
+            y = (mt[i] & self.UPPER) | (mt[(i + 1) % n] & self.LOWER)
+            mt[i] = mt[(i + m) % n] ^ (y >> 1) ^ (self.MATRIX if y & 1 else 0)
+        self.p = 0
+
+    def __call__(self) -> int:
+        if self.p >= self.N:
+            self._twist()
+        z = self.mt[self.p]
+        self.p += 1
+        z ^= (z >> 29) & 0x5555555555555555
+        z ^= (z << 17) & 0x71D67FFFEDA60000
+        z ^= (z << 37) & 0xFFF7EEE000000000
+        z ^= z >> 43
+        return z & self.MASK
+
+    def unit(self) -> float:
+        """uniform_real_distribution<double>(0, 1): libstdc++'s generate_canonical with one
+        64-bit draw -- the draw rounded to double, divided by 2^64, kept below 1."""
+        r = float(self()) / 18446744073709551616.0
+        return r if r < 1.0 else math.nextafter(1.0, 0.0)
+
+    def text(self) -> str:
+        return " ".join(str(w) for w in self.mt) + " " + str(self.p)
+
+    @classmethod
+    def from_text(cls, text: str) -> "MT19937_64":
+        words = [int(w) for w in text.split()]
+        if len(words) != cls.N + 1:
+            raise RuntimeError("invalid random-generator state in checkpoint")
+        e = cls(0)
+        e.mt, e.p = words[:cls.N], words[cls.N]
+        return e
+
+
+class DipolePort:
+    """DipoleManager (src/dipole.h:18-40) restated: the candidate scan is the C port's
+    (pvo_dipole_scan, bit-exact to src/dipole.cpp:49-78); the closest-first disjoint selection
+    (:79-100), the order-keeping compaction (:104-113) and the reinjection draws (:116-180)
+    follow here in the reference's order and arithmetic (Python's math functions are the C
+    library's)."""
+
+    SEED_MIX = 0xD1B54A32D192ED03     # src/dipole.cpp:29-30
+
+    def __init__(self, oracle: "Oracle", geo: Geometry, state=None):
+        self.oracle, self.geo = oracle, geo
+        self.removed, self.reinjected = (state[0], state[1]) if state else (0, 0)
+        if state and state[2]:
+            self.random = MT19937_64.from_text(state[2])
+        else:
+            self.random = MT19937_64(geo.random_seed ^ self.SEED_MIX)
+
+    def _position(self):
+        geo = self.geo
+        if geo.boundary == "periodic":
+            px = (self.random.unit() - 0.5) * geo.box_length_x
+            py = (self.random.unit() - 0.5) * geo.box_length_y
+            return px, py
+        radius = geo.disk_radius * math.sqrt(self.random.unit())
+        angle = 2.0 * math.pi * self.random.unit()
+        return radius * math.cos(angle), radius * math.sin(angle)
+
+    def _pair(self, population: int):
+        geo = self.geo
+        periodic = geo.boundary == "periodic"
+        area = (geo.box_length_x * geo.box_length_y if periodic
+                else math.pi * geo.disk_radius * geo.disk_radius)
+        spacing = math.sqrt(area / float(population))
+        first = self._position()
+        second = self._position()
+        if geo.dipole_reinjection == 2:
+            for _ in range(100000):
+                first = self._position()
+                angle = 2.0 * math.pi * self.random.unit()
+                second = (first[0] + spacing * math.cos(angle), first[1] + spacing * math.sin(angle))
+                if periodic:
+                    second = (math.remainder(second[0], geo.box_length_x),
+                              math.remainder(second[1], geo.box_length_y))
+                    break
+                if second[0] * second[0] + second[1] * second[1] < geo.disk_radius * geo.disk_radius:
+                    break
+            else:
+                raise RuntimeError("could not find a valid paired reinjection position")
+        return first, second
+
+    def process(self, x, y, g):
+        x, y, g = (np.array(a, dtype=np.float64) for a in (x, y, g))
+        n = x.size
+        geo = self.geo
+        if not geo.dipole_removal or n == 0:
+            return 0, x, y, g, self.state()
+        cands = sorted(self.oracle.dipole_scan(geo, x, y, g), key=lambda c: (c[2], c[0], c[1]))
+        selected = np.zeros(n, bool)
+        events = []
+        for a, b, _ in cands:
+            if selected[a] or (b < n and selected[b]):
+                continue
+            selected[a] = True
+            if b < n:
+                selected[b] = True
+                events.append((g[a], g[b], False))
+            else:
+                events.append((g[a], 0.0, True))
+        if not events:
+            return 0, x, y, g, self.state()
+        keep = ~selected
+        ox, oy, og = list(x[keep]), list(y[keep]), list(g[keep])
+        self.removed += len(events)
+        if geo.dipole_reinjection != 0:
+            for g1, g2, wall in events:
+                if wall:
+                    radius = geo.disk_radius * math.sqrt(self.random.unit())
+                    angle = 2.0 * math.pi * self.random.unit()
+                    ox.append(radius * math.cos(angle))
+                    oy.append(radius * math.sin(angle))
+                    og.append(g1)
+                    continue
+                first, second = self._pair(n)
+                ox += [first[0], second[0]]
+                oy += [first[1], second[1]]
+                og += [g1, g2]
+            self.reinjected += len(events)
+        return len(events), np.array(ox), np.array(oy), np.array(og), self.state()
+
+    def state(self):
+        return self.removed, self.reinjected, self.random.text()

@@ -282,6 +282,39 @@ int pvref_device_dopri5_step(void *handle, double dt, double *out) {
 
 // DipoleManager::process (src/dipole.cpp:42-127). Arrays are in/out with room for `capacity`
 // vortices; *n is updated to the surviving population. *events receives the return value.
+// DipoleManager(params, state) + process + state() (src/dipole.cpp:32-40, 42-127, 182-186): one
+// call of a manager restored from (*removed, *reinjected, engine_in); an empty engine_in keeps
+// the fresh seeding. The counts and the engine text after the call are written back.
+int pvref_dipole_process_state(const pvref_params *p, double *x, double *y, double *g,
+                               std::size_t *n, std::size_t capacity, std::size_t *events,
+                               std::uint64_t *removed, std::uint64_t *reinjected,
+                               const char *engine_in, char *engine_out,
+                               std::size_t engine_capacity) {
+    return guarded([&] {
+        const SimParams sp = toSimParams(p);
+        DipoleEventState in{static_cast<std::size_t>(*removed),
+                            static_cast<std::size_t>(*reinjected),
+                            engine_in ? std::string(engine_in) : std::string()};
+        DipoleManager manager(sp, in);
+        VortexSystem s = makeSystem(x, y, g, *n);
+        *events = manager.process(s);
+        if (s.size() > capacity)
+            throw std::runtime_error("dipole result exceeds capacity");
+        *n = s.size();
+        if (*n) {
+            std::memcpy(x, s.x.data(), *n * sizeof(double));
+            std::memcpy(y, s.y.data(), *n * sizeof(double));
+            std::memcpy(g, s.circulation.data(), *n * sizeof(double));
+        }
+        const DipoleEventState out = manager.state();
+        *removed = out.removedPairs;
+        *reinjected = out.reinjectedPairs;
+        if (out.randomEngineState.size() >= engine_capacity)
+            throw std::runtime_error("engine state exceeds capacity");
+        std::memcpy(engine_out, out.randomEngineState.c_str(), out.randomEngineState.size() + 1);
+    });
+}
+
 int pvref_dipole_process(const pvref_params *p, double *x, double *y, double *g, std::size_t *n,
                          std::size_t capacity, std::size_t *events) {
     return guarded([&] {

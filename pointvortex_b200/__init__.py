@@ -6,6 +6,8 @@ interface. Importing it without the built library raises ImportError.
 """
 from .kernel import (  # noqa: F401
     CudaError,
+    DeviceDipoleManager,
+    DipoleEventState,
     DiskKernel,
     DipoleCandidate,
     InfinitePlaneKernel,
@@ -28,7 +30,7 @@ from . import autotune as _autotune
 _autotune.load()  # the measured tuning table for this library, when present
 
 __all__ = [
-    "CudaError", "DiskKernel", "DipoleCandidate", "InfinitePlaneKernel", "Invariants",
+    "CudaError", "DeviceDipoleManager", "DipoleEventState", "DiskKernel", "DipoleCandidate", "InfinitePlaneKernel", "Invariants",
     "LogicError", "PeriodicBoxKernel", "StepResult", "VelocityField", "VelocityKernel",
     "VortexSystem", "backendName", "backendRuntimeDetails", "computeInvariants",
     "makeBackendKernel", "probePeak", "LIB_PATH",

@@ -54,6 +54,17 @@ class PvDipoleCandidate(ctypes.Structure):
     ]
 
 
+class PvDipoleConfig(ctypes.Structure):
+    _fields_ = [
+        ("removal", ctypes.c_int),
+        ("distance", ctypes.c_double),
+        ("reinjection", ctypes.c_int),
+        ("random_seed", ctypes.c_uint64),
+    ]
+
+
+REINJECTION = {"none": 0, "independent": 1, "paired": 2}
+
 PV_ERROR_CAPACITY = 6
 SIM_RUNNING, SIM_DONE, SIM_FAILED, SIM_BUDGET = 1, 2, 3, 4
 
@@ -120,6 +131,12 @@ SIGNATURES = {
     "pv_state_invariants": (_ST, [_CTX, _D]),
     "pv_dipole_scan": (_ST, [_CTX, ctypes.c_double, ctypes.POINTER(PvDipoleCandidate), _SZ,
                              ctypes.POINTER(_SZ)]),
+    "pv_dipole_configure": (_ST, [_CTX, ctypes.POINTER(PvDipoleConfig)]),
+    "pv_dipole_process": (_ST, [_CTX, ctypes.POINTER(_SZ)]),
+    "pv_dipole_state": (_ST, [_CTX, ctypes.POINTER(ctypes.c_uint64), ctypes.POINTER(ctypes.c_uint64),
+                              ctypes.c_char_p, _SZ, ctypes.POINTER(_SZ)]),
+    "pv_dipole_restore": (_ST, [_CTX, ctypes.c_uint64, ctypes.c_uint64, ctypes.c_char_p]),
+    "pv_download_circulation": (_ST, [_CTX, _D, _SZ]),
     "pv_state_size": (_ST, [_CTX, ctypes.POINTER(_SZ)]),
     "pv_evaluation_count": (_ST, [_CTX, ctypes.POINTER(ctypes.c_uint64)]),
     "pv_rk4_advance": (_ST, [_CTX, ctypes.c_double, ctypes.c_uint64]),

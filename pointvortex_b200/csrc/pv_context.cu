@@ -1269,6 +1269,18 @@ pv_status pv_dipole_restore(pv_context *ctx, uint64_t removed, uint64_t reinject
     return PV_OK;
 }
 
+pv_status pv_download_circulation(pv_context *ctx, double *circulation, size_t n) {
+    if (!ctx || (n && !circulation))
+        return PV_ERROR_INVALID_ARGUMENT;
+    pv_status st = require_state(ctx);
+    if (st != PV_OK)
+        return st;
+    if (n != ctx->n)
+        return fail(ctx, PV_ERROR_RUNTIME, "host and device vortex populations differ");
+    std::copy(ctx->gamma_host.begin(), ctx->gamma_host.end(), circulation);
+    return PV_OK;
+}
+
 pv_status pv_state_size(const pv_context *ctx, size_t *n) {
     if (!ctx || !n)
         return PV_ERROR_INVALID_ARGUMENT;

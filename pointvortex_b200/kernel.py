@@ -228,6 +228,20 @@ class VelocityKernel:
         vortices.x = x[:n].copy()
         vortices.y = y[:n].copy()
 
+    def downloadDeviceCirculation(self) -> np.ndarray:
+        """Circulations of the device state (they change when dipole events run on it)."""
+        n = self.stateSize()
+        g = np.empty(max(n, 1))
+        self._check(lib.pv_download_circulation(self._ctx, _ptr(g), n))
+        return g[:n].copy()
+
+    def downloadDeviceSystem(self) -> VortexSystem:
+        """The whole device state (positions and circulations) as a new VortexSystem."""
+        g = self.downloadDeviceCirculation()
+        s = VortexSystem(np.zeros(g.size), np.zeros(g.size), g)
+        self.downloadDeviceState(s)
+        return s
+
     def evaluateDeviceState(self) -> VelocityField:
         n = self.stateSize()
         u = np.empty(max(n, 1))
@@ -326,6 +340,56 @@ class DiskKernel(VelocityKernel):
 
     def __init__(self, radius: float, **kw):
         super().__init__(_lib.GEOMETRY_DISK, disk_radius=radius, **kw)
+
+
+@dataclass
+class DipoleEventState:
+    """src/dipole.h:12-16."""
+
+    removedPairs: int = 0
+    reinjectedPairs: int = 0
+    randomEngineState: str = ""
+
+
+class DeviceDipoleManager:
+    """DipoleManager (src/dipole.h:18-40) acting on a kernel's device-resident state.
+
+    process() is DipoleManager::process (src/dipole.cpp:42-127) with the candidate scan and the
+    survivor compaction on the GPU; only the candidate list crosses to the host, where the
+    closest-first selection and the reinjection draws (the reference's generator, seeded as the
+    reference seeds it) are made. After it the device population, its order and the generator
+    state equal what the reference's host code leaves. `state` restores a checkpointed
+    DipoleEventState (src/dipole.cpp:32-40)."""
+
+    def __init__(self, kernel: "VelocityKernel", removal: bool = True, distance: float = 0.01,
+                 reinjection: str = "none", random_seed: int = 1234567,
+                 state: Optional[DipoleEventState] = None):
+        if reinjection not in _lib.REINJECTION:
+            raise ValueError("dipoleReinjection must be none, independent, or paired")
+        self.kernel = kernel
+        cfg = _lib.PvDipoleConfig(int(bool(removal)), float(distance),
+                                  _lib.REINJECTION[reinjection], int(random_seed) & (2**64 - 1))
+        kernel._check(lib.pv_dipole_configure(kernel._ctx, ctypes.byref(cfg)))
+        if state is not None:
+            kernel._check(lib.pv_dipole_restore(kernel._ctx, state.removedPairs,
+                                                state.reinjectedPairs,
+                                                state.randomEngineState.encode()))
+
+    def process(self) -> int:
+        events = ctypes.c_size_t(0)
+        self.kernel._check(lib.pv_dipole_process(self.kernel._ctx, ctypes.byref(events)))
+        return int(events.value)
+
+    def state(self) -> DipoleEventState:
+        removed, reinjected = ctypes.c_uint64(0), ctypes.c_uint64(0)
+        length = ctypes.c_size_t(0)
+        lib.pv_dipole_state(self.kernel._ctx, ctypes.byref(removed), ctypes.byref(reinjected),
+                            None, 0, ctypes.byref(length))
+        buf = ctypes.create_string_buffer(length.value + 1)
+        self.kernel._check(lib.pv_dipole_state(self.kernel._ctx, ctypes.byref(removed),
+                                               ctypes.byref(reinjected), buf, len(buf),
+                                               ctypes.byref(length)))
+        return DipoleEventState(int(removed.value), int(reinjected.value), buf.value.decode())
 
 
 def computeInvariants(vortices: VortexSystem, kernel: VelocityKernel) -> Invariants:

@@ -61,14 +61,62 @@ def small_case(ref: Oracle, geo: Geometry, x, y, g, tag: str) -> None:
                           geo.absolute_tolerance, geo.relative_tolerance]))
 
 
+def planted_dipoles(boundary: str, n: int, seed: int):
+    """A state with ten planted close opposite-sign pairs (and, in the disk, vortices near the
+    wall): the input of the dipole-event fixtures."""
+    rng = np.random.default_rng(seed)
+    if boundary == "periodic":
+        x, y, g = ics.periodic_box(n, seed, 2 * np.pi)
+    else:
+        x, y, g = ics.disk(n, seed, 1.0, 0.999, gaussian=False)
+    for k in range(0, 20, 2):
+        x[k + 1] = x[k] + rng.uniform(-0.01, 0.01)
+        y[k + 1] = y[k] + rng.uniform(-0.01, 0.01)
+        g[k + 1] = -g[k]
+    if boundary == "periodic":
+        x = np.remainder(x + np.pi, 2 * np.pi) - np.pi
+    return x, y, g
+
+
+DIPOLE_EVENT_CASES = [(b, mode) for b in ("periodic", "disk") for mode in (0, 1, 2)]
+
+
+def dipole_event_geometry(boundary: str, mode: int) -> Geometry:
+    return Geometry(boundary, box_length_x=2 * np.pi, box_length_y=2 * np.pi, disk_radius=1.0,
+                    dipole_removal=True, dipole_removal_distance=0.02, dipole_reinjection=mode,
+                    random_seed=99)
+
+
+def dipole_event_fixtures(ref: Oracle) -> None:
+    """Three consecutive DipoleManager::process calls of one manager (removal, independent and
+    paired reinjection; periodic box and disk), with the counts and the generator text state
+    after each call."""
+    for boundary, mode in DIPOLE_EVENT_CASES:
+        geo = dipole_event_geometry(boundary, mode)
+        x, y, g = planted_dipoles(boundary, 400, 5)
+        out = {"x": x, "y": y, "g": g}
+        state = None
+        for call in range(3):
+            events, x, y, g, state = ref.dipole_events(geo, x, y, g, state)
+            out.update({f"events{call}": np.array([events]), f"x{call}": x, f"y{call}": y,
+                        f"g{call}": g, f"counts{call}": np.array(state[:2], dtype=np.uint64),
+                        f"engine{call}": np.array(state[2])})
+        save(f"dipole_events_{boundary}_{mode}.npz", **out)
+
+
 def main() -> int:
     ap = argparse.ArgumentParser()
     ap.add_argument("--reference", default="/root/reference")
+    ap.add_argument("--only", choices=["dipole_events"], default=None,
+                    help="regenerate one fixture family only")
     args = ap.parse_args()
     subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle"), "ref",
                     f"REF={args.reference}"], check=True)
     ref = Oracle("reference")
     t0 = time.time()
+    if args.only == "dipole_events":
+        dipole_event_fixtures(ref)
+        return 0
 
     # small cases, all three geometries (+ the core-radius plane)
     for tag, geo, (x, y, g) in [
@@ -133,6 +181,7 @@ def main() -> int:
         events, sx, sy, sg = ref.dipole_process(geo, x, y, g)
         save(f"dipole_{tag}.npz", x=x, y=y, g=g, events=np.array([events]), sx=sx, sy=sy, sg=sg,
              threshold=np.array([geo.dipole_removal_distance]))
+    dipole_event_fixtures(ref)
     print(f"done in {time.time() - t0:.1f} s")
     _ = rng
     return 0

@@ -142,3 +142,32 @@ def test_dipole_scan_matches_reference_process(port, reference, tag):
     assert events == ref_events == int(d["events"][0]) and events > 0
     keep = ~np.array(chosen)
     assert np.array_equal(d["x"][keep], sx) and np.array_equal(d["g"][keep], sg)
+
+
+def test_mt19937_64_known_answer():
+    """The C++ standard's required value: the 10000th draw of a default-constructed
+    std::mt19937_64 is 9981545732273789042 ([rand.predef])."""
+    from oracle.pyoracle import MT19937_64
+    e = MT19937_64()
+    for _ in range(9999):
+        e()
+    assert e() == 9981545732273789042
+
+
+@pytest.mark.parametrize("boundary,mode", [(b, m) for b in ("periodic", "disk") for m in (0, 1, 2)])
+def test_dipole_port_matches_reference_fixtures(port, boundary, mode):
+    """DipolePort (selection, compaction, reinjection draws, generator text state) against three
+    consecutive DipoleManager::process calls of the reference."""
+    from conftest import golden
+    from golden.make_golden import dipole_event_geometry
+    d = golden(f"dipole_events_{boundary}_{mode}.npz")
+    geo = dipole_event_geometry(boundary, mode)
+    x, y, g, state = d["x"], d["y"], d["g"], None
+    for call in range(3):
+        events, x, y, g, state = port.dipole_events(geo, x, y, g, state)
+        assert events == int(d[f"events{call}"][0])
+        assert np.array_equal(x, d[f"x{call}"]) and np.array_equal(y, d[f"y{call}"])
+        assert np.array_equal(g, d[f"g{call}"])
+        assert state[:2] == tuple(int(c) for c in d[f"counts{call}"])
+        assert state[2] == str(d[f"engine{call}"])
+    assert int(d["events0"][0]) > 0
