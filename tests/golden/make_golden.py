@@ -69,10 +69,11 @@ def planted_dipoles(boundary: str, n: int, seed: int):
         x, y, g = ics.periodic_box(n, seed, 2 * np.pi)
     else:
         x, y, g = ics.disk(n, seed, 1.0, 0.999, gaussian=False)
-    for k in range(0, 20, 2):
-        x[k + 1] = x[k] + rng.uniform(-0.01, 0.01)
-        y[k + 1] = y[k] + rng.uniform(-0.01, 0.01)
-        g[k + 1] = -g[k]
+    # move negative vortices next to positive ones (circulations untouched, so the periodic
+    # state keeps its zero total)
+    for a, b in zip(np.flatnonzero(g > 0)[:10], np.flatnonzero(g < 0)[:10]):
+        x[b] = x[a] + rng.uniform(-0.01, 0.01)
+        y[b] = y[a] + rng.uniform(-0.01, 0.01)
     if boundary == "periodic":
         x = np.remainder(x + np.pi, 2 * np.pi) - np.pi
     return x, y, g
