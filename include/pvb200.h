@@ -182,6 +182,32 @@ pv_status pv_dipole_state(const pv_context *ctx, uint64_t *removed, uint64_t *re
 pv_status pv_dipole_restore(pv_context *ctx, uint64_t removed, uint64_t reinjected,
                             const char *engine_state);
 
+/* ---- text output at GPU rates (the reference formats on the host with
+ *      std::ostream << std::setprecision(17)) ------------------------------------------------
+ * Rows are formatted on the GPU, one thread per vortex, with every double printed exactly as the
+ * reference's stream prints it (17 significant digits, correctly rounded, %g layout), packed on
+ * the GPU and copied to `out` in one transfer. *length = the frame's bytes; when capacity is
+ * smaller nothing is copied and PV_ERROR_CAPACITY is returned. n * PV_TRAJECTORY_ROW_MAX
+ * (n * PV_CHECKPOINT_ROW_MAX) bytes always suffice. No terminator is written. */
+#define PV_TRAJECTORY_ROW_MAX 192
+#define PV_CHECKPOINT_ROW_MAX 80
+
+/* The rows TrajectoryWriter::write (src/print.cpp:29-40) appends for one frame of the device
+ * state, "time,frame,index,x,y,circulation,u,v\n" per vortex, with the velocity evaluated on the
+ * device (evaluateDeviceState, as the driver's writeTrajectory does, src/main.cpp:251-258);
+ * fails like evaluateDeviceState on a non-finite velocity. */
+pv_status pv_format_trajectory(pv_context *ctx, double time, uint64_t frame, char *out,
+                               size_t capacity, size_t *length);
+/* The same rows for host arrays (TrajectoryWriter::write's own arguments). */
+pv_status pv_format_trajectory_host(pv_context *ctx, double time, uint64_t frame, const double *x,
+                                    const double *y, const double *circulation, const double *u,
+                                    const double *v, size_t n, char *out, size_t capacity,
+                                    size_t *length);
+/* The vortex block of writeCheckpoint (src/checkpoint.cpp:86-88) for the device state:
+ * "x y circulation\n" per vortex. */
+pv_status pv_format_checkpoint_vortices(pv_context *ctx, char *out, size_t capacity,
+                                        size_t *length);
+
 /* Circulations of the device state (they change only through pv_upload_state and
  * pv_dipole_process); n must equal the device population. No counterpart: the reference's
  * driver keeps the population on the host and processes dipoles there. */
@@ -298,8 +324,9 @@ pv_status pv_evaluate_device_noalloc(const pv_params *params, const double *x, c
 #define PV_KERNEL_STAGE 1      /* chunk reduction + stage position / combine / error + control */
 #define PV_KERNEL_ACCEPT 2     /* state update of an accepted step */
 #define PV_KERNEL_INVARIANTS 3 /* moments, Hamiltonian tiles, final sum */
-#define PV_KERNEL_DIPOLE 4     /* close-dipole candidate scan */
-#define PV_KERNEL_KINDS 5
+#define PV_KERNEL_DIPOLE 4     /* close-dipole candidate scan and survivor compaction */
+#define PV_KERNEL_OUTPUT 5     /* text formatting of trajectory / checkpoint rows */
+#define PV_KERNEL_KINDS 6
 
 typedef struct pv_kernel_stats {
     uint64_t launches[PV_KERNEL_KINDS];       /* kernels launched by this context */

@@ -256,6 +256,46 @@ class Oracle:
         return (events.value, xx[:k].copy(), yy[:k].copy(), gg[:k].copy(),
                 (removed.value, reinjected.value, out.value.decode()))
 
+    def write_trajectory(self, path: str, time: float, frame: int, x, y, g, u, v) -> bytes:
+        """TrajectoryWriter (src/print.cpp:24-40): header + one frame, written by the reference
+        into `path`; returns the file's bytes (reference only)."""
+        if self.kind == "port":
+            raise NotImplementedError("the reference's writer is its own ostream code")
+        arrs = [np.ascontiguousarray(a, dtype=np.float64) for a in (x, y, g, u, v)]
+        self.lib.pvref_write_trajectory.argtypes = [ctypes.c_char_p, ctypes.c_double,
+                                                    ctypes.c_size_t] + [_D] * 5 + [ctypes.c_size_t]
+        self._check(self.lib.pvref_write_trajectory(path.encode(), time, frame,
+                                                    *[_p(a) for a in arrs], arrs[0].size))
+        with open(path, "rb") as f:
+            return f.read()
+
+    def write_checkpoint(self, directory: str, geo: Geometry, x, y, g, initial, segment,
+                         dipole_state, schedule, progress) -> bytes:
+        """writeCheckpoint (src/checkpoint.cpp:23-102) by the reference; returns the bytes of
+        checkpoint_<outputIndex>.dat. dipole_state = (removed, reinjected, engine text);
+        schedule = the 5 OutputSchedule fields; progress = (time, suggestedTimeStep,
+        nextOutputTime, acceptedSteps, outputIndex, eventIndex)."""
+        if self.kind == "port":
+            raise NotImplementedError("the reference's writer is its own ostream code")
+        x, y, g = (np.ascontiguousarray(a, dtype=np.float64) for a in (x, y, g))
+        inv = np.array(initial, dtype=np.float64)
+        seg = np.array(segment, dtype=np.float64)
+        sched = np.array(schedule, dtype=np.float64)
+        pd = np.array(progress[:3], dtype=np.float64)
+        pi = np.array(progress[3:], dtype=np.uint64)
+        u64p = ctypes.POINTER(ctypes.c_uint64)
+        self.lib.pvref_write_checkpoint.argtypes = [
+            ctypes.c_char_p, ctypes.POINTER(_Params), _D, _D, _D, ctypes.c_size_t, _D, _D,
+            ctypes.c_uint64, ctypes.c_uint64, ctypes.c_char_p, _D, _D, u64p]
+        par = geo.c()
+        self._check(self.lib.pvref_write_checkpoint(
+            directory.encode(), ctypes.byref(par), _p(x), _p(y), _p(g), x.size, _p(inv), _p(seg),
+            int(dipole_state[0]), int(dipole_state[1]), dipole_state[2].encode(), _p(sched),
+            _p(pd), pi.ctypes.data_as(u64p)))
+        path = os.path.join(directory, "checkpoint_%08d.dat" % int(progress[4]))
+        with open(path, "rb") as f:
+            return f.read()
+
     def set_threads(self, n: int) -> None:
         if self.kind != "port":
             self.lib.pvref_set_threads(n)

@@ -14,6 +14,8 @@
 #include "backend.h"
 #include "compute.h"
 #include "dipole.h"
+#include "print.h"
+#include "checkpoint.h"
 #include "params.h"
 #include "timestep.h"
 
@@ -330,6 +332,46 @@ int pvref_dipole_process(const pvref_params *p, double *x, double *y, double *g,
             std::memcpy(y, s.y.data(), *n * sizeof(double));
             std::memcpy(g, s.circulation.data(), *n * sizeof(double));
         }
+    });
+}
+
+// TrajectoryWriter (src/print.cpp:24-40): a new file at path (overwritten) with its header and one
+// frame.
+int pvref_write_trajectory(const char *path, double time, std::size_t frame, const double *x,
+                           const double *y, const double *g, const double *u, const double *v,
+                           std::size_t n) {
+    return guarded([&] {
+        TrajectoryWriter writer(path, true);
+        VortexSystem s = makeSystem(x, y, g, n);
+        VelocityField vel;
+        vel.x.assign(u, u + n);
+        vel.y.assign(v, v + n);
+        writer.write(time, frame, s, vel);
+    });
+}
+
+// writeCheckpoint (src/checkpoint.cpp:23-102) into directory with the given records:
+// inv[0..4] initial and seg[0..4] segment invariants; sched[0..4] the OutputSchedule fields;
+// prog_d = (time, suggestedTimeStep, nextOutputTime); prog_i = (acceptedSteps, outputIndex,
+// eventIndex); the dipole state's counts and engine text.
+int pvref_write_checkpoint(const char *directory, const pvref_params *p, const double *x,
+                           const double *y, const double *g, std::size_t n, const double *inv,
+                           const double *seg, std::uint64_t removed, std::uint64_t reinjected,
+                           const char *engine, const double *sched, const double *prog_d,
+                           const std::uint64_t *prog_i) {
+    return guarded([&] {
+        const SimParams sp = toSimParams(p);
+        VortexSystem s = makeSystem(x, y, g, n);
+        const Invariants a{inv[0], inv[1], inv[2], inv[3], inv[4]};
+        const Invariants b{seg[0], seg[1], seg[2], seg[3], seg[4]};
+        const DipoleEventState d{static_cast<std::size_t>(removed),
+                                 static_cast<std::size_t>(reinjected), engine};
+        const OutputSchedule o{sched[0], sched[1], sched[2], sched[3], sched[4]};
+        const CheckpointProgress pr{prog_d[0], prog_d[1], prog_d[2],
+                                    static_cast<std::size_t>(prog_i[0]),
+                                    static_cast<std::size_t>(prog_i[1]),
+                                    static_cast<std::size_t>(prog_i[2])};
+        writeCheckpoint(directory, s, a, sp, b, d, o, pr, true);
     });
 }
 }

@@ -65,6 +65,9 @@ class PvDipoleConfig(ctypes.Structure):
 
 REINJECTION = {"none": 0, "independent": 1, "paired": 2}
 
+TRAJECTORY_ROW_MAX = 192   # PV_TRAJECTORY_ROW_MAX
+CHECKPOINT_ROW_MAX = 80    # PV_CHECKPOINT_ROW_MAX
+
 PV_ERROR_CAPACITY = 6
 SIM_RUNNING, SIM_DONE, SIM_FAILED, SIM_BUDGET = 1, 2, 3, 4
 
@@ -94,14 +97,14 @@ class PvBatchTotals(ctypes.Structure):
                 ("occupied_slots", ctypes.c_uint32)]
 
 
-KERNEL_KINDS = ("velocity", "stage", "accept", "invariants", "dipole")
+KERNEL_KINDS = ("velocity", "stage", "accept", "invariants", "dipole", "output")
 
 
 class PvKernelStats(ctypes.Structure):
     _fields_ = [
-        ("launches", ctypes.c_uint64 * 5),
-        ("timed_launches", ctypes.c_uint64 * 5),
-        ("milliseconds", ctypes.c_double * 5),
+        ("launches", ctypes.c_uint64 * 6),
+        ("timed_launches", ctypes.c_uint64 * 6),
+        ("milliseconds", ctypes.c_double * 6),
     ]
 
 
@@ -137,6 +140,11 @@ SIGNATURES = {
                               ctypes.c_char_p, _SZ, ctypes.POINTER(_SZ)]),
     "pv_dipole_restore": (_ST, [_CTX, ctypes.c_uint64, ctypes.c_uint64, ctypes.c_char_p]),
     "pv_download_circulation": (_ST, [_CTX, _D, _SZ]),
+    "pv_format_trajectory": (_ST, [_CTX, ctypes.c_double, ctypes.c_uint64, ctypes.c_char_p, _SZ,
+                                   ctypes.POINTER(_SZ)]),
+    "pv_format_trajectory_host": (_ST, [_CTX, ctypes.c_double, ctypes.c_uint64, _D, _D, _D, _D, _D,
+                                        _SZ, ctypes.c_char_p, _SZ, ctypes.POINTER(_SZ)]),
+    "pv_format_checkpoint_vortices": (_ST, [_CTX, ctypes.c_char_p, _SZ, ctypes.POINTER(_SZ)]),
     "pv_state_size": (_ST, [_CTX, ctypes.POINTER(_SZ)]),
     "pv_evaluation_count": (_ST, [_CTX, ctypes.POINTER(ctypes.c_uint64)]),
     "pv_rk4_advance": (_ST, [_CTX, ctypes.c_double, ctypes.c_uint64]),

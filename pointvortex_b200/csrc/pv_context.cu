@@ -109,6 +109,9 @@ struct pv_context {
     std::vector<double> gamma_host;  // the device state's circulations (they change only here)
     DeviceArray removed_index;
 
+    // text output (pv_format_*): row slots, row lengths, block offsets, the packed frame
+    DeviceArray fmt_stage, fmt_len, fmt_block, fmt_out;
+
     // launch accounting and optional per-launch CUDA-event timing (pv_set_profiling)
     bool profiling = false;
     uint64_t launches[PV_KERNEL_KINDS] = {};
@@ -123,7 +126,7 @@ struct pv_context {
     ~pv_context() {
         for (DeviceArray *a : {&x, &y, &gamma, &gs, &p0x, &p0y, &p1x, &p1y, &pu, &pv, &inv_scratch,
                                &inv_out, &cand, &ex, &ey, &eg, &egs, &eu, &ev, &epu, &epv,
-                               &removed_index})
+                               &removed_index, &fmt_stage, &fmt_len, &fmt_block, &fmt_out})
             a->release();
         for (int s = 0; s < 7; ++s) {
             kx[s].release();
@@ -733,6 +736,30 @@ pv_status pv_download_state(pv_context *ctx, double *x, double *y, size_t n) {
     return PV_OK;
 }
 
+namespace {
+// Enqueues the velocity of the device state into p1x / p1y (stage scratch; the stage velocities
+// and the FSAL derivative stay untouched) after clearing the control block. Not counted as a
+// stepping evaluation. The status is read by the caller's next read_control.
+pv_status enqueue_state_velocity(pv_context *ctx) {
+    pv_status st;
+    if ((st = reset_control(ctx)) != PV_OK)
+        return st;
+    if ((st = launch_eval(ctx, ctx->x.p, ctx->y.p)) != PV_OK)
+        return st;
+    --ctx->evaluations;
+    StageArgs s = stage_base(ctx);
+    s.mode = STAGE_REDUCE_ONLY;
+    s.s = 0;
+    s.kx[0] = ctx->p1x.p;
+    s.ky[0] = ctx->p1y.p;
+    s.ex = ctx->x.p;
+    s.ey = ctx->y.p;
+    PV_CUDA(ctx, counted(ctx, PV_KERNEL_STAGE, 1,
+                         [&] { return launch_stage(s, ctx->stream, ctx->sm_count); }));
+    return PV_OK;
+}
+} // namespace
+
 pv_status pv_evaluate_state(pv_context *ctx, double *u, double *v, size_t n) {
     if (!ctx)
         return PV_ERROR_INVALID_ARGUMENT;
@@ -744,20 +771,8 @@ pv_status pv_evaluate_state(pv_context *ctx, double *u, double *v, size_t n) {
     if (n == 0)
         return PV_OK;
     DeviceGuard guard(ctx->device);
-    if ((st = reset_control(ctx)) != PV_OK)
+    if ((st = enqueue_state_velocity(ctx)) != PV_OK)
         return st;
-    if ((st = launch_eval(ctx, ctx->x.p, ctx->y.p)) != PV_OK)
-        return st;
-    --ctx->evaluations; // not a stepping evaluation
-    // Reduce into the last stage slot's partner buffer p1 (scratch), leaving stages untouched.
-    StageArgs s = stage_base(ctx);
-    s.mode = STAGE_REDUCE_ONLY;
-    s.s = 0;
-    s.kx[0] = ctx->p1x.p;
-    s.ky[0] = ctx->p1y.p;
-    s.ex = ctx->x.p;
-    s.ey = ctx->y.p;
-    PV_CUDA(ctx, counted(ctx, PV_KERNEL_STAGE, 1, [&] { return launch_stage(s, ctx->stream, ctx->sm_count); }));
     PV_CUDA(ctx, cudaMemcpyAsync(u, ctx->p1x.p, n * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
     PV_CUDA(ctx, cudaMemcpyAsync(v, ctx->p1y.p, n * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
     if ((st = read_control(ctx)) != PV_OK)
@@ -1267,6 +1282,125 @@ pv_status pv_dipole_restore(pv_context *ctx, uint64_t removed, uint64_t reinject
     ctx->removed_pairs = removed;
     ctx->reinjected_pairs = reinjected;
     return PV_OK;
+}
+
+namespace {
+
+// Formats rows of (x, y, g[, u, v]) device arrays on the device and copies the packed text to
+// out when it fits. One synchronisation for the byte count (and the velocity status), one for the
+// copy.
+pv_status format_rows(pv_context *ctx, RowFormat f, char *out, size_t capacity, size_t *length,
+                      bool check_velocity) {
+    const size_t n = f.n;
+    const size_t blocks = (n + 255) / 256;
+    auto words = [](size_t bytes) { return (bytes + 7) / 8; };
+    PV_CUDA(ctx, ctx->fmt_stage.ensure(words(n * static_cast<size_t>(f.stride))));
+    PV_CUDA(ctx, ctx->fmt_out.ensure(words(n * static_cast<size_t>(f.stride))));
+    PV_CUDA(ctx, ctx->fmt_len.ensure(words(n * sizeof(uint32_t))));
+    PV_CUDA(ctx, ctx->fmt_block.ensure(blocks + 1));
+    char *dev_out = reinterpret_cast<char *>(ctx->fmt_out.p);
+    auto *block = reinterpret_cast<unsigned long long *>(ctx->fmt_block.p);
+    PV_CUDA(ctx, counted(ctx, PV_KERNEL_OUTPUT, 3, [&] {
+                return launch_format_rows(f, reinterpret_cast<char *>(ctx->fmt_stage.p),
+                                          reinterpret_cast<uint32_t *>(ctx->fmt_len.p), block,
+                                          dev_out, ctx->stream);
+            }));
+    auto *total = reinterpret_cast<unsigned long long *>(ctx->pinned);
+    PV_CUDA(ctx, cudaMemcpyAsync(total, block + blocks, sizeof(unsigned long long),
+                                 cudaMemcpyDeviceToHost, ctx->stream));
+    pv_status st;
+    if ((st = read_control(ctx)) != PV_OK)
+        return st;
+    if (check_velocity && (st = status_error(ctx, ctx->ctl_host->status)) != PV_OK)
+        return st;
+    *length = static_cast<size_t>(*total);
+    if (*length > capacity || (!out && *length))
+        return fail(ctx, PV_ERROR_CAPACITY, "output buffer is smaller than the formatted frame");
+    if (*length) {
+        PV_CUDA(ctx, cudaMemcpyAsync(out, dev_out, *length, cudaMemcpyDeviceToHost, ctx->stream));
+        PV_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    }
+    return PV_OK;
+}
+
+} // namespace
+
+pv_status pv_format_trajectory(pv_context *ctx, double time, uint64_t frame, char *out,
+                               size_t capacity, size_t *length) {
+    if (!ctx || !length)
+        return PV_ERROR_INVALID_ARGUMENT;
+    *length = 0;
+    pv_status st = require_state(ctx);
+    if (st != PV_OK)
+        return st;
+    if (ctx->n == 0)
+        return PV_OK;
+    DeviceGuard guard(ctx->device);
+    if ((st = enqueue_state_velocity(ctx)) != PV_OK)
+        return st;
+    RowFormat f{};
+    f.x = ctx->x.p;
+    f.y = ctx->y.p;
+    f.g = ctx->gamma.p;
+    f.u = ctx->p1x.p;
+    f.v = ctx->p1y.p;
+    f.n = ctx->n;
+    f.kind = ROWS_TRAJECTORY;
+    f.stride = kTrajectoryRowStride;
+    f.prefix_len = format_prefix(time, frame, f.prefix);
+    return format_rows(ctx, f, out, capacity, length, true);
+}
+
+pv_status pv_format_trajectory_host(pv_context *ctx, double time, uint64_t frame, const double *x,
+                                    const double *y, const double *circulation, const double *u,
+                                    const double *v, size_t n, char *out, size_t capacity,
+                                    size_t *length) {
+    if (!ctx || !length || (n && (!x || !y || !circulation || !u || !v)))
+        return PV_ERROR_INVALID_ARGUMENT;
+    *length = 0;
+    if (n == 0)
+        return PV_OK;
+    DeviceGuard guard(ctx->device);
+    const size_t np = padded(n);
+    for (DeviceArray *a : {&ctx->ex, &ctx->ey, &ctx->eg, &ctx->eu, &ctx->ev})
+        PV_CUDA(ctx, a->ensure(np));
+    const size_t bytes = n * sizeof(double);
+    const double *src[5] = {x, y, circulation, u, v};
+    DeviceArray *dst[5] = {&ctx->ex, &ctx->ey, &ctx->eg, &ctx->eu, &ctx->ev};
+    for (int k = 0; k < 5; ++k)
+        PV_CUDA(ctx, cudaMemcpyAsync(dst[k]->p, src[k], bytes, cudaMemcpyHostToDevice, ctx->stream));
+    RowFormat f{};
+    f.x = ctx->ex.p;
+    f.y = ctx->ey.p;
+    f.g = ctx->eg.p;
+    f.u = ctx->eu.p;
+    f.v = ctx->ev.p;
+    f.n = n;
+    f.kind = ROWS_TRAJECTORY;
+    f.stride = kTrajectoryRowStride;
+    f.prefix_len = format_prefix(time, frame, f.prefix);
+    return format_rows(ctx, f, out, capacity, length, false);
+}
+
+pv_status pv_format_checkpoint_vortices(pv_context *ctx, char *out, size_t capacity,
+                                        size_t *length) {
+    if (!ctx || !length)
+        return PV_ERROR_INVALID_ARGUMENT;
+    *length = 0;
+    pv_status st = require_state(ctx);
+    if (st != PV_OK)
+        return st;
+    if (ctx->n == 0)
+        return PV_OK;
+    DeviceGuard guard(ctx->device);
+    RowFormat f{};
+    f.x = ctx->x.p;
+    f.y = ctx->y.p;
+    f.g = ctx->gamma.p;
+    f.n = ctx->n;
+    f.kind = ROWS_CHECKPOINT;
+    f.stride = kCheckpointRowStride;
+    return format_rows(ctx, f, out, capacity, length, false);
 }
 
 pv_status pv_download_circulation(pv_context *ctx, double *circulation, size_t n) {

@@ -114,6 +114,27 @@ cudaError_t launch_compact_survivors(const double *x, const double *y, const dou
                                      size_t m, double *ox, double *oy, double *og, double *ogs,
                                      cudaStream_t stream);
 
+// ---- text output (pv_output.cu) -----------------------------------------------------------------
+enum RowKind { ROWS_TRAJECTORY = 0, ROWS_CHECKPOINT = 1 };
+constexpr int kTrajectoryRowStride = 192;  // time(24),frame(20),index(20) and five doubles(5 x 25)
+constexpr int kCheckpointRowStride = 80;   // three doubles (3 x 25)
+
+struct RowFormat {
+    const double *x, *y, *g, *u, *v;
+    size_t n;
+    int kind;        // RowKind
+    int stride;      // staging bytes per row
+    int prefix_len;  // trajectory rows: "time,frame," formatted once
+    char prefix[48];
+};
+// "time,frame," as the trajectory rows begin; returns its length (at most 46).
+int format_prefix(double time, uint64_t frame, char *out);
+// Formats rows [0, f.n) into staging (f.stride bytes each), then packs them into out;
+// block_sums needs ceil(n / 256) + 1 entries and receives the frame's byte count at
+// block_sums[ceil(n / 256)].
+cudaError_t launch_format_rows(const RowFormat &f, char *staging, uint32_t *lengths,
+                               unsigned long long *block_sums, char *out, cudaStream_t stream);
+
 // ---- shared host helpers (pv_context.cu) -------------------------------------------------------
 // Kernel-constructor validation and fast-path constants of a parameter set.
 int make_geometry_consts(const struct pv_params &p, GeometryConsts &g, std::string &message);

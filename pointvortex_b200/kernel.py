@@ -242,6 +242,40 @@ class VelocityKernel:
         self.downloadDeviceState(s)
         return s
 
+    # -- text output formatted on the GPU (the reference's setprecision(17) streams) ----------
+    def _formatted(self, call, n_rows: int, row_max: int) -> bytes:
+        cap = max(n_rows * row_max, 1)
+        buf = ctypes.create_string_buffer(cap)
+        length = ctypes.c_size_t(0)
+        self._check(call(buf, cap, ctypes.byref(length)))
+        return buf.raw[:length.value]
+
+    def formatTrajectory(self, time: float, frame: int) -> bytes:
+        """The rows TrajectoryWriter::write (src/print.cpp:29-40) appends for the device state,
+        with the velocity evaluated on the device."""
+        return self._formatted(lambda b, c, l: lib.pv_format_trajectory(self._ctx, time, frame, b,
+                                                                           c, l),
+                               self.stateSize(), _lib.TRAJECTORY_ROW_MAX)
+
+    def formatTrajectoryHost(self, time: float, frame: int, vortices: VortexSystem,
+                             velocity: VelocityField) -> bytes:
+        """The same rows for host arrays."""
+        x, y, g = self._arrays(vortices)
+        u, v = _f64(velocity.x), _f64(velocity.y)
+        if not (u.size == v.size == x.size):
+            raise ValueError("velocity and vortex arrays have different lengths")
+        return self._formatted(
+            lambda b, c, l: lib.pv_format_trajectory_host(self._ctx, time, frame, _ptr(x), _ptr(y),
+                                                          _ptr(g), _ptr(u), _ptr(v), x.size, b, c,
+                                                          l),
+            x.size, _lib.TRAJECTORY_ROW_MAX)
+
+    def formatCheckpointVortices(self) -> bytes:
+        """The "x y circulation" block of writeCheckpoint (src/checkpoint.cpp:86-88) for the
+        device state."""
+        return self._formatted(lambda b, c, l: lib.pv_format_checkpoint_vortices(self._ctx, b, c, l),
+                               self.stateSize(), _lib.CHECKPOINT_ROW_MAX)
+
     def evaluateDeviceState(self) -> VelocityField:
         n = self.stateSize()
         u = np.empty(max(n, 1))

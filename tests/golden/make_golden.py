@@ -105,10 +105,51 @@ def dipole_event_fixtures(ref: Oracle) -> None:
         save(f"dipole_events_{boundary}_{mode}.npz", **out)
 
 
+def output_inputs():
+    """Inputs of the writer fixtures: a periodic state with velocities, with awkward values
+    (negative zero, integers, powers of ten, subnormals, huge and tiny magnitudes) mixed in."""
+    x, y, g = ics.periodic_box(300, 31, 2 * np.pi)
+    rng = np.random.default_rng(32)
+    u = rng.normal(0.0, 50.0, 300)
+    v = rng.normal(0.0, 50.0, 300) * 10.0 ** rng.integers(-12, 12, 300)
+    odd = np.array([0.0, -0.0, 1.0, -1.0, 1e-5, 1e-4, 1e16, 1e17, 123456789012345678.0, 5e-324,
+                    1.7976931348623157e308, 0.1, 2.5, 1e21, -3.0e-310])
+    u[:odd.size] = odd
+    v[-odd.size:] = odd[::-1]
+    return x, y, g, u, v
+
+
+OUTPUT_GEOMETRY = dict(boundary="periodic", box_length_x=2 * np.pi, box_length_y=2 * np.pi,
+                       dipole_removal=True, dipole_removal_distance=1e-3)
+OUTPUT_RECORDS = dict(initial=[0.0, 0.123, -0.456, 7.0, -0.0123456789],
+                      segment=[0.0, 0.1230000001, -0.4559999, 7.1, -0.012345],
+                      schedule=[0.1, 0.05, 0.25, 0.35, 0.5],
+                      progress=[0.3, 1.2345e-6, 0.4, 1234, 3, 7])
+
+
+def output_fixtures(ref: Oracle) -> None:
+    """The reference's TrajectoryWriter (one frame) and writeCheckpoint files, as bytes."""
+    import tempfile
+    x, y, g, u, v = output_inputs()
+    with tempfile.TemporaryDirectory() as tmp:
+        traj = ref.write_trajectory(os.path.join(tmp, "trajectory.csv"), 0.3, 7, x, y, g, u, v)
+        geo = Geometry(**OUTPUT_GEOMETRY)
+        engine = ref.dipole_events(Geometry("periodic", box_length_x=2 * np.pi,
+                                            box_length_y=2 * np.pi, dipole_removal=True,
+                                            dipole_removal_distance=1e-3, random_seed=5),
+                                   x, y, g)[4][2]
+        r = OUTPUT_RECORDS
+        ckpt = ref.write_checkpoint(tmp, geo, x, y, g, r["initial"], r["segment"],
+                                    (2, 1, engine), r["schedule"], r["progress"])
+    save("writers_periodic_n300.npz", x=x, y=y, g=g, u=u, v=v,
+         trajectory=np.frombuffer(traj, dtype=np.uint8),
+         checkpoint=np.frombuffer(ckpt, dtype=np.uint8), engine=np.array(engine))
+
+
 def main() -> int:
     ap = argparse.ArgumentParser()
     ap.add_argument("--reference", default="/root/reference")
-    ap.add_argument("--only", choices=["dipole_events"], default=None,
+    ap.add_argument("--only", choices=["dipole_events", "output"], default=None,
                     help="regenerate one fixture family only")
     args = ap.parse_args()
     subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle"), "ref",
@@ -117,6 +158,9 @@ def main() -> int:
     t0 = time.time()
     if args.only == "dipole_events":
         dipole_event_fixtures(ref)
+        return 0
+    if args.only == "output":
+        output_fixtures(ref)
         return 0
 
     # small cases, all three geometries (+ the core-radius plane)
@@ -183,6 +227,7 @@ def main() -> int:
         save(f"dipole_{tag}.npz", x=x, y=y, g=g, events=np.array([events]), sx=sx, sy=sy, sg=sg,
              threshold=np.array([geo.dipole_removal_distance]))
     dipole_event_fixtures(ref)
+    output_fixtures(ref)
     print(f"done in {time.time() - t0:.1f} s")
     _ = rng
     return 0
