@@ -49,6 +49,10 @@ METRIC = "pair-interactions/s"
 # exact m = +-1, +-2 pairs (18), the m = 3..5 expansion (6) and the m = +-6 terms (5); per axis
 # the combination, reciprocal and update (16).
 FLOPS_PER_PAIR_PERIODIC = 240
+# DRAM bytes (read + write) of one launch of the periodic pair kernel at this workload, from one
+# ncu capture (dram__bytes_read.sum 139.0 KB, dram__bytes_write.sum 0 B, with ncu's cache flush
+# before the launch): the sources are read once, everything else stays in L2.
+TRAFFIC_BYTES_PER_LAUNCH = 139008
 
 
 def rank_info():
@@ -235,7 +239,10 @@ def run_ours(args):
             "e2e": e2e,
             "gpu_launches": int(launches),
             "roofline": {"bound": "fp64", "achieved": achieved, "peak": peak,
-                         "unit": "TFLOP/s", "frac": achieved / peak, "traffic": None,
+                         "unit": "TFLOP/s", "frac": achieved / peak,
+                         "traffic": TRAFFIC_BYTES_PER_LAUNCH,
+                         "traffic_note": "DRAM bytes per launch (ncu); the algorithmic minimum "
+                                         "is the 24N-byte source read, 98304 B",
                          "kernel": "velocity_kernel<PeriodicPair>",
                          "flops_per_pair": FLOPS_PER_PAIR_PERIODIC,
                          "ms_per_launch": per_launch_ms, "launches": v_timed,
@@ -504,6 +511,66 @@ def run_serving(budget: int = 10) -> dict:
     return out
 
 
+def run_output(reps: int = 10) -> dict:
+    """The reference's text output at GPU rates: one trajectory frame (TrajectoryWriter::write,
+    velocity evaluated on the device) and one checkpoint vortex block of the N = 16384 disk
+    workload state, formatted on the GPU, copied to the host and written to a file; wall clock
+    per frame, plus the formatting kernels' own time from their launch events."""
+    import tempfile
+    import pointvortex_b200 as pv
+    from pointvortex_b200 import ics
+    x, y, g = ics.workload_state("disk_rk4_n16384")
+    k = pv.DiskKernel(1.0)
+    k.uploadDeviceState(pv.VortexSystem(x, y, g))
+    out = {"workload": "disk_n16384", "rows": int(x.size)}
+    with tempfile.TemporaryDirectory() as tmp:
+        path = os.path.join(tmp, "trajectory.csv")
+        for name, call in (("trajectory_frame", lambda: k.formatTrajectory(0.1, 1)),
+                           ("checkpoint_block", k.formatCheckpointVortices)):
+            with open(path, "wb") as f:
+                for _ in range(3):
+                    f.write(call())
+                k.setProfiling(True)
+                k.resetKernelStats()
+                t0 = time.perf_counter()
+                for _ in range(reps):
+                    text = call()
+                    f.write(text)
+                    f.flush()
+                sec = (time.perf_counter() - t0) / reps
+                stats = k.kernelStats()
+                k.setProfiling(False)
+            launches, timed, ms = stats["output"]
+            kernel_ms = ms / max(timed, 1)
+            out[name] = {"ms_per_frame": sec * 1e3, "bytes": len(text),
+                         "formatting_kernels_ms": kernel_ms,
+                         "formatted_GB_per_s": len(text) / (kernel_ms * 1e-3) / 1e9}
+        vel = k.evaluateDeviceState()
+    out["inputs"] = (x, y, g, vel.x, vel.y)
+    return out
+
+
+def cpu_baseline_output(inputs, reps: int = 3) -> dict:
+    """The reference's own TrajectoryWriter (src/print.cpp, compiled into oracle/_ref) writing
+    the same frame on the host: the CPU baseline of the output row."""
+    import tempfile
+    from oracle.pyoracle import Oracle
+    try:
+        ref = Oracle("reference")
+    except FileNotFoundError as exc:
+        return {"unavailable": str(exc)[:200]}
+    x, y, g, u, v = inputs
+    with tempfile.TemporaryDirectory() as tmp:
+        path = os.path.join(tmp, "trajectory.csv")
+        ref.write_trajectory(path, 0.1, 1, x, y, g, u, v)
+        t0 = time.perf_counter()
+        for _ in range(reps):
+            ref.write_trajectory(path, 0.1, 1, x, y, g, u, v)
+        sec = (time.perf_counter() - t0) / reps
+    return {"ms_per_frame": sec * 1e3, "kind": "reference", "cores": 1,
+            "sample": f"TrajectoryWriter::write of the same {x.size}-row frame into a new file"}
+
+
 def summarize_launches(path: str) -> str:
     """Per-kernel launches, total time and share of an ncu launch list
     (`ncu --metrics gpu__time_duration.sum --csv --log-file <path> ...`), as a Markdown table."""
@@ -576,6 +643,14 @@ def main(argv=None):
             result["serving"] = run_serving()
         except Exception as exc:
             result["serving"] = {"error": str(exc)[:200]}
+        try:
+            out = run_output()
+            inputs = out.pop("inputs")
+            if not args.no_cpu_baseline:
+                out["reference_cpu"] = cpu_baseline_output(inputs)
+            result["output"] = out
+        except Exception as exc:
+            result["output"] = {"error": str(exc)[:200]}
     if rank == 0:
         if not args.no_cpu_baseline and world == 1:
             result["cpu_baseline"] = cpu_baseline()
