@@ -10,7 +10,7 @@
 // Status codes of the C ABI become the reference's exception types, with the library's message:
 // PV_ERROR_INVALID_ARGUMENT -> std::invalid_argument, PV_ERROR_OUT_OF_RANGE -> std::out_of_range,
 // PV_ERROR_LOGIC -> std::logic_error, anything else -> std::runtime_error.
-#include "backend.h"
+#include "backend_b200.h"
 
 #include "pvb200.h"
 
@@ -102,8 +102,39 @@ class B200Kernel final : public VelocityKernel {
     }
 
     void downloadDeviceState(VortexSystem &vortices) const override {
-        check(pv_download_state(ctx_, vortices.x.data(), vortices.y.data(), vortices.size()));
+        std::size_t n = vortices.size();
+        if (dipolesOnDevice_) {
+            // dipole events on the device may have changed the population and its circulations
+            check(pv_state_size(ctx_, &n));
+            vortices.resize(n);
+            check(pv_download_circulation(ctx_, vortices.circulation.data(), n));
+        }
+        check(pv_download_state(ctx_, vortices.x.data(), vortices.y.data(), n));
         vortices.validate();
+    }
+
+    // DipoleManager::process (src/dipole.cpp:42-127) on the device state, for the driver patch
+    // that keeps the population on the GPU. `state` carries the manager's counts and generator
+    // text in and out, so the host DipoleManager can be rebuilt from it. Returns the events.
+    std::size_t processDipolesOnDevice(const SimParams &p, DipoleEventState &state) {
+        if (!dipolesOnDevice_) {
+            const pv_dipole_config c{p.dipoleRemoval ? 1 : 0, p.dipoleRemovalDistance,
+                                     static_cast<int>(p.dipoleReinjection), p.randomSeed};
+            check(pv_dipole_configure(ctx_, &c));
+            check(pv_dipole_restore(ctx_, state.removedPairs, state.reinjectedPairs,
+                                    state.randomEngineState.c_str()));
+            dipolesOnDevice_ = true;
+        }
+        std::size_t events = 0;
+        check(pv_dipole_process(ctx_, &events));
+        std::uint64_t removed = 0, reinjected = 0;
+        std::size_t length = 0;
+        pv_dipole_state(ctx_, &removed, &reinjected, nullptr, 0, &length);
+        std::string text(length + 1, '\0');
+        check(pv_dipole_state(ctx_, &removed, &reinjected, text.data(), text.size(), &length));
+        text.resize(length);
+        state = {static_cast<std::size_t>(removed), static_cast<std::size_t>(reinjected), text};
+        return events;
     }
 
     void evaluateDeviceState(VelocityField &velocity) const override {
@@ -131,9 +162,19 @@ class B200Kernel final : public VelocityKernel {
             raise(st, pv_last_error(ctx_));
     }
     pv_context *ctx_ = nullptr;
+    bool dipolesOnDevice_ = false;
 };
 
 } // namespace
+
+bool b200ProcessDipoles(VelocityKernel &kernel, const SimParams &params, DipoleEventState &state,
+                        std::size_t &events) {
+    auto *b200 = dynamic_cast<B200Kernel *>(&kernel);
+    if (!b200)
+        return false;
+    events = b200->processDipolesOnDevice(params, state);
+    return true;
+}
 
 void backendInitialize(int &, char **&) {}
 void backendFinalize() {}

@@ -106,3 +106,15 @@ def test_cli_dipole_removal_and_restart(tmp_path):
                 f"restartFile {os.path.join(right, 'checkpoints', ckpt)}\nrunDirectory {restart}\n")
     r = subprocess.run([B200, params], capture_output=True, text=True, timeout=120)
     assert r.returncode == 0, r.stdout + r.stderr
+
+
+PLUGIN_DIPOLES = os.path.join(ROOT, "oracle", "_ref", "plugin_dipoles")
+
+
+@pytest.mark.skipif(not os.path.exists(PLUGIN_DIPOLES), reason="make -C oracle plugin-test")
+def test_backend_dipole_hook_matches_reference_manager():
+    """b200ProcessDipoles through the backend translation unit against the reference's host
+    DipoleManager: removal, independent and paired reinjection, periodic box and disk, three
+    consecutive calls each."""
+    r = subprocess.run([PLUGIN_DIPOLES], capture_output=True, text=True, timeout=120)
+    assert r.returncode == 0 and r.stdout.strip().endswith("OK"), r.stdout + r.stderr
