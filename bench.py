@@ -497,9 +497,13 @@ def run_serving(budget: int = 10) -> dict:
     the one-request-at-a-time FIFO loop beside it on the middle stream."""
     from pointvortex_b200.serve import Server, one_at_a_time, poisson_stream
     out = {"step_budget": budget, "streams": []}
-    for rate, count in ((10.0, 30), (100.0, 200), (1000.0, 600)):
+    for rate, count, policy in ((10.0, 30, "split"), (100.0, 200, "split"), (100.0, 200, "fifo"),
+                                (1000.0, 600, "split")):
         reqs = poisson_stream(count, rate, seed=int(rate), max_steps=budget)
-        server = Server(capacity_vortices=4_000_000, max_slots=1024, attempts_per_tick=2)
+        # split: the expensive batch takes one attempt per tick, the cheap one 16 (measured best
+        # of a sweep of 1-2 / 8-32 attempts and 2^22-2^26 split points on the 100 req/s stream)
+        server = Server(capacity_vortices=4_000_000, max_slots=1024,
+                        attempts_per_tick=1 if policy == "split" else 2, policy=policy)
         summary = server.serve(reqs)
         server.close()
         summary["rate_per_s"] = rate

@@ -1,10 +1,15 @@
 """Continuous-batching solve server over the batched ensemble engine.
 
 A request is one solve: (geometry, N, seed, t_end, tolerance). The server keeps every admitted
-state resident in one device arena. New requests are admitted whenever a slot and arena room (the
+state resident in a device arena. New requests are admitted whenever a slot and arena room (the
 HBM budget) are free, including while others are mid-flight, and they join the next batched
 DOPRI5 attempt. Finished solves are retired, their final states downloaded and handed to a
 callback (streamed), and their room freed. Latency is measured from arrival to retirement.
+
+In a lock-step attempt every simulation advances once, so a batch moves at the pace of its most
+expensive member. With policy "split" the server also admits by estimated work: cheap requests
+(one evaluation at most `split_work` plane-pair units) go to their own batch, which takes several
+attempts for each attempt of the batch holding the expensive ones.
 
 `one_at_a_time()` is the comparison loop: the same requests, FIFO, each solved alone with the
 single-simulation context API (one simulation per launch, plain FP64).
@@ -52,6 +57,17 @@ class Completion:
     time: float
     x: Optional[np.ndarray] = None
     y: Optional[np.ndarray] = None
+    pairs: float = 0.0            # pair interactions evaluated for this request
+
+
+# Relative cost of one ordered pair by geometry, from the measured FP64 pair rates of the
+# single-simulation kernels (plane 1.5e12, disk 5.3e11, periodic 9.6e10 pairs/s).
+PAIR_COST = {"infinite": 1.0, "disk": 2.9, "periodic": 15.8}
+
+
+def work(req: "Request") -> float:
+    """Estimated cost of one velocity evaluation of the request, in plane-pair units."""
+    return PAIR_COST[req.geometry] * float(req.n) * float(req.n)
 
 
 def poisson_stream(n_requests: int, rate: float, seed: int, n_min: int = 32, n_max: int = 32768,
@@ -74,47 +90,90 @@ def poisson_stream(n_requests: int, rate: float, seed: int, n_min: int = 32, n_m
     return out
 
 
-class Server:
-    def __init__(self, capacity_vortices: int, max_slots: int, attempts_per_tick: int = 4,
-                 device: int = 0, keep_states: bool = False):
+class _Lane:
+    """One batch with its own FIFO queue of arrived requests."""
+
+    def __init__(self, capacity_vortices: int, max_slots: int, device: int, attempts: int):
         self.batch = Batch(capacity_vortices, max_slots, device)
-        self.attempts_per_tick = attempts_per_tick
-        self.keep_states = keep_states
-        self.queue: list = []          # (arrival, rid, request) min-heap, FIFO by arrival
+        self.attempts = attempts
+        self.ready: list = []            # (arrival, rid, request), arrival order
         self.running: dict[int, tuple] = {}
+
+
+class Server:
+    """Continuous batching. policy "fifo": one batch, requests admitted in arrival order.
+    policy "split" (admission by estimated work): requests whose evaluation costs at most
+    `split_work` plane-pair units go to a small-request batch that takes `small_attempts`
+    attempts for each attempt of the large-request batch, so that short requests are not held to
+    the pace of the largest ones in a lock-step attempt. Within a batch the order is FIFO."""
+
+    def __init__(self, capacity_vortices: int, max_slots: int, attempts_per_tick: int = 4,
+                 device: int = 0, keep_states: bool = False, policy: str = "fifo",
+                 split_work: float = 2.0 ** 26, small_attempts: int = 16,
+                 small_fraction: float = 0.25):
+        if policy not in ("fifo", "split"):
+            raise ValueError("policy must be fifo or split")
+        self.policy = policy
+        self.keep_states = keep_states
+        self.split_work = split_work
+        self.arrivals: list = []         # (arrival, rid, request) min-heap
         self.completions: list[Completion] = []
+        if policy == "fifo":
+            self.lanes = [_Lane(capacity_vortices, max_slots, device, attempts_per_tick)]
+        else:
+            small_cap = max(int(capacity_vortices * small_fraction), 4096)
+            small_slots = max(max_slots // 2, 1)
+            self.lanes = [_Lane(small_cap, small_slots, device, small_attempts),
+                          _Lane(capacity_vortices - small_cap, max(max_slots - small_slots, 1),
+                                device, attempts_per_tick)]
+
+    @property
+    def batch(self) -> Batch:
+        return self.lanes[0].batch
 
     def submit(self, req: Request) -> None:
-        heapq.heappush(self.queue, (req.arrival, req.rid, req))
+        heapq.heappush(self.arrivals, (req.arrival, req.rid, req))
+
+    def _lane_of(self, req: Request) -> _Lane:
+        if self.policy == "split" and work(req) > self.split_work:
+            return self.lanes[1]
+        return self.lanes[0]
 
     def _admit(self, now: float) -> int:
+        while self.arrivals and self.arrivals[0][0] <= now:
+            item = heapq.heappop(self.arrivals)
+            self._lane_of(item[2]).ready.append(item)
         admitted = 0
-        while self.queue and self.queue[0][0] <= now:
-            _, _, req = self.queue[0]
-            x, y, g = req.state()
-            try:
-                sid = self.batch.add(geometry_params(req.geometry), x, y, g, req.t_end, dt=req.dt,
-                                     atol=req.atol, rtol=req.rtol, max_steps=req.max_steps)
-            except CapacityError:
-                break                   # wait for room: head-of-line, arrival order kept
-            heapq.heappop(self.queue)
-            self.running[sid] = (req, now)
-            admitted += 1
+        for lane in self.lanes:
+            while lane.ready:
+                _, _, req = lane.ready[0]
+                x, y, g = req.state()
+                try:
+                    sid = lane.batch.add(geometry_params(req.geometry), x, y, g, req.t_end,
+                                         dt=req.dt, atol=req.atol, rtol=req.rtol,
+                                         max_steps=req.max_steps)
+                except CapacityError:
+                    break               # wait for room: head-of-line, arrival order kept
+                lane.ready.pop(0)
+                lane.running[sid] = (req, now)
+                admitted += 1
         return admitted
 
-    def _retire(self, now: float, on_complete) -> int:
+    def _retire(self, lane: _Lane, now: float, on_complete) -> int:
         done = 0
-        for sid in list(self.running):
-            info = self.batch.info(sid)
+        for sid in list(lane.running):
+            info = lane.batch.info(sid)
             if info.state == "running":
                 continue
-            req, _ = self.running.pop(sid)
+            req, _ = lane.running.pop(sid)
             x = y = None
             if self.keep_states or on_complete is not None:
-                x, y = self.batch.result(sid)
-            self.batch.release(sid)
+                x, y = lane.batch.result(sid)
+            lane.batch.release(sid)
+            evals = 6 * (info.acceptedSteps + info.rejectedSteps) + 1
             c = Completion(req.rid, info.state, now - req.arrival, info.acceptedSteps, info.time,
-                           x if self.keep_states else None, y if self.keep_states else None)
+                           x if self.keep_states else None, y if self.keep_states else None,
+                           float(evals) * req.n * (req.n - 1))
             self.completions.append(c)
             if on_complete is not None:
                 on_complete(c, x, y)
@@ -129,21 +188,26 @@ class Server:
         start = clock()
         total = len(requests)
         while len(self.completions) < total:
-            now = clock() - start
-            self._admit(now)
-            if not self.running:
-                if self.queue:
-                    wait = self.queue[0][0] - (clock() - start)
+            self._admit(clock() - start)
+            busy = [lane for lane in self.lanes if lane.running]
+            if not busy:
+                if self.arrivals:
+                    wait = self.arrivals[0][0] - (clock() - start)
                     if wait > 0:
                         time.sleep(min(wait, 0.01))
                 continue
-            self.batch.advance(self.attempts_per_tick)
-            self._retire(clock() - start, on_complete)
+            for lane in busy:
+                lane.batch.advance(lane.attempts)
+                self._retire(lane, clock() - start, on_complete)
+                self._admit(clock() - start)
         elapsed = clock() - start
-        return summarize(self.completions, elapsed)
+        out = summarize(self.completions, elapsed)
+        out["policy"] = self.policy
+        return out
 
     def close(self):
-        self.batch.close()
+        for lane in self.lanes:
+            lane.batch.close()
 
 
 def summarize(completions: list[Completion], elapsed: float) -> dict:
@@ -151,8 +215,10 @@ def summarize(completions: list[Completion], elapsed: float) -> dict:
     states = {}
     for c in completions:
         states[c.state] = states.get(c.state, 0) + 1
+    pairs = sum(c.pairs for c in completions)
     return {"requests": len(completions), "elapsed_s": elapsed,
             "solves_per_s": len(completions) / elapsed if elapsed > 0 else 0.0,
+            "pair_interactions_per_s": pairs / elapsed if elapsed > 0 else 0.0,
             "p50_latency_s": float(np.percentile(lat, 50)),
             "p99_latency_s": float(np.percentile(lat, 99)), "states": states}
 
@@ -174,6 +240,7 @@ def one_at_a_time(requests: list[Request], device: int = 0, clock=time.perf_coun
         x, y, g = req.state()
         k.uploadDeviceState(VortexSystem(x, y, g))
         t, dt, steps, state = 0.0, min(max(req.dt, 1e-12), 0.1), 0, "done"
+        evals_before = k.evaluationCount
         try:
             while t < req.t_end:
                 if req.max_steps and steps >= req.max_steps:
@@ -187,5 +254,7 @@ def one_at_a_time(requests: list[Request], device: int = 0, clock=time.perf_coun
                     t = req.t_end
         except (RuntimeError, ValueError):
             state = "failed"
-        out.append(Completion(req.rid, state, clock() - start - req.arrival, steps, t))
+        evals = k.evaluationCount - evals_before
+        out.append(Completion(req.rid, state, clock() - start - req.arrival, steps, t,
+                              pairs=float(evals) * req.n * (req.n - 1)))
     return summarize(out, clock() - start)

@@ -50,3 +50,23 @@ def test_one_at_a_time_baseline_agrees():
     for req in reqs:
         info, _ = alone(req)
         assert info.state in ("done", "budget", "failed")
+
+
+def test_split_policy_results_equal_alone_results():
+    """Admission by estimated work (two batches, cheap requests advanced faster) changes when a
+    request runs, never what it computes."""
+    reqs = poisson_stream(16, rate=400.0, seed=11, n_min=32, n_max=3000, t_end_range=(0.01, 0.02),
+                          rtols=(1e-6, 1e-9), max_steps=30)
+    server = Server(capacity_vortices=20000, max_slots=8, attempts_per_tick=1, keep_states=True,
+                    policy="split", split_work=2.0 ** 18, small_attempts=4)
+    summary = server.serve(reqs)
+    server.close()
+    assert summary["requests"] == len(reqs) and summary["policy"] == "split"
+    assert len(server.lanes) == 2
+    by_id = {c.rid: c for c in server.completions}
+    for req in reqs:
+        c = by_id[req.rid]
+        info, (x, y) = alone(req)
+        assert c.state == info.state and c.accepted_steps == info.acceptedSteps, req
+        assert np.array_equal(c.x, x) and np.array_equal(c.y, y), req
+        assert c.pairs > 0
