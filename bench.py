@@ -49,6 +49,9 @@ METRIC = "pair-interactions/s"
 # exact m = +-1, +-2 pairs (18), the m = 3..5 expansion (6) and the m = +-6 terms (5); per axis
 # the combination, reciprocal and update (16).
 FLOPS_PER_PAIR_PERIODIC = 240
+# The symmetric form evaluates each unordered pair once and applies it to both vortices: the same
+# 240 plus two more FMA updates (the source's reaction) per unordered pair.
+FLOPS_PER_UNORDERED_PAIR_SYMMETRIC = 244
 # DRAM bytes (read + write) of one launch of the periodic pair kernel at this workload, from one
 # ncu capture (dram__bytes_read.sum 139.0 KB, dram__bytes_write.sum 0 B, with ncu's cache flush
 # before the launch): the sources are read once, everything else stays in L2.
@@ -209,7 +212,14 @@ def run_ours(args):
     v_launch, v_timed, v_ms = stats["velocity"]
     per_launch_ms = v_ms / max(v_timed, 1)
     # every timed velocity launch is one evaluation of the step loop: its pairs over its time
-    achieved = FLOPS_PER_PAIR_PERIODIC * pairs_local / (v_ms * 1e-3) / 1e12
+    plan = k.statePlan()
+    if plan["symmetric"]:
+        flops_per_ordered_pair = FLOPS_PER_UNORDERED_PAIR_SYMMETRIC / 2.0
+        kernel_name = "periodic_symmetric_kernel"
+    else:
+        flops_per_ordered_pair = FLOPS_PER_PAIR_PERIODIC
+        kernel_name = "velocity_kernel<PeriodicPair>"
+    achieved = flops_per_ordered_pair * pairs_local / (v_ms * 1e-3) / 1e12
     # measured FP64 FMA peak of this GPU (36.8 TFLOP/s at 1965 MHz on this pool's B200s when
     # the probe is skipped, e.g. under a profiler)
     peak = 36.83 if args.no_peak_probe else pv.probePeak("fp64", local) / 1e12
@@ -243,8 +253,10 @@ def run_ours(args):
                          "traffic": TRAFFIC_BYTES_PER_LAUNCH,
                          "traffic_note": "DRAM bytes per launch (ncu); the algorithmic minimum "
                                          "is the 24N-byte source read, 98304 B",
-                         "kernel": "velocity_kernel<PeriodicPair>",
-                         "flops_per_pair": FLOPS_PER_PAIR_PERIODIC,
+                         "kernel": kernel_name,
+                         "flops_per_pair": flops_per_ordered_pair,
+                         "flops_note": "algorithmic flops per ordered pair of the launched "
+                                       "kernel (the symmetric form: 244 per unordered pair)",
                          "ms_per_launch": per_launch_ms, "launches": v_timed,
                          "peak_source": "measured FP64 FMA probe (pv_probe_peak) on this GPU"},
             "kernel_ms": {kk: vv[2] for kk, vv in stats.items()},
@@ -363,9 +375,11 @@ def run_reference(args):
                     "d2h_bytes_per_step": 0}}
 
 
-def run_kernel_case(spec: str, evals: int, precision: str = "fp64") -> dict:
+def run_kernel_case(spec: str, evals: int, precision: str = "fp64", ordered: bool = False) -> dict:
     """Velocity evaluations only (no stepping), for kernel timing and ncu captures:
-    spec = "geometry:N" with geometry infinite | periodic | disk; precision fp64 | fp32c."""
+    spec = "geometry:N" with geometry infinite | periodic | disk; precision fp64 | fp32c.
+    ordered: evaluate host arrays (always the ordered-pair kernel) instead of the device state
+    (the symmetric kernel where the plan uses it)."""
     import torch
     import pointvortex_b200 as pv
     from pointvortex_b200 import ics
@@ -385,19 +399,22 @@ def run_kernel_case(spec: str, evals: int, precision: str = "fp64") -> dict:
         k = pv.DiskKernel(1.0, precision=prec)
         flops = 33
     k.uploadDeviceState(pv.VortexSystem(x, y, g))
+    symmetric = k.statePlan()["symmetric"] and not ordered
+    run = (lambda: k.evaluate(x, y, g)) if ordered else k.evaluateDeviceState
     for _ in range(2):
-        k.evaluateDeviceState()
+        run()
     k.setProfiling(True)
     k.resetKernelStats()
     for _ in range(evals):
-        k.evaluateDeviceState()
+        run()
     st = k.kernelStats()["velocity"]
     ms = st[2] / max(st[1], 1)
     pairs = n * (n - 1)
+    work = (FLOPS_PER_UNORDERED_PAIR_SYMMETRIC * pairs / 2) if symmetric else flops * pairs
     torch.cuda.synchronize()
-    return {"case": spec, "precision": precision, "evaluations": evals, "ms_per_evaluation": ms,
-            "pairs_per_s": pairs / (ms * 1e-3), "formula_flops_per_pair": flops,
-            "tflops": flops * pairs / (ms * 1e-3) / 1e12}
+    return {"case": spec, "precision": precision, "kernel": "symmetric" if symmetric else "ordered",
+            "evaluations": evals, "ms_per_evaluation": ms, "pairs_per_s": pairs / (ms * 1e-3),
+            "formula_flops_per_pair": flops, "tflops": work / (ms * 1e-3) / 1e12}
 
 
 def run_reference_cuda(evals: int = 3, steps: int = 3) -> dict:
@@ -615,6 +632,8 @@ def main(argv=None):
     ap.add_argument("--evals", type=int, default=10)
     ap.add_argument("--precision", choices=["fp64", "fp32c"], default="fp64",
                     help="precision form of --kernel-case")
+    ap.add_argument("--ordered", action="store_true",
+                    help="--kernel-case on host arrays: the ordered-pair kernel")
     ap.add_argument("--reference-cuda", action="store_true",
                     help="time the reference's own CUDA backend on the workload (own process)")
     ap.add_argument("--summarize-launches", default=None, metavar="CSV",
@@ -630,7 +649,8 @@ def main(argv=None):
         print(json.dumps(run_reference_cuda()), flush=True)
         return 0
     if args.kernel_case:
-        print(json.dumps(run_kernel_case(args.kernel_case, args.evals, args.precision)), flush=True)
+        print(json.dumps(run_kernel_case(args.kernel_case, args.evals, args.precision,
+                                         args.ordered)), flush=True)
         return 0
     if args.impl == "reference":
         out = run_reference(args)

@@ -213,6 +213,17 @@ pv_status pv_format_checkpoint_vortices(pv_context *ctx, char *out, size_t capac
  * driver keeps the population on the host and processes dipoles there. */
 pv_status pv_download_circulation(pv_context *ctx, double *circulation, size_t n);
 
+/* How the context evaluates its device state (no reference counterpart; for benchmarks and
+ * profiles). symmetric = 1: the periodic box is evaluated once per unordered pair (each pair's
+ * series serves both vortices); rows = partial-sum rows the stage reduction adds. */
+typedef struct pv_plan_info {
+    int symmetric;
+    int rows;
+    int targets_per_thread; /* ordered kernel */
+    int chunk;              /* ordered kernel: sources per work item */
+} pv_plan_info;
+pv_status pv_state_plan(const pv_context *ctx, pv_plan_info *info);
+
 /* Population of the device state. */
 pv_status pv_state_size(const pv_context *ctx, size_t *n);
 /* Velocity evaluations made so far by the stepping hooks (the reference's CountingKernel,

@@ -65,6 +65,11 @@ class PvDipoleConfig(ctypes.Structure):
 
 REINJECTION = {"none": 0, "independent": 1, "paired": 2}
 
+class PvPlanInfo(ctypes.Structure):
+    _fields_ = [("symmetric", ctypes.c_int), ("rows", ctypes.c_int),
+                ("targets_per_thread", ctypes.c_int), ("chunk", ctypes.c_int)]
+
+
 TRAJECTORY_ROW_MAX = 192   # PV_TRAJECTORY_ROW_MAX
 CHECKPOINT_ROW_MAX = 80    # PV_CHECKPOINT_ROW_MAX
 
@@ -145,6 +150,7 @@ SIGNATURES = {
     "pv_format_trajectory_host": (_ST, [_CTX, ctypes.c_double, ctypes.c_uint64, _D, _D, _D, _D, _D,
                                         _SZ, ctypes.c_char_p, _SZ, ctypes.POINTER(_SZ)]),
     "pv_format_checkpoint_vortices": (_ST, [_CTX, ctypes.c_char_p, _SZ, ctypes.POINTER(_SZ)]),
+    "pv_state_plan": (_ST, [_CTX, ctypes.POINTER(PvPlanInfo)]),
     "pv_state_size": (_ST, [_CTX, ctypes.POINTER(_SZ)]),
     "pv_evaluation_count": (_ST, [_CTX, ctypes.POINTER(ctypes.c_uint64)]),
     "pv_rk4_advance": (_ST, [_CTX, ctypes.c_double, ctypes.c_uint64]),

@@ -91,7 +91,10 @@ struct pv_context {
     DeviceArray x, y, gamma, gs;     // state and scaled circulations
     DeviceArray p0x, p0y, p1x, p1y;  // stage positions (ping-pong)
     DeviceArray kx[7], ky[7];        // stage velocities
-    DeviceArray pu, pv;              // chunk partials
+    DeviceArray pu, pv;              // chunk partials (or symmetric-kernel rows)
+    SymmetricPlan sym{};             // periodic FP64: one evaluation per unordered pair
+    DeviceArray sym_items, sym_counter;
+    int sym_items_blocks = 0;        // the block count the item table was built for
     DeviceArray inv_scratch, inv_out;
     DeviceArray cand;                // dipole candidates (3 doubles-worth each)
     DeviceControl *ctl = nullptr;    // device control block
@@ -126,7 +129,8 @@ struct pv_context {
     ~pv_context() {
         for (DeviceArray *a : {&x, &y, &gamma, &gs, &p0x, &p0y, &p1x, &p1y, &pu, &pv, &inv_scratch,
                                &inv_out, &cand, &ex, &ey, &eg, &egs, &eu, &ev, &epu, &epv,
-                               &removed_index, &fmt_stage, &fmt_len, &fmt_block, &fmt_out})
+                               &removed_index, &fmt_stage, &fmt_len, &fmt_block, &fmt_out,
+                               &sym_items, &sym_counter})
             a->release();
         for (int s = 0; s < 7; ++s) {
             kx[s].release();
@@ -376,6 +380,17 @@ std::vector<double> scaled(const GeometryConsts &g, const double *gamma, size_t 
 
 // Velocity of the state positions (px, py) into k_s via partials + stage kernel.
 pv_status launch_eval(pv_context *c, const double *px, const double *py) {
+    if (c->sym.enabled()) {
+        PV_CUDA(c, counted(c, PV_KERNEL_VELOCITY, 1, [&] {
+                    return launch_periodic_symmetric(
+                        px, py, c->gs.p, c->n, c->sym,
+                        reinterpret_cast<const unsigned *>(c->sym_items.p),
+                        reinterpret_cast<unsigned *>(c->sym_counter.p), c->pu.p, c->pv.p,
+                        padded(c->n), c->gc, c->stream);
+                }));
+        ++c->evaluations;
+        return PV_OK;
+    }
     EvalArgs a{};
     a.tx = px;
     a.ty = py;
@@ -405,7 +420,7 @@ StageArgs stage_base(pv_context *c) {
     StageArgs s{};
     s.n = c->n;
     s.reduce = 1;
-    s.num_chunks = c->plan.num_chunks;
+    s.num_chunks = c->sym.enabled() ? c->sym.blocks : c->plan.num_chunks;
     s.stride = padded(c->n);
     s.pu = c->pu.p;
     s.pv = c->pv.p;
@@ -431,9 +446,24 @@ pv_status ensure_state_capacity(pv_context *c, size_t n) {
         PV_CUDA(c, c->ky[s].ensure(np));
     }
     c->plan = plan_evaluation(c->gc.geometry, n, n, c->sm_count, 0, c->params.precision);
-    const size_t partial = static_cast<size_t>(c->plan.num_chunks) * np;
+    c->sym = SymmetricPlan{};
+    if (c->gc.geometry == GEO_PERIODIC && c->params.precision == PV_PRECISION_FP64)
+        c->sym = plan_symmetric(n, c->sm_count);
+    const size_t rows = c->sym.enabled() ? static_cast<size_t>(c->sym.blocks)
+                                         : static_cast<size_t>(c->plan.num_chunks);
+    const size_t partial = rows * np;
     PV_CUDA(c, c->pu.ensure(partial));
     PV_CUDA(c, c->pv.ensure(partial));
+    if (c->sym.enabled() && c->sym_items_blocks != c->sym.blocks) {
+        std::vector<unsigned> items(c->sym.items);
+        symmetric_items(c->sym, items.data());
+        PV_CUDA(c, c->sym_items.ensure((items.size() + 1) / 2));
+        PV_CUDA(c, c->sym_counter.ensure(1));
+        PV_CUDA(c, cudaMemcpyAsync(c->sym_items.p, items.data(), items.size() * sizeof(unsigned),
+                                   cudaMemcpyHostToDevice, c->stream));
+        PV_CUDA(c, cudaStreamSynchronize(c->stream));
+        c->sym_items_blocks = c->sym.blocks;
+    }
     return PV_OK;
 }
 
@@ -1412,6 +1442,16 @@ pv_status pv_download_circulation(pv_context *ctx, double *circulation, size_t n
     if (n != ctx->n)
         return fail(ctx, PV_ERROR_RUNTIME, "host and device vortex populations differ");
     std::copy(ctx->gamma_host.begin(), ctx->gamma_host.end(), circulation);
+    return PV_OK;
+}
+
+pv_status pv_state_plan(const pv_context *ctx, pv_plan_info *info) {
+    if (!ctx || !info)
+        return PV_ERROR_INVALID_ARGUMENT;
+    info->symmetric = ctx->sym.enabled() ? 1 : 0;
+    info->rows = ctx->sym.enabled() ? ctx->sym.blocks : ctx->plan.num_chunks;
+    info->targets_per_thread = ctx->plan.per_thread;
+    info->chunk = ctx->plan.chunk;
     return PV_OK;
 }
 

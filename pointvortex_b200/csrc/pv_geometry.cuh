@@ -147,10 +147,13 @@ struct PeriodicPair {
         }
     }
 
-    template <bool CHECK>
-    __device__ __forceinline__ static void pair(const GeometryConsts &g, double tx, double ty,
-                                                double sx, double sy, double sg, bool self,
-                                                double &u, double &v) {
+    // The pair's terms without its circulation: the target's velocity changes by
+    // u -= g_s * au / bu, v += g_s * av / bv. Exchanging target and source negates x^ and y^
+    // exactly (remainder is odd), which negates au and av and leaves bu and bv unchanged, bit for
+    // bit: every quantity below is an exactly odd or even function of (x^, y^).
+    __device__ __forceinline__ static void terms(const GeometryConsts &g, double tx, double ty,
+                                                 double sx, double sy, double &au, double &bu,
+                                                 double &av, double &bv) {
         const double xh = g.wave * exact_remainder(tx - sx, g.lx, g.inv_lx, g.half_lx);
         const double yh = g.wave * exact_remainder(ty - sy, g.ly, g.inv_ly, g.half_ly);
         double shx, chx, snx, csx, shy, chy, sny, csy;
@@ -164,26 +167,28 @@ struct PeriodicPair {
         const double sin_y = 2.0 * sny * csy;
         const double sinh_x = 2.0 * shx * chx;          // sinh x^
         const double sinh_y = 2.0 * shy * chy;
-        double d0u = 2.0 * fma(shx, shx, sny * sny);
-        double d0v = 2.0 * fma(shy, shy, snx * snx);
-        if (CHECK && self) { // the self pair contributes exactly 0 in the reference (sin 0 = 0)
-            d0u = 1.0;
-            d0v = 1.0;
-        }
+        const double d0u = 2.0 * fma(shx, shx, sny * sny);
+        const double d0v = 2.0 * fma(shy, shy, snx * snx);
         double nu, du, ru, nv, dv, rv;
         image_sum(g, xh, cosh_x, sinh_x, cos_y, nu, du, ru);
         image_sum(g, yh, cosh_y, sinh_y, cos_x, nv, dv, rv);
         // 1/d0 + num/den + rest = (den + d0 (num + den rest)) / (d0 den)
-        const double numer_u = fma(d0u, fma(du, ru, nu), du);
-        const double numer_v = fma(d0v, fma(dv, rv, nv), dv);
-        double cu = sg * sin_y * numer_u;
-        double cv = sg * sin_x * numer_v;
-        if (CHECK && self) {
-            cu = 0.0;
-            cv = 0.0;
-        }
-        u = fma(-cu, rcp_refined(d0u * du), u);
-        v = fma(cv, rcp_refined(d0v * dv), v);
+        au = sin_y * fma(d0u, fma(du, ru, nu), du);
+        av = sin_x * fma(d0v, fma(dv, rv, nv), dv);
+        bu = d0u * du;
+        bv = d0v * dv;
+    }
+
+    template <bool CHECK>
+    __device__ __forceinline__ static void pair(const GeometryConsts &g, double tx, double ty,
+                                                double sx, double sy, double sg, bool self,
+                                                double &u, double &v) {
+        if (CHECK && self) // the self pair contributes exactly 0 in the reference (sin 0 = 0)
+            return;
+        double au, bu, av, bv;
+        terms(g, tx, ty, sx, sy, au, bu, av, bv);
+        u = fma(-(sg * au), rcp_refined(bu), u);
+        v = fma(sg * av, rcp_refined(bv), v);
     }
 };
 

@@ -1,0 +1,198 @@
+// pv_symmetric.cu — the periodic-box velocity of a whole population evaluated once per unordered
+// pair.
+//
+// The reference evaluates every ordered pair (src/compute.cpp:203-256). The Weiss–McWilliams pair
+// term is antisymmetric: exchanging target and source negates x^ and y^ exactly (IEEE remainder
+// is odd), and every quantity of PeriodicPair::terms is an exactly odd or even function of them,
+// so the source's term is the target's with the other circulation and the opposite sign, bit for
+// bit. One evaluation of the transcendental series therefore serves both vortices, and the work
+// per velocity evaluation halves. Only the order of summation differs from the ordered-pair
+// kernel.
+//
+// Work decomposition (warp-level, persistent):
+//   * vortices form blocks of 32a (a = 1..16 sub-blocks of 32); an item is a block pair (I, J),
+//     I <= J, taken by one warp from an atomic queue;
+//   * for a sub-block pair each lane holds one target; the 32 sources and their accumulated
+//     reactions rotate through the lanes by shuffles, so in 32 steps every (target, source) pair
+//     is met once and every source comes back to its home lane;
+//   * sub-blocks on the diagonal of a diagonal item are evaluated one-sided (31 rotations, the
+//     self pair skipped: it contributes exactly 0 in the reference, sin 0 = 0);
+//   * partial sums go to rows of a [blocks][N] array: vortices of block I receive row J from item
+//     (I, J), vortices of block J receive row I, and each (row, vortex) is written exactly once,
+//     so the stage kernel's fixed-order sum over rows keeps results deterministic.
+#include "pv_internal.h"
+
+#include <algorithm>
+
+namespace pvb {
+
+namespace {
+
+constexpr int kThreads = 128;  // 4 independent warps per CTA
+
+__device__ __forceinline__ double rotate(double v, int from) {
+    return __shfl_sync(0xffffffffu, v, from);
+}
+
+__device__ __forceinline__ void kernel_values(const GeometryConsts &g, double tx, double ty,
+                                              double sx, double sy, double &ku, double &kv) {
+    double au, bu, av, bv;
+    PeriodicPair::terms(g, tx, ty, sx, sy, au, bu, av, bv);
+    ku = au * rcp_refined(bu);
+    kv = av * rcp_refined(bv);
+}
+
+__global__ void __launch_bounds__(kThreads)
+    periodic_symmetric_kernel(const double *__restrict__ x, const double *__restrict__ y,
+                              const double *__restrict__ gs, size_t n, int a,
+                              const unsigned *__restrict__ items, unsigned n_items,
+                              unsigned *counter, double *__restrict__ pu,
+                              double *__restrict__ pv, size_t stride, GeometryConsts g) {
+    extern __shared__ double2 reaction_smem[];
+    const int lane = threadIdx.x & 31;
+    double2 *reaction = reaction_smem + (threadIdx.x >> 5) * a * 32;  // this warp's sources
+    const int next = (lane + 1) & 31;
+    const size_t block_len = static_cast<size_t>(32) * a;
+    for (;;) {
+        unsigned item = 0;
+        if (lane == 0)
+            item = atomicAdd(counter, 1u);
+        item = __shfl_sync(0xffffffffu, item, 0);
+        if (item >= n_items)
+            break;
+        const unsigned packed = items[item];
+        const unsigned I = packed >> 16, J = packed & 0xffffu;
+        const bool diagonal = I == J;
+        for (int jb = 0; jb < a; ++jb)
+            reaction[jb * 32 + lane] = make_double2(0.0, 0.0);
+        __syncwarp();
+        for (int ib = 0; ib < a; ++ib) {
+            const size_t ti = I * block_len + static_cast<size_t>(ib) * 32 + lane;
+            const bool t_ok = ti < n;
+            const double tx = t_ok ? x[ti] : 0.0, ty = t_ok ? y[ti] : 0.0;
+            const double tg = t_ok ? gs[ti] : 0.0;
+            double u = 0.0, v = 0.0;
+            for (int jb = diagonal ? ib : 0; jb < a; ++jb) {
+                const size_t sj = J * block_len + static_cast<size_t>(jb) * 32 + lane;
+                int s_ok = sj < n ? 1 : 0;
+                double sx = s_ok ? x[sj] : 0.0, sy = s_ok ? y[sj] : 0.0;
+                double sg = s_ok ? gs[sj] : 0.0;
+                if (diagonal && jb == ib) {
+                    // ordered pairs (lane, lane + k), k = 1..31, target side only
+                    for (int k = 1; k < 32; ++k) {
+                        sx = rotate(sx, next);
+                        sy = rotate(sy, next);
+                        sg = rotate(sg, next);
+                        s_ok = __shfl_sync(0xffffffffu, s_ok, next);
+                        if (t_ok && s_ok) {
+                            double ku, kv;
+                            kernel_values(g, tx, ty, sx, sy, ku, kv);
+                            u = fma(-sg, ku, u);
+                            v = fma(sg, kv, v);
+                        }
+                    }
+                    continue;
+                }
+                double ru = reaction[jb * 32 + lane].x, rv = reaction[jb * 32 + lane].y;
+                for (int k = 0; k < 32; ++k) {
+                    if (t_ok && s_ok) {
+                        double ku, kv;
+                        kernel_values(g, tx, ty, sx, sy, ku, kv);
+                        u = fma(-sg, ku, u);  // target: -g_s K
+                        v = fma(sg, kv, v);
+                        ru = fma(tg, ku, ru);  // source: the exchanged pair, +g_t K
+                        rv = fma(-tg, kv, rv);
+                    }
+                    sx = rotate(sx, next);
+                    sy = rotate(sy, next);
+                    sg = rotate(sg, next);
+                    ru = rotate(ru, next);
+                    rv = rotate(rv, next);
+                    s_ok = __shfl_sync(0xffffffffu, s_ok, next);
+                }
+                reaction[jb * 32 + lane] = make_double2(ru, rv);  // home again after 32 steps
+            }
+            if (diagonal) {  // reactions from the sub-blocks before this one in the same block
+                const double2 r = reaction[ib * 32 + lane];
+                u += r.x;
+                v += r.y;
+            }
+            if (t_ok) {
+                pu[J * stride + ti] = u;
+                pv[J * stride + ti] = v;
+            }
+        }
+        if (!diagonal) {
+            for (int jb = 0; jb < a; ++jb) {
+                const size_t sj = J * block_len + static_cast<size_t>(jb) * 32 + lane;
+                if (sj < n) {
+                    const double2 r = reaction[jb * 32 + lane];
+                    pu[I * stride + sj] = r.x;
+                    pv[I * stride + sj] = r.y;
+                }
+            }
+        }
+        __syncwarp();
+    }
+}
+
+int resident_ctas(int a) {
+    static int cached[17] = {};
+    if (a < 1 || a > 16)
+        return 1;
+    if (!cached[a]) {
+        int blocks = 0;
+        const size_t smem = static_cast<size_t>(kThreads / 32) * a * 32 * sizeof(double2);
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, periodic_symmetric_kernel,
+                                                          kThreads, smem) != cudaSuccess ||
+            blocks < 1)
+            blocks = 1;
+        cached[a] = blocks;
+    }
+    return cached[a];
+}
+
+}  // namespace
+
+SymmetricPlan plan_symmetric(size_t n, int sm_count) {
+    SymmetricPlan p{};
+    if (n < kSymmetricMinN)
+        return p;
+    // the smallest block that keeps the partial rows within kSymmetricPartialBytes
+    const size_t np = (n + 255) & ~static_cast<size_t>(255);
+    for (int a = 1; a <= 16; a *= 2) {
+        const size_t blocks = (n + 32 * static_cast<size_t>(a) - 1) / (32 * static_cast<size_t>(a));
+        if (blocks > 0xffffu)
+            continue;
+        if (blocks * np * 2 * sizeof(double) <= kSymmetricPartialBytes || a == 16) {
+            p.a = a;
+            p.blocks = static_cast<int>(blocks);
+            p.items = static_cast<unsigned>(blocks * (blocks + 1) / 2);
+            p.grid = std::max(sm_count, 1) * resident_ctas(a);
+            return p;
+        }
+    }
+    return SymmetricPlan{};
+}
+
+void symmetric_items(const SymmetricPlan &p, unsigned *out) {
+    size_t k = 0;
+    for (unsigned i = 0; i < static_cast<unsigned>(p.blocks); ++i)
+        for (unsigned j = i; j < static_cast<unsigned>(p.blocks); ++j)
+            out[k++] = (i << 16) | j;
+}
+
+cudaError_t launch_periodic_symmetric(const double *x, const double *y, const double *gs, size_t n,
+                                      const SymmetricPlan &p, const unsigned *items,
+                                      unsigned *counter, double *pu, double *pv, size_t stride,
+                                      const GeometryConsts &g, cudaStream_t stream) {
+    cudaError_t e = cudaMemsetAsync(counter, 0, sizeof(unsigned), stream);
+    if (e != cudaSuccess)
+        return e;
+    const size_t smem = static_cast<size_t>(kThreads / 32) * p.a * 32 * sizeof(double2);
+    periodic_symmetric_kernel<<<p.grid, kThreads, smem, stream>>>(x, y, gs, n, p.a, items, p.items,
+                                                                  counter, pu, pv, stride, g);
+    return cudaGetLastError();
+}
+
+}  // namespace pvb

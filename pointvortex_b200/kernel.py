@@ -324,6 +324,14 @@ class VelocityKernel:
         out.sort(key=lambda c: (c.distanceSquared, c.first, c.second))
         return out
 
+    def statePlan(self) -> dict:
+        """How the device state is evaluated (pv_state_plan): symmetric (once per unordered
+        pair), partial rows, and the ordered kernel's targets per thread and chunk."""
+        info = _lib.PvPlanInfo()
+        self._check(lib.pv_state_plan(self._ctx, ctypes.byref(info)))
+        return {"symmetric": bool(info.symmetric), "rows": info.rows,
+                "targets_per_thread": info.targets_per_thread, "chunk": info.chunk}
+
     @property
     def evaluationCount(self) -> int:
         c = ctypes.c_uint64(0)
