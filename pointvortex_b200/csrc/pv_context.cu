@@ -319,6 +319,22 @@ pv_status make_consts(const pv_params &p, GeometryConsts &g, std::string &messag
         }
         g.k6 = g.has6 ? 2.0 * std::exp(-12.0 * kPi) : 0.0;
         g.shift6 = 2.0 * kPi * static_cast<double>(6);
+        // |x^| <= pi (1 + 2^-52), so x^ - shift6 < 0 < x^ + shift6 and the reference's tests
+        // |x^ - shift6| <= 40 and |x^ + shift6| <= 40 are monotone in x^: find their end points
+        // with the same rounded subtraction and addition.
+        volatile double s6 = g.shift6;  // keep the rounded operations as written
+        double lo = -40.0 + g.shift6;
+        while (std::fabs(lo - s6) <= 40.0)
+            lo = std::nextafter(lo, -1e300);
+        while (!(std::fabs(lo - s6) <= 40.0))
+            lo = std::nextafter(lo, 1e300);
+        double hi = 40.0 - g.shift6;
+        while (std::fabs(hi + s6) <= 40.0)
+            hi = std::nextafter(hi, 1e300);
+        while (!(std::fabs(hi + s6) <= 40.0))
+            hi = std::nextafter(hi, -1e300);
+        g.lo6 = lo;
+        g.hi6 = hi;
         return PV_OK;
     }
     if (p.geometry == PV_GEOMETRY_DISK) {

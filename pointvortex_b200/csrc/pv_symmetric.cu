@@ -37,7 +37,7 @@ __device__ __forceinline__ double rotate(double v, int from) {
 __device__ __forceinline__ void kernel_values(const GeometryConsts &g, double tx, double ty,
                                               double sx, double sy, double &ku, double &kv) {
     double au, bu, av, bv;
-    PeriodicPair::terms(g, tx, ty, sx, sy, au, bu, av, bv);
+    PeriodicPair::terms<true>(g, tx, ty, sx, sy, au, bu, av, bv);  // half sines: see gs2 below
     ku = au * rcp_refined(bu);
     kv = av * rcp_refined(bv);
 }
@@ -70,13 +70,13 @@ __global__ void __launch_bounds__(kThreads)
             const size_t ti = I * block_len + static_cast<size_t>(ib) * 32 + lane;
             const bool t_ok = ti < n;
             const double tx = t_ok ? x[ti] : 0.0, ty = t_ok ? y[ti] : 0.0;
-            const double tg = t_ok ? gs[ti] : 0.0;
+            const double tg = t_ok ? 2.0 * gs[ti] : 0.0;  // doubled: the terms carry half sines
             double u = 0.0, v = 0.0;
             for (int jb = diagonal ? ib : 0; jb < a; ++jb) {
                 const size_t sj = J * block_len + static_cast<size_t>(jb) * 32 + lane;
                 int s_ok = sj < n ? 1 : 0;
                 double sx = s_ok ? x[sj] : 0.0, sy = s_ok ? y[sj] : 0.0;
-                double sg = s_ok ? gs[sj] : 0.0;
+                double sg = s_ok ? 2.0 * gs[sj] : 0.0;
                 if (diagonal && jb == ib) {
                     // ordered pairs (lane, lane + k), k = 1..31, target side only
                     for (int k = 1; k < 32; ++k) {
