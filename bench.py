@@ -461,7 +461,8 @@ def run_reference_cuda(evals: int = 3, steps: int = 3) -> dict:
             "note": "wall clock per call; the backend synchronises after every evaluation"}
 
 
-def run_ensemble(n_sims: int = 512, budget: int = 10, seed: int = 7) -> dict:
+def run_ensemble(n_sims: int = 512, budget: int = 10, seed: int = 7,
+                 precision: str = "fp64") -> dict:
     """Batched ensemble: n_sims independent simulations, N log-uniform in [64, 8192], geometry
     round-robin (infinite / periodic 2 pi / disk R = 1), balanced +-1 circulations, DOPRI5 with
     rtol 1e-8 to t_end = 0.5, each with an accepted-step budget (the workloads are chaotic, so
@@ -489,7 +490,8 @@ def run_ensemble(n_sims: int = 512, budget: int = 10, seed: int = 7) -> dict:
     b = Batch(total + 256 * (n_sims + 1), n_sims, max_steps=budget)
     torch.cuda.synchronize()
     t0 = time.perf_counter()
-    ids = [b.add(geometry_params(geo), *st, 0.5, dt=1e-3, atol=1e-10, rtol=1e-8)
+    ids = [b.add(geometry_params(geo, precision=precision), *st, 0.5, dt=1e-3, atol=1e-10,
+                 rtol=1e-8)
            for (geo, n, sd), st in zip(specs, states)]
     attempts = b.run()
     finished = {}
@@ -504,7 +506,8 @@ def run_ensemble(n_sims: int = 512, budget: int = 10, seed: int = 7) -> dict:
     b.close()
     return {"simulations": n_sims, "vortices": total, "step_budget": budget,
             "attempts": attempts, "seconds": elapsed, "solves_per_s": n_sims / elapsed,
-            "pair_interactions_per_s": pairs / elapsed, "states": finished, "dtype": "f64",
+            "pair_interactions_per_s": pairs / elapsed, "states": finished,
+            "dtype": "f64" if precision == "fp64" else "f32 compensated (f64 state and control)",
             "note": "one arena, lock-step DOPRI5 attempts, CUDA-graph replay per attempt"}
 
 
@@ -661,6 +664,7 @@ def main(argv=None):
     if rank == 0 and world == 1 and not args.no_extras:
         try:
             result["ensemble"] = run_ensemble()
+            result["ensemble_fp32c"] = run_ensemble(precision="fp32c")
         except Exception as exc:
             result["ensemble"] = {"error": str(exc)[:200]}
         try:

@@ -1,8 +1,8 @@
 """Batched ensembles over libpvb200's pv_batch_* API.
 
-Many independent simulations (each: geometry, population, tolerances, end time) share one device
-arena and advance in lock-step DOPRI5 attempts, each with its own step size. A simulation's result
-is the same alone and in any mix.
+Many independent simulations (each: geometry, population, precision form, tolerances, end time)
+share one device arena and advance in lock-step DOPRI5 attempts, each with its own step size. A
+simulation's result is the same alone and in any mix.
 """
 from __future__ import annotations
 
@@ -34,12 +34,18 @@ class SimInfo:
     population: int
 
 
+PRECISIONS = {"fp64": _lib.PRECISION_FP64, "fp32c": _lib.PRECISION_FP32C}
+
+
 def geometry_params(boundary: str, core_radius: float = 0.0, box_length: float = 2.0 * np.pi,
-                    image_layers: int = 8, disk_radius: float = 1.0) -> _lib.PvParams:
+                    image_layers: int = 8, disk_radius: float = 1.0,
+                    precision: str = "fp64") -> _lib.PvParams:
+    """Parameters of one batched simulation; precision "fp64" (plain) or "fp32c" (the
+    FP32-compensated form)."""
     g = {"infinite": _lib.GEOMETRY_INFINITE, "periodic": _lib.GEOMETRY_PERIODIC,
          "disk": _lib.GEOMETRY_DISK}[boundary]
     return _lib.PvParams(g, core_radius, box_length, box_length, image_layers, disk_radius,
-                         _lib.PRECISION_FP64)
+                         PRECISIONS[precision])
 
 
 class Batch:

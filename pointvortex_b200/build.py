@@ -20,7 +20,8 @@ LIB = os.path.join(HERE, "libpvb200.so")
 OBJ_DIR = os.path.join(HERE, "_build")
 SOURCES = ["pv_velocity.cu", "pv_velocity32.cu", "pv_stepping.cu", "pv_invariants.cu", "pv_dipole.cu", "pv_context.cu",
            "pv_noalloc.cu", "pv_batch.cu", "pv_output.cu", "pv_symmetric.cu"]
-HEADERS = ["pv_common.cuh", "pv_geometry.cuh", "pv_format.cuh", "pv_internal.h"]
+HEADERS = ["pv_common.cuh", "pv_geometry.cuh", "pv_format.cuh", "pv_pair32.cuh", "pv_symmetric.cuh",
+           "pv_internal.h"]
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",
     "-O3", "-lineinfo", "-std=c++17",

@@ -9,7 +9,11 @@
 //     (simulation, block of 128 threads x T targets, chunk of sources) items with an atomic counter. The
 //     items are sorted by cost (periodic pairs cost ~15x plane pairs), so the longest go first.
 //     Each CTA copies the item's geometry constants to shared memory and runs the same TMA-staged
-//     tile loop and pair functions as the single-simulation kernel;
+//     tile loop and pair functions as the single-simulation kernel. FP64 periodic simulations
+//     from N = 2048 instead take (simulation, block I, block J) items of 128 x 128 evaluated once
+//     per unordered pair (the warp tiles of pv_symmetric.cuh, reactions summed across the CTA's
+//     warps in fixed order). Simulations in the FP32-compensated form drain a second queue, in a
+//     second launch, with the pair terms of pv_pair32.cuh;
 //   * stage: one 256-element block per slice of a simulation reduces that simulation's chunk
 //     partials in fixed order, then forms the next stage position or the DOPRI5 error;
 //   * control: one thread per simulation runs the step-size control, the rejection cap, the end
@@ -21,6 +25,8 @@
 // simulation stops with its own status; the others are untouched.
 #include "pvb200.h"
 #include "pv_internal.h"
+#include "pv_pair32.cuh"
+#include "pv_symmetric.cuh"
 
 #include <algorithm>
 #include <cmath>
@@ -36,6 +42,7 @@ namespace {
 constexpr int kBlock = 128;          // threads per velocity CTA
 constexpr int kTileB = 256;          // sources per shared-memory stage
 constexpr size_t kAlign = 256;       // arena granularity (elements)
+constexpr int kCounters = 16;        // work-queue counters: two launches per velocity stage
 
 // Targets per thread by geometry (as the single-simulation plan uses them): the plane's cheap
 // pairs share each staged source among 4 targets, the disk's among 2.
@@ -54,8 +61,10 @@ struct SimDesc {
     unsigned long long part_off;  // first element of its chunk partials
     unsigned n;
     unsigned pad_n;
-    unsigned num_chunks;
+    unsigned num_chunks;          // partial rows (chunks, or 128-blocks of the symmetric form)
     unsigned chunk;
+    int precision;                // PV_PRECISION_*
+    int symmetric;                // FP64 periodic evaluated once per unordered pair
 };
 
 struct SimControl {
@@ -73,12 +82,17 @@ struct SimControl {
     double atol, rtol, dtmin, dtmax;
 };
 
+enum ItemKind : unsigned { ITEM_ORDERED = 0, ITEM_SYMMETRIC = 1 };
+
 struct Item {
     unsigned sim;
-    unsigned tb;
-    unsigned chunk;
-    unsigned pad0;
+    unsigned tb;     // target block (symmetric: block I)
+    unsigned chunk;  // source chunk (symmetric: block J >= I)
+    unsigned kind;   // ItemKind
 };
+
+// Symmetric-form rows: blocks of kBlock vortices (constexpr helper for host and device)
+constexpr unsigned symmetric_rows(unsigned n) { return (n + 127u) / 128u; }
 
 struct SliceEntry { // one 256-element slice of one simulation (stage / accept kernels)
     unsigned sim;
@@ -206,6 +220,175 @@ __device__ __forceinline__ void run_item(const GeometryConsts &g, const double *
         }
 }
 
+// One 128 x 128 block pair of a periodic FP64 simulation, once per unordered pair: warp w holds
+// targets I*128 + 32w + lane and meets the four 32-source sub-tiles of block J in turn. Targets'
+// sums go to row J, the sources' reactions (summed over the four warps in fixed order) to row I.
+// A diagonal item (I == J) is evaluated one-sided. red_u / red_v: 4 x 128 doubles of shared memory.
+__device__ __forceinline__ void run_symmetric_item(const GeometryConsts &g, const double *px,
+                                                   const double *py, const double *sgs, size_t n,
+                                                   unsigned I, unsigned J, double *pu, double *pv,
+                                                   size_t pad_n, double *red_u, double *red_v) {
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const bool diagonal = I == J;
+    const size_t ti = static_cast<size_t>(I) * kBlock + static_cast<size_t>(w) * 32 + lane;
+    const bool t_ok = ti < n;
+    const double tx = t_ok ? px[ti] : 0.0, ty = t_ok ? py[ti] : 0.0;
+    const double tg2 = t_ok ? 2.0 * sgs[ti] : 0.0;  // doubled: the terms carry half sines
+    double u = 0.0, v = 0.0;
+    for (int qq = 0; qq < 4; ++qq) {
+        const int q = (w + qq) & 3;
+        const size_t sj = static_cast<size_t>(J) * kBlock + static_cast<size_t>(q) * 32 + lane;
+        const int s_ok = sj < n ? 1 : 0;
+        const double sx = s_ok ? px[sj] : 0.0, sy = s_ok ? py[sj] : 0.0;
+        const double sg2 = s_ok ? 2.0 * sgs[sj] : 0.0;
+        if (diagonal) {
+            sym::one_sided_tile(g, tx, ty, t_ok, sx, sy, sg2, s_ok, q == w, u, v);
+        } else {
+            double ru = 0.0, rv = 0.0;
+            sym::react_tile(g, tx, ty, tg2, t_ok, sx, sy, sg2, s_ok, u, v, ru, rv);
+            red_u[w * kBlock + q * 32 + lane] = ru;
+            red_v[w * kBlock + q * 32 + lane] = rv;
+        }
+    }
+    if (t_ok) {
+        pu[static_cast<size_t>(J) * pad_n + ti] = u;
+        pv[static_cast<size_t>(J) * pad_n + ti] = v;
+    }
+    if (!diagonal) {
+        __syncthreads();
+        const size_t sj = static_cast<size_t>(J) * kBlock + threadIdx.x;
+        if (sj < n) {
+            double su = red_u[threadIdx.x], sv = red_v[threadIdx.x];
+            for (int k = 1; k < 4; ++k) {
+                su += red_u[k * kBlock + threadIdx.x];
+                sv += red_v[k * kBlock + threadIdx.x];
+            }
+            pu[static_cast<size_t>(I) * pad_n + sj] = su;
+            pv[static_cast<size_t>(I) * pad_n + sj] = sv;
+        }
+        __syncthreads();
+    }
+}
+
+// The FP32-compensated form of run_item: the staged FP64 tile is split once per CTA into
+// double-float FP32 coordinates; FP32 sums are promoted into FP64 every f32::kFlush sources.
+template <int GEO, int T>
+__device__ __forceinline__ void run_item32(const GeometryConsts &g, const double *px,
+                                           const double *py, const double *sgs, size_t src0,
+                                           size_t src1, size_t blk0, size_t blk1, double *pu,
+                                           double *pv, size_t out0, double (*s_x)[kTileB],
+                                           double (*s_y)[kTileB], double (*s_g)[kTileB],
+                                           float4 *s_f, float *s_gf, uint64_t *bars,
+                                           uint32_t &seq, int *timeout_status, bool &timed_out) {
+    const int tid = threadIdx.x;
+    const f32::F32Geometry f = f32::make_f32(g);
+    f32::Target32 tg[T];
+    float u[T], v[T];
+    double ud[T], vd[T];
+    size_t ti[T];
+#pragma unroll
+    for (int k = 0; k < T; ++k) {
+        ti[k] = blk0 + static_cast<size_t>(k) * kBlock + tid;
+        const bool ok = ti[k] < blk1;
+        tg[k].x = ok ? px[ti[k]] : 0.0;
+        tg[k].y = ok ? py[ti[k]] : 0.0;
+        tg[k].xh = static_cast<float>(tg[k].x);
+        tg[k].xl = static_cast<float>(tg[k].x - static_cast<double>(tg[k].xh));
+        tg[k].yh = static_cast<float>(tg[k].y);
+        tg[k].yl = static_cast<float>(tg[k].y - static_cast<double>(tg[k].yh));
+        u[k] = v[k] = 0.0f;
+        ud[k] = vd[k] = 0.0;
+    }
+    const int ntiles = src1 > src0 ? static_cast<int>((src1 - src0 + kTileB - 1) / kTileB) : 0;
+    const uint32_t seq0 = seq;
+    auto issue = [&](int t) {
+        const int st = (seq0 + t) & 1;
+        const size_t j0 = src0 + static_cast<size_t>(t) * kTileB;
+        const int cnt = static_cast<int>(min(static_cast<size_t>(kTileB), src1 - j0));
+        const int even = cnt & ~1;
+        fence_proxy_async_smem();
+        mbar_arrive_expect_tx(&bars[st], static_cast<uint32_t>(3 * even * sizeof(double)));
+        if (even) {
+            const uint32_t bytes = static_cast<uint32_t>(even * sizeof(double));
+            bulk_g2s(s_x[st], px + j0, bytes, &bars[st]);
+            bulk_g2s(s_y[st], py + j0, bytes, &bars[st]);
+            bulk_g2s(s_g[st], sgs + j0, bytes, &bars[st]);
+        }
+        if (cnt & 1) {
+            s_x[st][cnt - 1] = px[j0 + cnt - 1];
+            s_y[st][cnt - 1] = py[j0 + cnt - 1];
+            s_g[st][cnt - 1] = sgs[j0 + cnt - 1];
+        }
+    };
+    if (tid == 0) {
+        if (ntiles > 0)
+            issue(0);
+        if (ntiles > 1)
+            issue(1);
+    }
+    __syncthreads();
+    for (int t = 0; t < ntiles; ++t) {
+        const uint32_t k = seq0 + t;
+        const int st = k & 1;
+        const bool ok = mbar_wait_bounded(&bars[st], (k >> 1) & 1, timeout_status);
+        if (__syncthreads_or(!ok)) {
+            timed_out = true;
+            return;
+        }
+        const size_t j0 = src0 + static_cast<size_t>(t) * kTileB;
+        const int cnt = static_cast<int>(min(static_cast<size_t>(kTileB), src1 - j0));
+        for (int j = tid; j < cnt; j += kBlock) {
+            const double xj = s_x[st][j], yj = s_y[st][j];
+            const float xh = static_cast<float>(xj), yh = static_cast<float>(yj);
+            s_f[j] = make_float4(xh, yh, static_cast<float>(xj - static_cast<double>(xh)),
+                                 static_cast<float>(yj - static_cast<double>(yh)));
+            s_gf[j] = static_cast<float>(s_g[st][j]);
+        }
+        __syncthreads();
+        const bool diagonal = j0 < blk1 && blk0 < j0 + cnt;
+        for (int jb = 0; jb < cnt; jb += f32::kFlush) {
+            const int je = min(cnt, jb + f32::kFlush);
+            if (diagonal) {
+#pragma unroll 1
+                for (int j = jb; j < je; ++j) {
+                    const float4 sf = s_f[j];
+                    const float gf = s_gf[j];
+#pragma unroll
+                    for (int q = 0; q < T; ++q)
+                        f32::pair32<GEO, true>(f, g, tg[q], sf, gf, s_x[st][j], s_y[st][j],
+                                               s_g[st][j], ti[q] == j0 + j, u[q], v[q], ud[q], vd[q]);
+                }
+            } else {
+#pragma unroll 2
+                for (int j = jb; j < je; ++j) {
+                    const float4 sf = s_f[j];
+                    const float gf = s_gf[j];
+#pragma unroll
+                    for (int q = 0; q < T; ++q)
+                        f32::pair32<GEO, false>(f, g, tg[q], sf, gf, s_x[st][j], s_y[st][j],
+                                                s_g[st][j], false, u[q], v[q], ud[q], vd[q]);
+                }
+            }
+#pragma unroll
+            for (int q = 0; q < T; ++q) {
+                ud[q] += static_cast<double>(u[q]);
+                vd[q] += static_cast<double>(v[q]);
+                u[q] = v[q] = 0.0f;
+            }
+        }
+        __syncthreads();
+        if (tid == 0 && t + 2 < ntiles)
+            issue(t + 2);
+    }
+    seq = seq0 + ntiles;
+#pragma unroll
+    for (int q = 0; q < T; ++q)
+        if (ti[q] < blk1) {
+            pu[out0 + ti[q]] = ud[q];
+            pv[out0 + ti[q]] = vd[q];
+        }
+}
+
 struct VelocityBatchArgs {
     const Item *items;
     unsigned n_items;
@@ -218,10 +401,15 @@ struct VelocityBatchArgs {
     int *timeout_status;
 };
 
+// PREC = PV_PRECISION_FP64: ordered and symmetric items; PREC = PV_PRECISION_FP32C: the
+// compensated form's ordered items.
+template <int PREC>
 __global__ void __launch_bounds__(kBlock) batch_velocity_kernel(const VelocityBatchArgs a) {
     __shared__ alignas(128) double s_x[2][kTileB];
     __shared__ alignas(128) double s_y[2][kTileB];
     __shared__ alignas(128) double s_g[2][kTileB];
+    __shared__ alignas(16) float4 s_f[PREC == PV_PRECISION_FP32C ? kTileB : 1];
+    __shared__ float s_gf[PREC == PV_PRECISION_FP32C ? kTileB : 1];
     __shared__ alignas(8) uint64_t bars[2];
     __shared__ GeometryConsts s_geo;
     __shared__ unsigned s_item;
@@ -257,27 +445,54 @@ __global__ void __launch_bounds__(kBlock) batch_velocity_kernel(const VelocityBa
         px += d.off;
         py += d.off;
         const double *sgs = a.arena.gs + d.off;
+        double *pu = a.arena.pu + d.part_off;
+        double *pv = a.arena.pv + d.part_off;
+        if (PREC == PV_PRECISION_FP64 && it.kind == ITEM_SYMMETRIC) {
+            // the TMA ring is idle between items: its buffers hold the cross-warp reactions
+            run_symmetric_item(s_geo, px, py, sgs, d.n, it.tb, it.chunk, pu, pv, d.pad_n,
+                               &s_x[0][0], &s_y[0][0]);
+            __syncthreads();
+            continue;
+        }
         const size_t src0 = static_cast<size_t>(it.chunk) * d.chunk;
         const size_t src1 = min(src0 + d.chunk, static_cast<size_t>(d.n));
         const size_t per_block = static_cast<size_t>(kBlock) * targets_per_thread(s_geo.geometry);
         const size_t blk0 = static_cast<size_t>(it.tb) * per_block;
         const size_t blk1 = min(blk0 + per_block, static_cast<size_t>(d.n));
-        double *pu = a.arena.pu + d.part_off;
-        double *pv = a.arena.pv + d.part_off;
         const size_t out0 = static_cast<size_t>(it.chunk) * d.pad_n;
-        switch (s_geo.geometry) {
-        case GEO_INFINITE:
-            run_item<InfinitePair, 4>(s_geo, px, py, sgs, src0, src1, blk0, blk1, pu, pv, out0, s_x,
-                                   s_y, s_g, bars, seq, a.timeout_status, timed_out);
-            break;
-        case GEO_PERIODIC:
-            run_item<PeriodicPair, 1>(s_geo, px, py, sgs, src0, src1, blk0, blk1, pu, pv, out0, s_x,
-                                   s_y, s_g, bars, seq, a.timeout_status, timed_out);
-            break;
-        default:
-            run_item<DiskPair, 2>(s_geo, px, py, sgs, src0, src1, blk0, blk1, pu, pv, out0, s_x, s_y,
-                               s_g, bars, seq, a.timeout_status, timed_out);
-            break;
+        if (PREC == PV_PRECISION_FP32C) {
+            switch (s_geo.geometry) {
+            case GEO_INFINITE:
+                run_item32<GEO_INFINITE, 4>(s_geo, px, py, sgs, src0, src1, blk0, blk1, pu, pv,
+                                            out0, s_x, s_y, s_g, s_f, s_gf, bars, seq,
+                                            a.timeout_status, timed_out);
+                break;
+            case GEO_PERIODIC:
+                run_item32<GEO_PERIODIC, 1>(s_geo, px, py, sgs, src0, src1, blk0, blk1, pu, pv,
+                                            out0, s_x, s_y, s_g, s_f, s_gf, bars, seq,
+                                            a.timeout_status, timed_out);
+                break;
+            default:
+                run_item32<GEO_DISK, 2>(s_geo, px, py, sgs, src0, src1, blk0, blk1, pu, pv, out0,
+                                        s_x, s_y, s_g, s_f, s_gf, bars, seq, a.timeout_status,
+                                        timed_out);
+                break;
+            }
+        } else {
+            switch (s_geo.geometry) {
+            case GEO_INFINITE:
+                run_item<InfinitePair, 4>(s_geo, px, py, sgs, src0, src1, blk0, blk1, pu, pv, out0,
+                                          s_x, s_y, s_g, bars, seq, a.timeout_status, timed_out);
+                break;
+            case GEO_PERIODIC:
+                run_item<PeriodicPair, 1>(s_geo, px, py, sgs, src0, src1, blk0, blk1, pu, pv, out0,
+                                          s_x, s_y, s_g, bars, seq, a.timeout_status, timed_out);
+                break;
+            default:
+                run_item<DiskPair, 2>(s_geo, px, py, sgs, src0, src1, blk0, blk1, pu, pv, out0,
+                                      s_x, s_y, s_g, bars, seq, a.timeout_status, timed_out);
+                break;
+            }
         }
         if (timed_out)
             return;
@@ -483,14 +698,16 @@ struct pv_batch {
     size_t slices_cap = 0;
     unsigned *d_counters = nullptr;    // one queue counter per velocity launch of an attempt
     int *d_timeout = nullptr;
-    int resident = 1;
+    int resident = 1;                  // FP64 velocity CTAs per SM
+    int resident32 = 1;                // FP32C velocity CTAs per SM
     std::vector<SimDesc> descs;
     std::vector<int> slot_used;
     std::map<size_t, size_t> free_elems;  // offset -> length (elements), arena
     std::map<size_t, size_t> free_parts;  // offset -> length, partials
     std::vector<std::pair<size_t, size_t>> sim_ranges, part_ranges;
     bool tables_dirty = true;
-    unsigned n_items = 0, n_slices = 0;
+    unsigned n_items = 0, n_slices = 0;  // n_items = FP64 items, then n_items32 FP32C items
+    unsigned n_items32 = 0;
     uint64_t attempts = 0, evaluations_pairs = 0;
     cudaGraphExec_t attempt_graph = nullptr; // one captured attempt for the current tables
     bool use_graph = true;
@@ -554,35 +771,51 @@ void give(std::map<size_t, size_t> &free, size_t off, size_t len) {
     }
 }
 
-// Rebuilds the work queue (items sorted by cost) and the slice table for the running simulations.
+// Rebuilds the work queues (items sorted by cost; FP64 first, then FP32C) and the slice table for
+// the running simulations.
 pv_status rebuild_tables(pv_batch *b) {
-    std::vector<Item> items;
-    std::vector<double> cost;
+    std::vector<Item> items[2];
+    std::vector<double> cost[2];
     std::vector<SliceEntry> slices;
     for (unsigned s = 0; s < b->max_sims; ++s) {
         if (b->slot_used[s] != SIM_RUNNING)
             continue;
         const SimDesc &d = b->descs[s];
-        const unsigned per_block = kBlock * targets_per_thread(d.g.geometry);
-        const unsigned tbs = (d.n + per_block - 1) / per_block;
+        const int q = d.precision == PV_PRECISION_FP32C ? 1 : 0;
         const double w = d.g.geometry == GEO_PERIODIC ? 15.0 : (d.g.geometry == GEO_DISK ? 2.7 : 1.0);
-        for (unsigned tb = 0; tb < tbs; ++tb)
-            for (unsigned ch = 0; ch < d.num_chunks; ++ch) {
-                items.push_back({s, tb, ch, 0});
-                const double nt = std::min<double>(per_block, d.n - tb * double(per_block));
-                const double ns = std::min<double>(d.chunk, d.n - ch * double(d.chunk));
-                cost.push_back(w * nt * ns);
-            }
+        if (d.symmetric) {
+            const unsigned nb = symmetric_rows(d.n);
+            for (unsigned I = 0; I < nb; ++I)
+                for (unsigned J = I; J < nb; ++J) {
+                    items[q].push_back({s, I, J, ITEM_SYMMETRIC});
+                    const double ni = std::min<double>(kBlock, d.n - I * double(kBlock));
+                    const double nj = std::min<double>(kBlock, d.n - J * double(kBlock));
+                    cost[q].push_back(w * ni * nj);
+                }
+        } else {
+            const unsigned per_block = kBlock * targets_per_thread(d.g.geometry);
+            const unsigned tbs = (d.n + per_block - 1) / per_block;
+            for (unsigned tb = 0; tb < tbs; ++tb)
+                for (unsigned ch = 0; ch < d.num_chunks; ++ch) {
+                    items[q].push_back({s, tb, ch, ITEM_ORDERED});
+                    const double nt = std::min<double>(per_block, d.n - tb * double(per_block));
+                    const double ns = std::min<double>(d.chunk, d.n - ch * double(d.chunk));
+                    cost[q].push_back(w * nt * ns);
+                }
+        }
         for (unsigned st = 0; st < d.n; st += 256)
             slices.push_back({s, st});
     }
-    std::vector<size_t> order(items.size());
-    for (size_t i = 0; i < order.size(); ++i)
-        order[i] = i;
-    std::stable_sort(order.begin(), order.end(), [&](size_t a, size_t c) { return cost[a] > cost[c]; });
-    std::vector<Item> sorted(items.size());
-    for (size_t i = 0; i < order.size(); ++i)
-        sorted[i] = items[order[i]];
+    std::vector<Item> sorted;
+    for (int q = 0; q < 2; ++q) {
+        std::vector<size_t> order(items[q].size());
+        for (size_t i = 0; i < order.size(); ++i)
+            order[i] = i;
+        std::stable_sort(order.begin(), order.end(),
+                         [&](size_t a, size_t c) { return cost[q][a] > cost[q][c]; });
+        for (size_t i : order)
+            sorted.push_back(items[q][i]);
+    }
     if (sorted.size() > b->items_cap) {
         cudaFree(b->d_items);
         b->d_items = nullptr;
@@ -602,7 +835,8 @@ pv_status rebuild_tables(pv_batch *b) {
         PVB_CUDA(b, cudaMemcpyAsync(b->d_slices, slices.data(), slices.size() * sizeof(SliceEntry),
                                     cudaMemcpyHostToDevice, b->stream));
     PVB_CUDA(b, cudaStreamSynchronize(b->stream));
-    b->n_items = static_cast<unsigned>(sorted.size());
+    b->n_items = static_cast<unsigned>(items[0].size());
+    b->n_items32 = static_cast<unsigned>(items[1].size());
     b->n_slices = static_cast<unsigned>(slices.size());
     b->tables_dirty = false;
     return PV_OK;
@@ -618,27 +852,38 @@ StageCoefs stage_coefs() {
     return c;
 }
 
+// The velocity of one stage: the FP64 queue, then the FP32C queue (counters 2s and 2s + 1).
 pv_status launch_velocity_stage(pv_batch *b, int stage, int only_without_fsal, int counter) {
     VelocityBatchArgs a{};
-    a.items = b->d_items;
-    a.n_items = b->n_items;
-    a.counter = b->d_counters + counter;
     a.descs = b->d_descs;
     a.ctl = b->d_ctl;
     a.arena = b->arena;
     a.stage = stage;
     a.only_without_fsal = only_without_fsal;
     a.timeout_status = b->d_timeout;
-    const unsigned grid = static_cast<unsigned>(std::max(1, b->sm_count * b->resident));
-    batch_velocity_kernel<<<grid, kBlock, 0, b->stream>>>(a);
-    PVB_CUDA(b, cudaGetLastError());
+    if (b->n_items) {
+        a.items = b->d_items;
+        a.n_items = b->n_items;
+        a.counter = b->d_counters + 2 * counter;
+        const unsigned grid = static_cast<unsigned>(std::max(1, b->sm_count * b->resident));
+        batch_velocity_kernel<PV_PRECISION_FP64><<<grid, kBlock, 0, b->stream>>>(a);
+        PVB_CUDA(b, cudaGetLastError());
+    }
+    if (b->n_items32) {
+        a.items = b->d_items + b->n_items;
+        a.n_items = b->n_items32;
+        a.counter = b->d_counters + 2 * counter + 1;
+        const unsigned grid = static_cast<unsigned>(std::max(1, b->sm_count * b->resident32));
+        batch_velocity_kernel<PV_PRECISION_FP32C><<<grid, kBlock, 0, b->stream>>>(a);
+        PVB_CUDA(b, cudaGetLastError());
+    }
     return PV_OK;
 }
 
 pv_status enqueue_attempt(pv_batch *b) {
-    if (b->n_items == 0)
+    if (b->n_items + b->n_items32 == 0)
         return PV_OK;
-    PVB_CUDA(b, cudaMemsetAsync(b->d_counters, 0, 8 * sizeof(unsigned), b->stream));
+    PVB_CUDA(b, cudaMemsetAsync(b->d_counters, 0, kCounters * sizeof(unsigned), b->stream));
     const StageCoefs coefs = stage_coefs();
     pv_status st;
     if ((st = launch_velocity_stage(b, 0, 1, 0)) != PV_OK)
@@ -672,7 +917,7 @@ pv_status capture_attempt(pv_batch *b) {
         cudaGraphExecDestroy(b->attempt_graph);
         b->attempt_graph = nullptr;
     }
-    if (!b->use_graph || b->n_items == 0)
+    if (!b->use_graph || b->n_items + b->n_items32 == 0)
         return PV_OK;
     cudaGraph_t graph = nullptr;
     PVB_CUDA(b, cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
@@ -725,10 +970,13 @@ pv_status pv_batch_create(const pv_batch_config *config, pv_batch **out) {
     cudaError_t e;
     if ((e = cudaDeviceGetAttribute(&b->sm_count, cudaDevAttrMultiProcessorCount, b->device)) != cudaSuccess)
         return bail(e, "cudaDeviceGetAttribute");
-    if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b->resident, batch_velocity_kernel, kBlock, 0)) !=
-        cudaSuccess)
+    if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+             &b->resident, batch_velocity_kernel<PV_PRECISION_FP64>, kBlock, 0)) != cudaSuccess ||
+        (e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+             &b->resident32, batch_velocity_kernel<PV_PRECISION_FP32C>, kBlock, 0)) != cudaSuccess)
         return bail(e, "cudaOccupancyMaxActiveBlocksPerMultiprocessor");
     b->resident = std::max(1, b->resident);
+    b->resident32 = std::max(1, b->resident32);
     if ((e = cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking)) != cudaSuccess)
         return bail(e, "cudaStreamCreate");
     b->capacity = round_up(config->capacity_vortices, kAlign) + kAlign * b->max_sims;
@@ -763,7 +1011,7 @@ pv_status pv_batch_create(const pv_batch_config *config, pv_batch **out) {
     if ((e = cudaMalloc(&b->d_descs, b->max_sims * sizeof(SimDesc))) != cudaSuccess ||
         (e = cudaMalloc(&b->d_ctl, b->max_sims * sizeof(SimControl))) != cudaSuccess ||
         (e = cudaMallocHost(&b->h_ctl, b->max_sims * sizeof(SimControl))) != cudaSuccess ||
-        (e = cudaMalloc(&b->d_counters, 8 * sizeof(unsigned))) != cudaSuccess ||
+        (e = cudaMalloc(&b->d_counters, kCounters * sizeof(unsigned))) != cudaSuccess ||
         (e = cudaMalloc(&b->d_timeout, sizeof(int))) != cudaSuccess)
         return bail(e, "cudaMalloc(batch tables)");
     std::memset(b->h_ctl, 0, b->max_sims * sizeof(SimControl));
@@ -830,9 +1078,16 @@ pv_status pv_batch_add(pv_batch *b, const pv_params *params, const double *x, co
         }
     if (slot == b->max_sims)
         return bfail(b, PV_ERROR_CAPACITY, "no free simulation slot");
+    if (params->precision != PV_PRECISION_FP64 && params->precision != PV_PRECISION_FP32C)
+        return bfail(b, PV_ERROR_INVALID_ARGUMENT, "unknown precision form");
     const size_t pad = round_up(n, kAlign);
     const size_t chunk = chunk_for(n);
-    const unsigned chunks = static_cast<unsigned>((n + chunk - 1) / chunk);
+    // FP64 periodic populations from kSymmetricMinN up: once per unordered pair, one partial row
+    // per 128-block (a function of n only, so the choice never depends on the batch)
+    const bool symmetric = params->precision == PV_PRECISION_FP64 && g.geometry == GEO_PERIODIC &&
+                           n >= kSymmetricMinN;
+    const unsigned chunks = symmetric ? symmetric_rows(static_cast<unsigned>(n))
+                                      : static_cast<unsigned>((n + chunk - 1) / chunk);
     size_t off = 0, poff = 0;
     if (!take(b->free_elems, pad, off))
         return bfail(b, PV_ERROR_CAPACITY, "the batch arena has no room for this population");
@@ -848,6 +1103,8 @@ pv_status pv_batch_add(pv_batch *b, const pv_params *params, const double *x, co
     d.pad_n = static_cast<unsigned>(pad);
     d.num_chunks = chunks;
     d.chunk = static_cast<unsigned>(chunk);
+    d.precision = params->precision;
+    d.symmetric = symmetric ? 1 : 0;
     b->descs[slot] = d;
     b->sim_ranges[slot] = {off, pad};
     b->part_ranges[slot] = {poff, pad * chunks};
@@ -896,7 +1153,7 @@ pv_status pv_batch_advance(pv_batch *b, uint32_t attempts, uint32_t *running) {
             if ((st = capture_attempt(b)) != PV_OK)
                 return st;
         }
-        if (b->n_items == 0)
+        if (b->n_items + b->n_items32 == 0)
             break;
         if (b->attempt_graph)
             PVB_CUDA(b, cudaGraphLaunch(b->attempt_graph, b->stream));
@@ -974,7 +1231,7 @@ pv_status pv_batch_status(pv_batch *b, pv_batch_totals *totals) {
     if (!b || !totals)
         return PV_ERROR_INVALID_ARGUMENT;
     totals->attempts = b->attempts;
-    totals->work_items = b->n_items;
+    totals->work_items = b->n_items + b->n_items32;
     size_t free_elems = 0;
     for (auto &kv : b->free_elems)
         free_elems += kv.second;

@@ -21,6 +21,7 @@
 //     (I, J), vortices of block J receive row I, and each (row, vortex) is written exactly once,
 //     so the stage kernel's fixed-order sum over rows keeps results deterministic.
 #include "pv_internal.h"
+#include "pv_symmetric.cuh"
 
 #include <algorithm>
 
@@ -29,18 +30,6 @@ namespace pvb {
 namespace {
 
 constexpr int kThreads = 128;  // 4 independent warps per CTA
-
-__device__ __forceinline__ double rotate(double v, int from) {
-    return __shfl_sync(0xffffffffu, v, from);
-}
-
-__device__ __forceinline__ void kernel_values(const GeometryConsts &g, double tx, double ty,
-                                              double sx, double sy, double &ku, double &kv) {
-    double au, bu, av, bv;
-    PeriodicPair::terms<true>(g, tx, ty, sx, sy, au, bu, av, bv);  // half sines: see gs2 below
-    ku = au * rcp_refined(bu);
-    kv = av * rcp_refined(bv);
-}
 
 __global__ void __launch_bounds__(kThreads)
     periodic_symmetric_kernel(const double *__restrict__ x, const double *__restrict__ y,
@@ -51,7 +40,6 @@ __global__ void __launch_bounds__(kThreads)
     extern __shared__ double2 reaction_smem[];
     const int lane = threadIdx.x & 31;
     double2 *reaction = reaction_smem + (threadIdx.x >> 5) * a * 32;  // this warp's sources
-    const int next = (lane + 1) & 31;
     const size_t block_len = static_cast<size_t>(32) * a;
     for (;;) {
         unsigned item = 0;
@@ -65,52 +53,24 @@ __global__ void __launch_bounds__(kThreads)
         const bool diagonal = I == J;
         for (int jb = 0; jb < a; ++jb)
             reaction[jb * 32 + lane] = make_double2(0.0, 0.0);
-        __syncwarp();
         for (int ib = 0; ib < a; ++ib) {
             const size_t ti = I * block_len + static_cast<size_t>(ib) * 32 + lane;
             const bool t_ok = ti < n;
             const double tx = t_ok ? x[ti] : 0.0, ty = t_ok ? y[ti] : 0.0;
-            const double tg = t_ok ? 2.0 * gs[ti] : 0.0;  // doubled: the terms carry half sines
+            const double tg2 = t_ok ? 2.0 * gs[ti] : 0.0;  // doubled: the terms carry half sines
             double u = 0.0, v = 0.0;
             for (int jb = diagonal ? ib : 0; jb < a; ++jb) {
                 const size_t sj = J * block_len + static_cast<size_t>(jb) * 32 + lane;
-                int s_ok = sj < n ? 1 : 0;
-                double sx = s_ok ? x[sj] : 0.0, sy = s_ok ? y[sj] : 0.0;
-                double sg = s_ok ? 2.0 * gs[sj] : 0.0;
+                const int s_ok = sj < n ? 1 : 0;
+                const double sx = s_ok ? x[sj] : 0.0, sy = s_ok ? y[sj] : 0.0;
+                const double sg2 = s_ok ? 2.0 * gs[sj] : 0.0;
                 if (diagonal && jb == ib) {
-                    // ordered pairs (lane, lane + k), k = 1..31, target side only
-                    for (int k = 1; k < 32; ++k) {
-                        sx = rotate(sx, next);
-                        sy = rotate(sy, next);
-                        sg = rotate(sg, next);
-                        s_ok = __shfl_sync(0xffffffffu, s_ok, next);
-                        if (t_ok && s_ok) {
-                            double ku, kv;
-                            kernel_values(g, tx, ty, sx, sy, ku, kv);
-                            u = fma(-sg, ku, u);
-                            v = fma(sg, kv, v);
-                        }
-                    }
+                    sym::one_sided_tile(g, tx, ty, t_ok, sx, sy, sg2, s_ok, true, u, v);
                     continue;
                 }
                 double ru = reaction[jb * 32 + lane].x, rv = reaction[jb * 32 + lane].y;
-                for (int k = 0; k < 32; ++k) {
-                    if (t_ok && s_ok) {
-                        double ku, kv;
-                        kernel_values(g, tx, ty, sx, sy, ku, kv);
-                        u = fma(-sg, ku, u);  // target: -g_s K
-                        v = fma(sg, kv, v);
-                        ru = fma(tg, ku, ru);  // source: the exchanged pair, +g_t K
-                        rv = fma(-tg, kv, rv);
-                    }
-                    sx = rotate(sx, next);
-                    sy = rotate(sy, next);
-                    sg = rotate(sg, next);
-                    ru = rotate(ru, next);
-                    rv = rotate(rv, next);
-                    s_ok = __shfl_sync(0xffffffffu, s_ok, next);
-                }
-                reaction[jb * 32 + lane] = make_double2(ru, rv);  // home again after 32 steps
+                sym::react_tile(g, tx, ty, tg2, t_ok, sx, sy, sg2, s_ok, u, v, ru, rv);
+                reaction[jb * 32 + lane] = make_double2(ru, rv);
             }
             if (diagonal) {  // reactions from the sub-blocks before this one in the same block
                 const double2 r = reaction[ib * 32 + lane];

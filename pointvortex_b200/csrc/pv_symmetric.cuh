@@ -1,0 +1,75 @@
+// pv_symmetric.cuh — warp tiles of the periodic box evaluated once per unordered pair, shared by
+// the single-simulation kernel (pv_symmetric.cu) and the batched ensembles (pv_batch.cu).
+//
+// A tile is 32 targets (one per lane) against 32 sources. The sources, with the reactions they
+// accumulate, rotate one lane per step by shuffles; after 32 steps every (target, source) pair has
+// been met once and every source is back in its home lane. The pair terms are exactly odd under
+// exchanging target and source (PeriodicPair::terms), so one evaluation gives the target's term
+// and, with the other circulation and the opposite sign, the source's. The terms carry half sines
+// (PeriodicPair::terms<true>), so callers pass doubled scaled circulations: 2 * Gamma * 0.5/L.
+#pragma once
+
+#include "pv_geometry.cuh"
+
+namespace pvb {
+namespace sym {
+
+__device__ __forceinline__ double rotate(double v, int from) {
+    return __shfl_sync(0xffffffffu, v, from);
+}
+
+__device__ __forceinline__ void kernel_values(const GeometryConsts &g, double tx, double ty,
+                                              double sx, double sy, double &ku, double &kv) {
+    double au, bu, av, bv;
+    PeriodicPair::terms<true>(g, tx, ty, sx, sy, au, bu, av, bv);
+    ku = au * rcp_refined(bu);
+    kv = av * rcp_refined(bv);
+}
+
+// Targets (tx, ty, tg2) against the sources held in the lanes (sx, sy, sg2 and their reactions
+// ru, rv); adds the targets' sums to u, v and the sources' to ru, rv. Sources end at home.
+__device__ __forceinline__ void react_tile(const GeometryConsts &g, double tx, double ty,
+                                           double tg2, bool t_ok, double sx, double sy,
+                                           double sg2, int s_ok, double &u, double &v, double &ru,
+                                           double &rv) {
+    const int next = (threadIdx.x + 1) & 31;
+    for (int k = 0; k < 32; ++k) {
+        if (t_ok && s_ok) {
+            double ku, kv;
+            kernel_values(g, tx, ty, sx, sy, ku, kv);
+            u = fma(-sg2, ku, u);   // target: -g_s K
+            v = fma(sg2, kv, v);
+            ru = fma(tg2, ku, ru);  // source: the exchanged pair, +g_t K
+            rv = fma(-tg2, kv, rv);
+        }
+        sx = rotate(sx, next);
+        sy = rotate(sy, next);
+        sg2 = rotate(sg2, next);
+        ru = rotate(ru, next);
+        rv = rotate(rv, next);
+        s_ok = __shfl_sync(0xffffffffu, s_ok, next);
+    }
+}
+
+// Target side only. same_block: the sources are the targets' own lanes, so the self pair (k = 0)
+// is skipped; it contributes exactly 0 in the reference (sin 0 = 0).
+__device__ __forceinline__ void one_sided_tile(const GeometryConsts &g, double tx, double ty,
+                                               bool t_ok, double sx, double sy, double sg2,
+                                               int s_ok, bool same_block, double &u, double &v) {
+    const int next = (threadIdx.x + 1) & 31;
+    for (int k = 0; k < 32; ++k) {
+        if (t_ok && s_ok && !(same_block && k == 0)) {
+            double ku, kv;
+            kernel_values(g, tx, ty, sx, sy, ku, kv);
+            u = fma(-sg2, ku, u);
+            v = fma(sg2, kv, v);
+        }
+        sx = rotate(sx, next);
+        sy = rotate(sy, next);
+        sg2 = rotate(sg2, next);
+        s_ok = __shfl_sync(0xffffffffu, s_ok, next);
+    }
+}
+
+}  // namespace sym
+}  // namespace pvb

@@ -34,11 +34,15 @@ def state(boundary, n, seed):
 
 
 def run_batch(items, capacity=20000, slots=16, **kw):
+    """items: (boundary, n, seed, t_end[, precision])."""
     b = Batch(capacity, slots)
     ids = []
-    for boundary, n, seed, t_end in items:
+    for item in items:
+        boundary, n, seed, t_end = item[:4]
+        precision = item[4] if len(item) > 4 else "fp64"
         x, y, g = state(boundary, n, seed)
-        ids.append(b.add(geometry_params(boundary), x, y, g, t_end, **{**SOLVE, **kw}))
+        ids.append(b.add(geometry_params(boundary, precision=precision), x, y, g, t_end,
+                         **{**SOLVE, **kw}))
     b.run()
     out = [(b.info(i), b.result(i)) for i in ids]
     b.close()
@@ -127,3 +131,44 @@ def test_admission_validation():
     g[0] += 1.0
     with pytest.raises(ValueError, match="zero total circulation"):
         b.add(geometry_params("periodic"), x, y, g, 0.01, **SOLVE)
+
+
+def mixed_forms():
+    """FP64 periodic from N = 2048 runs once per unordered pair; fp32c items drain their own
+    queue in a second launch per stage."""
+    return [
+        ("periodic", 2100, 7, 0.0004),
+        ("infinite", 700, 8, 0.002, "fp32c"),
+        ("periodic", 512, 9, 0.002, "fp32c"),
+        ("disk", 600, 15, 0.002, "fp32c"),
+        ("infinite", 500, 11, 0.002),
+    ]
+
+
+def test_alone_equals_in_the_mix_across_forms():
+    mixed = run_batch(mixed_forms(), capacity=40000)
+    for k, spec in enumerate(mixed_forms()):
+        (info_a, (xa, ya)) = run_batch([spec], capacity=40000)[0]
+        info_m, (xm, ym) = mixed[k]
+        assert info_a.state == "done" and info_m.state == "done", (spec, info_a, info_m)
+        assert info_a.acceptedSteps == info_m.acceptedSteps
+        assert np.array_equal(xa, xm) and np.array_equal(ya, ym), spec
+
+
+def test_symmetric_batch_matches_oracle_driver(reference):
+    spec = mixed_forms()[0]
+    (info, (x, y)), = run_batch([spec], capacity=40000)
+    rx, ry, steps = oracle_driver(reference, *spec)
+    assert info.acceptedSteps == steps, info
+    assert position_error(x, y, rx, ry) <= 1e-9
+
+
+def test_fp32c_batch_tracks_fp64():
+    """The compensated form against the plain form over the same solves: FP32-level terms move
+    the vortices by ~1e-7 at most over these few steps."""
+    forms = [s for s in mixed_forms() if len(s) > 4]
+    fp32 = run_batch(forms, capacity=40000)
+    fp64 = run_batch([s[:4] for s in forms], capacity=40000)
+    for spec, (i32, (x32, y32)), (i64, (x64, y64)) in zip(forms, fp32, fp64):
+        assert i32.state == i64.state == "done", spec
+        assert np.max(np.hypot(x32 - x64, y32 - y64)) < 1e-6, spec
