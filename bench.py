@@ -520,8 +520,9 @@ def run_serving(budget: int = 10) -> dict:
     for rate, count, policy in ((10.0, 30, "split"), (100.0, 200, "split"), (100.0, 200, "fifo"),
                                 (1000.0, 600, "split")):
         reqs = poisson_stream(count, rate, seed=int(rate), max_steps=budget)
-        # split: the expensive batch takes one attempt per tick, the cheap one 16 (measured best
-        # of a sweep of 1-2 / 8-32 attempts and 2^22-2^26 split points on the 100 req/s stream)
+        # split: two batches driven by two host threads on two streams, the expensive one one
+        # attempt per call, the cheap one 16 (the best p50 of a sweep of 1-4 / 2-16 attempts
+        # on the 100 req/s stream at equal throughput)
         server = Server(capacity_vortices=4_000_000, max_slots=1024,
                         attempts_per_tick=1 if policy == "split" else 2, policy=policy)
         summary = server.serve(reqs)

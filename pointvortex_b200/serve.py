@@ -17,6 +17,7 @@ single-simulation context API (one simulation per launch, plain FP64).
 from __future__ import annotations
 
 import heapq
+import threading
 import time
 from dataclasses import dataclass, field
 from typing import Callable, Optional
@@ -139,25 +140,31 @@ class Server:
             return self.lanes[1]
         return self.lanes[0]
 
-    def _admit(self, now: float) -> int:
+    def _route(self, now: float) -> None:
+        """Moves the requests that have arrived into their lane's ready list (arrival order)."""
         while self.arrivals and self.arrivals[0][0] <= now:
             item = heapq.heappop(self.arrivals)
             self._lane_of(item[2]).ready.append(item)
+
+    def _admit_lane(self, lane: _Lane, now: float) -> int:
         admitted = 0
-        for lane in self.lanes:
-            while lane.ready:
-                _, _, req = lane.ready[0]
-                x, y, g = req.state()
-                try:
-                    sid = lane.batch.add(geometry_params(req.geometry), x, y, g, req.t_end,
-                                         dt=req.dt, atol=req.atol, rtol=req.rtol,
-                                         max_steps=req.max_steps)
-                except CapacityError:
-                    break               # wait for room: head-of-line, arrival order kept
-                lane.ready.pop(0)
-                lane.running[sid] = (req, now)
-                admitted += 1
+        while lane.ready:
+            _, _, req = lane.ready[0]
+            x, y, g = req.state()
+            try:
+                sid = lane.batch.add(geometry_params(req.geometry), x, y, g, req.t_end,
+                                     dt=req.dt, atol=req.atol, rtol=req.rtol,
+                                     max_steps=req.max_steps)
+            except CapacityError:
+                break                   # wait for room: head-of-line, arrival order kept
+            lane.ready.pop(0)
+            lane.running[sid] = (req, now)
+            admitted += 1
         return admitted
+
+    def _admit(self, now: float) -> int:
+        self._route(now)
+        return sum(self._admit_lane(lane, now) for lane in self.lanes)
 
     def _retire(self, lane: _Lane, now: float, on_complete) -> int:
         done = 0
@@ -182,28 +189,65 @@ class Server:
 
     def serve(self, requests: list[Request], on_complete: Optional[Callable] = None,
               clock=time.perf_counter) -> dict:
-        """Runs the stream in real time: a request becomes visible at its arrival time."""
+        """Runs the stream in real time: a request becomes visible at its arrival time. With
+        policy "split" each batch is driven by its own host thread on its own CUDA stream, so the
+        cheap requests' attempts run beside the expensive batch's instead of between them."""
         for r in requests:
             self.submit(r)
         start = clock()
         total = len(requests)
-        while len(self.completions) < total:
-            self._admit(clock() - start)
-            busy = [lane for lane in self.lanes if lane.running]
-            if not busy:
-                if self.arrivals:
-                    wait = self.arrivals[0][0] - (clock() - start)
-                    if wait > 0:
-                        time.sleep(min(wait, 0.01))
-                continue
-            for lane in busy:
+        if total == 0:
+            pass
+        elif self.policy == "split":
+            self._serve_threads(total, on_complete, clock, start)
+        else:
+            lane = self.lanes[0]
+            while len(self.completions) < total:
+                self._admit(clock() - start)
+                if not lane.running:
+                    if self.arrivals:
+                        wait = self.arrivals[0][0] - (clock() - start)
+                        if wait > 0:
+                            time.sleep(min(wait, 0.01))
+                    continue
                 lane.batch.advance(lane.attempts)
                 self._retire(lane, clock() - start, on_complete)
-                self._admit(clock() - start)
         elapsed = clock() - start
         out = summarize(self.completions, elapsed)
         out["policy"] = self.policy
         return out
+
+    def _serve_threads(self, total: int, on_complete, clock, start: float) -> None:
+        lock = threading.Lock()
+        finished = threading.Event()
+        errors: list = []
+
+        def drive(lane: _Lane) -> None:
+            try:
+                while not finished.is_set():
+                    with lock:
+                        self._route(clock() - start)
+                        self._admit_lane(lane, clock() - start)
+                        idle = not lane.running
+                    if idle:
+                        time.sleep(0.0005)
+                        continue
+                    lane.batch.advance(lane.attempts)   # the GIL is released during the call
+                    with lock:
+                        self._retire(lane, clock() - start, on_complete)
+                        if len(self.completions) >= total:
+                            finished.set()
+            except BaseException as exc:  # surfaced to the caller below
+                errors.append(exc)
+                finished.set()
+
+        threads = [threading.Thread(target=drive, args=(lane,), daemon=True) for lane in self.lanes]
+        for t in threads:
+            t.start()
+        for t in threads:
+            t.join()
+        if errors:
+            raise errors[0]
 
     def close(self):
         for lane in self.lanes:
