@@ -18,7 +18,8 @@
 namespace pvb {
 
 namespace {
-constexpr int kDT = 128;
+constexpr int kDT = 128;  // targets per block
+constexpr int kDS = 32;   // sources per block
 
 __device__ __forceinline__ void push(DipoleCandidateDev *out, size_t capacity,
                                      unsigned long long *count, unsigned long long a,
@@ -31,33 +32,37 @@ __device__ __forceinline__ void push(DipoleCandidateDev *out, size_t capacity,
     }
 }
 
+// Block (source tile of kDS, target block of kDT): every unordered pair i < j once. Short source
+// tiles give many CTAs, so the scan hides its latency at small N too.
 __global__ void __launch_bounds__(kDT)
     dipole_scan_kernel(const double *x, const double *y, const double *g, size_t n,
                        GeometryConsts gc, double thr2, DipoleCandidateDev *out, size_t capacity,
                        unsigned long long *count) {
-    const int I = blockIdx.y, J = blockIdx.x;
-    if (J < I)
+    const size_t i0 = static_cast<size_t>(blockIdx.y) * kDT;
+    const size_t j0 = static_cast<size_t>(blockIdx.x) * kDS;
+    if (j0 + kDS <= i0 + 1)  // every source of the tile precedes every target of the block
         return;
-    __shared__ double sx[kDT], sy[kDT], sg[kDT];
-    const size_t j0 = static_cast<size_t>(J) * kDT;
-    const size_t jl = j0 + threadIdx.x;
-    sx[threadIdx.x] = jl < n ? x[jl] : 0.0;
-    sy[threadIdx.x] = jl < n ? y[jl] : 0.0;
-    sg[threadIdx.x] = jl < n ? g[jl] : 0.0;
+    __shared__ double sx[kDS], sy[kDS], sg[kDS];
+    if (threadIdx.x < kDS) {
+        const size_t jl = j0 + threadIdx.x;
+        sx[threadIdx.x] = jl < n ? x[jl] : 0.0;
+        sy[threadIdx.x] = jl < n ? y[jl] : 0.0;
+        sg[threadIdx.x] = jl < n ? g[jl] : 0.0;
+    }
     __syncthreads();
-    const size_t i = static_cast<size_t>(I) * kDT + threadIdx.x;
+    const size_t i = i0 + threadIdx.x;
     if (i >= n)
         return;
     const double xi = x[i], yi = y[i], gi = g[i];
     if (gi == 0.0)
         return;
     const bool periodic = gc.geometry == GEO_PERIODIC;
-    const int jcount = static_cast<int>(min(static_cast<size_t>(kDT), n - j0));
-    const int jstart = (I == J) ? static_cast<int>(threadIdx.x) + 1 : 0;
+    const int jcount = static_cast<int>(min(static_cast<size_t>(kDS), n - j0));
     const bool neg_i = signbit(gi);
-    for (int jj = jstart; jj < jcount; ++jj) {
+#pragma unroll 4
+    for (int jj = 0; jj < jcount; ++jj) {
         const double gj = sg[jj];
-        if (gj == 0.0 || neg_i == static_cast<bool>(signbit(gj)))
+        if (j0 + jj <= i || gj == 0.0 || neg_i == static_cast<bool>(signbit(gj)))
             continue;
         double dx = xi - sx[jj], dy = yi - sy[jj];
         if (periodic) {
@@ -68,7 +73,8 @@ __global__ void __launch_bounds__(kDT)
         if (d2 < thr2)
             push(out, capacity, count, i, j0 + jj, d2);
     }
-    if (gc.geometry == GEO_DISK && I == J) {
+    // the wall image of each target once: in the block whose source tile starts at the target block
+    if (gc.geometry == GEO_DISK && j0 == i0) {
         const double r2 = __dadd_rn(__dmul_rn(xi, xi), __dmul_rn(yi, yi));
         if (r2 > 0.0) {
             const double image = __ddiv_rn(__dsub_rn(gc.radius2, r2), __dsqrt_rn(r2));
@@ -127,8 +133,10 @@ cudaError_t launch_dipole_scan(const double *x, const double *y, const double *g
     cudaError_t e = cudaMemsetAsync(count, 0, sizeof(unsigned long long), stream);
     if (e != cudaSuccess || n == 0)
         return e;
-    const size_t nt = (n + kDT - 1) / kDT;
-    const dim3 grid(static_cast<unsigned>(nt), static_cast<unsigned>(nt));
+    const size_t nt = (n + kDT - 1) / kDT, ns = (n + kDS - 1) / kDS;
+    if (nt > 65535)
+        return cudaErrorInvalidValue;
+    const dim3 grid(static_cast<unsigned>(ns), static_cast<unsigned>(nt));
     dipole_scan_kernel<<<grid, kDT, 0, stream>>>(x, y, gamma, n, g, threshold * threshold, out,
                                                  capacity, count);
     return cudaGetLastError();

@@ -64,10 +64,90 @@ __device__ void dopri_control(DeviceControl *ctl) {
 }
 } // namespace
 
+// Everything a stage does for one target once its velocity (ku, kv) is summed: the slow path of
+// a non-finite sum, the stage velocity, and the stage position / RK4 combination / DOPRI5 error.
 template <int MODE>
+__device__ __forceinline__ void finish_target(const StageArgs &a, size_t i, double ku, double kv,
+                                              double dt, double &local_max) {
+    if (a.reduce) {
+        if (!isfinite(ku) || !isfinite(kv)) {
+            const int verdict =
+                slow_target(a.g, a.ex, a.ey, a.gamma, a.n_src, a.t_offset + i, ku, kv);
+            if (verdict == ST_COINCIDENT || (verdict && !a.nonfinite_ok))
+                set_status(&a.ctl->status, verdict);
+        }
+        a.kx[a.s][i] = ku;
+        a.ky[a.s][i] = kv;
+    }
+    if (MODE == STAGE_POSITION) {
+        // makeStage, src/timestep.cpp:19-30 (zero coefficients add an exact zero: skipped)
+        double dx = 0.0, dy = 0.0;
+        for (int j = 0; j < a.ncoef; ++j) {
+            const double c = a.coef[j];
+            if (c == 0.0)
+                continue;
+            const double kxj = j == a.s ? ku : a.kx[j][i];
+            const double kyj = j == a.s ? kv : a.ky[j][i];
+            dx = __dadd_rn(dx, __dmul_rn(c, kxj));
+            dy = __dadd_rn(dy, __dmul_rn(c, kyj));
+        }
+        const double nx = __dadd_rn(a.x0[i], __dmul_rn(dt, dx));
+        const double ny = __dadd_rn(a.y0[i], __dmul_rn(dt, dy));
+        a.xt[i] = nx;
+        a.yt[i] = ny;
+        validate_position(a, nx, ny);
+    } else if (MODE == STAGE_RK4_COMBINE) {
+        // src/timestep.cpp:52-57: x0 + dt * (k1 + 2 k2 + 2 k3 + k4) / 6
+        const double sx = __dadd_rn(__dadd_rn(__dadd_rn(a.kx[0][i], __dmul_rn(2.0, a.kx[1][i])),
+                                              __dmul_rn(2.0, a.kx[2][i])),
+                                    ku);
+        const double sy = __dadd_rn(__dadd_rn(__dadd_rn(a.ky[0][i], __dmul_rn(2.0, a.ky[1][i])),
+                                              __dmul_rn(2.0, a.ky[2][i])),
+                                    kv);
+        const double nx = __dadd_rn(a.x0[i], __ddiv_rn(__dmul_rn(dt, sx), 6.0));
+        const double ny = __dadd_rn(a.y0[i], __ddiv_rn(__dmul_rn(dt, sy), 6.0));
+        a.xt[i] = nx;
+        a.yt[i] = ny;
+        if (!isfinite(nx) || !isfinite(ny))
+            set_status(&a.ctl->status, ST_NONFINITE_POSITION);
+    } else if (MODE == STAGE_DOPRI_ERROR) {
+        // src/timestep.cpp:78-95: xt holds the fifth-order point y5 (stage 7's position).
+        double xe = 0.0, ye = 0.0;
+        for (int j = 0; j < 7; ++j) {
+            const double w = a.w[j];
+            if (w == 0.0)
+                continue;
+            const double h = __dmul_rn(dt, w);
+            const double kxj = j == a.s ? ku : a.kx[j][i];
+            const double kyj = j == a.s ? kv : a.ky[j][i];
+            xe = __dadd_rn(xe, __dmul_rn(h, kxj));
+            ye = __dadd_rn(ye, __dmul_rn(h, kyj));
+        }
+        const double x5 = a.xt[i], y5 = a.yt[i];
+        const double xs = __dadd_rn(a.ctl->absolute_tolerance,
+                                    __dmul_rn(a.ctl->relative_tolerance,
+                                              max_ref(fabs(a.x0[i]), fabs(x5))));
+        const double ys = __dadd_rn(a.ctl->absolute_tolerance,
+                                    __dmul_rn(a.ctl->relative_tolerance,
+                                              max_ref(fabs(a.y0[i]), fabs(y5))));
+        if (!isfinite(xe) || !isfinite(ye) || !isfinite(xs) || !isfinite(ys) || !(xs > 0.0) ||
+            !(ys > 0.0)) {
+            set_status(&a.ctl->status, ST_DOPRI_NONFINITE);
+        } else {
+            local_max = max_ref(local_max, __ddiv_rn(fabs(xe), xs));
+            local_max = max_ref(local_max, __ddiv_rn(fabs(ye), ys));
+        }
+    }
+}
+
+// WIDE: many partial rows (the symmetric kernel's). A block then covers 32 targets with 8 row
+// groups: warp g sums rows g, g + 8, ... (coalesced over the 32 targets), and warp 0 adds the 8
+// group sums in fixed order. Otherwise one thread per target sums its rows in order.
+template <int MODE, bool WIDE>
 __global__ void __launch_bounds__(256) stage_kernel(const StageArgs a) {
     __shared__ int s_status;
     __shared__ double s_max[8];
+    __shared__ double s_u[WIDE ? 8 : 1][32], s_v[WIDE ? 8 : 1][32];
     const int tid = threadIdx.x;
     if (tid == 0)
         s_status = *reinterpret_cast<volatile int *>(&a.ctl->status);
@@ -77,86 +157,46 @@ __global__ void __launch_bounds__(256) stage_kernel(const StageArgs a) {
 
     const double dt = a.dt_from_control ? a.ctl->dt : a.dt;
     double local_max = 0.0;
-    for (size_t i = blockIdx.x * static_cast<size_t>(blockDim.x) + tid; i < a.n;
-         i += static_cast<size_t>(gridDim.x) * blockDim.x) {
-        double ku, kv;
-        if (a.reduce) {
-            ku = 0.0;
-            kv = 0.0;
-            for (int c = 0; c < a.num_chunks; ++c) {
-                ku += a.pu[static_cast<size_t>(c) * a.stride + i];
-                kv += a.pv[static_cast<size_t>(c) * a.stride + i];
+    if (WIDE) {
+        const int lane = tid & 31, group = tid >> 5;
+        for (size_t base = static_cast<size_t>(blockIdx.x) * 32; base < a.n;
+             base += static_cast<size_t>(gridDim.x) * 32) {
+            const size_t i = base + lane;
+            double su = 0.0, sv = 0.0;
+            if (i < a.n)
+                for (int c = group; c < a.num_chunks; c += 8) {
+                    su += a.pu[static_cast<size_t>(c) * a.stride + i];
+                    sv += a.pv[static_cast<size_t>(c) * a.stride + i];
+                }
+            s_u[group][lane] = su;
+            s_v[group][lane] = sv;
+            __syncthreads();
+            if (group == 0 && i < a.n) {
+                double ku = s_u[0][lane], kv = s_v[0][lane];
+                for (int g = 1; g < 8; ++g) {
+                    ku += s_u[g][lane];
+                    kv += s_v[g][lane];
+                }
+                finish_target<MODE>(a, i, ku, kv, dt, local_max);
             }
-            if (!isfinite(ku) || !isfinite(kv)) {
-                const int verdict =
-                    slow_target(a.g, a.ex, a.ey, a.gamma, a.n_src, a.t_offset + i, ku, kv);
-                if (verdict == ST_COINCIDENT || (verdict && !a.nonfinite_ok))
-                    set_status(&a.ctl->status, verdict);
-            }
-            a.kx[a.s][i] = ku;
-            a.ky[a.s][i] = kv;
-        } else {
-            ku = a.kx[a.s][i];
-            kv = a.ky[a.s][i];
+            __syncthreads();
         }
-        if (MODE == STAGE_POSITION) {
-            // makeStage, src/timestep.cpp:19-30 (zero coefficients add an exact zero: skipped)
-            double dx = 0.0, dy = 0.0;
-            for (int j = 0; j < a.ncoef; ++j) {
-                const double c = a.coef[j];
-                if (c == 0.0)
-                    continue;
-                const double kxj = j == a.s ? ku : a.kx[j][i];
-                const double kyj = j == a.s ? kv : a.ky[j][i];
-                dx = __dadd_rn(dx, __dmul_rn(c, kxj));
-                dy = __dadd_rn(dy, __dmul_rn(c, kyj));
-            }
-            const double nx = __dadd_rn(a.x0[i], __dmul_rn(dt, dx));
-            const double ny = __dadd_rn(a.y0[i], __dmul_rn(dt, dy));
-            a.xt[i] = nx;
-            a.yt[i] = ny;
-            validate_position(a, nx, ny);
-        } else if (MODE == STAGE_RK4_COMBINE) {
-            // src/timestep.cpp:52-57: x0 + dt * (k1 + 2 k2 + 2 k3 + k4) / 6
-            const double sx = __dadd_rn(__dadd_rn(__dadd_rn(a.kx[0][i], __dmul_rn(2.0, a.kx[1][i])),
-                                                  __dmul_rn(2.0, a.kx[2][i])),
-                                        ku);
-            const double sy = __dadd_rn(__dadd_rn(__dadd_rn(a.ky[0][i], __dmul_rn(2.0, a.ky[1][i])),
-                                                  __dmul_rn(2.0, a.ky[2][i])),
-                                        kv);
-            const double nx = __dadd_rn(a.x0[i], __ddiv_rn(__dmul_rn(dt, sx), 6.0));
-            const double ny = __dadd_rn(a.y0[i], __ddiv_rn(__dmul_rn(dt, sy), 6.0));
-            a.xt[i] = nx;
-            a.yt[i] = ny;
-            if (!isfinite(nx) || !isfinite(ny))
-                set_status(&a.ctl->status, ST_NONFINITE_POSITION);
-        } else if (MODE == STAGE_DOPRI_ERROR) {
-            // src/timestep.cpp:78-95: xt holds the fifth-order point y5 (stage 7's position).
-            double xe = 0.0, ye = 0.0;
-            for (int j = 0; j < 7; ++j) {
-                const double w = a.w[j];
-                if (w == 0.0)
-                    continue;
-                const double h = __dmul_rn(dt, w);
-                const double kxj = j == a.s ? ku : a.kx[j][i];
-                const double kyj = j == a.s ? kv : a.ky[j][i];
-                xe = __dadd_rn(xe, __dmul_rn(h, kxj));
-                ye = __dadd_rn(ye, __dmul_rn(h, kyj));
-            }
-            const double x5 = a.xt[i], y5 = a.yt[i];
-            const double xs = __dadd_rn(a.ctl->absolute_tolerance,
-                                        __dmul_rn(a.ctl->relative_tolerance,
-                                                  max_ref(fabs(a.x0[i]), fabs(x5))));
-            const double ys = __dadd_rn(a.ctl->absolute_tolerance,
-                                        __dmul_rn(a.ctl->relative_tolerance,
-                                                  max_ref(fabs(a.y0[i]), fabs(y5))));
-            if (!isfinite(xe) || !isfinite(ye) || !isfinite(xs) || !isfinite(ys) ||
-                !(xs > 0.0) || !(ys > 0.0)) {
-                set_status(&a.ctl->status, ST_DOPRI_NONFINITE);
+    } else {
+        for (size_t i = blockIdx.x * static_cast<size_t>(blockDim.x) + tid; i < a.n;
+             i += static_cast<size_t>(gridDim.x) * blockDim.x) {
+            double ku, kv;
+            if (a.reduce) {
+                ku = 0.0;
+                kv = 0.0;
+                for (int c = 0; c < a.num_chunks; ++c) {
+                    ku += a.pu[static_cast<size_t>(c) * a.stride + i];
+                    kv += a.pv[static_cast<size_t>(c) * a.stride + i];
+                }
             } else {
-                local_max = max_ref(local_max, __ddiv_rn(fabs(xe), xs));
-                local_max = max_ref(local_max, __ddiv_rn(fabs(ye), ys));
+                ku = a.kx[a.s][i];
+                kv = a.ky[a.s][i];
             }
+            finish_target<MODE>(a, i, ku, kv, dt, local_max);
         }
     }
 
@@ -207,25 +247,35 @@ unsigned grid_for(size_t n, int sm_count) {
 }
 } // namespace
 
+// Partial rows from which a block of 32 targets x 8 row groups beats one thread per target.
+constexpr int kWideRows = 32;
+
+template <int MODE>
+cudaError_t launch_stage_mode(const StageArgs &a, cudaStream_t stream, int sm_count) {
+    if (a.reduce && a.num_chunks >= kWideRows) {
+        const size_t blocks = (a.n + 31) / 32;
+        const size_t cap = static_cast<size_t>(sm_count > 0 ? sm_count : 148) * 8;
+        const unsigned grid = static_cast<unsigned>(blocks < 1 ? 1 : (blocks < cap ? blocks : cap));
+        stage_kernel<MODE, true><<<grid, 256, 0, stream>>>(a);
+    } else {
+        stage_kernel<MODE, false><<<grid_for(a.n, sm_count), 256, 0, stream>>>(a);
+    }
+    return cudaGetLastError();
+}
+
 cudaError_t launch_stage(const StageArgs &a, cudaStream_t stream, int sm_count) {
-    const unsigned grid = grid_for(a.n, sm_count);
     switch (a.mode) {
     case STAGE_REDUCE_ONLY:
-        stage_kernel<STAGE_REDUCE_ONLY><<<grid, 256, 0, stream>>>(a);
-        break;
+        return launch_stage_mode<STAGE_REDUCE_ONLY>(a, stream, sm_count);
     case STAGE_POSITION:
-        stage_kernel<STAGE_POSITION><<<grid, 256, 0, stream>>>(a);
-        break;
+        return launch_stage_mode<STAGE_POSITION>(a, stream, sm_count);
     case STAGE_RK4_COMBINE:
-        stage_kernel<STAGE_RK4_COMBINE><<<grid, 256, 0, stream>>>(a);
-        break;
+        return launch_stage_mode<STAGE_RK4_COMBINE>(a, stream, sm_count);
     case STAGE_DOPRI_ERROR:
-        stage_kernel<STAGE_DOPRI_ERROR><<<grid, 256, 0, stream>>>(a);
-        break;
+        return launch_stage_mode<STAGE_DOPRI_ERROR>(a, stream, sm_count);
     default:
         return cudaErrorInvalidValue;
     }
-    return cudaGetLastError();
 }
 
 cudaError_t launch_accept(double *x, double *y, const double *xt, const double *yt, double *k0x,
