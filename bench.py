@@ -520,11 +520,10 @@ def run_serving(budget: int = 10) -> dict:
     for rate, count, policy in ((10.0, 30, "split"), (100.0, 200, "split"), (100.0, 200, "fifo"),
                                 (1000.0, 600, "split")):
         reqs = poisson_stream(count, rate, seed=int(rate), max_steps=budget)
-        # split: two batches driven by two host threads on two streams, the expensive one one
-        # attempt per call, the cheap one 16 (the best p50 of a sweep of 1-4 / 2-16 attempts
-        # on the 100 req/s stream at equal throughput)
+        # split: cheap requests batched (16 attempts per call), expensive ones one at a time on
+        # single-simulation contexts (4 steps per call), driven by two host threads
         server = Server(capacity_vortices=4_000_000, max_slots=1024,
-                        attempts_per_tick=1 if policy == "split" else 2, policy=policy)
+                        attempts_per_tick=4 if policy == "split" else 2, policy=policy)
         summary = server.serve(reqs)
         server.close()
         summary["rate_per_s"] = rate

@@ -514,9 +514,14 @@ struct StageBatchArgs {
 
 __global__ void __launch_bounds__(256) batch_stage_kernel(const StageBatchArgs a) {
     __shared__ double s_max[8];
+    __shared__ int s_skip;
     const SliceEntry sl = a.slices[blockIdx.x];
     SimControl &c = a.ctl[sl.sim];
-    if (c.state != SIM_RUNNING || c.status != 0)
+    // one decision for the whole block (other blocks may raise the status meanwhile)
+    if (threadIdx.x == 0)
+        s_skip = c.state != SIM_RUNNING || *reinterpret_cast<volatile int *>(&c.status) != 0;
+    __syncthreads();
+    if (s_skip)
         return;
     const SimDesc &d = a.descs[sl.sim];
     const size_t i = sl.start + threadIdx.x;
@@ -526,15 +531,50 @@ __global__ void __launch_bounds__(256) batch_stage_kernel(const StageBatchArgs a
     const double *ey = (s == 0 ? a.arena.y : a.arena.py[(s - 1) & 1]) + d.off;
     const double dt = c.dt_attempt;
     double local_max = 0.0;
+    const bool reduce = s > 0 || !c.fsal;  // uniform over the block: one simulation per slice
+    double wide_u = 0.0, wide_v = 0.0;
+    if (reduce && d.num_chunks >= 32) {
+        // many partial rows (symmetric items): for each 32 targets of the slice, the 8 warps
+        // each sum every 8th row, coalesced, and the targets' own warp adds the 8 group sums
+        // in fixed order
+        __shared__ double s_u[8][32], s_v[8][32];
+        const int lane = threadIdx.x & 31, group = threadIdx.x >> 5;
+        for (int pass = 0; pass < 8; ++pass) {
+            const size_t t = sl.start + static_cast<size_t>(pass) * 32 + lane;
+            double su = 0.0, sv = 0.0;
+            if (t < d.n)
+                for (unsigned ch = group; ch < d.num_chunks; ch += 8) {
+                    su += a.arena.pu[d.part_off + static_cast<size_t>(ch) * d.pad_n + t];
+                    sv += a.arena.pv[d.part_off + static_cast<size_t>(ch) * d.pad_n + t];
+                }
+            s_u[group][lane] = su;
+            s_v[group][lane] = sv;
+            __syncthreads();
+            if (group == pass) {
+                wide_u = s_u[0][lane];
+                wide_v = s_v[0][lane];
+                for (int g = 1; g < 8; ++g) {
+                    wide_u += s_u[g][lane];
+                    wide_v += s_v[g][lane];
+                }
+            }
+            __syncthreads();
+        }
+    }
     if (inside) {
         const size_t e = d.off + i;
         double ku, kv;
-        if (s > 0 || !c.fsal) {
+        if (reduce) {
             ku = 0.0;
             kv = 0.0;
-            for (unsigned ch = 0; ch < d.num_chunks; ++ch) {
-                ku += a.arena.pu[d.part_off + static_cast<size_t>(ch) * d.pad_n + i];
-                kv += a.arena.pv[d.part_off + static_cast<size_t>(ch) * d.pad_n + i];
+            if (d.num_chunks >= 32) {
+                ku = wide_u;
+                kv = wide_v;
+            } else {
+                for (unsigned ch = 0; ch < d.num_chunks; ++ch) {
+                    ku += a.arena.pu[d.part_off + static_cast<size_t>(ch) * d.pad_n + i];
+                    kv += a.arena.pv[d.part_off + static_cast<size_t>(ch) * d.pad_n + i];
+                }
             }
             if (!isfinite(ku) || !isfinite(kv)) {
                 const int verdict = slow_target(d.g, ex, ey, a.arena.gamma + d.off, d.n, i, ku, kv);

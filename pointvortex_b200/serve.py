@@ -100,18 +100,134 @@ class _Lane:
         self.ready: list = []            # (arrival, rid, request), arrival order
         self.running: dict[int, tuple] = {}
 
+    def admit(self, server: "Server", now: float) -> int:
+        return server._admit_lane(self, now)
+
+    def advance(self) -> None:
+        self.batch.advance(self.attempts)
+
+    def retire(self, server: "Server", now: float, on_complete) -> int:
+        return server._retire(self, now, on_complete)
+
+    def close(self) -> None:
+        self.batch.close()
+
+
+class _Solver:
+    """The reference driver's DOPRI5 loop (src/main.cpp:310-343, without output events) for one
+    request on a single-simulation context: its own step size, end-time landing and budget."""
+
+    def __init__(self, kernels: dict, req: Request):
+        from .kernel import VortexSystem
+        self.req = req
+        self.k = kernels[req.geometry]
+        x, y, g = req.state()
+        self.k.uploadDeviceState(VortexSystem(x, y, g))
+        self.t, self.dt, self.steps = 0.0, min(max(req.dt, 1e-12), 0.1), 0
+        self.state: Optional[str] = None
+        self.evals0 = self.k.evaluationCount
+
+    def step(self) -> bool:
+        """One accepted step; True once the solve has ended (done, budget or failed)."""
+        req = self.req
+        if self.t >= req.t_end:
+            self.state = "done"
+            return True
+        if req.max_steps and self.steps >= req.max_steps:
+            self.state = "budget"
+            return True
+        try:
+            r = self.k.deviceDopri5Step(min(self.dt, req.t_end - self.t), req.atol, req.rtol,
+                                        1e-12, 0.1)
+        except (RuntimeError, ValueError):
+            self.state = "failed"
+            return True
+        self.t += r.acceptedTimeStep
+        self.dt = r.suggestedTimeStep
+        self.steps += 1
+        if self.t + 16 * np.finfo(float).eps * abs(self.t) >= req.t_end:
+            self.t = req.t_end
+        return False
+
+    def pairs(self) -> float:
+        return float(self.k.evaluationCount - self.evals0) * self.req.n * (self.req.n - 1)
+
+    def positions(self):
+        from .kernel import VortexSystem
+        n = self.k.stateSize()
+        st = VortexSystem(np.zeros(n), np.zeros(n), np.zeros(n))
+        self.k.downloadDeviceState(st)
+        return st.x, st.y
+
+
+def _contexts(device: int) -> dict:
+    from .kernel import DiskKernel, InfinitePlaneKernel, PeriodicBoxKernel
+    return {"infinite": InfinitePlaneKernel(0.0, device=device),
+            "periodic": PeriodicBoxKernel(2 * np.pi, 2 * np.pi, 8, device=device),
+            "disk": DiskKernel(1.0, device=device)}
+
+
+class _ContextLane:
+    """Expensive requests, one at a time, each on a single-simulation context: one such request
+    fills the GPU by itself, and the context runs the fastest kernels for it (the periodic box
+    once per unordered pair)."""
+
+    def __init__(self, device: int, steps_per_call: int):
+        self.kernels = _contexts(device)
+        self.steps_per_call = steps_per_call
+        self.ready: list = []
+        self.current: Optional[tuple] = None   # (solver, admitted at)
+        self.running: dict = {}
+
+    def admit(self, server: "Server", now: float) -> int:
+        if self.current is not None or not self.ready:
+            return 0
+        _, _, req = self.ready.pop(0)
+        self.current = (_Solver(self.kernels, req), now)
+        self.running = {req.rid: self.current}
+        return 1
+
+    def advance(self) -> None:
+        solver = self.current[0]
+        for _ in range(self.steps_per_call):
+            if solver.step():
+                break
+
+    def retire(self, server: "Server", now: float, on_complete) -> int:
+        solver = self.current[0]
+        if solver.state is None:
+            return 0
+        req = solver.req
+        x = y = None
+        if server.keep_states or on_complete is not None:
+            x, y = solver.positions()
+        c = Completion(req.rid, solver.state, now - req.arrival, solver.steps, solver.t,
+                       x if server.keep_states else None, y if server.keep_states else None,
+                       solver.pairs())
+        server.completions.append(c)
+        if on_complete is not None:
+            on_complete(c, x, y)
+        self.current = None
+        self.running = {}
+        return 1
+
+    def close(self) -> None:
+        for k in self.kernels.values():
+            k.close()
+
 
 class Server:
     """Continuous batching. policy "fifo": one batch, requests admitted in arrival order.
     policy "split" (admission by estimated work): requests whose evaluation costs at most
-    `split_work` plane-pair units go to a small-request batch that takes `small_attempts`
-    attempts for each attempt of the large-request batch, so that short requests are not held to
-    the pace of the largest ones in a lock-step attempt. Within a batch the order is FIFO."""
+    `split_work` plane-pair units go to the batch, which takes `small_attempts` attempts per
+    call; the expensive ones, each of which fills the GPU alone, are solved one at a time on
+    single-simulation contexts (`attempts_per_tick` steps per call). Two host threads drive the
+    two on their own streams, so cheap requests are never held to the pace of an expensive one.
+    Within each the order is FIFO."""
 
     def __init__(self, capacity_vortices: int, max_slots: int, attempts_per_tick: int = 4,
                  device: int = 0, keep_states: bool = False, policy: str = "fifo",
-                 split_work: float = 2.0 ** 26, small_attempts: int = 16,
-                 small_fraction: float = 0.25):
+                 split_work: float = 2.0 ** 26, small_attempts: int = 16):
         if policy not in ("fifo", "split"):
             raise ValueError("policy must be fifo or split")
         self.policy = policy
@@ -122,11 +238,8 @@ class Server:
         if policy == "fifo":
             self.lanes = [_Lane(capacity_vortices, max_slots, device, attempts_per_tick)]
         else:
-            small_cap = max(int(capacity_vortices * small_fraction), 4096)
-            small_slots = max(max_slots // 2, 1)
-            self.lanes = [_Lane(small_cap, small_slots, device, small_attempts),
-                          _Lane(capacity_vortices - small_cap, max(max_slots - small_slots, 1),
-                                device, attempts_per_tick)]
+            self.lanes = [_Lane(capacity_vortices, max_slots, device, small_attempts),
+                          _ContextLane(device, attempts_per_tick)]
 
     @property
     def batch(self) -> Batch:
@@ -135,7 +248,7 @@ class Server:
     def submit(self, req: Request) -> None:
         heapq.heappush(self.arrivals, (req.arrival, req.rid, req))
 
-    def _lane_of(self, req: Request) -> _Lane:
+    def _lane_of(self, req: Request):
         if self.policy == "split" and work(req) > self.split_work:
             return self.lanes[1]
         return self.lanes[0]
@@ -222,19 +335,19 @@ class Server:
         finished = threading.Event()
         errors: list = []
 
-        def drive(lane: _Lane) -> None:
+        def drive(lane) -> None:
             try:
                 while not finished.is_set():
                     with lock:
                         self._route(clock() - start)
-                        self._admit_lane(lane, clock() - start)
+                        lane.admit(self, clock() - start)
                         idle = not lane.running
                     if idle:
                         time.sleep(0.0005)
                         continue
-                    lane.batch.advance(lane.attempts)   # the GIL is released during the call
+                    lane.advance()   # the GIL is released inside the library calls
                     with lock:
-                        self._retire(lane, clock() - start, on_complete)
+                        lane.retire(self, clock() - start, on_complete)
                         if len(self.completions) >= total:
                             finished.set()
             except BaseException as exc:  # surfaced to the caller below
@@ -251,7 +364,7 @@ class Server:
 
     def close(self):
         for lane in self.lanes:
-            lane.batch.close()
+            lane.close()
 
 
 def summarize(completions: list[Completion], elapsed: float) -> dict:
@@ -270,35 +383,18 @@ def summarize(completions: list[Completion], elapsed: float) -> dict:
 def one_at_a_time(requests: list[Request], device: int = 0, clock=time.perf_counter) -> dict:
     """FIFO baseline: each request solved alone through the single-simulation context API
     (pv_upload_state + pv_dopri5_step per step), in arrival order."""
-    from .kernel import DiskKernel, InfinitePlaneKernel, PeriodicBoxKernel, VortexSystem
-    kernels = {"infinite": InfinitePlaneKernel(0.0, device=device),
-               "periodic": PeriodicBoxKernel(2 * np.pi, 2 * np.pi, 8, device=device),
-               "disk": DiskKernel(1.0, device=device)}
+    kernels = _contexts(device)
     out = []
     start = clock()
     for req in sorted(requests, key=lambda r: r.arrival):
         now = clock() - start
         if req.arrival > now:
             time.sleep(req.arrival - now)
-        k = kernels[req.geometry]
-        x, y, g = req.state()
-        k.uploadDeviceState(VortexSystem(x, y, g))
-        t, dt, steps, state = 0.0, min(max(req.dt, 1e-12), 0.1), 0, "done"
-        evals_before = k.evaluationCount
-        try:
-            while t < req.t_end:
-                if req.max_steps and steps >= req.max_steps:
-                    state = "budget"
-                    break
-                r = k.deviceDopri5Step(min(dt, req.t_end - t), req.atol, req.rtol, 1e-12, 0.1)
-                t += r.acceptedTimeStep
-                dt = r.suggestedTimeStep
-                steps += 1
-                if t + 16 * np.finfo(float).eps * abs(t) >= req.t_end:
-                    t = req.t_end
-        except (RuntimeError, ValueError):
-            state = "failed"
-        evals = k.evaluationCount - evals_before
-        out.append(Completion(req.rid, state, clock() - start - req.arrival, steps, t,
-                              pairs=float(evals) * req.n * (req.n - 1)))
+        solver = _Solver(kernels, req)
+        while not solver.step():
+            pass
+        out.append(Completion(req.rid, solver.state, clock() - start - req.arrival, solver.steps,
+                              solver.t, pairs=solver.pairs()))
+    for k in kernels.values():
+        k.close()
     return summarize(out, clock() - start)
