@@ -463,8 +463,8 @@ pv_status ensure_state_capacity(pv_context *c, size_t n) {
     }
     c->plan = plan_evaluation(c->gc.geometry, n, n, c->sm_count, 0, c->params.precision);
     c->sym = SymmetricPlan{};
-    if (c->gc.geometry == GEO_PERIODIC && c->params.precision == PV_PRECISION_FP64)
-        c->sym = plan_symmetric(n, c->sm_count);
+    if (c->gc.geometry == GEO_PERIODIC)
+        c->sym = plan_symmetric(n, c->sm_count, c->params.precision);
     const size_t rows = c->sym.enabled() ? static_cast<size_t>(c->sym.blocks)
                                          : static_cast<size_t>(c->plan.num_chunks);
     const size_t partial = rows * np;

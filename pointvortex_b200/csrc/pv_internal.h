@@ -54,11 +54,12 @@ struct SymmetricPlan {
     int blocks = 0;      // partial rows
     unsigned items = 0;  // block pairs (I <= J)
     int grid = 0;        // persistent CTAs
+    int precision = 0;   // PV_PRECISION_FP64 or PV_PRECISION_FP32C
     bool enabled() const { return a > 0; }
 };
 constexpr size_t kSymmetricMinN = 2048;                            // below: the ordered kernel
 constexpr size_t kSymmetricPartialBytes = static_cast<size_t>(256) << 20;
-SymmetricPlan plan_symmetric(size_t n, int sm_count);
+SymmetricPlan plan_symmetric(size_t n, int sm_count, int precision);
 void symmetric_items(const SymmetricPlan &p, unsigned *out);  // p.items packed (I << 16) | J
 cudaError_t launch_periodic_symmetric(const double *x, const double *y, const double *gs, size_t n,
                                       const SymmetricPlan &p, const unsigned *items,

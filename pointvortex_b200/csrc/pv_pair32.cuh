@@ -114,6 +114,31 @@ struct Target32 {
     double x, y;
 };
 
+// The periodic pair's terms without its circulation, in FP32: the target's velocity changes by
+// u -= g_s ku, v += g_s kv. t and s are (x_hi, y_hi, x_lo, y_lo). Exchanging target and source
+// negates the displacement exactly, and every quantity below is an exactly odd or even function
+// of it, so ku and kv are exactly odd: the symmetric kernels use one evaluation for both.
+__device__ __forceinline__ void periodic_values32(const F32Geometry &f, const float4 t,
+                                                  const float4 s, float &ku, float &kv) {
+    const float dx = (t.x - s.x) + (t.z - s.z);
+    const float dy = (t.y - s.y) + (t.w - s.w);
+    const float hx = half_angle_f32(f, dx), hy = half_angle_f32(f, dy);
+    float shx, chx, snx, csx, shy, chy, sny, csy;
+    shcs_f32(hx, shx, chx, snx, csx);
+    shcs_f32(hy, shy, chy, sny, csy);
+    const float cosh_x = fmaf(2.0f * shx, shx, 1.0f), cosh_y = fmaf(2.0f * shy, shy, 1.0f);
+    const float cos_x = fmaf(-2.0f * snx, snx, 1.0f), cos_y = fmaf(-2.0f * sny, sny, 1.0f);
+    const float sin_x = 2.0f * snx * csx, sin_y = 2.0f * sny * csy;
+    const float sinh_x = 2.0f * shx * chx, sinh_y = 2.0f * shy * chy;
+    const float d0u = 2.0f * fmaf(shx, shx, sny * sny);
+    const float d0v = 2.0f * fmaf(shy, shy, snx * snx);
+    float nu, du, ru, nv, dv, rv;
+    image_sum_f32(f, hx, cosh_x, sinh_x, cos_y, nu, du, ru);
+    image_sum_f32(f, hy, cosh_y, sinh_y, cos_x, nv, dv, rv);
+    ku = sin_y * fmaf(d0u, fmaf(du, ru, nu), du) * rcp_approx_f32(d0u * du);
+    kv = sin_x * fmaf(d0v, fmaf(dv, rv, nv), dv) * rcp_approx_f32(d0v * dv);
+}
+
 template <int GEO, bool CHECK>
 __device__ __forceinline__ void pair32(const F32Geometry &f, const GeometryConsts &g,
                                        const Target32 &t, const float4 s, float sgf, double sxd,

@@ -20,6 +20,7 @@
 //   * partial sums go to rows of a [blocks][N] array: vortices of block I receive row J from item
 //     (I, J), vortices of block J receive row I, and each (row, vortex) is written exactly once,
 //     so the stage kernel's fixed-order sum over rows keeps results deterministic.
+#include "pvb200.h"
 #include "pv_internal.h"
 #include "pv_symmetric.cuh"
 
@@ -96,25 +97,111 @@ __global__ void __launch_bounds__(kThreads)
     }
 }
 
-int resident_ctas(int a) {
-    static int cached[17] = {};
+// The FP32-compensated form of the same decomposition: the pair terms on the FP32 pipe from
+// double-float coordinates; each tile's FP32 sums (32 sources) are promoted into FP64.
+__global__ void __launch_bounds__(kThreads)
+    periodic_symmetric32_kernel(const double *__restrict__ x, const double *__restrict__ y,
+                                const double *__restrict__ gs, size_t n, int a,
+                                const unsigned *__restrict__ items, unsigned n_items,
+                                unsigned *counter, double *__restrict__ pu,
+                                double *__restrict__ pv, size_t stride, GeometryConsts g) {
+    extern __shared__ double2 reaction_smem[];
+    __shared__ float4 src_f[kThreads];
+    __shared__ float src_g[kThreads];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    double2 *reaction = reaction_smem + warp * a * 32;
+    float4 *sf = src_f + warp * 32;
+    float *sgf = src_g + warp * 32;
+    const f32::F32Geometry f = f32::make_f32(g);
+    const size_t block_len = static_cast<size_t>(32) * a;
+    for (;;) {
+        unsigned item = 0;
+        if (lane == 0)
+            item = atomicAdd(counter, 1u);
+        item = __shfl_sync(0xffffffffu, item, 0);
+        if (item >= n_items)
+            break;
+        const unsigned packed = items[item];
+        const unsigned I = packed >> 16, J = packed & 0xffffu;
+        const bool diagonal = I == J;
+        for (int jb = 0; jb < a; ++jb)
+            reaction[jb * 32 + lane] = make_double2(0.0, 0.0);
+        for (int ib = 0; ib < a; ++ib) {
+            const size_t t0 = I * block_len + static_cast<size_t>(ib) * 32;
+            const size_t ti = t0 + lane;
+            const bool t_ok = ti < n;
+            const float4 t = sym::split32(t_ok ? x[ti] : 0.0, t_ok ? y[ti] : 0.0);
+            const float tg = t_ok ? static_cast<float>(gs[ti]) : 0.0f;
+            double ud = 0.0, vd = 0.0;
+            for (int jb = diagonal ? ib : 0; jb < a; ++jb) {
+                const size_t j0 = J * block_len + static_cast<size_t>(jb) * 32;
+                const size_t sj = j0 + lane;
+                const int s_count = j0 < n ? static_cast<int>(min(static_cast<size_t>(32), n - j0)) : 0;
+                __syncwarp();  // the previous tile's reads of the buffer are done
+                sf[lane] = sym::split32(sj < n ? x[sj] : 0.0, sj < n ? y[sj] : 0.0);
+                sgf[lane] = sj < n ? static_cast<float>(gs[sj]) : 0.0f;
+                __syncwarp();
+                float u = 0.0f, v = 0.0f;
+                if (diagonal && jb == ib) {
+                    sym::one_sided_tile32(f, t, t_ok, sf, sgf, s_count, true, u, v);
+                } else {
+                    float ru = 0.0f, rv = 0.0f;
+                    sym::react_tile32(f, t, tg, t_ok, sf, sgf, s_count, u, v, ru, rv);
+                    double2 r = reaction[jb * 32 + lane];
+                    r.x += static_cast<double>(ru);
+                    r.y += static_cast<double>(rv);
+                    reaction[jb * 32 + lane] = r;
+                }
+                ud += static_cast<double>(u);
+                vd += static_cast<double>(v);
+            }
+            if (diagonal) {
+                const double2 r = reaction[ib * 32 + lane];
+                ud += r.x;
+                vd += r.y;
+            }
+            if (t_ok) {
+                pu[J * stride + ti] = ud;
+                pv[J * stride + ti] = vd;
+            }
+        }
+        if (!diagonal) {
+            for (int jb = 0; jb < a; ++jb) {
+                const size_t sj = J * block_len + static_cast<size_t>(jb) * 32 + lane;
+                if (sj < n) {
+                    const double2 r = reaction[jb * 32 + lane];
+                    pu[I * stride + sj] = r.x;
+                    pv[I * stride + sj] = r.y;
+                }
+            }
+        }
+        __syncwarp();
+    }
+}
+
+int resident_ctas(int a, int precision) {
+    static int cached[2][17] = {};
     if (a < 1 || a > 16)
         return 1;
-    if (!cached[a]) {
+    const int q = precision == PV_PRECISION_FP32C ? 1 : 0;
+    if (!cached[q][a]) {
         int blocks = 0;
         const size_t smem = static_cast<size_t>(kThreads / 32) * a * 32 * sizeof(double2);
-        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, periodic_symmetric_kernel,
-                                                          kThreads, smem) != cudaSuccess ||
-            blocks < 1)
+        const cudaError_t e =
+            q ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, periodic_symmetric32_kernel,
+                                                              kThreads, smem)
+              : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, periodic_symmetric_kernel,
+                                                              kThreads, smem);
+        if (e != cudaSuccess || blocks < 1)
             blocks = 1;
-        cached[a] = blocks;
+        cached[q][a] = blocks;
     }
-    return cached[a];
+    return cached[q][a];
 }
 
 }  // namespace
 
-SymmetricPlan plan_symmetric(size_t n, int sm_count) {
+SymmetricPlan plan_symmetric(size_t n, int sm_count, int precision) {
     SymmetricPlan p{};
     if (n < kSymmetricMinN)
         return p;
@@ -128,7 +215,8 @@ SymmetricPlan plan_symmetric(size_t n, int sm_count) {
             p.a = a;
             p.blocks = static_cast<int>(blocks);
             p.items = static_cast<unsigned>(blocks * (blocks + 1) / 2);
-            p.grid = std::max(sm_count, 1) * resident_ctas(a);
+            p.grid = std::max(sm_count, 1) * resident_ctas(a, precision);
+            p.precision = precision;
             return p;
         }
     }
@@ -150,8 +238,12 @@ cudaError_t launch_periodic_symmetric(const double *x, const double *y, const do
     if (e != cudaSuccess)
         return e;
     const size_t smem = static_cast<size_t>(kThreads / 32) * p.a * 32 * sizeof(double2);
-    periodic_symmetric_kernel<<<p.grid, kThreads, smem, stream>>>(x, y, gs, n, p.a, items, p.items,
-                                                                  counter, pu, pv, stride, g);
+    if (p.precision == PV_PRECISION_FP32C)
+        periodic_symmetric32_kernel<<<p.grid, kThreads, smem, stream>>>(
+            x, y, gs, n, p.a, items, p.items, counter, pu, pv, stride, g);
+    else
+        periodic_symmetric_kernel<<<p.grid, kThreads, smem, stream>>>(
+            x, y, gs, n, p.a, items, p.items, counter, pu, pv, stride, g);
     return cudaGetLastError();
 }
 

@@ -10,6 +10,7 @@
 #pragma once
 
 #include "pv_geometry.cuh"
+#include "pv_pair32.cuh"
 
 namespace pvb {
 namespace sym {
@@ -69,6 +70,53 @@ __device__ __forceinline__ void one_sided_tile(const GeometryConsts &g, double t
         sg2 = rotate(sg2, next);
         s_ok = __shfl_sync(0xffffffffu, s_ok, next);
     }
+}
+
+// FP32-compensated tiles: the 32 sources (hi/lo coordinates and FP32 circulation) sit in this
+// warp's shared buffer, read at index (lane + k) & 31; only their FP32 reactions rotate through
+// the lanes. The callers promote the FP32 sums of each tile into FP64.
+__device__ __forceinline__ void react_tile32(const f32::F32Geometry &f, const float4 t, float tg,
+                                             bool t_ok, const float4 *sf, const float *sg,
+                                             int s_count, float &u, float &v, float &ru,
+                                             float &rv) {
+    const int lane = threadIdx.x & 31, next = (lane + 1) & 31;
+    for (int k = 0; k < 32; ++k) {
+        const int j = (lane + k) & 31;
+        if (t_ok && j < s_count) {
+            float ku, kv;
+            f32::periodic_values32(f, t, sf[j], ku, kv);
+            const float g = sg[j];
+            u = fmaf(-g, ku, u);
+            v = fmaf(g, kv, v);
+            ru = fmaf(tg, ku, ru);
+            rv = fmaf(-tg, kv, rv);
+        }
+        ru = __shfl_sync(0xffffffffu, ru, next);
+        rv = __shfl_sync(0xffffffffu, rv, next);
+    }
+}
+
+__device__ __forceinline__ void one_sided_tile32(const f32::F32Geometry &f, const float4 t,
+                                                 bool t_ok, const float4 *sf, const float *sg,
+                                                 int s_count, bool same_block, float &u,
+                                                 float &v) {
+    const int lane = threadIdx.x & 31;
+    for (int k = same_block ? 1 : 0; k < 32; ++k) {
+        const int j = (lane + k) & 31;
+        if (t_ok && j < s_count) {
+            float ku, kv;
+            f32::periodic_values32(f, t, sf[j], ku, kv);
+            u = fmaf(-sg[j], ku, u);
+            v = fmaf(sg[j], kv, v);
+        }
+    }
+}
+
+// (x_hi, y_hi, x_lo, y_lo) of a double position.
+__device__ __forceinline__ float4 split32(double x, double y) {
+    const float xh = static_cast<float>(x), yh = static_cast<float>(y);
+    return make_float4(xh, yh, static_cast<float>(x - static_cast<double>(xh)),
+                       static_cast<float>(y - static_cast<double>(yh)));
 }
 
 }  // namespace sym

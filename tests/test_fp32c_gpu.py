@@ -79,3 +79,23 @@ def test_fp32c_steps_track_fp64():
     # five steps of 1e-4 with Gaussian circulations (speeds up to ~1e3): FP32-level velocity
     # differences move the vortices by ~1e-7 at most
     assert np.max(np.hypot(out[0].x - out[1].x, out[0].y - out[1].y)) < 1e-6
+
+
+@pytest.mark.parametrize("n", [2082, 4096])
+def test_fp32c_symmetric_periodic_against_fp64_oracle(reference, n):
+    """From N = 2048 the compensated periodic evaluation of the device state runs once per
+    unordered pair (its FP32 terms are exactly odd as well); same bounds as the ordered form."""
+    x, y, g = state("periodic", n, 70 + n)
+    k = kernel("periodic")
+    k.uploadDeviceState(pv.VortexSystem(x, y, g))
+    assert k.statePlan()["symmetric"]
+    f = k.evaluateDeviceState()
+    geo = Geometry("periodic", box_length_x=2 * np.pi, box_length_y=2 * np.pi)
+    ur, vr = reference.evaluate(geo, x, y, g)
+    err = normalized_error(f.x, f.y, ur, vr)
+    mx, rms = BOUNDS["periodic"]
+    print(f"symmetric periodic n={n}: fp32c error max {err.max():.2e} "
+          f"rms {np.sqrt(np.mean(err**2)):.2e}")
+    assert err.max() <= mx and np.sqrt(np.mean(err ** 2)) <= rms
+    ordered = k.evaluate(x, y, g)   # host arrays: the ordered FP32C kernel
+    assert normalized_error(f.x, f.y, ordered.x, ordered.y).max() <= mx
