@@ -535,6 +535,70 @@ def run_serving(budget: int = 10) -> dict:
     return out
 
 
+def run_other_configs() -> dict:
+    """The other single-simulation configurations, timed on the device (CUDA events of the
+    library's launches):
+    * infinite plane N = 1024, RK4 dt = 1e-3, 100 steps (pv_rk4_advance): pair-interactions/s
+      and the invariants' drift over the run;
+    * disk N = 16384 (Gaussian circulations), plain FP64 and FP32-compensated evaluations:
+      pair-interactions/s of each and the FP32C velocity's error against the FP64 one. Its RK4
+      run at dt = 5e-4 leaves the disk at step 1 in the reference, and here alike (reported)."""
+    import torch
+    import pointvortex_b200 as pv
+    from pointvortex_b200 import ics
+    out = {}
+    x, y, g = ics.workload_state("infinite_rk4_n1024")
+    k = pv.InfinitePlaneKernel(0.0)
+    k.uploadDeviceState(pv.VortexSystem(x, y, g))
+    inv0 = k.stateInvariants()
+    k.rk4Advance(1e-3, 5)
+    k.uploadDeviceState(pv.VortexSystem(x, y, g))
+    start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    stream = torch.cuda.ExternalStream(k.cudaStream())
+    start.record(stream)
+    k.rk4Advance(1e-3, 100)
+    stop.record(stream)
+    torch.cuda.synchronize()
+    ms = start.elapsed_time(stop)
+    inv1 = k.stateInvariants()
+    out["infinite_rk4_n1024"] = {
+        "steps": 100, "ms": ms, "ms_per_step": ms / 100,
+        "pair_interactions_per_s": 400 * 1024 * 1023 / (ms * 1e-3),
+        "drift": {"circulation": inv1.circulation - inv0.circulation,
+                  "linear_impulse_x": inv1.linearImpulseX - inv0.linearImpulseX,
+                  "linear_impulse_y": inv1.linearImpulseY - inv0.linearImpulseY,
+                  "angular_impulse": inv1.angularImpulse - inv0.angularImpulse,
+                  "hamiltonian": inv1.hamiltonian - inv0.hamiltonian},
+        "note": "the 100 steps are one CUDA graph of a step replayed (pv_rk4_advance)"}
+    x, y, g = ics.workload_state("disk_rk4_n16384")
+    forms = {}
+    vel = {}
+    for name, prec in (("fp64", 0), ("fp32c", 1)):
+        kd = pv.DiskKernel(1.0, precision=prec)
+        kd.uploadDeviceState(pv.VortexSystem(x, y, g))
+        kd.evaluateDeviceState()
+        kd.setProfiling(True)
+        kd.resetKernelStats()
+        for _ in range(10):
+            vel[name] = kd.evaluateDeviceState()
+        st = kd.kernelStats()["velocity"]
+        per = st[2] / max(st[1], 1)
+        forms[name] = {"ms_per_evaluation": per, "pair_interactions_per_s": 16384 * 16383 / (per * 1e-3)}
+        try:
+            kd.deviceRk4Step(5e-4)
+            forms[name]["rk4_step_1"] = "ok"
+        except (RuntimeError, ValueError) as exc:
+            forms[name]["rk4_step_1"] = str(exc)
+    a, b = vel["fp64"], vel["fp32c"]
+    mag = np.hypot(a.x, a.y)
+    scale = np.maximum(mag, np.sqrt(np.mean(mag * mag)))
+    err = np.hypot(b.x - a.x, b.y - a.y) / scale
+    forms["fp32c_vs_fp64_error"] = {"max": float(err.max()), "rms": float(np.sqrt(np.mean(err ** 2)))}
+    forms["speedup"] = forms["fp32c"]["pair_interactions_per_s"] / forms["fp64"]["pair_interactions_per_s"]
+    out["disk_n16384"] = forms
+    return out
+
+
 def run_output(reps: int = 10) -> dict:
     """The reference's text output at GPU rates: one trajectory frame (TrajectoryWriter::write,
     velocity evaluated on the device) and one checkpoint vortex block of the N = 16384 disk
@@ -671,6 +735,10 @@ def main(argv=None):
             result["serving"] = run_serving()
         except Exception as exc:
             result["serving"] = {"error": str(exc)[:200]}
+        try:
+            result["other_configs"] = run_other_configs()
+        except Exception as exc:
+            result["other_configs"] = {"error": str(exc)[:200]}
         try:
             out = run_output()
             inputs = out.pop("inputs")

@@ -899,9 +899,51 @@ pv_status pv_rk4_advance(pv_context *ctx, double dt, uint64_t steps) {
     DeviceGuard guard(ctx->device);
     if ((st = reset_control(ctx)) != PV_OK)
         return st;
-    for (uint64_t k = 0; k < steps; ++k)
-        if ((st = enqueue_rk4(ctx, dt)) != PV_OK)
+    if (ctx->profiling || steps < 4) {
+        for (uint64_t k = 0; k < steps; ++k)
+            if ((st = enqueue_rk4(ctx, dt)) != PV_OK)
+                return st;
+    } else {
+        // one step (9 launches at small N, each a few microseconds) captured as a CUDA graph
+        // and replayed: the step loop is launch-bound below N ~ 10^4
+        uint64_t launches0[PV_KERNEL_KINDS];
+        std::copy(ctx->launches, ctx->launches + PV_KERNEL_KINDS, launches0);
+        const uint64_t evals0 = ctx->evaluations;
+        cudaGraph_t graph = nullptr;
+        cudaGraphExec_t exec = nullptr;
+        PV_CUDA(ctx, cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
+        st = enqueue_rk4(ctx, dt);
+        const cudaError_t e = cudaStreamEndCapture(ctx->stream, &graph);
+        if (st != PV_OK || e != cudaSuccess) {
+            if (graph)
+                cudaGraphDestroy(graph);
+            return st != PV_OK ? st
+                               : fail(ctx, PV_ERROR_CUDA,
+                                      std::string("cudaStreamEndCapture: ") + cudaGetErrorString(e));
+        }
+        const cudaError_t ei = cudaGraphInstantiate(&exec, graph, 0);
+        cudaGraphDestroy(graph);
+        if (ei != cudaSuccess)
+            return fail(ctx, PV_ERROR_CUDA,
+                        std::string("cudaGraphInstantiate: ") + cudaGetErrorString(ei));
+        for (uint64_t k = 0; k < steps; ++k) {
+            const cudaError_t el = cudaGraphLaunch(exec, ctx->stream);
+            if (el != cudaSuccess) {
+                cudaGraphExecDestroy(exec);
+                return fail(ctx, PV_ERROR_CUDA,
+                            std::string("cudaGraphLaunch: ") + cudaGetErrorString(el));
+            }
+        }
+        // the capture counted one step's launches and evaluations
+        for (int kind = 0; kind < PV_KERNEL_KINDS; ++kind)
+            ctx->launches[kind] += (ctx->launches[kind] - launches0[kind]) * (steps - 1);
+        ctx->evaluations += (ctx->evaluations - evals0) * (steps - 1);
+        st = read_control(ctx);
+        cudaGraphExecDestroy(exec);
+        if (st != PV_OK)
             return st;
+        return status_error(ctx, ctx->ctl_host->status);
+    }
     if ((st = read_control(ctx)) != PV_OK)
         return st;
     return status_error(ctx, ctx->ctl_host->status);
