@@ -92,6 +92,7 @@ struct pv_context {
     DeviceArray p0x, p0y, p1x, p1y;  // stage positions (ping-pong)
     DeviceArray kx[7], ky[7];        // stage velocities
     DeviceArray pu, pv;              // chunk partials (or symmetric-kernel rows)
+    cudaGraphExec_t attempt_graph = nullptr; // one DOPRI5 attempt with a valid FSAL derivative
     SymmetricPlan sym{};             // periodic FP64: one evaluation per unordered pair
     DeviceArray sym_items, sym_counter;
     int sym_items_blocks = 0;        // the block count the item table was built for
@@ -111,6 +112,10 @@ struct pv_context {
     uint64_t removed_pairs = 0, reinjected_pairs = 0;
     std::vector<double> gamma_host;  // the device state's circulations (they change only here)
     DeviceArray removed_index;
+    // With removal configured, every DOPRI5 attempt also scans its accepted state for dipoles in
+    // the same synchronisation; pv_dipole_process then needs no GPU work when none was found.
+    bool prescan_valid = false;        // the device state is the one the last scan saw
+    unsigned long long prescan_count = 0;
 
     // text output (pv_format_*): row slots, row lengths, block offsets, the packed frame
     DeviceArray fmt_stage, fmt_len, fmt_block, fmt_out;
@@ -123,10 +128,18 @@ struct pv_context {
     struct Timer {
         cudaEvent_t start, stop;
         int kind;
+        bool in_graph;  // recorded by the captured attempt on every replay; owned by it
     };
     std::vector<Timer> pending, pool;
+    bool capturing = false;             // counted() during a graph capture
+    std::vector<Timer> capture_timers;  // the timers a capture recorded
+    std::vector<Timer> graph_timers;    // those of attempt_graph
+    bool graph_profiled = false;        // attempt_graph records per-launch events
+    std::vector<const void *> graph_key; // buffers and plan attempt_graph was captured for
 
     ~pv_context() {
+        if (attempt_graph)
+            cudaGraphExecDestroy(attempt_graph);
         for (DeviceArray *a : {&x, &y, &gamma, &gs, &p0x, &p0y, &p1x, &p1y, &pu, &pv, &inv_scratch,
                                &inv_out, &cand, &ex, &ey, &eg, &egs, &eu, &ev, &epu, &epv,
                                &removed_index, &fmt_stage, &fmt_len, &fmt_block, &fmt_out,
@@ -143,6 +156,9 @@ struct pv_context {
         if (pinned)
             cudaFreeHost(pinned);
         for (auto &t : pending)
+            if (!t.in_graph)
+                pool.push_back(t);
+        for (auto &t : graph_timers)
             pool.push_back(t);
         for (auto &t : pool) {
             cudaEventDestroy(t.start);
@@ -204,11 +220,16 @@ template <class F> cudaError_t counted(pv_context *c, int kind, int count, F &&l
             return e;
     }
     t.kind = kind;
-    cudaEventRecord(t.start, c->stream);
-    const cudaError_t e = launch();
-    cudaEventRecord(t.stop, c->stream);
-    c->pending.push_back(t);
-    return e;
+    t.in_graph = c->capturing;
+    // inside a capture the records become event-record nodes that fire on every replay
+    const unsigned flags = c->capturing ? cudaEventRecordExternal : cudaEventRecordDefault;
+    cudaError_t e = cudaEventRecordWithFlags(t.start, c->stream, flags);
+    if (e != cudaSuccess)
+        return e;
+    e = launch();
+    const cudaError_t e2 = cudaEventRecordWithFlags(t.stop, c->stream, flags);
+    (c->capturing ? c->capture_timers : c->pending).push_back(t);
+    return e != cudaSuccess ? e : e2;
 }
 
 // Folds the timings of completed launches into the totals (call after a stream synchronisation).
@@ -219,7 +240,8 @@ void collect_timers(pv_context *c) {
             c->milliseconds[t.kind] += ms;
             ++c->timed[t.kind];
         }
-        c->pool.push_back(t);
+        if (!t.in_graph)
+            c->pool.push_back(t);
     }
     c->pending.clear();
 }
@@ -451,6 +473,42 @@ StageArgs stage_base(pv_context *c) {
     s.ctl = c->ctl;
     s.g = c->gc;
     return s;
+}
+
+// A captured attempt bakes in the population, the plan and the buffer addresses.
+void drop_graphs(pv_context *c) {
+    if (c->attempt_graph) {
+        cudaGraphExecDestroy(c->attempt_graph);
+        c->attempt_graph = nullptr;
+    }
+    for (auto &t : c->graph_timers)
+        c->pool.push_back(t);
+    c->graph_timers.clear();
+    c->graph_key.clear();
+}
+
+// What a captured attempt depends on: the population, the plan and every buffer it touches.
+std::vector<const void *> attempt_key(const pv_context *c) {
+    std::vector<const void *> k = {reinterpret_cast<const void *>(c->n),
+                                   reinterpret_cast<const void *>(
+                                       static_cast<uintptr_t>(c->profiling ? 1 : 0)),
+                                   reinterpret_cast<const void *>(
+                                       static_cast<uintptr_t>(c->plan.num_chunks)),
+                                   reinterpret_cast<const void *>(
+                                       static_cast<uintptr_t>(c->sym.blocks)),
+                                   c->x.p, c->y.p, c->gamma.p, c->gs.p, c->p0x.p, c->p0y.p,
+                                   c->p1x.p, c->p1y.p, c->pu.p, c->pv.p, c->sym_items.p,
+                                   c->sym_counter.p, c->ctl, c->cand.p,
+                                   reinterpret_cast<const void *>(static_cast<uintptr_t>(
+                                       c->dipole_configured && c->dipole.removal ? 1 : 0))};
+    uint64_t bits;
+    std::memcpy(&bits, &c->dipole.distance, sizeof bits);
+    k.push_back(reinterpret_cast<const void *>(static_cast<uintptr_t>(bits)));
+    for (int s = 0; s < 7; ++s) {
+        k.push_back(c->kx[s].p);
+        k.push_back(c->ky[s].p);
+    }
+    return k;
 }
 
 pv_status ensure_state_capacity(pv_context *c, size_t n) {
@@ -751,6 +809,7 @@ pv_status pv_upload_state(pv_context *ctx, const double *x, const double *y,
         return st;
     ctx->n = n;
     ctx->fsal_valid = false;
+    ctx->prescan_valid = false;
     ctx->state_valid = true;
     ctx->gamma_host.assign(circulation, circulation + n);
     if (n == 0)
@@ -873,6 +932,7 @@ pv_status pv_rk4_step(pv_context *ctx, double dt) {
     if (st != PV_OK)
         return st;
     ctx->fsal_valid = false;
+    ctx->prescan_valid = false;
     if (ctx->n == 0)
         return PV_OK;
     DeviceGuard guard(ctx->device);
@@ -894,6 +954,7 @@ pv_status pv_rk4_advance(pv_context *ctx, double dt, uint64_t steps) {
     if (st != PV_OK)
         return st;
     ctx->fsal_valid = false;
+    ctx->prescan_valid = false;
     if (ctx->n == 0 || steps == 0)
         return PV_OK;
     DeviceGuard guard(ctx->device);
@@ -949,6 +1010,68 @@ pv_status pv_rk4_advance(pv_context *ctx, double dt, uint64_t steps) {
     return status_error(ctx, ctx->ctl_host->status);
 }
 
+namespace {
+// One DOPRI5 attempt (src/timestep.cpp:62-120) on the context stream: k0 when it is not cached,
+// stages 1..6 with their positions, the error norm and step control of the last stage, and the
+// accept kernel. Everything it needs from the host is in the control block.
+pv_status enqueue_dopri_attempt(pv_context *ctx, bool need_k0) {
+    double *pos_x[2] = {ctx->p0x.p, ctx->p1x.p};
+    double *pos_y[2] = {ctx->p0y.p, ctx->p1y.p};
+    double w[7];
+    for (int j = 0; j < 7; ++j)
+        w[j] = kB5[j] - kB4[j];
+    pv_status st;
+    const double *px = ctx->x.p, *py = ctx->y.p;
+    if (need_k0 && (st = launch_eval(ctx, px, py)) != PV_OK)
+        return st;
+    for (int s = 0; s < 7; ++s) {
+        if (s > 0 && (st = launch_eval(ctx, px, py)) != PV_OK)
+            return st;
+        StageArgs a = stage_base(ctx);
+        a.s = s;
+        a.reduce = (s > 0 || need_k0) ? 1 : 0;
+        a.ex = px;
+        a.ey = py;
+        a.dt_from_control = 1;
+        if (s < 6) {
+            a.mode = STAGE_POSITION;
+            a.ncoef = s + 1;
+            for (int j = 0; j <= s; ++j)
+                a.coef[j] = kDopri[s + 1][j];
+            a.xt = pos_x[s & 1];
+            a.yt = pos_y[s & 1];
+        } else {
+            a.mode = STAGE_DOPRI_ERROR;
+            a.xt = const_cast<double *>(px); // y5, the position k6 was evaluated at
+            a.yt = const_cast<double *>(py);
+            for (int j = 0; j < 7; ++j)
+                a.w[j] = w[j];
+        }
+        PV_CUDA(ctx, counted(ctx, PV_KERNEL_STAGE, 1,
+                             [&] { return launch_stage(a, ctx->stream, ctx->sm_count); }));
+        if (s < 6) {
+            px = a.xt;
+            py = a.yt;
+        }
+    }
+    PV_CUDA(ctx, counted(ctx, PV_KERNEL_ACCEPT, 1, [&] {
+                return launch_accept(ctx->x.p, ctx->y.p, px, py, ctx->kx[0].p, ctx->ky[0].p,
+                                     ctx->kx[6].p, ctx->ky[6].p, ctx->n, 1, ctx->ctl, ctx->stream);
+            }));
+    if (ctx->dipole_configured && ctx->dipole.removal) {
+        // the dipole scan of the accepted state (the kernel returns at once after a rejection)
+        auto *dev = reinterpret_cast<DipoleCandidateDev *>(ctx->cand.p);
+        auto *dev_count = reinterpret_cast<unsigned long long *>(&ctx->ctl->dipole_count);
+        PV_CUDA(ctx, counted(ctx, PV_KERNEL_DIPOLE, 1, [&] {
+                    return launch_dipole_scan(ctx->x.p, ctx->y.p, ctx->gamma.p, ctx->n, ctx->gc,
+                                              ctx->dipole.distance, dev, ctx->cand.cap / 3,
+                                              dev_count, ctx->stream, ctx->ctl);
+                }));
+    }
+    return PV_OK;
+}
+} // namespace
+
 pv_status pv_dopri5_step(pv_context *ctx, double dt, double absolute_tolerance,
                          double relative_tolerance, double minimum_time_step,
                          double maximum_time_step, pv_step_result *result) {
@@ -980,50 +1103,68 @@ pv_status pv_dopri5_step(pv_context *ctx, double dt, double absolute_tolerance,
     ctx->ctl_host->maximum_time_step = maximum_time_step;
     PV_CUDA(ctx, cudaMemcpyAsync(ctx->ctl, ctx->ctl_host, sizeof(DeviceControl),
                                  cudaMemcpyHostToDevice, ctx->stream));
-    double *pos_x[2] = {ctx->p0x.p, ctx->p1x.p};
-    double *pos_y[2] = {ctx->p0y.p, ctx->p1y.p};
-    double w[7];
-    for (int j = 0; j < 7; ++j)
-        w[j] = kB5[j] - kB4[j];
+    ctx->prescan_valid = false;
+    const bool prescan = ctx->dipole_configured && ctx->dipole.removal;
+    if (prescan)
+        PV_CUDA(ctx, ctx->cand.ensure(3 * 64));
     bool need_k0 = !ctx->fsal_valid;
     for (int attempt = 0; attempt < 40; ++attempt) {
-        const double *px = ctx->x.p, *py = ctx->y.p;
-        if (need_k0 && (st = launch_eval(ctx, px, py)) != PV_OK)
-            return st;
-        for (int s = 0; s < 7; ++s) {
-            if (s > 0 && (st = launch_eval(ctx, px, py)) != PV_OK)
+        if (need_k0) {
+            if ((st = enqueue_dopri_attempt(ctx, need_k0)) != PV_OK)
                 return st;
-            StageArgs a = stage_base(ctx);
-            a.s = s;
-            a.reduce = (s > 0 || need_k0) ? 1 : 0;
-            a.ex = px;
-            a.ey = py;
-            a.dt_from_control = 1;
-            if (s < 6) {
-                a.mode = STAGE_POSITION;
-                a.ncoef = s + 1;
-                for (int j = 0; j <= s; ++j)
-                    a.coef[j] = kDopri[s + 1][j];
-                a.xt = pos_x[s & 1];
-                a.yt = pos_y[s & 1];
-            } else {
-                a.mode = STAGE_DOPRI_ERROR;
-                a.xt = const_cast<double *>(px); // y5, the position k6 was evaluated at
-                a.yt = const_cast<double *>(py);
-                for (int j = 0; j < 7; ++j)
-                    a.w[j] = w[j];
+        } else {
+            // the FSAL attempt is the same launch sequence every time (dt lives in the control
+            // block): one CUDA graph, captured again only when the population, the plan, a
+            // buffer or the profiling switch changes. With profiling on, the capture holds the
+            // per-launch events, which every replay records.
+            const std::vector<const void *> key = attempt_key(ctx);
+            if (ctx->attempt_graph && key != ctx->graph_key)
+                drop_graphs(ctx);
+            if (!ctx->attempt_graph) {
+                const uint64_t evals0 = ctx->evaluations;
+                uint64_t launches0[PV_KERNEL_KINDS];
+                std::copy(ctx->launches, ctx->launches + PV_KERNEL_KINDS, launches0);
+                cudaGraph_t graph = nullptr;
+                PV_CUDA(ctx, cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
+                ctx->capturing = true;
+                ctx->capture_timers.clear();
+                st = enqueue_dopri_attempt(ctx, false);
+                ctx->capturing = false;
+                const cudaError_t e = cudaStreamEndCapture(ctx->stream, &graph);
+                ctx->graph_timers.swap(ctx->capture_timers);
+                ctx->capture_timers.clear();
+                if (st != PV_OK || e != cudaSuccess) {
+                    if (graph)
+                        cudaGraphDestroy(graph);
+                    drop_graphs(ctx);
+                    return st != PV_OK ? st
+                                       : fail(ctx, PV_ERROR_CUDA, std::string("cudaStreamEndCapture: ") +
+                                                                      cudaGetErrorString(e));
+                }
+                const cudaError_t ei = cudaGraphInstantiate(&ctx->attempt_graph, graph, 0);
+                cudaGraphDestroy(graph);
+                if (ei != cudaSuccess) {
+                    ctx->attempt_graph = nullptr;
+                    drop_graphs(ctx);
+                    return fail(ctx, PV_ERROR_CUDA,
+                                std::string("cudaGraphInstantiate: ") + cudaGetErrorString(ei));
+                }
+                // the capture counted; the launch below counts again
+                ctx->evaluations = evals0;
+                std::copy(launches0, launches0 + PV_KERNEL_KINDS, ctx->launches);
+                ctx->graph_key = key;
             }
-            PV_CUDA(ctx, counted(ctx, PV_KERNEL_STAGE, 1, [&] { return launch_stage(a, ctx->stream, ctx->sm_count); }));
-            if (s < 6) {
-                px = a.xt;
-                py = a.yt;
-            }
+            PV_CUDA(ctx, cudaGraphLaunch(ctx->attempt_graph, ctx->stream));
+            for (const auto &t : ctx->graph_timers)
+                ctx->pending.push_back(t);
+            ctx->evaluations += 6;
+            ctx->launches[PV_KERNEL_VELOCITY] += 6;
+            ctx->launches[PV_KERNEL_STAGE] += 7;
+            ctx->launches[PV_KERNEL_ACCEPT] += 1;
+            if (prescan)
+                ctx->launches[PV_KERNEL_DIPOLE] += 1;
         }
         need_k0 = false;
-        PV_CUDA(ctx, counted(ctx, PV_KERNEL_ACCEPT, 1, [&] {
-                    return launch_accept(ctx->x.p, ctx->y.p, px, py, ctx->kx[0].p, ctx->ky[0].p,
-                                         ctx->kx[6].p, ctx->ky[6].p, ctx->n, 1, ctx->ctl, ctx->stream);
-                }));
         if ((st = read_control(ctx)) != PV_OK)
             return st;
         if (ctx->ctl_host->status != 0) {
@@ -1032,6 +1173,8 @@ pv_status pv_dopri5_step(pv_context *ctx, double dt, double absolute_tolerance,
         }
         if (ctx->ctl_host->accepted) {
             ctx->fsal_valid = true;
+            ctx->prescan_valid = prescan;
+            ctx->prescan_count = ctx->ctl_host->dipole_count;
             result->accepted_time_step = ctx->ctl_host->result[0];
             result->suggested_time_step = ctx->ctl_host->result[1];
             result->normalized_error = ctx->ctl_host->result[2];
@@ -1194,6 +1337,7 @@ pv_status pv_dipole_configure(pv_context *ctx, const pv_dipole_config *config) {
                     "dipole reinjection is available only for periodic and disk geometries");
     ctx->dipole = *config;
     ctx->dipole_configured = true;
+    ctx->prescan_valid = false;
     // DipoleManager seeds its engine with the run seed mixed by this constant
     // (src/dipole.cpp:29-30); runs and checkpoints stay interchangeable only with the same seeding
     ctx->dipole_random.seed(config->random_seed ^ 0xd1b54a32d192ed03ULL);
@@ -1213,6 +1357,9 @@ pv_status pv_dipole_process(pv_context *ctx, size_t *events) {
     const size_t n = ctx->n;
     if (!ctx->dipole.removal || n == 0)
         return PV_OK;
+    if (ctx->prescan_valid && ctx->prescan_count == 0)
+        return PV_OK;  // the last accepted DOPRI5 attempt scanned this very state: no candidate
+    ctx->prescan_valid = false;
     std::vector<pv_dipole_candidate> cands;
     if ((st = scan_all(ctx, ctx->dipole.distance, cands)) != PV_OK)
         return st;

@@ -37,7 +37,9 @@ __device__ __forceinline__ void push(DipoleCandidateDev *out, size_t capacity,
 __global__ void __launch_bounds__(kDT)
     dipole_scan_kernel(const double *x, const double *y, const double *g, size_t n,
                        GeometryConsts gc, double thr2, DipoleCandidateDev *out, size_t capacity,
-                       unsigned long long *count) {
+                       unsigned long long *count, const DeviceControl *gate) {
+    if (gate && !gate->accepted)  // after a DOPRI5 attempt: only the accepted state is scanned
+        return;
     const size_t i0 = static_cast<size_t>(blockIdx.y) * kDT;
     const size_t j0 = static_cast<size_t>(blockIdx.x) * kDS;
     if (j0 + kDS <= i0 + 1)  // every source of the tile precedes every target of the block
@@ -129,7 +131,8 @@ __global__ void probe_ffma(int iterations, double *sink) {
 cudaError_t launch_dipole_scan(const double *x, const double *y, const double *gamma, size_t n,
                                const GeometryConsts &g, double threshold,
                                DipoleCandidateDev *out, size_t capacity,
-                               unsigned long long *count, cudaStream_t stream) {
+                               unsigned long long *count, cudaStream_t stream,
+                               const DeviceControl *gate) {
     cudaError_t e = cudaMemsetAsync(count, 0, sizeof(unsigned long long), stream);
     if (e != cudaSuccess || n == 0)
         return e;
@@ -138,7 +141,7 @@ cudaError_t launch_dipole_scan(const double *x, const double *y, const double *g
         return cudaErrorInvalidValue;
     const dim3 grid(static_cast<unsigned>(ns), static_cast<unsigned>(nt));
     dipole_scan_kernel<<<grid, kDT, 0, stream>>>(x, y, gamma, n, g, threshold * threshold, out,
-                                                 capacity, count);
+                                                 capacity, count, gate);
     return cudaGetLastError();
 }
 

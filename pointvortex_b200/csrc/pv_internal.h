@@ -124,7 +124,8 @@ struct DipoleCandidateDev {
 cudaError_t launch_dipole_scan(const double *x, const double *y, const double *gamma, size_t n,
                                const GeometryConsts &g, double threshold,
                                DipoleCandidateDev *out, size_t capacity,
-                               unsigned long long *count, cudaStream_t stream);
+                               unsigned long long *count, cudaStream_t stream,
+                               const DeviceControl *gate = nullptr);  // gate: scan iff accepted
 
 // Order-preserving removal of the sorted indices removed[0, m) from (x, y, g, gs)[0, n) into
 // (ox, oy, og, ogs)[0, n - m).

@@ -110,3 +110,25 @@ def test_disabled_removal_is_a_no_op():
     k.uploadDeviceState(pv.VortexSystem(d["x"], d["y"], d["g"]))
     dm = pv.DeviceDipoleManager(k, removal=False, distance=0.02)
     assert dm.process() == 0 and k.stateSize() == d["x"].size
+
+
+@pytest.mark.parametrize("planted", [True, False])
+def test_scan_fused_into_the_step(planted):
+    """With removal configured, each DOPRI5 attempt also scans its accepted state; process()
+    after the step must give what a fresh scan of that state gives (events, population, order)."""
+    from conftest import golden
+    d = golden("dipole_events_periodic_0.npz")
+    x, y, g = (d["x"], d["y"], d["g"]) if planted else (d["x0"], d["y0"], d["g0"])
+    fused = kernel_for("periodic")
+    fused.uploadDeviceState(pv.VortexSystem(x, y, g))
+    dm = manager(fused, 0)
+    fused.deviceDopri5Step(1e-7, 1e-12, 1e-9, 1e-12, 0.1)
+    stepped = fused.downloadDeviceSystem()
+    events = dm.process()
+    after = fused.downloadDeviceSystem()
+    fresh = kernel_for("periodic")
+    fresh.uploadDeviceState(stepped)
+    want = manager(fresh, 0).process()
+    expect = fresh.downloadDeviceSystem()
+    assert events == want and (events > 0) == planted
+    assert np.array_equal(after.x, expect.x) and np.array_equal(after.circulation, expect.circulation)
