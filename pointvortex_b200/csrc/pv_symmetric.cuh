@@ -29,13 +29,16 @@ __device__ __forceinline__ void kernel_values(const GeometryConsts &g, double tx
 
 // Targets (tx, ty, tg2) against the sources held in the lanes (sx, sy, sg2 and their reactions
 // ru, rv); adds the targets' sums to u, v and the sources' to ru, rv. Sources end at home.
-__device__ __forceinline__ void react_tile(const GeometryConsts &g, double tx, double ty,
-                                           double tg2, bool t_ok, double sx, double sy,
-                                           double sg2, int s_ok, double &u, double &v, double &ru,
-                                           double &rv) {
+// FULL: all 32 targets and sources exist (every tile but the last block's), no predicates.
+template <bool FULL>
+__device__ __forceinline__ void react_tile_t(const GeometryConsts &g, double tx, double ty,
+                                             double tg2, bool t_ok, double sx, double sy,
+                                             double sg2, int s_ok, double &u, double &v,
+                                             double &ru, double &rv) {
     const int next = (threadIdx.x + 1) & 31;
+#pragma unroll 2
     for (int k = 0; k < 32; ++k) {
-        if (t_ok && s_ok) {
+        if (FULL || (t_ok && s_ok)) {
             double ku, kv;
             kernel_values(g, tx, ty, sx, sy, ku, kv);
             u = fma(-sg2, ku, u);   // target: -g_s K
@@ -48,8 +51,19 @@ __device__ __forceinline__ void react_tile(const GeometryConsts &g, double tx, d
         sg2 = rotate(sg2, next);
         ru = rotate(ru, next);
         rv = rotate(rv, next);
-        s_ok = __shfl_sync(0xffffffffu, s_ok, next);
+        if (!FULL)
+            s_ok = __shfl_sync(0xffffffffu, s_ok, next);
     }
+}
+
+__device__ __forceinline__ void react_tile(const GeometryConsts &g, double tx, double ty,
+                                           double tg2, bool t_ok, double sx, double sy,
+                                           double sg2, int s_ok, double &u, double &v, double &ru,
+                                           double &rv) {
+    if (__all_sync(0xffffffffu, t_ok && s_ok))
+        react_tile_t<true>(g, tx, ty, tg2, t_ok, sx, sy, sg2, s_ok, u, v, ru, rv);
+    else
+        react_tile_t<false>(g, tx, ty, tg2, t_ok, sx, sy, sg2, s_ok, u, v, ru, rv);
 }
 
 // Target side only. same_block: the sources are the targets' own lanes, so the self pair (k = 0)
@@ -75,14 +89,16 @@ __device__ __forceinline__ void one_sided_tile(const GeometryConsts &g, double t
 // FP32-compensated tiles: the 32 sources (hi/lo coordinates and FP32 circulation) sit in this
 // warp's shared buffer, read at index (lane + k) & 31; only their FP32 reactions rotate through
 // the lanes. The callers promote the FP32 sums of each tile into FP64.
-__device__ __forceinline__ void react_tile32(const f32::F32Geometry &f, const float4 t, float tg,
-                                             bool t_ok, const float4 *sf, const float *sg,
-                                             int s_count, float &u, float &v, float &ru,
-                                             float &rv) {
+template <bool FULL>
+__device__ __forceinline__ void react_tile32_t(const f32::F32Geometry &f, const float4 t, float tg,
+                                               bool t_ok, const float4 *sf, const float *sg,
+                                               int s_count, float &u, float &v, float &ru,
+                                               float &rv) {
     const int lane = threadIdx.x & 31, next = (lane + 1) & 31;
+#pragma unroll 2
     for (int k = 0; k < 32; ++k) {
         const int j = (lane + k) & 31;
-        if (t_ok && j < s_count) {
+        if (FULL || (t_ok && j < s_count)) {
             float ku, kv;
             f32::periodic_values32(f, t, sf[j], ku, kv);
             const float g = sg[j];
@@ -94,6 +110,16 @@ __device__ __forceinline__ void react_tile32(const f32::F32Geometry &f, const fl
         ru = __shfl_sync(0xffffffffu, ru, next);
         rv = __shfl_sync(0xffffffffu, rv, next);
     }
+}
+
+__device__ __forceinline__ void react_tile32(const f32::F32Geometry &f, const float4 t, float tg,
+                                             bool t_ok, const float4 *sf, const float *sg,
+                                             int s_count, float &u, float &v, float &ru,
+                                             float &rv) {
+    if (__all_sync(0xffffffffu, t_ok && s_count == 32))
+        react_tile32_t<true>(f, t, tg, t_ok, sf, sg, s_count, u, v, ru, rv);
+    else
+        react_tile32_t<false>(f, t, tg, t_ok, sf, sg, s_count, u, v, ru, rv);
 }
 
 __device__ __forceinline__ void one_sided_tile32(const f32::F32Geometry &f, const float4 t,
