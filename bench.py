@@ -52,10 +52,10 @@ FLOPS_PER_PAIR_PERIODIC = 240
 # The symmetric form evaluates each unordered pair once and applies it to both vortices: the same
 # 240 plus two more FMA updates (the source's reaction) per unordered pair.
 FLOPS_PER_UNORDERED_PAIR_SYMMETRIC = 244
-# DRAM bytes (read + write) of one launch of the periodic pair kernel at this workload, from one
-# ncu capture (dram__bytes_read.sum 139.0 KB, dram__bytes_write.sum 0 B, with ncu's cache flush
-# before the launch): the sources are read once, everything else stays in L2.
-TRAFFIC_BYTES_PER_LAUNCH = 139008
+# DRAM bytes (read + write) of one launch of the symmetric periodic kernel at this workload, from
+# one ncu capture (dram__bytes_read.sum 174.8 KB, dram__bytes_write.sum 0 B, with ncu's cache
+# flush before the launch): the sources are read once, the partial rows stay in L2.
+TRAFFIC_BYTES_PER_LAUNCH = 174848
 
 
 def rank_info():
