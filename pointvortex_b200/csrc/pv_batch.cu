@@ -9,8 +9,8 @@
 //     (simulation, block of 128 threads x T targets, chunk of sources) items with an atomic counter. The
 //     items are sorted by cost (periodic pairs cost ~15x plane pairs), so the longest go first.
 //     Each CTA copies the item's geometry constants to shared memory and runs the same TMA-staged
-//     tile loop and pair functions as the single-simulation kernel. FP64 periodic simulations
-//     from N = 2048 instead take (simulation, block I, block J) items of 128 x 128 evaluated once
+//     tile loop and pair functions as the single-simulation kernel. Periodic simulations (both
+//     forms) from N = 2048 instead take (simulation, block I, block J) items of 128 x 128 evaluated once
 //     per unordered pair (the warp tiles of pv_symmetric.cuh, reactions summed across the CTA's
 //     warps in fixed order). Simulations in the FP32-compensated form drain a second queue, in a
 //     second launch, with the pair terms of pv_pair32.cuh;
@@ -64,7 +64,7 @@ struct SimDesc {
     unsigned num_chunks;          // partial rows (chunks, or 128-blocks of the symmetric form)
     unsigned chunk;
     int precision;                // PV_PRECISION_*
-    int symmetric;                // FP64 periodic evaluated once per unordered pair
+    int symmetric;                // periodic, evaluated once per unordered pair (either form)
 };
 
 struct SimControl {
@@ -270,6 +270,66 @@ __device__ __forceinline__ void run_symmetric_item(const GeometryConsts &g, cons
     }
 }
 
+// The FP32-compensated form of run_symmetric_item: each warp stages the 32 sources of its current
+// sub-tile (hi/lo coordinates, FP32 circulation) in its own shared buffer; FP32 sums of each
+// 32 x 32 tile are promoted into FP64.
+__device__ __forceinline__ void run_symmetric_item32(const GeometryConsts &g, const double *px,
+                                                     const double *py, const double *sgs,
+                                                     size_t n, unsigned I, unsigned J,
+                                                     double *pu, double *pv, size_t pad_n,
+                                                     double *red_u, double *red_v, float4 *s_f,
+                                                     float *s_gf) {
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const bool diagonal = I == J;
+    const f32::F32Geometry f = f32::make_f32(g);
+    float4 *sf = s_f + w * 32;
+    float *sg = s_gf + w * 32;
+    const size_t ti = static_cast<size_t>(I) * kBlock + static_cast<size_t>(w) * 32 + lane;
+    const bool t_ok = ti < n;
+    const float4 t = sym::split32(t_ok ? px[ti] : 0.0, t_ok ? py[ti] : 0.0);
+    const float tg = t_ok ? static_cast<float>(sgs[ti]) : 0.0f;
+    double ud = 0.0, vd = 0.0;
+    for (int qq = 0; qq < 4; ++qq) {
+        const int q = (w + qq) & 3;
+        const size_t j0 = static_cast<size_t>(J) * kBlock + static_cast<size_t>(q) * 32;
+        const size_t sj = j0 + lane;
+        const int s_count = j0 < n ? static_cast<int>(min(static_cast<size_t>(32), n - j0)) : 0;
+        __syncwarp();
+        sf[lane] = sym::split32(sj < n ? px[sj] : 0.0, sj < n ? py[sj] : 0.0);
+        sg[lane] = sj < n ? static_cast<float>(sgs[sj]) : 0.0f;
+        __syncwarp();
+        float u = 0.0f, v = 0.0f;
+        if (diagonal) {
+            sym::one_sided_tile32(f, t, t_ok, sf, sg, s_count, q == w, u, v);
+        } else {
+            float ru = 0.0f, rv = 0.0f;
+            sym::react_tile32(f, t, tg, t_ok, sf, sg, s_count, u, v, ru, rv);
+            red_u[w * kBlock + q * 32 + lane] = static_cast<double>(ru);
+            red_v[w * kBlock + q * 32 + lane] = static_cast<double>(rv);
+        }
+        ud += static_cast<double>(u);
+        vd += static_cast<double>(v);
+    }
+    if (t_ok) {
+        pu[static_cast<size_t>(J) * pad_n + ti] = ud;
+        pv[static_cast<size_t>(J) * pad_n + ti] = vd;
+    }
+    if (!diagonal) {
+        __syncthreads();
+        const size_t sj = static_cast<size_t>(J) * kBlock + threadIdx.x;
+        if (sj < n) {
+            double su = red_u[threadIdx.x], sv = red_v[threadIdx.x];
+            for (int k = 1; k < 4; ++k) {
+                su += red_u[k * kBlock + threadIdx.x];
+                sv += red_v[k * kBlock + threadIdx.x];
+            }
+            pu[static_cast<size_t>(I) * pad_n + sj] = su;
+            pv[static_cast<size_t>(I) * pad_n + sj] = sv;
+        }
+        __syncthreads();
+    }
+}
+
 // The FP32-compensated form of run_item: the staged FP64 tile is split once per CTA into
 // double-float FP32 coordinates; FP32 sums are promoted into FP64 every f32::kFlush sources.
 template <int GEO, int T>
@@ -447,10 +507,14 @@ __global__ void __launch_bounds__(kBlock) batch_velocity_kernel(const VelocityBa
         const double *sgs = a.arena.gs + d.off;
         double *pu = a.arena.pu + d.part_off;
         double *pv = a.arena.pv + d.part_off;
-        if (PREC == PV_PRECISION_FP64 && it.kind == ITEM_SYMMETRIC) {
+        if (it.kind == ITEM_SYMMETRIC) {
             // the TMA ring is idle between items: its buffers hold the cross-warp reactions
-            run_symmetric_item(s_geo, px, py, sgs, d.n, it.tb, it.chunk, pu, pv, d.pad_n,
-                               &s_x[0][0], &s_y[0][0]);
+            if constexpr (PREC == PV_PRECISION_FP32C)
+                run_symmetric_item32(s_geo, px, py, sgs, d.n, it.tb, it.chunk, pu, pv, d.pad_n,
+                                     &s_x[0][0], &s_y[0][0], s_f, s_gf);
+            else
+                run_symmetric_item(s_geo, px, py, sgs, d.n, it.tb, it.chunk, pu, pv, d.pad_n,
+                                   &s_x[0][0], &s_y[0][0]);
             __syncthreads();
             continue;
         }
@@ -1122,10 +1186,9 @@ pv_status pv_batch_add(pv_batch *b, const pv_params *params, const double *x, co
         return bfail(b, PV_ERROR_INVALID_ARGUMENT, "unknown precision form");
     const size_t pad = round_up(n, kAlign);
     const size_t chunk = chunk_for(n);
-    // FP64 periodic populations from kSymmetricMinN up: once per unordered pair, one partial row
+    // periodic populations from kSymmetricMinN up: once per unordered pair, one partial row
     // per 128-block (a function of n only, so the choice never depends on the batch)
-    const bool symmetric = params->precision == PV_PRECISION_FP64 && g.geometry == GEO_PERIODIC &&
-                           n >= kSymmetricMinN;
+    const bool symmetric = g.geometry == GEO_PERIODIC && n >= kSymmetricMinN;
     const unsigned chunks = symmetric ? symmetric_rows(static_cast<unsigned>(n))
                                       : static_cast<unsigned>((n + chunk - 1) / chunk);
     size_t off = 0, poff = 0;

@@ -134,10 +134,11 @@ def test_admission_validation():
 
 
 def mixed_forms():
-    """FP64 periodic from N = 2048 runs once per unordered pair; fp32c items drain their own
-    queue in a second launch per stage."""
+    """Periodic from N = 2048 runs once per unordered pair (both forms); fp32c items drain their
+    own queue in a second launch per stage."""
     return [
         ("periodic", 2100, 7, 0.0004),
+        ("periodic", 2200, 13, 0.0004, "fp32c"),
         ("infinite", 700, 8, 0.002, "fp32c"),
         ("periodic", 512, 9, 0.002, "fp32c"),
         ("disk", 600, 15, 0.002, "fp32c"),
