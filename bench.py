@@ -461,16 +461,9 @@ def run_reference_cuda(evals: int = 3, steps: int = 3) -> dict:
             "note": "wall clock per call; the backend synchronises after every evaluation"}
 
 
-def run_ensemble(n_sims: int = 512, budget: int = 10, seed: int = 7,
-                 precision: str = "fp64") -> dict:
-    """Batched ensemble: n_sims independent simulations, N log-uniform in [64, 8192], geometry
-    round-robin (infinite / periodic 2 pi / disk R = 1), balanced +-1 circulations, DOPRI5 with
-    rtol 1e-8 to t_end = 0.5, each with an accepted-step budget (the workloads are chaotic, so
-    unbudgeted work per simulation is unbounded). Timed from the first admission to the last
-    result download."""
-    import torch
-    from pointvortex_b200 import ics
-    from pointvortex_b200.batch import Batch, geometry_params
+def ensemble_specs(n_sims: int = 512, seed: int = 7) -> list:
+    """The cfg-4 ensemble: N log-uniform in [64, 8192], geometry round-robin (infinite /
+    periodic 2 pi / disk R = 1), one seed per simulation."""
     rng = np.random.default_rng(seed)
     geos = ("infinite", "periodic", "disk")
     specs = []
@@ -478,6 +471,16 @@ def run_ensemble(n_sims: int = 512, budget: int = 10, seed: int = 7,
         n = int(np.exp(rng.uniform(np.log(64), np.log(8192))))
         n += n % 2
         specs.append((geos[k % 3], n, 1000 + k))
+    return specs
+
+
+def solve_batch(specs, budget: int, precision: str, device: int = 0):
+    """Solves the given (geometry, N, seed) simulations in one batch: balanced +-1 circulations,
+    DOPRI5 with rtol 1e-8 to t_end = 0.5, an accepted-step budget each. Returns (per-simulation
+    (state, pairs), attempts, seconds from the first admission to the last result download)."""
+    import torch
+    from pointvortex_b200 import ics
+    from pointvortex_b200.batch import Batch, geometry_params
     states = []
     for geo, n, sd in specs:
         if geo == "periodic":
@@ -487,28 +490,75 @@ def run_ensemble(n_sims: int = 512, budget: int = 10, seed: int = 7,
         else:
             states.append(ics.infinite_plane(n, sd))
     total = sum(n for _, n, _ in specs)
-    b = Batch(total + 256 * (n_sims + 1), n_sims, max_steps=budget)
+    b = Batch(total + 256 * (len(specs) + 1), max(len(specs), 1), device, max_steps=budget)
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     ids = [b.add(geometry_params(geo, precision=precision), *st, 0.5, dt=1e-3, atol=1e-10,
                  rtol=1e-8)
            for (geo, n, sd), st in zip(specs, states)]
-    attempts = b.run()
-    finished = {}
-    pairs = 0.0
+    attempts = b.run() if ids else 0
+    out = []
     for sid, (geo, n, sd) in zip(ids, specs):
         info = b.info(sid)
         b.result(sid)
-        finished[info.state] = finished.get(info.state, 0) + 1
         evals = 6 * (info.acceptedSteps + info.rejectedSteps) + 1
-        pairs += evals * n * (n - 1)
+        out.append((info.state, float(evals) * n * (n - 1)))
     elapsed = time.perf_counter() - t0
     b.close()
-    return {"simulations": n_sims, "vortices": total, "step_budget": budget,
+    return out, attempts, elapsed
+
+
+def run_ensemble(n_sims: int = 512, budget: int = 10, seed: int = 7,
+                 precision: str = "fp64") -> dict:
+    """Batched ensemble (cfg-4) on one GPU, each simulation with an accepted-step budget (the
+    workloads are chaotic, so unbudgeted work per simulation is unbounded)."""
+    specs = ensemble_specs(n_sims, seed)
+    results, attempts, elapsed = solve_batch(specs, budget, precision)
+    finished = {}
+    for state, _ in results:
+        finished[state] = finished.get(state, 0) + 1
+    pairs = sum(p for _, p in results)
+    return {"simulations": n_sims, "vortices": sum(n for _, n, _ in specs), "step_budget": budget,
             "attempts": attempts, "seconds": elapsed, "solves_per_s": n_sims / elapsed,
             "pair_interactions_per_s": pairs / elapsed, "states": finished,
             "dtype": "f64" if precision == "fp64" else "f32 compensated (f64 state and control)",
             "note": "one arena, lock-step DOPRI5 attempts, CUDA-graph replay per attempt"}
+
+
+def run_ensemble_sharded(rank: int, world: int, device: int, n_sims: int = 512, budget: int = 10,
+                         seed: int = 7) -> dict | None:
+    """The same ensemble over `world` GPUs as replicas of the batch engine: each rank solves its
+    share of the simulations (cost-balanced partition), only the results go to rank 0. The time
+    is the slowest rank's."""
+    import torch.distributed as dist
+    from pointvortex_b200.shard import run_sharded, simulation_cost, torch_gather
+    specs = ensemble_specs(n_sims, seed)
+    timing = {}
+
+    def run_local(mine):
+        # never raises: every rank must reach the gathers
+        try:
+            results, _, elapsed = solve_batch([s for _, s in mine], budget, "fp64", device)
+        except Exception as exc:
+            timing["error"] = str(exc)[:200]
+            return []
+        timing["seconds"] = elapsed
+        return [(i, r) for (i, _), r in zip(mine, results)]
+
+    dist.barrier()
+    merged = run_sharded(specs, lambda s: simulation_cost(s[0], s[1]), run_local, rank, world,
+                         torch_gather)
+    seconds = max(torch_gather(timing.get("seconds", 0.0)))
+    errors = [e for e in torch_gather(timing.get("error")) if e]
+    if rank != 0:
+        return None
+    if errors or any(m is None for m in merged):
+        return {"error": (errors or ["a rank returned no results"])[0]}
+    pairs = sum(p for _, p in merged)
+    return {"simulations": n_sims, "ranks": world, "seconds": seconds,
+            "solves_per_s": n_sims / seconds, "pair_interactions_per_s": pairs / seconds,
+            "note": "replicas: one batch engine per GPU, cost-balanced partition, results "
+                    "gathered once"}
 
 
 def run_serving(budget: int = 10) -> dict:
@@ -725,6 +775,13 @@ def main(argv=None):
             print(json.dumps(out), flush=True)
         return 0
     result, k = run_ours(args)
+    if world > 1 and not args.no_extras:
+        try:  # every rank takes part (collectives in the same order everywhere)
+            sharded = run_ensemble_sharded(rank, world, int(os.environ.get("LOCAL_RANK", "0")))
+        except Exception as exc:
+            sharded = {"error": str(exc)[:200]}
+        if rank == 0:
+            result["ensemble_sharded"] = sharded
     if rank == 0 and world == 1 and not args.no_extras:
         try:
             result["ensemble"] = run_ensemble()
