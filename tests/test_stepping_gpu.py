@@ -177,3 +177,28 @@ def test_empty_population():
     k.deviceRk4Step(1e-3)
     r = k.deviceDopri5Step(1e-3, 1e-10, 1e-8, 1e-12, 0.1)
     assert r.acceptedTimeStep == 1e-3 and r.suggestedTimeStep == 5e-3 and r.rejectedSteps == 0
+
+
+def test_dopri_graph_replay_equals_launches_and_profiling():
+    """The FSAL attempt is replayed as a captured CUDA graph (with per-launch event nodes when
+    profiling): steps with profiling on and off give identical states and step results."""
+    import pointvortex_b200 as pv
+    from pointvortex_b200 import ics
+    x, y, g = ics.periodic_box(2100, 31)
+    out = []
+    for profiling in (False, True):
+        k = pv.PeriodicBoxKernel(2 * np.pi, 2 * np.pi, 8)
+        k.setProfiling(profiling)
+        k.uploadDeviceState(pv.VortexSystem(x, y, g))
+        dt, results = 1e-4, []
+        for _ in range(6):
+            r = k.deviceDopri5Step(dt, 1e-12, 1e-9, 1e-12, 0.1)
+            results.append((r.acceptedTimeStep, r.rejectedSteps))
+            dt = r.suggestedTimeStep
+        s = k.downloadDeviceSystem()
+        stats = k.kernelStats()
+        out.append((results, s.x, s.y, stats))
+    (r0, x0, y0, _), (r1, x1, y1, st1) = out
+    assert r0 == r1 and np.array_equal(x0, x1) and np.array_equal(y0, y1)
+    launches, timed, ms = st1["velocity"]
+    assert launches == timed and ms > 0  # every replayed launch was timed by its graph events
