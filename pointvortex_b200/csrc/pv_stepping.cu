@@ -140,14 +140,19 @@ __device__ __forceinline__ void finish_target(const StageArgs &a, size_t i, doub
     }
 }
 
-// WIDE: many partial rows (the symmetric kernel's). A block then covers 32 targets with 8 row
-// groups: warp g sums rows g, g + 8, ... (coalesced over the 32 targets), and warp 0 adds the 8
-// group sums in fixed order. Otherwise one thread per target sums its rows in order.
+// WIDE: many partial rows (the symmetric kernel's). A block then covers kWideTargets targets with
+// 256 / kWideTargets row groups: thread (group, t) sums rows group, group + groups, ...
+// (coalesced over the targets), and the threads of group 0 add the group sums in fixed order.
+// Otherwise one thread per target sums its rows in order.
+constexpr int kWideTargets = 16;
+constexpr int kWideGroups = 256 / kWideTargets;
+
 template <int MODE, bool WIDE>
 __global__ void __launch_bounds__(256) stage_kernel(const StageArgs a) {
     __shared__ int s_status;
     __shared__ double s_max[8];
-    __shared__ double s_u[WIDE ? 8 : 1][32], s_v[WIDE ? 8 : 1][32];
+    __shared__ double s_u[WIDE ? kWideGroups : 1][kWideTargets],
+        s_v[WIDE ? kWideGroups : 1][kWideTargets];
     const int tid = threadIdx.x;
     if (tid == 0)
         s_status = *reinterpret_cast<volatile int *>(&a.ctl->status);
@@ -158,13 +163,13 @@ __global__ void __launch_bounds__(256) stage_kernel(const StageArgs a) {
     const double dt = a.dt_from_control ? a.ctl->dt : a.dt;
     double local_max = 0.0;
     if (WIDE) {
-        const int lane = tid & 31, group = tid >> 5;
-        for (size_t base = static_cast<size_t>(blockIdx.x) * 32; base < a.n;
-             base += static_cast<size_t>(gridDim.x) * 32) {
+        const int lane = tid % kWideTargets, group = tid / kWideTargets;
+        for (size_t base = static_cast<size_t>(blockIdx.x) * kWideTargets; base < a.n;
+             base += static_cast<size_t>(gridDim.x) * kWideTargets) {
             const size_t i = base + lane;
             double su = 0.0, sv = 0.0;
             if (i < a.n)
-                for (int c = group; c < a.num_chunks; c += 8) {
+                for (int c = group; c < a.num_chunks; c += kWideGroups) {
                     su += a.pu[static_cast<size_t>(c) * a.stride + i];
                     sv += a.pv[static_cast<size_t>(c) * a.stride + i];
                 }
@@ -173,7 +178,7 @@ __global__ void __launch_bounds__(256) stage_kernel(const StageArgs a) {
             __syncthreads();
             if (group == 0 && i < a.n) {
                 double ku = s_u[0][lane], kv = s_v[0][lane];
-                for (int g = 1; g < 8; ++g) {
+                for (int g = 1; g < kWideGroups; ++g) {
                     ku += s_u[g][lane];
                     kv += s_v[g][lane];
                 }
@@ -253,7 +258,7 @@ constexpr int kWideRows = 32;
 template <int MODE>
 cudaError_t launch_stage_mode(const StageArgs &a, cudaStream_t stream, int sm_count) {
     if (a.reduce && a.num_chunks >= kWideRows) {
-        const size_t blocks = (a.n + 31) / 32;
+        const size_t blocks = (a.n + kWideTargets - 1) / kWideTargets;
         const size_t cap = static_cast<size_t>(sm_count > 0 ? sm_count : 148) * 8;
         const unsigned grid = static_cast<unsigned>(blocks < 1 ? 1 : (blocks < cap ? blocks : cap));
         stage_kernel<MODE, true><<<grid, 256, 0, stream>>>(a);
