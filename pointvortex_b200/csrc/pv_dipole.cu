@@ -61,19 +61,21 @@ __global__ void __launch_bounds__(kDT)
     const bool periodic = gc.geometry == GEO_PERIODIC;
     const int jcount = static_cast<int>(min(static_cast<size_t>(kDS), n - j0));
     const bool neg_i = signbit(gi);
+    // every pair's distance first (no divergence); the order and sign conditions only for the
+    // rare pair closer than the threshold
 #pragma unroll 4
     for (int jj = 0; jj < jcount; ++jj) {
-        const double gj = sg[jj];
-        if (j0 + jj <= i || gj == 0.0 || neg_i == static_cast<bool>(signbit(gj)))
-            continue;
         double dx = xi - sx[jj], dy = yi - sy[jj];
         if (periodic) {
             dx = exact_remainder(dx, gc.lx, gc.inv_lx, gc.half_lx);
             dy = exact_remainder(dy, gc.ly, gc.inv_ly, gc.half_ly);
         }
         const double d2 = __dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy));
-        if (d2 < thr2)
-            push(out, capacity, count, i, j0 + jj, d2);
+        if (d2 < thr2) {
+            const double gj = sg[jj];
+            if (j0 + jj > i && gj != 0.0 && neg_i != static_cast<bool>(signbit(gj)))
+                push(out, capacity, count, i, j0 + jj, d2);
+        }
     }
     // the wall image of each target once: in the block whose source tile starts at the target block
     if (gc.geometry == GEO_DISK && j0 == i0) {
