@@ -25,6 +25,7 @@
 #include "pv_symmetric.cuh"
 
 #include <algorithm>
+#include <atomic>
 
 namespace pvb {
 
@@ -180,11 +181,11 @@ __global__ void __launch_bounds__(kThreads)
 }
 
 int resident_ctas(int a, int precision) {
-    static int cached[2][17] = {};
+    static std::atomic<int> cached[2][17] = {};  // host threads may ask at once
     if (a < 1 || a > 16)
         return 1;
     const int q = precision == PV_PRECISION_FP32C ? 1 : 0;
-    if (!cached[q][a]) {
+    if (!cached[q][a].load(std::memory_order_relaxed)) {
         int blocks = 0;
         const size_t smem = static_cast<size_t>(kThreads / 32) * a * 32 * sizeof(double2);
         const cudaError_t e =
@@ -194,9 +195,9 @@ int resident_ctas(int a, int precision) {
                                                               kThreads, smem);
         if (e != cudaSuccess || blocks < 1)
             blocks = 1;
-        cached[q][a] = blocks;
+        cached[q][a].store(blocks, std::memory_order_relaxed);
     }
-    return cached[q][a];
+    return cached[q][a].load(std::memory_order_relaxed);
 }
 
 }  // namespace

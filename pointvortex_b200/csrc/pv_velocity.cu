@@ -17,6 +17,7 @@
 #include "pv_internal.h"
 
 #include <algorithm>
+#include <atomic>
 
 namespace pvb {
 
@@ -179,16 +180,20 @@ cudaError_t launch_pair(const EvalArgs &a, const EvalPlan &p, cudaStream_t strea
 
 namespace {
 // Resident CTAs per SM of one kernel instance (registers and shared memory decide it).
+// (Contexts on several host threads may ask at once: the cache is an atomic, and a repeated
+// query gives the same value.)
 template <class Pair, int T> int resident_ctas() {
-    static int cached = -1;
-    if (cached < 0) {
+    static std::atomic<int> cached{-1};
+    int v = cached.load(std::memory_order_relaxed);
+    if (v < 0) {
         int blocks = 0;
         if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, velocity_kernel<Pair, 128, T>,
                                                           128, 0) != cudaSuccess || blocks < 1)
             blocks = 1;
-        cached = blocks;
+        cached.store(blocks, std::memory_order_relaxed);
+        v = blocks;
     }
-    return cached;
+    return v;
 }
 
 template <class Pair> int resident_for(int per_thread) {
@@ -199,7 +204,8 @@ template <class Pair> int resident_for(int per_thread) {
 
 namespace {
 // Autotuner table: targets per thread for (geometry, precision, floor(log2 N)); 0 = heuristic.
-int g_tuning[3][2][40] = {};
+// Atomic entries: a table update may run beside evaluations on other host threads.
+std::atomic<int> g_tuning[3][2][40] = {};
 } // namespace
 
 int tuning_lookup(int geometry, int precision, size_t n) {
@@ -208,14 +214,14 @@ int tuning_lookup(int geometry, int precision, size_t n) {
     int bucket = 0;
     while ((size_t(2) << bucket) <= n && bucket < 39)
         ++bucket;
-    return g_tuning[geometry][precision][bucket];
+    return g_tuning[geometry][precision][bucket].load(std::memory_order_relaxed);
 }
 
 bool tuning_store(int geometry, int precision, int log2_n, int per_thread) {
     if (geometry < 0 || geometry > 2 || precision < 0 || precision > 1 || log2_n < 0 ||
         log2_n >= 40 || (per_thread != 0 && per_thread != 1 && per_thread != 2 && per_thread != 4))
         return false;
-    g_tuning[geometry][precision][log2_n] = per_thread;
+    g_tuning[geometry][precision][log2_n].store(per_thread, std::memory_order_relaxed);
     return true;
 }
 
