@@ -58,7 +58,8 @@ struct SymmetricPlan {
     bool enabled() const { return a > 0; }
 };
 constexpr size_t kSymmetricMinN = 2048;                            // below: the ordered kernel
-constexpr size_t kSymmetricPartialBytes = static_cast<size_t>(256) << 20;
+constexpr size_t kSymmetricPartialBytes = static_cast<size_t>(256) << 20;  // a grows past this
+constexpr size_t kSymmetricPartialBytesMax = static_cast<size_t>(4) << 30;  // beyond: ordered kernel
 SymmetricPlan plan_symmetric(size_t n, int sm_count, int precision);
 void symmetric_items(const SymmetricPlan &p, unsigned *out);  // p.items packed (I << 16) | J
 cudaError_t launch_periodic_symmetric(const double *x, const double *y, const double *gs, size_t n,

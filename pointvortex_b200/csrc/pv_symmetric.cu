@@ -206,13 +206,15 @@ SymmetricPlan plan_symmetric(size_t n, int sm_count, int precision) {
     SymmetricPlan p{};
     if (n < kSymmetricMinN)
         return p;
-    // the smallest block that keeps the partial rows within kSymmetricPartialBytes
+    // the smallest block that keeps the partial rows within kSymmetricPartialBytes, or the largest
+    // block up to kSymmetricPartialBytesMax (N ~ 3.7e5); beyond that the ordered kernel runs
     const size_t np = (n + 255) & ~static_cast<size_t>(255);
     for (int a = 1; a <= 16; a *= 2) {
         const size_t blocks = (n + 32 * static_cast<size_t>(a) - 1) / (32 * static_cast<size_t>(a));
         if (blocks > 0xffffu)
             continue;
-        if (blocks * np * 2 * sizeof(double) <= kSymmetricPartialBytes || a == 16) {
+        const size_t bytes = blocks * np * 2 * sizeof(double);
+        if (bytes <= kSymmetricPartialBytes || (a == 16 && bytes <= kSymmetricPartialBytesMax)) {
             p.a = a;
             p.blocks = static_cast<int>(blocks);
             p.items = static_cast<unsigned>(blocks * (blocks + 1) / 2);
