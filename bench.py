@@ -52,6 +52,11 @@ FLOPS_PER_PAIR_PERIODIC = 240
 # The symmetric form evaluates each unordered pair once and applies it to both vortices: the same
 # 240 plus two more FMA updates (the source's reaction) per unordered pair.
 FLOPS_PER_UNORDERED_PAIR_SYMMETRIC = 244
+# The plane in the same count: an ordered pair is 11 (displacement 2, r^2 3, reciprocal 1, scale
+# 1, two FMA updates 4); the symmetric form spends 16 per unordered pair (the shared displacement,
+# r^2 and reciprocal, the two kernel values 2, four FMA updates 8).
+FLOPS_PER_PAIR_PLANE = 11
+FLOPS_PER_UNORDERED_PAIR_PLANE_SYMMETRIC = 16
 # DRAM bytes (read + write) of one launch of the symmetric periodic kernel at this workload, from
 # one ncu capture (dram__bytes_read.sum 174.8 KB, dram__bytes_write.sum 0 B, with ncu's cache
 # flush before the launch): the sources are read once, the partial rows stay in L2.
@@ -389,15 +394,15 @@ def run_kernel_case(spec: str, evals: int, precision: str = "fp64", ordered: boo
     if geo == "infinite":
         x, y, g = ics.infinite_plane(n, 1)
         k = pv.InfinitePlaneKernel(0.0, precision=prec)
-        flops = 11
+        flops, flops_sym = FLOPS_PER_PAIR_PLANE, FLOPS_PER_UNORDERED_PAIR_PLANE_SYMMETRIC
     elif geo == "periodic":
         x, y, g = ics.periodic_box(n, 2, LENGTH)
         k = pv.PeriodicBoxKernel(LENGTH, LENGTH, LAYERS, precision=prec)
-        flops = FLOPS_PER_PAIR_PERIODIC
+        flops, flops_sym = FLOPS_PER_PAIR_PERIODIC, FLOPS_PER_UNORDERED_PAIR_SYMMETRIC
     else:
         x, y, g = ics.disk(n, 3, 1.0)
         k = pv.DiskKernel(1.0, precision=prec)
-        flops = 33
+        flops, flops_sym = 33, None
     k.uploadDeviceState(pv.VortexSystem(x, y, g))
     symmetric = k.statePlan()["symmetric"] and not ordered
     run = (lambda: k.evaluate(x, y, g)) if ordered else k.evaluateDeviceState
@@ -410,11 +415,12 @@ def run_kernel_case(spec: str, evals: int, precision: str = "fp64", ordered: boo
     st = k.kernelStats()["velocity"]
     ms = st[2] / max(st[1], 1)
     pairs = n * (n - 1)
-    work = (FLOPS_PER_UNORDERED_PAIR_SYMMETRIC * pairs / 2) if symmetric else flops * pairs
+    work = (flops_sym * pairs / 2) if symmetric else flops * pairs
     torch.cuda.synchronize()
     return {"case": spec, "precision": precision, "kernel": "symmetric" if symmetric else "ordered",
             "evaluations": evals, "ms_per_evaluation": ms, "pairs_per_s": pairs / (ms * 1e-3),
-            "formula_flops_per_pair": flops, "tflops": work / (ms * 1e-3) / 1e12}
+            "formula_flops_per_pair": flops, "tflops": work / (ms * 1e-3) / 1e12,
+            "ordered_equivalent_tflops": flops * pairs / (ms * 1e-3) / 1e12}
 
 
 def run_reference_cuda(evals: int = 3, steps: int = 3) -> dict:

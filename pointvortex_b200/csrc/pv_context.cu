@@ -93,7 +93,7 @@ struct pv_context {
     DeviceArray kx[7], ky[7];        // stage velocities
     DeviceArray pu, pv;              // chunk partials (or symmetric-kernel rows)
     cudaGraphExec_t attempt_graph = nullptr; // one DOPRI5 attempt with a valid FSAL derivative
-    SymmetricPlan sym{};             // periodic FP64: one evaluation per unordered pair
+    SymmetricPlan sym{};             // one evaluation per unordered pair (when planned)
     DeviceArray sym_items, sym_counter;
     int sym_items_blocks = 0;        // the block count the item table was built for
     DeviceArray inv_scratch, inv_out;
@@ -420,7 +420,7 @@ std::vector<double> scaled(const GeometryConsts &g, const double *gamma, size_t 
 pv_status launch_eval(pv_context *c, const double *px, const double *py) {
     if (c->sym.enabled()) {
         PV_CUDA(c, counted(c, PV_KERNEL_VELOCITY, 1, [&] {
-                    return launch_periodic_symmetric(
+                    return launch_symmetric(
                         px, py, c->gs.p, c->n, c->sym,
                         reinterpret_cast<const unsigned *>(c->sym_items.p),
                         reinterpret_cast<unsigned *>(c->sym_counter.p), c->pu.p, c->pv.p,
@@ -520,9 +520,7 @@ pv_status ensure_state_capacity(pv_context *c, size_t n) {
         PV_CUDA(c, c->ky[s].ensure(np));
     }
     c->plan = plan_evaluation(c->gc.geometry, n, n, c->sm_count, 0, c->params.precision);
-    c->sym = SymmetricPlan{};
-    if (c->gc.geometry == GEO_PERIODIC)
-        c->sym = plan_symmetric(n, c->sm_count, c->params.precision);
+    c->sym = plan_symmetric(n, c->sm_count, c->params.precision, c->gc.geometry);
     const size_t rows = c->sym.enabled() ? static_cast<size_t>(c->sym.blocks)
                                          : static_cast<size_t>(c->plan.num_chunks);
     const size_t partial = rows * np;

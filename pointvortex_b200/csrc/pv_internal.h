@@ -47,25 +47,30 @@ cudaError_t launch_velocity(const EvalArgs &a, const EvalPlan &p, cudaStream_t s
 // The FP32-compensated precision form (pv_velocity32.cu): same arguments, same partial layout.
 cudaError_t launch_velocity_fp32c(const EvalArgs &a, const EvalPlan &p, cudaStream_t stream);
 
-// The periodic box evaluated once per unordered pair (pv_symmetric.cu) for a whole population
-// (targets = sources). Partial rows: `blocks` rows of the same layout as the chunk partials.
+// The periodic box (FP64, FP32C) and the infinite plane (FP64) evaluated once per unordered pair
+// (pv_symmetric.cu) for a whole population (targets = sources). Partial rows: `blocks` rows of
+// the same layout as the chunk partials.
 struct SymmetricPlan {
     int a = 0;           // 32-vortex sub-blocks per block; 0: not used
     int blocks = 0;      // partial rows
     unsigned items = 0;  // block pairs (I <= J)
     int grid = 0;        // persistent CTAs
     int precision = 0;   // PV_PRECISION_FP64 or PV_PRECISION_FP32C
+    int geometry = 0;    // GEO_PERIODIC or GEO_INFINITE
+    int targets = 1;     // targets per lane off the diagonal (the plane: 4 or 8)
     bool enabled() const { return a > 0; }
 };
-constexpr size_t kSymmetricMinN = 2048;                            // below: the ordered kernel
+constexpr size_t kSymmetricMinN = 2048;       // periodic box below: the ordered kernel
+constexpr size_t kSymmetricPlaneMinN = 16384;   // infinite plane below: the ordered kernel
+constexpr size_t kSymmetricPlaneWideN = 32768;  // the plane from here: 8 targets per lane
 constexpr size_t kSymmetricPartialBytes = static_cast<size_t>(256) << 20;  // a grows past this
 constexpr size_t kSymmetricPartialBytesMax = static_cast<size_t>(4) << 30;  // beyond: ordered kernel
-SymmetricPlan plan_symmetric(size_t n, int sm_count, int precision);
+SymmetricPlan plan_symmetric(size_t n, int sm_count, int precision, int geometry);
 void symmetric_items(const SymmetricPlan &p, unsigned *out);  // p.items packed (I << 16) | J
-cudaError_t launch_periodic_symmetric(const double *x, const double *y, const double *gs, size_t n,
-                                      const SymmetricPlan &p, const unsigned *items,
-                                      unsigned *counter, double *pu, double *pv, size_t stride,
-                                      const GeometryConsts &g, cudaStream_t stream);
+cudaError_t launch_symmetric(const double *x, const double *y, const double *gs, size_t n,
+                             const SymmetricPlan &p, const unsigned *items, unsigned *counter,
+                             double *pu, double *pv, size_t stride, const GeometryConsts &g,
+                             cudaStream_t stream);
 
 // ---- stage kernels (reduction, stage positions, RK4 combine, DOPRI5 error and control) ------
 enum StageMode : int {

@@ -1,13 +1,13 @@
-// pv_symmetric.cu — the periodic-box velocity of a whole population evaluated once per unordered
-// pair.
+// pv_symmetric.cu — the velocity of a whole population evaluated once per unordered pair: the
+// periodic box (FP64 and FP32-compensated) and the infinite plane (FP64).
 //
-// The reference evaluates every ordered pair (src/compute.cpp:203-256). The Weiss–McWilliams pair
-// term is antisymmetric: exchanging target and source negates x^ and y^ exactly (IEEE remainder
-// is odd), and every quantity of PeriodicPair::terms is an exactly odd or even function of them,
-// so the source's term is the target's with the other circulation and the opposite sign, bit for
-// bit. One evaluation of the transcendental series therefore serves both vortices, and the work
-// per velocity evaluation halves. Only the order of summation differs from the ordered-pair
-// kernel.
+// The reference evaluates every ordered pair (src/compute.cpp:203-256 for the box, :88-133 for
+// the plane). The Weiss–McWilliams pair term is antisymmetric: exchanging target and source
+// negates x^ and y^ exactly (IEEE remainder is odd), and every quantity of PeriodicPair::terms is
+// an exactly odd or even function of them, so the source's term is the target's with the other
+// circulation and the opposite sign, bit for bit. The plane's (dy, dx) / (r^2 + eps^2) is odd in
+// the same way. One evaluation therefore serves both vortices, and the work per velocity
+// evaluation halves. Only the order of summation differs from the ordered-pair kernel.
 //
 // Work decomposition (warp-level, persistent):
 //   * vortices form blocks of 32a (a = 1..16 sub-blocks of 32); an item is a block pair (I, J),
@@ -16,7 +16,9 @@
 //     reactions rotate through the lanes by shuffles, so in 32 steps every (target, source) pair
 //     is met once and every source comes back to its home lane;
 //   * sub-blocks on the diagonal of a diagonal item are evaluated one-sided (31 rotations, the
-//     self pair skipped: it contributes exactly 0 in the reference, sin 0 = 0);
+//     self pair skipped, as in the reference);
+//   * the plane's pair term is cheap next to the five shuffles of a rotation step, so off the
+//     diagonal each lane holds 4 or 8 targets against the rotating sources;
 //   * partial sums go to rows of a [blocks][N] array: vortices of block I receive row J from item
 //     (I, J), vortices of block J receive row I, and each (row, vortex) is written exactly once,
 //     so the stage kernel's fixed-order sum over rows keeps results deterministic.
@@ -33,12 +35,15 @@ namespace {
 
 constexpr int kThreads = 128;  // 4 independent warps per CTA
 
+// P: the pair kernel (sym::PeriodicSym, sym::PlaneSym). T: targets per lane in the items off the
+// diagonal (a multiple of T sub-blocks per block); diagonal items hold one target per lane.
+template <class P, int T>
 __global__ void __launch_bounds__(kThreads)
-    periodic_symmetric_kernel(const double *__restrict__ x, const double *__restrict__ y,
-                              const double *__restrict__ gs, size_t n, int a,
-                              const unsigned *__restrict__ items, unsigned n_items,
-                              unsigned *counter, double *__restrict__ pu,
-                              double *__restrict__ pv, size_t stride, GeometryConsts g) {
+    symmetric_kernel(const double *__restrict__ x, const double *__restrict__ y,
+                     const double *__restrict__ gs, size_t n, int a,
+                     const unsigned *__restrict__ items, unsigned n_items, unsigned *counter,
+                     double *__restrict__ pu, double *__restrict__ pv, size_t stride,
+                     GeometryConsts g) {
     extern __shared__ double2 reaction_smem[];
     const int lane = threadIdx.x & 31;
     double2 *reaction = reaction_smem + (threadIdx.x >> 5) * a * 32;  // this warp's sources
@@ -55,33 +60,75 @@ __global__ void __launch_bounds__(kThreads)
         const bool diagonal = I == J;
         for (int jb = 0; jb < a; ++jb)
             reaction[jb * 32 + lane] = make_double2(0.0, 0.0);
-        for (int ib = 0; ib < a; ++ib) {
-            const size_t ti = I * block_len + static_cast<size_t>(ib) * 32 + lane;
-            const bool t_ok = ti < n;
-            const double tx = t_ok ? x[ti] : 0.0, ty = t_ok ? y[ti] : 0.0;
-            const double tg2 = t_ok ? 2.0 * gs[ti] : 0.0;  // doubled: the terms carry half sines
-            double u = 0.0, v = 0.0;
-            for (int jb = diagonal ? ib : 0; jb < a; ++jb) {
-                const size_t sj = J * block_len + static_cast<size_t>(jb) * 32 + lane;
-                const int s_ok = sj < n ? 1 : 0;
-                const double sx = s_ok ? x[sj] : 0.0, sy = s_ok ? y[sj] : 0.0;
-                const double sg2 = s_ok ? 2.0 * gs[sj] : 0.0;
-                if (diagonal && jb == ib) {
-                    sym::one_sided_tile(g, tx, ty, t_ok, sx, sy, sg2, s_ok, true, u, v);
-                    continue;
+        if (T > 1 && !diagonal) {
+            for (int ib = 0; ib < a; ib += T) {
+                double tx[T], ty[T], tg[T], u[T], v[T];
+                bool t_ok[T], all_ok = true;
+#pragma unroll
+                for (int t = 0; t < T; ++t) {
+                    const size_t ti = I * block_len + static_cast<size_t>(ib + t) * 32 + lane;
+                    t_ok[t] = ti < n;
+                    all_ok = all_ok && t_ok[t];
+                    tx[t] = t_ok[t] ? x[ti] : 0.0;
+                    ty[t] = t_ok[t] ? y[ti] : 0.0;
+                    tg[t] = t_ok[t] ? P::kScale * gs[ti] : 0.0;
+                    u[t] = 0.0;
+                    v[t] = 0.0;
                 }
-                double ru = reaction[jb * 32 + lane].x, rv = reaction[jb * 32 + lane].y;
-                sym::react_tile(g, tx, ty, tg2, t_ok, sx, sy, sg2, s_ok, u, v, ru, rv);
-                reaction[jb * 32 + lane] = make_double2(ru, rv);
+                for (int jb = 0; jb < a; ++jb) {
+                    const size_t sj = J * block_len + static_cast<size_t>(jb) * 32 + lane;
+                    const int s_ok = sj < n ? 1 : 0;
+                    const double sx = s_ok ? x[sj] : 0.0, sy = s_ok ? y[sj] : 0.0;
+                    const double sg = s_ok ? P::kScale * gs[sj] : 0.0;
+                    double ru = reaction[jb * 32 + lane].x, rv = reaction[jb * 32 + lane].y;
+                    if (__all_sync(0xffffffffu, all_ok && s_ok)) {
+                        sym::react_tiles_full<P, T>(g, tx, ty, tg, sx, sy, sg, u, v, ru, rv);
+                    } else {
+#pragma unroll
+                        for (int t = 0; t < T; ++t)
+                            sym::react_tile<P>(g, tx[t], ty[t], tg[t], t_ok[t], sx, sy, sg, s_ok,
+                                               u[t], v[t], ru, rv);
+                    }
+                    reaction[jb * 32 + lane] = make_double2(ru, rv);
+                }
+#pragma unroll
+                for (int t = 0; t < T; ++t) {
+                    const size_t ti = I * block_len + static_cast<size_t>(ib + t) * 32 + lane;
+                    if (t_ok[t]) {
+                        pu[J * stride + ti] = u[t];
+                        pv[J * stride + ti] = v[t];
+                    }
+                }
             }
-            if (diagonal) {  // reactions from the sub-blocks before this one in the same block
-                const double2 r = reaction[ib * 32 + lane];
-                u += r.x;
-                v += r.y;
-            }
-            if (t_ok) {
-                pu[J * stride + ti] = u;
-                pv[J * stride + ti] = v;
+        } else {
+            for (int ib = 0; ib < a; ++ib) {
+                const size_t ti = I * block_len + static_cast<size_t>(ib) * 32 + lane;
+                const bool t_ok = ti < n;
+                const double tx = t_ok ? x[ti] : 0.0, ty = t_ok ? y[ti] : 0.0;
+                const double tg = t_ok ? P::kScale * gs[ti] : 0.0;
+                double u = 0.0, v = 0.0;
+                for (int jb = diagonal ? ib : 0; jb < a; ++jb) {
+                    const size_t sj = J * block_len + static_cast<size_t>(jb) * 32 + lane;
+                    const int s_ok = sj < n ? 1 : 0;
+                    const double sx = s_ok ? x[sj] : 0.0, sy = s_ok ? y[sj] : 0.0;
+                    const double sg = s_ok ? P::kScale * gs[sj] : 0.0;
+                    if (diagonal && jb == ib) {
+                        sym::one_sided_tile<P>(g, tx, ty, t_ok, sx, sy, sg, s_ok, true, u, v);
+                        continue;
+                    }
+                    double ru = reaction[jb * 32 + lane].x, rv = reaction[jb * 32 + lane].y;
+                    sym::react_tile<P>(g, tx, ty, tg, t_ok, sx, sy, sg, s_ok, u, v, ru, rv);
+                    reaction[jb * 32 + lane] = make_double2(ru, rv);
+                }
+                if (diagonal) {  // reactions from the sub-blocks before this one in the same block
+                    const double2 r = reaction[ib * 32 + lane];
+                    u += r.x;
+                    v += r.y;
+                }
+                if (t_ok) {
+                    pu[J * stride + ti] = u;
+                    pv[J * stride + ti] = v;
+                }
             }
         }
         if (!diagonal) {
@@ -180,36 +227,62 @@ __global__ void __launch_bounds__(kThreads)
     }
 }
 
-int resident_ctas(int a, int precision) {
-    static std::atomic<int> cached[2][17] = {};  // host threads may ask at once
-    if (a < 1 || a > 16)
+// Targets per lane of the plane's items off the diagonal: 4 below kSymmetricPlaneWideN, 8 from
+// there up. Eight divide the shuffles per pair further but hold 168 registers (3 CTAs per SM), and
+// their blocks of at least 8 sub-blocks leave too few items to balance below that size.
+constexpr int kPlaneTargets = 4;
+constexpr int kPlaneTargetsWide = 8;
+
+enum SymKernel : int { SYM_PERIODIC = 0, SYM_PERIODIC32 = 1, SYM_PLANE = 2, SYM_PLANE_WIDE = 3 };
+
+int kernel_of(const SymmetricPlan &p) {
+    if (p.geometry == GEO_INFINITE)
+        return p.targets == kPlaneTargetsWide ? SYM_PLANE_WIDE : SYM_PLANE;
+    return p.precision == PV_PRECISION_FP32C ? SYM_PERIODIC32 : SYM_PERIODIC;
+}
+
+int resident_ctas(int a, int kernel) {
+    static std::atomic<int> cached[4][17] = {};  // host threads may ask at once
+    if (a < 1 || a > 16 || kernel < 0 || kernel > 3)
         return 1;
-    const int q = precision == PV_PRECISION_FP32C ? 1 : 0;
-    if (!cached[q][a].load(std::memory_order_relaxed)) {
+    if (!cached[kernel][a].load(std::memory_order_relaxed)) {
         int blocks = 0;
         const size_t smem = static_cast<size_t>(kThreads / 32) * a * 32 * sizeof(double2);
-        const cudaError_t e =
-            q ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, periodic_symmetric32_kernel,
-                                                              kThreads, smem)
-              : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, periodic_symmetric_kernel,
+        cudaError_t e;
+        if (kernel == SYM_PERIODIC32)
+            e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, periodic_symmetric32_kernel,
                                                               kThreads, smem);
+        else if (kernel == SYM_PLANE)
+            e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+                &blocks, symmetric_kernel<sym::PlaneSym, kPlaneTargets>, kThreads, smem);
+        else if (kernel == SYM_PLANE_WIDE)
+            e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+                &blocks, symmetric_kernel<sym::PlaneSym, kPlaneTargetsWide>, kThreads, smem);
+        else
+            e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+                &blocks, symmetric_kernel<sym::PeriodicSym, 1>, kThreads, smem);
         if (e != cudaSuccess || blocks < 1)
             blocks = 1;
-        cached[q][a].store(blocks, std::memory_order_relaxed);
+        cached[kernel][a].store(blocks, std::memory_order_relaxed);
     }
-    return cached[q][a].load(std::memory_order_relaxed);
+    return cached[kernel][a].load(std::memory_order_relaxed);
 }
 
 }  // namespace
 
-SymmetricPlan plan_symmetric(size_t n, int sm_count, int precision) {
+SymmetricPlan plan_symmetric(size_t n, int sm_count, int precision, int geometry) {
     SymmetricPlan p{};
-    if (n < kSymmetricMinN)
+    const bool plane = geometry == GEO_INFINITE;
+    if (plane ? (precision != PV_PRECISION_FP64 || n < kSymmetricPlaneMinN)
+              : (geometry != GEO_PERIODIC || n < kSymmetricMinN))
         return p;
     // the smallest block that keeps the partial rows within kSymmetricPartialBytes, or the largest
-    // block up to kSymmetricPartialBytesMax (N ~ 3.7e5); beyond that the ordered kernel runs
+    // block up to kSymmetricPartialBytesMax (N ~ 3.7e5); beyond that the ordered kernel runs. The
+    // plane's blocks hold at least as many sub-blocks as a lane holds targets.
+    const int targets =
+        plane ? (n >= kSymmetricPlaneWideN ? kPlaneTargetsWide : kPlaneTargets) : 1;
     const size_t np = (n + 255) & ~static_cast<size_t>(255);
-    for (int a = 1; a <= 16; a *= 2) {
+    for (int a = targets; a <= 16; a *= 2) {
         const size_t blocks = (n + 32 * static_cast<size_t>(a) - 1) / (32 * static_cast<size_t>(a));
         if (blocks > 0xffffu)
             continue;
@@ -218,8 +291,10 @@ SymmetricPlan plan_symmetric(size_t n, int sm_count, int precision) {
             p.a = a;
             p.blocks = static_cast<int>(blocks);
             p.items = static_cast<unsigned>(blocks * (blocks + 1) / 2);
-            p.grid = std::max(sm_count, 1) * resident_ctas(a, precision);
             p.precision = precision;
+            p.geometry = geometry;
+            p.targets = targets;
+            p.grid = std::max(sm_count, 1) * resident_ctas(a, kernel_of(p));
             return p;
         }
     }
@@ -233,20 +308,32 @@ void symmetric_items(const SymmetricPlan &p, unsigned *out) {
             out[k++] = (i << 16) | j;
 }
 
-cudaError_t launch_periodic_symmetric(const double *x, const double *y, const double *gs, size_t n,
-                                      const SymmetricPlan &p, const unsigned *items,
-                                      unsigned *counter, double *pu, double *pv, size_t stride,
-                                      const GeometryConsts &g, cudaStream_t stream) {
+cudaError_t launch_symmetric(const double *x, const double *y, const double *gs, size_t n,
+                             const SymmetricPlan &p, const unsigned *items, unsigned *counter,
+                             double *pu, double *pv, size_t stride, const GeometryConsts &g,
+                             cudaStream_t stream) {
     cudaError_t e = cudaMemsetAsync(counter, 0, sizeof(unsigned), stream);
     if (e != cudaSuccess)
         return e;
     const size_t smem = static_cast<size_t>(kThreads / 32) * p.a * 32 * sizeof(double2);
-    if (p.precision == PV_PRECISION_FP32C)
+    switch (kernel_of(p)) {
+    case SYM_PERIODIC32:
         periodic_symmetric32_kernel<<<p.grid, kThreads, smem, stream>>>(
             x, y, gs, n, p.a, items, p.items, counter, pu, pv, stride, g);
-    else
-        periodic_symmetric_kernel<<<p.grid, kThreads, smem, stream>>>(
+        break;
+    case SYM_PLANE:
+        symmetric_kernel<sym::PlaneSym, kPlaneTargets><<<p.grid, kThreads, smem, stream>>>(
             x, y, gs, n, p.a, items, p.items, counter, pu, pv, stride, g);
+        break;
+    case SYM_PLANE_WIDE:
+        symmetric_kernel<sym::PlaneSym, kPlaneTargetsWide><<<p.grid, kThreads, smem, stream>>>(
+            x, y, gs, n, p.a, items, p.items, counter, pu, pv, stride, g);
+        break;
+    default:
+        symmetric_kernel<sym::PeriodicSym, 1><<<p.grid, kThreads, smem, stream>>>(
+            x, y, gs, n, p.a, items, p.items, counter, pu, pv, stride, g);
+        break;
+    }
     return cudaGetLastError();
 }
 

@@ -1,12 +1,13 @@
-// pv_symmetric.cuh — warp tiles of the periodic box evaluated once per unordered pair, shared by
-// the single-simulation kernel (pv_symmetric.cu) and the batched ensembles (pv_batch.cu).
+// pv_symmetric.cuh — warp tiles evaluated once per unordered pair (periodic box, infinite plane),
+// shared by the single-simulation kernels (pv_symmetric.cu) and the batched ensembles
+// (pv_batch.cu).
 //
 // A tile is 32 targets (one per lane) against 32 sources. The sources, with the reactions they
 // accumulate, rotate one lane per step by shuffles; after 32 steps every (target, source) pair has
 // been met once and every source is back in its home lane. The pair terms are exactly odd under
-// exchanging target and source (PeriodicPair::terms), so one evaluation gives the target's term
-// and, with the other circulation and the opposite sign, the source's. The terms carry half sines
-// (PeriodicPair::terms<true>), so callers pass doubled scaled circulations: 2 * Gamma * 0.5/L.
+// exchanging target and source, so one evaluation gives the target's term and, with the other
+// circulation and the opposite sign, the source's. Callers pass the scaled circulations times
+// the policy's kScale (the periodic terms carry half sines: 2 * Gamma * 0.5/L).
 #pragma once
 
 #include "pv_geometry.cuh"
@@ -19,36 +20,55 @@ __device__ __forceinline__ double rotate(double v, int from) {
     return __shfl_sync(0xffffffffu, v, from);
 }
 
-__device__ __forceinline__ void kernel_values(const GeometryConsts &g, double tx, double ty,
-                                              double sx, double sy, double &ku, double &kv) {
-    double au, bu, av, bv;
-    PeriodicPair::terms<true>(g, tx, ty, sx, sy, au, bu, av, bv);
-    ku = au * rcp_refined(bu);
-    kv = av * rcp_refined(bv);
-}
+// Pair kernels K of the geometries evaluated this way: the target's velocity changes by
+// u -= c_s K_u, v += c_s K_v and the source's by u += c_t K_u, v -= c_t K_v, where c is the
+// stored scaled circulation times kScale.
+struct PeriodicSym {
+    // the terms carry half sines (PeriodicPair::terms<true>): circulations are doubled
+    static constexpr double kScale = 2.0;
+    __device__ __forceinline__ static void values(const GeometryConsts &g, double tx, double ty,
+                                                  double sx, double sy, double &ku, double &kv) {
+        double au, bu, av, bv;
+        PeriodicPair::terms<true>(g, tx, ty, sx, sy, au, bu, av, bv);
+        ku = au * rcp_refined(bu);
+        kv = av * rcp_refined(bv);
+    }
+};
 
-// Targets (tx, ty, tg2) against the sources held in the lanes (sx, sy, sg2 and their reactions
+// The infinite plane (InfinitePair): K = (dy, dx) / (r^2 + eps^2), exactly odd in (dx, dy).
+struct PlaneSym {
+    static constexpr double kScale = 1.0;
+    __device__ __forceinline__ static void values(const GeometryConsts &g, double tx, double ty,
+                                                  double sx, double sy, double &ku, double &kv) {
+        const double dx = tx - sx, dy = ty - sy;
+        const double inv = rcp_refined(fma(dx, dx, fma(dy, dy, g.eps2)));
+        ku = dy * inv;
+        kv = dx * inv;
+    }
+};
+
+// Targets (tx, ty, tg) against the sources held in the lanes (sx, sy, sg and their reactions
 // ru, rv); adds the targets' sums to u, v and the sources' to ru, rv. Sources end at home.
 // FULL: all 32 targets and sources exist (every tile but the last block's), no predicates.
-template <bool FULL>
+template <class P, bool FULL>
 __device__ __forceinline__ void react_tile_t(const GeometryConsts &g, double tx, double ty,
-                                             double tg2, bool t_ok, double sx, double sy,
-                                             double sg2, int s_ok, double &u, double &v,
+                                             double tg, bool t_ok, double sx, double sy,
+                                             double sg, int s_ok, double &u, double &v,
                                              double &ru, double &rv) {
     const int next = (threadIdx.x + 1) & 31;
 #pragma unroll 2
     for (int k = 0; k < 32; ++k) {
         if (FULL || (t_ok && s_ok)) {
             double ku, kv;
-            kernel_values(g, tx, ty, sx, sy, ku, kv);
-            u = fma(-sg2, ku, u);   // target: -g_s K
-            v = fma(sg2, kv, v);
-            ru = fma(tg2, ku, ru);  // source: the exchanged pair, +g_t K
-            rv = fma(-tg2, kv, rv);
+            P::values(g, tx, ty, sx, sy, ku, kv);
+            u = fma(-sg, ku, u);   // target: -c_s K
+            v = fma(sg, kv, v);
+            ru = fma(tg, ku, ru);  // source: the exchanged pair, +c_t K
+            rv = fma(-tg, kv, rv);
         }
         sx = rotate(sx, next);
         sy = rotate(sy, next);
-        sg2 = rotate(sg2, next);
+        sg = rotate(sg, next);
         ru = rotate(ru, next);
         rv = rotate(rv, next);
         if (!FULL)
@@ -56,32 +76,62 @@ __device__ __forceinline__ void react_tile_t(const GeometryConsts &g, double tx,
     }
 }
 
+template <class P = PeriodicSym>
 __device__ __forceinline__ void react_tile(const GeometryConsts &g, double tx, double ty,
-                                           double tg2, bool t_ok, double sx, double sy,
-                                           double sg2, int s_ok, double &u, double &v, double &ru,
+                                           double tg, bool t_ok, double sx, double sy, double sg,
+                                           int s_ok, double &u, double &v, double &ru,
                                            double &rv) {
     if (__all_sync(0xffffffffu, t_ok && s_ok))
-        react_tile_t<true>(g, tx, ty, tg2, t_ok, sx, sy, sg2, s_ok, u, v, ru, rv);
+        react_tile_t<P, true>(g, tx, ty, tg, t_ok, sx, sy, sg, s_ok, u, v, ru, rv);
     else
-        react_tile_t<false>(g, tx, ty, tg2, t_ok, sx, sy, sg2, s_ok, u, v, ru, rv);
+        react_tile_t<P, false>(g, tx, ty, tg, t_ok, sx, sy, sg, s_ok, u, v, ru, rv);
+}
+
+// T targets per lane (T sub-blocks of targets) against one sub-block of 32 sources, every target
+// and source present. Each rotation step serves T pairs, so the shuffles (five doubles a step)
+// per pair fall by T: for a cheap pair term (the plane's) they would otherwise bound the tile.
+template <class P, int T>
+__device__ __forceinline__ void react_tiles_full(const GeometryConsts &g, const double (&tx)[T],
+                                                 const double (&ty)[T], const double (&tg)[T],
+                                                 double sx, double sy, double sg, double (&u)[T],
+                                                 double (&v)[T], double &ru, double &rv) {
+    const int next = (threadIdx.x + 1) & 31;
+#pragma unroll 2
+    for (int k = 0; k < 32; ++k) {
+#pragma unroll
+        for (int t = 0; t < T; ++t) {
+            double ku, kv;
+            P::values(g, tx[t], ty[t], sx, sy, ku, kv);
+            u[t] = fma(-sg, ku, u[t]);
+            v[t] = fma(sg, kv, v[t]);
+            ru = fma(tg[t], ku, ru);
+            rv = fma(-tg[t], kv, rv);
+        }
+        sx = rotate(sx, next);
+        sy = rotate(sy, next);
+        sg = rotate(sg, next);
+        ru = rotate(ru, next);
+        rv = rotate(rv, next);
+    }
 }
 
 // Target side only. same_block: the sources are the targets' own lanes, so the self pair (k = 0)
-// is skipped; it contributes exactly 0 in the reference (sin 0 = 0).
+// is skipped; the reference skips it too (and in the periodic box it contributes exactly 0).
+template <class P = PeriodicSym>
 __device__ __forceinline__ void one_sided_tile(const GeometryConsts &g, double tx, double ty,
-                                               bool t_ok, double sx, double sy, double sg2,
+                                               bool t_ok, double sx, double sy, double sg,
                                                int s_ok, bool same_block, double &u, double &v) {
     const int next = (threadIdx.x + 1) & 31;
     for (int k = 0; k < 32; ++k) {
         if (t_ok && s_ok && !(same_block && k == 0)) {
             double ku, kv;
-            kernel_values(g, tx, ty, sx, sy, ku, kv);
-            u = fma(-sg2, ku, u);
-            v = fma(sg2, kv, v);
+            P::values(g, tx, ty, sx, sy, ku, kv);
+            u = fma(-sg, ku, u);
+            v = fma(sg, kv, v);
         }
         sx = rotate(sx, next);
         sy = rotate(sy, next);
-        sg2 = rotate(sg2, next);
+        sg = rotate(sg, next);
         s_ok = __shfl_sync(0xffffffffu, s_ok, next);
     }
 }

@@ -1,13 +1,14 @@
-"""The periodic box evaluated once per unordered pair (the device-state path from N = 2048 up):
-against the oracle and against the ordered-pair kernel, on ragged populations, with more than one
-sub-block per block (N = 24000), deterministic, and with the reference's errors."""
+"""The periodic box and the infinite plane evaluated once per unordered pair (the device-state
+path from N = 2048 and N = 16384 up): against the oracle and against the ordered-pair kernel, on
+ragged populations, with more than one sub-block per block, deterministic, and with the
+reference's errors."""
 import numpy as np
 import pytest
 
 import pointvortex_b200 as pv
 from conftest import golden, normalized_error
 from oracle.pyoracle import Geometry
-from pointvortex_b200 import ics
+from pointvortex_b200 import _lib, ics
 
 pytestmark = pytest.mark.gpu
 
@@ -79,3 +80,86 @@ def test_symmetric_coincident_pair_is_the_reference_error(port):
 def test_small_populations_use_the_ordered_kernel():
     x, y, g = ics.periodic_box(1024, 2, L)
     assert not kernel_with(x, y, g).statePlan()["symmetric"]
+
+
+# ---- the infinite plane (FP64 from N = 16384 up: four targets per lane off the diagonal, eight
+# from N = 32768 up) -----------------------------------------------------------------------------
+
+def plane_kernel_with(x, y, g, core=0.0):
+    k = pv.InfinitePlaneKernel(core)
+    k.uploadDeviceState(pv.VortexSystem(x, y, g))
+    return k
+
+
+@pytest.mark.parametrize("n,core", [(16384, 0.0), (16400, 0.0), (20000, 0.05)])
+def test_plane_symmetric_matches_oracle(reference, n, core):
+    """16400 and 20000 end in a ragged block (128-vortex blocks); 0.05 is a core radius."""
+    x, y, g = ics.infinite_plane(n, 70 + n)
+    k = plane_kernel_with(x, y, g, core)
+    plan = k.statePlan()
+    assert plan["symmetric"] and plan["rows"] == (n + 127) // 128
+    vel = k.evaluateDeviceState()
+    u, v = reference.evaluate(Geometry("infinite", core_radius=core), x, y, g)
+    assert normalized_error(vel.x, vel.y, u, v).max() <= 1e-12
+
+
+@pytest.mark.parametrize("n", [33000, 40000])
+def test_plane_symmetric_wide_against_ordered_and_oracle(port, n):
+    """Eight targets per lane (256-vortex blocks, ragged last block): all targets against the
+    ordered-pair kernel, the first and the last ones against the oracle."""
+    x, y, g = ics.infinite_plane(n, 17)
+    k = plane_kernel_with(x, y, g)
+    plan = k.statePlan()
+    assert plan["symmetric"] and plan["rows"] == (n + 255) // 256
+    vel = k.evaluateDeviceState()
+    ordered = k.evaluate(x, y, g)
+    assert normalized_error(vel.x, vel.y, ordered.x, ordered.y).max() <= 1e-12
+    geo = Geometry("infinite")
+    for t0, t1 in ((0, 40), (n - 40, n)):
+        u, v = port.evaluate_range(geo, x, y, g, t0, t1)
+        assert normalized_error(vel.x[t0:t1], vel.y[t0:t1], u, v).max() <= 1e-12
+
+
+def test_plane_symmetric_is_deterministic():
+    x, y, g = ics.infinite_plane(17000, 4)
+    k = plane_kernel_with(x, y, g)
+    a = k.evaluateDeviceState()
+    b = k.evaluateDeviceState()
+    assert np.array_equal(a.x, b.x) and np.array_equal(a.y, b.y)
+
+
+@pytest.mark.parametrize("n,i,j", [(16384, 7, 16000), (16384, 130, 131), (33000, 9, 32990)])
+def test_plane_symmetric_coincident_pair_is_the_reference_error(port, n, i, j):
+    """Off the diagonal and inside one sub-block; the oracle's error comes from a 64-vortex system
+    with the same coincidence."""
+    x, y, g = ics.infinite_plane(n, 5)
+    x[i], y[i] = x[j], y[j]
+    k = plane_kernel_with(x, y, g)
+    xs, ys, gs = ics.infinite_plane(64, 5)
+    xs[3], ys[3] = xs[40], ys[40]
+    with pytest.raises(RuntimeError) as want:
+        port.evaluate(Geometry("infinite"), xs, ys, gs)
+    with pytest.raises(RuntimeError) as got:
+        k.evaluateDeviceState()
+    assert str(got.value) == str(want.value)
+
+
+def test_plane_coincident_pair_with_core_is_finite(reference):
+    x, y, g = ics.infinite_plane(16384, 6)
+    x[9], y[9] = x[5000], y[5000]
+    k = plane_kernel_with(x, y, g, 0.01)
+    vel = k.evaluateDeviceState()
+    u, v = reference.evaluate(Geometry("infinite", core_radius=0.01), x, y, g)
+    assert normalized_error(vel.x, vel.y, u, v).max() <= 1e-12
+
+
+def test_small_plane_populations_use_the_ordered_kernel():
+    x, y, g = ics.infinite_plane(16000, 2)
+    assert not plane_kernel_with(x, y, g).statePlan()["symmetric"]
+
+
+def test_plane_fp32c_uses_the_ordered_kernel():
+    x, y, g = ics.infinite_plane(17000, 2)
+    k = pv.InfinitePlaneKernel(0.0, precision=_lib.PRECISION_FP32C)
+    k.uploadDeviceState(pv.VortexSystem(x, y, g))
+    assert not k.statePlan()["symmetric"]
