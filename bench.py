@@ -178,34 +178,45 @@ def run_ours(args):
     torch.cuda.synchronize()
 
     # timed region: CUDA events on the library's own stream bracket each step (kernels, copies
-    # and the gaps while the host reads the step-control word back); the library additionally
-    # brackets every launch with events so that the dominant kernel can be timed on its own
-    k.setProfiling(True)
+    # and the gaps while the host reads the step-control word back)
+    k.setProfiling(False)
     k.resetKernelStats()
-    evals = 0
-    pairs = 0.0
     lib_stream = torch.cuda.ExternalStream(k.cudaStream(), device=f"cuda:{local}")
-    events = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
-              for _ in range(args.steps)]
-    if world > 1:
-        torch.distributed.barrier()
-    torch.cuda.synchronize()
-    with ClockSampler(local) as clocks:
+
+    def run_steps(dt, record):
+        evals, pairs = 0, 0.0
+        events = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+                  for _ in range(args.steps)] if record else None
         for s in range(args.steps):
             flush_l2(flush)
             torch.cuda.synchronize()
             n_step = k.stateSize()       # the evaluations of a step run before its removals
-            events[s][0].record(lib_stream)
+            if record:
+                events[s][0].record(lib_stream)
             dt, e = dopri_step(k, dt, dipoles)
-            events[s][1].record(lib_stream)
+            if record:
+                events[s][1].record(lib_stream)
             evals += e
             pairs += e * n_step * (n_step - 1)
         torch.cuda.synchronize()
-    step_ms = [a.elapsed_time(b) for a, b in events]
-    stats = k.kernelStats()
-    k.setProfiling(False)
+        step_ms = [a.elapsed_time(b) for a, b in events] if record else None
+        return dt, evals, pairs, step_ms
+
+    if world > 1:
+        torch.distributed.barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clocks:
+        dt, evals, pairs, step_ms = run_steps(dt, True)
+        launches = sum(v[0] for v in k.kernelStats().values())
+        # kernel pass: the same number of steps again with every launch bracketed by events
+        # inside the library (pv_set_profiling). Those events are extra nodes of the attempt
+        # graph and lengthen the step, so this pass only times the kernels.
+        k.setProfiling(True)
+        k.resetKernelStats()
+        dt, _, pairs_profiled, _ = run_steps(dt, False)
+        stats = k.kernelStats()
+        k.setProfiling(False)
     total_ms = float(np.sum(step_ms))
-    pairs_local = pairs
     total_ms, pairs = combine_ranks(total_ms, pairs, f"cuda:{local}")
     value = pairs / (total_ms * 1e-3)
 
@@ -214,21 +225,20 @@ def run_ours(args):
     e2e = measure_e2e(k, dt, max(10, args.steps // 4), local, SEED + rank)
 
     # roofline of the dominant kernel (the tiled periodic pair kernel), from its launch events
+    # in the kernel pass: every timed velocity launch is one evaluation, its pairs over its time
     v_launch, v_timed, v_ms = stats["velocity"]
     per_launch_ms = v_ms / max(v_timed, 1)
-    # every timed velocity launch is one evaluation of the step loop: its pairs over its time
     plan = k.statePlan()
     if plan["symmetric"]:
         flops_per_ordered_pair = FLOPS_PER_UNORDERED_PAIR_SYMMETRIC / 2.0
-        kernel_name = "periodic_symmetric_kernel"
+        kernel_name = "symmetric_kernel<PeriodicSym, 1>"
     else:
         flops_per_ordered_pair = FLOPS_PER_PAIR_PERIODIC
         kernel_name = "velocity_kernel<PeriodicPair>"
-    achieved = flops_per_ordered_pair * pairs_local / (v_ms * 1e-3) / 1e12
+    achieved = flops_per_ordered_pair * pairs_profiled / (v_ms * 1e-3) / 1e12
     # measured FP64 FMA peak of this GPU (36.8 TFLOP/s at 1965 MHz on this pool's B200s when
     # the probe is skipped, e.g. under a profiler)
     peak = 36.83 if args.no_peak_probe else pv.probePeak("fp64", local) / 1e12
-    launches = sum(v[0] for v in stats.values())
 
     result = None
     if rank == 0:
@@ -263,6 +273,9 @@ def run_ours(args):
                          "flops_note": "algorithmic flops per ordered pair of the launched "
                                        "kernel (the symmetric form: 244 per unordered pair)",
                          "ms_per_launch": per_launch_ms, "launches": v_timed,
+                         "timing": "CUDA events around each launch on the library stream, in a "
+                                   "second pass of the same number of steps right after the "
+                                   "timed one",
                          "peak_source": "measured FP64 FMA probe (pv_probe_peak) on this GPU"},
             "kernel_ms": {kk: vv[2] for kk, vv in stats.items()},
             "clocks": clocks.summary(),
