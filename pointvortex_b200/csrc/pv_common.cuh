@@ -45,6 +45,15 @@ struct DeviceControl {
 };
 static_assert(sizeof(DeviceControl) == 256, "control block is one 256-byte line");
 
+// Programmatic dependent launch. The kernels of a step are launched so that the next one may be
+// scheduled while the previous one drains (launch_pdl); each of them first waits until the grid
+// before it has completed and its memory is visible, then lets its own successor be scheduled.
+// Without a programmatic predecessor the wait returns at once.
+__device__ __forceinline__ void pdl_enter() {
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+
 __device__ __forceinline__ void set_status(int *status, int code) { atomicMax(status, code); }
 // For end-of-operation checks that the reference makes only when nothing failed earlier.
 __device__ __forceinline__ void set_status_if_clean(int *status, int code) {

@@ -531,6 +531,7 @@ pv_status ensure_state_capacity(pv_context *c, size_t n) {
         symmetric_items(c->sym, items.data());
         PV_CUDA(c, c->sym_items.ensure((items.size() + 1) / 2));
         PV_CUDA(c, c->sym_counter.ensure(1));
+        PV_CUDA(c, cudaMemsetAsync(c->sym_counter.p, 0, 2 * sizeof(unsigned), c->stream));
         PV_CUDA(c, cudaMemcpyAsync(c->sym_items.p, items.data(), items.size() * sizeof(unsigned),
                                    cudaMemcpyHostToDevice, c->stream));
         PV_CUDA(c, cudaStreamSynchronize(c->stream));

@@ -38,6 +38,7 @@ __global__ void __launch_bounds__(kDT)
     dipole_scan_kernel(const double *x, const double *y, const double *g, size_t n,
                        GeometryConsts gc, double thr2, DipoleCandidateDev *out, size_t capacity,
                        unsigned long long *count, const DeviceControl *gate) {
+    pdl_enter();
     if (gate && !gate->accepted)  // after a DOPRI5 attempt: only the accepted state is scanned
         return;
     const size_t i0 = static_cast<size_t>(blockIdx.y) * kDT;
@@ -135,16 +136,23 @@ cudaError_t launch_dipole_scan(const double *x, const double *y, const double *g
                                DipoleCandidateDev *out, size_t capacity,
                                unsigned long long *count, cudaStream_t stream,
                                const DeviceControl *gate) {
-    cudaError_t e = cudaMemsetAsync(count, 0, sizeof(unsigned long long), stream);
-    if (e != cudaSuccess || n == 0)
-        return e;
+    // Gated (inside a DOPRI5 attempt): the count is the control block's, which the attempt's
+    // step control has zeroed, so no memset node splits the attempt's chain of kernels.
+    if (gate && count != &gate->dipole_count)
+        return cudaErrorInvalidValue;
+    if (!gate) {
+        const cudaError_t e = cudaMemsetAsync(count, 0, sizeof(unsigned long long), stream);
+        if (e != cudaSuccess)
+            return e;
+    }
+    if (n == 0)
+        return cudaSuccess;
     const size_t nt = (n + kDT - 1) / kDT, ns = (n + kDS - 1) / kDS;
     if (nt > 65535)
         return cudaErrorInvalidValue;
     const dim3 grid(static_cast<unsigned>(ns), static_cast<unsigned>(nt));
-    dipole_scan_kernel<<<grid, kDT, 0, stream>>>(x, y, gamma, n, g, threshold * threshold, out,
-                                                 capacity, count, gate);
-    return cudaGetLastError();
+    return launch_pdl(dipole_scan_kernel, grid, dim3(kDT), 0, stream, x, y, gamma, n, g,
+                      threshold * threshold, out, capacity, count, gate);
 }
 
 namespace {

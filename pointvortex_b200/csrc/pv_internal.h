@@ -11,6 +11,25 @@
 
 namespace pvb {
 
+// Launches a kernel that may be scheduled while the previous kernel of the stream drains
+// (programmatic stream serialization); the kernel calls pdl_enter() before touching memory, which
+// waits for that kernel to complete. In a stream capture the launch becomes a programmatic edge.
+template <typename... Params, typename... Args>
+cudaError_t launch_pdl(void (*kernel)(Params...), dim3 grid, dim3 block, size_t smem,
+                       cudaStream_t stream, Args... args) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = stream;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, kernel, static_cast<Params>(args)...);
+}
+
 // ---- velocity evaluation ---------------------------------------------------------------------
 // One launch evaluates targets [t_begin, t_end) against sources [0, n_src). The source range is
 // cut into `num_chunks` chunks; work item (target block, chunk) writes its partial sums to
@@ -67,6 +86,7 @@ constexpr size_t kSymmetricPartialBytes = static_cast<size_t>(256) << 20;  // a 
 constexpr size_t kSymmetricPartialBytesMax = static_cast<size_t>(4) << 30;  // beyond: ordered kernel
 SymmetricPlan plan_symmetric(size_t n, int sm_count, int precision, int geometry);
 void symmetric_items(const SymmetricPlan &p, unsigned *out);  // p.items packed (I << 16) | J
+// counter: two words, zero before the first launch; each launch leaves them zero again.
 cudaError_t launch_symmetric(const double *x, const double *y, const double *gs, size_t n,
                              const SymmetricPlan &p, const unsigned *items, unsigned *counter,
                              double *pu, double *pv, size_t stride, const GeometryConsts &g,

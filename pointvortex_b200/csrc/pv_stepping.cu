@@ -61,6 +61,7 @@ __device__ void dopri_control(DeviceControl *ctl) {
     }
     ctl->err_bits = 0ull;
     ctl->blocks_done = 0u;
+    ctl->dipole_count = 0ull;  // the attempt's gated dipole scan counts from here
 }
 } // namespace
 
@@ -153,6 +154,7 @@ __global__ void __launch_bounds__(256) stage_kernel(const StageArgs a) {
     __shared__ double s_max[8];
     __shared__ double s_u[WIDE ? kWideGroups : 1][kWideTargets],
         s_v[WIDE ? kWideGroups : 1][kWideTargets];
+    pdl_enter();
     const int tid = threadIdx.x;
     if (tid == 0)
         s_status = *reinterpret_cast<volatile int *>(&a.ctl->status);
@@ -231,6 +233,7 @@ __global__ void __launch_bounds__(256)
     accept_kernel(double *x, double *y, const double *xt, const double *yt, double *k0x,
                   double *k0y, const double *k6x, const double *k6y, size_t n, int dopri,
                   const DeviceControl *ctl) {
+    pdl_enter();
     if (ctl->status != 0 || (dopri && !ctl->accepted))
         return;
     for (size_t i = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; i < n;
@@ -261,11 +264,10 @@ cudaError_t launch_stage_mode(const StageArgs &a, cudaStream_t stream, int sm_co
         const size_t blocks = (a.n + kWideTargets - 1) / kWideTargets;
         const size_t cap = static_cast<size_t>(sm_count > 0 ? sm_count : 148) * 8;
         const unsigned grid = static_cast<unsigned>(blocks < 1 ? 1 : (blocks < cap ? blocks : cap));
-        stage_kernel<MODE, true><<<grid, 256, 0, stream>>>(a);
-    } else {
-        stage_kernel<MODE, false><<<grid_for(a.n, sm_count), 256, 0, stream>>>(a);
+        return launch_pdl(stage_kernel<MODE, true>, dim3(grid), dim3(256), 0, stream, a);
     }
-    return cudaGetLastError();
+    return launch_pdl(stage_kernel<MODE, false>, dim3(grid_for(a.n, sm_count)), dim3(256), 0,
+                      stream, a);
 }
 
 cudaError_t launch_stage(const StageArgs &a, cudaStream_t stream, int sm_count) {
@@ -286,9 +288,8 @@ cudaError_t launch_stage(const StageArgs &a, cudaStream_t stream, int sm_count) 
 cudaError_t launch_accept(double *x, double *y, const double *xt, const double *yt, double *k0x,
                           double *k0y, const double *k6x, const double *k6y, size_t n, int dopri,
                           DeviceControl *ctl, cudaStream_t stream) {
-    accept_kernel<<<grid_for(n, 0), 256, 0, stream>>>(x, y, xt, yt, k0x, k0y, k6x, k6y, n, dopri,
-                                                       ctl);
-    return cudaGetLastError();
+    return launch_pdl(accept_kernel, dim3(grid_for(n, 0)), dim3(256), 0, stream, x, y, xt, yt, k0x,
+                      k0y, k6x, k6y, n, dopri, ctl);
 }
 
 } // namespace pvb

@@ -35,6 +35,21 @@ namespace {
 
 constexpr int kThreads = 128;  // 4 independent warps per CTA
 
+// The work queue resets itself at the end of a launch, so no memset precedes the kernel:
+// counter[0] hands out items and counter[1] counts the warps that found the queue empty. Every warp
+// draws exactly one ticket past the end, and only after that increments counter[1]; the warp that
+// brings counter[1] to the grid's warp count is the last to touch either word, and zeroes both.
+__device__ __forceinline__ void release_queue(unsigned *counter) {
+    if ((threadIdx.x & 31) != 0)
+        return;
+    const unsigned warps = gridDim.x * (kThreads / 32);
+    __threadfence();
+    if (atomicAdd(counter + 1, 1u) == warps - 1) {
+        atomicExch(counter, 0u);
+        atomicExch(counter + 1, 0u);
+    }
+}
+
 // P: the pair kernel (sym::PeriodicSym, sym::PlaneSym). T: targets per lane in the items off the
 // diagonal (a multiple of T sub-blocks per block); diagonal items hold one target per lane.
 template <class P, int T>
@@ -45,6 +60,7 @@ __global__ void __launch_bounds__(kThreads)
                      double *__restrict__ pu, double *__restrict__ pv, size_t stride,
                      GeometryConsts g) {
     extern __shared__ double2 reaction_smem[];
+    pdl_enter();
     const int lane = threadIdx.x & 31;
     double2 *reaction = reaction_smem + (threadIdx.x >> 5) * a * 32;  // this warp's sources
     const size_t block_len = static_cast<size_t>(32) * a;
@@ -143,6 +159,7 @@ __global__ void __launch_bounds__(kThreads)
         }
         __syncwarp();
     }
+    release_queue(counter);
 }
 
 // The FP32-compensated form of the same decomposition: the pair terms on the FP32 pipe from
@@ -156,6 +173,7 @@ __global__ void __launch_bounds__(kThreads)
     extern __shared__ double2 reaction_smem[];
     __shared__ float4 src_f[kThreads];
     __shared__ float src_g[kThreads];
+    pdl_enter();
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     double2 *reaction = reaction_smem + warp * a * 32;
     float4 *sf = src_f + warp * 32;
@@ -225,6 +243,7 @@ __global__ void __launch_bounds__(kThreads)
         }
         __syncwarp();
     }
+    release_queue(counter);
 }
 
 // Targets per lane of the plane's items off the diagonal: 4 below kSymmetricPlaneWideN, 8 from
@@ -312,29 +331,22 @@ cudaError_t launch_symmetric(const double *x, const double *y, const double *gs,
                              const SymmetricPlan &p, const unsigned *items, unsigned *counter,
                              double *pu, double *pv, size_t stride, const GeometryConsts &g,
                              cudaStream_t stream) {
-    cudaError_t e = cudaMemsetAsync(counter, 0, sizeof(unsigned), stream);
-    if (e != cudaSuccess)
-        return e;
     const size_t smem = static_cast<size_t>(kThreads / 32) * p.a * 32 * sizeof(double2);
+    const dim3 grid(static_cast<unsigned>(p.grid)), block(kThreads);
     switch (kernel_of(p)) {
     case SYM_PERIODIC32:
-        periodic_symmetric32_kernel<<<p.grid, kThreads, smem, stream>>>(
-            x, y, gs, n, p.a, items, p.items, counter, pu, pv, stride, g);
-        break;
+        return launch_pdl(periodic_symmetric32_kernel, grid, block, smem, stream, x, y, gs, n, p.a,
+                          items, p.items, counter, pu, pv, stride, g);
     case SYM_PLANE:
-        symmetric_kernel<sym::PlaneSym, kPlaneTargets><<<p.grid, kThreads, smem, stream>>>(
-            x, y, gs, n, p.a, items, p.items, counter, pu, pv, stride, g);
-        break;
+        return launch_pdl(symmetric_kernel<sym::PlaneSym, kPlaneTargets>, grid, block, smem,
+                          stream, x, y, gs, n, p.a, items, p.items, counter, pu, pv, stride, g);
     case SYM_PLANE_WIDE:
-        symmetric_kernel<sym::PlaneSym, kPlaneTargetsWide><<<p.grid, kThreads, smem, stream>>>(
-            x, y, gs, n, p.a, items, p.items, counter, pu, pv, stride, g);
-        break;
+        return launch_pdl(symmetric_kernel<sym::PlaneSym, kPlaneTargetsWide>, grid, block, smem,
+                          stream, x, y, gs, n, p.a, items, p.items, counter, pu, pv, stride, g);
     default:
-        symmetric_kernel<sym::PeriodicSym, 1><<<p.grid, kThreads, smem, stream>>>(
-            x, y, gs, n, p.a, items, p.items, counter, pu, pv, stride, g);
-        break;
+        return launch_pdl(symmetric_kernel<sym::PeriodicSym, 1>, grid, block, smem, stream, x, y,
+                          gs, n, p.a, items, p.items, counter, pu, pv, stride, g);
     }
-    return cudaGetLastError();
 }
 
 }  // namespace pvb

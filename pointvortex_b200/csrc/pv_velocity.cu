@@ -31,6 +31,7 @@ __global__ void __launch_bounds__(B) velocity_kernel(const EvalArgs a) {
     __shared__ alignas(8) uint64_t bars[2];
     __shared__ int s_status;
 
+    pdl_enter();
     const int tid = threadIdx.x;
     if (tid == 0)
         s_status = *reinterpret_cast<volatile int *>(a.status);
@@ -159,8 +160,8 @@ cudaError_t launch_t(const EvalArgs &a, const EvalPlan &p, cudaStream_t stream) 
     constexpr int B = 128;
     if (p.block != B)
         return cudaErrorInvalidConfiguration;
-    velocity_kernel<Pair, B, T><<<static_cast<unsigned>(p.items()), B, 0, stream>>>(a);
-    return cudaGetLastError();
+    return launch_pdl(velocity_kernel<Pair, B, T>, dim3(static_cast<unsigned>(p.items())), dim3(B),
+                      0, stream, a);
 }
 
 template <class Pair>

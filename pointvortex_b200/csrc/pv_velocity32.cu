@@ -39,6 +39,7 @@ __global__ void __launch_bounds__(B) velocity32_kernel(const EvalArgs a) {
     __shared__ alignas(8) uint64_t bars[2];
     __shared__ int s_status;
 
+    pdl_enter();
     const int tid = threadIdx.x;
     if (tid == 0)
         s_status = *reinterpret_cast<volatile int *>(a.status);
@@ -168,8 +169,8 @@ __global__ void __launch_bounds__(B) velocity32_kernel(const EvalArgs a) {
 }
 
 template <int GEO, int T> cudaError_t launch32_t(const EvalArgs &a, const EvalPlan &p, cudaStream_t s) {
-    velocity32_kernel<GEO, 128, T><<<static_cast<unsigned>(p.items()), 128, 0, s>>>(a);
-    return cudaGetLastError();
+    return launch_pdl(velocity32_kernel<GEO, 128, T>, dim3(static_cast<unsigned>(p.items())),
+                      dim3(128), 0, s, a);
 }
 
 template <int GEO> cudaError_t launch32_geo(const EvalArgs &a, const EvalPlan &p, cudaStream_t s) {
