@@ -57,6 +57,40 @@ def test_symmetric_with_sub_blocks_against_ordered_and_oracle(port):
     assert normalized_error(vel.x[n - 40:], vel.y[n - 40:], u, v).max() <= 1e-12
 
 
+@pytest.mark.parametrize("n", [3000, 4100, 8192])
+def test_symmetric_one_sub_block_against_ordered_and_oracle(port, n):
+    """One sub-block per block (ragged last block at 3000 and 4100): every target against the
+    ordered-pair kernel, three ranges against the oracle, and a repeated evaluation bit for
+    bit."""
+    x, y, g = ics.periodic_box(n, 31 + n, L)
+    k = kernel_with(x, y, g)
+    plan = k.statePlan()
+    assert plan["symmetric"] and plan["rows"] == (n + 31) // 32
+    vel = k.evaluateDeviceState()
+    ordered = k.evaluate(x, y, g)
+    assert normalized_error(vel.x, vel.y, ordered.x, ordered.y).max() <= 1e-12
+    geo = Geometry("periodic", box_length_x=L, box_length_y=L)
+    for t0, t1 in ((0, 48), (n // 2 - 24, n // 2 + 24), (n - 48, n)):
+        u, v = port.evaluate_range(geo, x, y, g, t0, t1)
+        assert normalized_error(vel.x[t0:t1], vel.y[t0:t1], u, v).max() <= 1e-12
+    again = k.evaluateDeviceState()
+    assert np.array_equal(vel.x, again.x) and np.array_equal(vel.y, again.y)
+
+
+def test_symmetric_coincident_pair_across_blocks_is_the_reference_error(port):
+    x, y, g = ics.periodic_box(4096, 8, L)
+    x[100], y[100] = x[3900], y[3900]
+    k = kernel_with(x, y, g)
+    xs, ys, gs = ics.periodic_box(64, 8, L)
+    xs[3], ys[3] = xs[40], ys[40]
+    geo = Geometry("periodic", box_length_x=L, box_length_y=L)
+    with pytest.raises(RuntimeError) as want:
+        port.evaluate(geo, xs, ys, gs)
+    with pytest.raises(RuntimeError) as got:
+        k.evaluateDeviceState()
+    assert str(got.value) == str(want.value)
+
+
 def test_symmetric_is_deterministic():
     x, y, g = ics.periodic_box(5000, 3, L)
     k = kernel_with(x, y, g)
