@@ -66,7 +66,7 @@ cudaError_t launch_velocity(const EvalArgs &a, const EvalPlan &p, cudaStream_t s
 // The FP32-compensated precision form (pv_velocity32.cu): same arguments, same partial layout.
 cudaError_t launch_velocity_fp32c(const EvalArgs &a, const EvalPlan &p, cudaStream_t stream);
 
-// The periodic box (FP64, FP32C) and the infinite plane (FP64) evaluated once per unordered pair
+// The periodic box and the infinite plane (FP64, FP32C) evaluated once per unordered pair
 // (pv_symmetric.cu) for a whole population (targets = sources). Partial rows: `blocks` rows of
 // the same layout as the chunk partials.
 struct SymmetricPlan {
@@ -81,6 +81,7 @@ struct SymmetricPlan {
 };
 constexpr size_t kSymmetricMinN = 2048;       // periodic box below: the ordered kernel
 constexpr size_t kSymmetricPlaneMinN = 16384;   // infinite plane below: the ordered kernel
+constexpr size_t kSymmetricPlane32MinN = 16384; // the same for the FP32-compensated plane
 constexpr size_t kSymmetricPlaneWideN = 32768;  // the plane from here: 8 targets per lane
 constexpr size_t kSymmetricPartialBytes = static_cast<size_t>(256) << 20;  // a grows past this
 constexpr size_t kSymmetricPartialBytesMax = static_cast<size_t>(4) << 30;  // beyond: ordered kernel

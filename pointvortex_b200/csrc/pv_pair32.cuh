@@ -139,6 +139,31 @@ __device__ __forceinline__ void periodic_values32(const F32Geometry &f, const fl
     kv = sin_x * fmaf(d0v, fmaf(dv, rv, nv), dv) * rcp_approx_f32(d0v * dv);
 }
 
+// The plane's kernel values in FP32: K = (dy, dx) / (r^2 + eps^2) from the double-float
+// displacement. Exactly odd under exchanging target and source, as periodic_values32.
+__device__ __forceinline__ void plane_values32(const F32Geometry &f, const float4 t,
+                                               const float4 s, float &ku, float &kv) {
+    const float dx = (t.x - s.x) + (t.z - s.z);
+    const float dy = (t.y - s.y) + (t.w - s.w);
+    const float inv = rcp_approx_f32(fmaf(dx, dx, fmaf(dy, dy, f.eps2)));
+    ku = dy * inv;
+    kv = dx * inv;
+}
+
+// The pair kernels of the FP32 symmetric tiles (circulations enter unscaled).
+struct Periodic32 {
+    __device__ __forceinline__ static void values(const F32Geometry &f, const float4 t,
+                                                  const float4 s, float &ku, float &kv) {
+        periodic_values32(f, t, s, ku, kv);
+    }
+};
+struct Plane32 {
+    __device__ __forceinline__ static void values(const F32Geometry &f, const float4 t,
+                                                  const float4 s, float &ku, float &kv) {
+        plane_values32(f, t, s, ku, kv);
+    }
+};
+
 template <int GEO, bool CHECK>
 __device__ __forceinline__ void pair32(const F32Geometry &f, const GeometryConsts &g,
                                        const Target32 &t, const float4 s, float sgf, double sxd,

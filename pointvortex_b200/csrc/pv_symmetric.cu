@@ -1,5 +1,5 @@
 // pv_symmetric.cu — the velocity of a whole population evaluated once per unordered pair: the
-// periodic box (FP64 and FP32-compensated) and the infinite plane (FP64).
+// periodic box and the infinite plane, each in FP64 and in the FP32-compensated form.
 //
 // The reference evaluates every ordered pair (src/compute.cpp:203-256 for the box, :88-133 for
 // the plane). The Weiss–McWilliams pair term is antisymmetric: exchanging target and source
@@ -163,13 +163,17 @@ __global__ void __launch_bounds__(kThreads)
 }
 
 // The FP32-compensated form of the same decomposition: the pair terms on the FP32 pipe from
-// double-float coordinates; each tile's FP32 sums (32 sources) are promoted into FP64.
+// double-float coordinates; each tile's FP32 sums (32 sources) are promoted into FP64. The
+// sources of a tile sit in this warp's shared buffer and only the FP32 reactions rotate.
+// V: the pair kernel (f32::Periodic32, f32::Plane32). T: targets per lane in the items off the
+// diagonal, as in symmetric_kernel.
+template <class V, int T>
 __global__ void __launch_bounds__(kThreads)
-    periodic_symmetric32_kernel(const double *__restrict__ x, const double *__restrict__ y,
-                                const double *__restrict__ gs, size_t n, int a,
-                                const unsigned *__restrict__ items, unsigned n_items,
-                                unsigned *counter, double *__restrict__ pu,
-                                double *__restrict__ pv, size_t stride, GeometryConsts g) {
+    symmetric32_kernel(const double *__restrict__ x, const double *__restrict__ y,
+                       const double *__restrict__ gs, size_t n, int a,
+                       const unsigned *__restrict__ items, unsigned n_items, unsigned *counter,
+                       double *__restrict__ pu, double *__restrict__ pv, size_t stride,
+                       GeometryConsts g) {
     extern __shared__ double2 reaction_smem[];
     __shared__ float4 src_f[kThreads];
     __shared__ float src_g[kThreads];
@@ -192,43 +196,109 @@ __global__ void __launch_bounds__(kThreads)
         const bool diagonal = I == J;
         for (int jb = 0; jb < a; ++jb)
             reaction[jb * 32 + lane] = make_double2(0.0, 0.0);
-        for (int ib = 0; ib < a; ++ib) {
-            const size_t t0 = I * block_len + static_cast<size_t>(ib) * 32;
-            const size_t ti = t0 + lane;
-            const bool t_ok = ti < n;
-            const float4 t = sym::split32(t_ok ? x[ti] : 0.0, t_ok ? y[ti] : 0.0);
-            const float tg = t_ok ? static_cast<float>(gs[ti]) : 0.0f;
-            double ud = 0.0, vd = 0.0;
-            for (int jb = diagonal ? ib : 0; jb < a; ++jb) {
-                const size_t j0 = J * block_len + static_cast<size_t>(jb) * 32;
-                const size_t sj = j0 + lane;
-                const int s_count = j0 < n ? static_cast<int>(min(static_cast<size_t>(32), n - j0)) : 0;
-                __syncwarp();  // the previous tile's reads of the buffer are done
-                sf[lane] = sym::split32(sj < n ? x[sj] : 0.0, sj < n ? y[sj] : 0.0);
-                sgf[lane] = sj < n ? static_cast<float>(gs[sj]) : 0.0f;
-                __syncwarp();
-                float u = 0.0f, v = 0.0f;
-                if (diagonal && jb == ib) {
-                    sym::one_sided_tile32(f, t, t_ok, sf, sgf, s_count, true, u, v);
-                } else {
-                    float ru = 0.0f, rv = 0.0f;
-                    sym::react_tile32(f, t, tg, t_ok, sf, sgf, s_count, u, v, ru, rv);
-                    double2 r = reaction[jb * 32 + lane];
-                    r.x += static_cast<double>(ru);
-                    r.y += static_cast<double>(rv);
-                    reaction[jb * 32 + lane] = r;
+        if (T > 1 && !diagonal) {
+            for (int ib = 0; ib < a; ib += T) {
+                float4 t[T];
+                float tg[T];
+                bool t_ok[T], all_ok = true;
+                double ud[T], vd[T];
+#pragma unroll
+                for (int q = 0; q < T; ++q) {
+                    const size_t ti = I * block_len + static_cast<size_t>(ib + q) * 32 + lane;
+                    t_ok[q] = ti < n;
+                    all_ok = all_ok && t_ok[q];
+                    t[q] = sym::split32(t_ok[q] ? x[ti] : 0.0, t_ok[q] ? y[ti] : 0.0);
+                    tg[q] = t_ok[q] ? static_cast<float>(gs[ti]) : 0.0f;
+                    ud[q] = 0.0;
+                    vd[q] = 0.0;
                 }
-                ud += static_cast<double>(u);
-                vd += static_cast<double>(v);
+                for (int jb = 0; jb < a; ++jb) {
+                    const size_t j0 = J * block_len + static_cast<size_t>(jb) * 32;
+                    const size_t sj = j0 + lane;
+                    const int s_count =
+                        j0 < n ? static_cast<int>(min(static_cast<size_t>(32), n - j0)) : 0;
+                    __syncwarp();  // the previous tile's reads of the buffer are done
+                    sf[lane] = sym::split32(sj < n ? x[sj] : 0.0, sj < n ? y[sj] : 0.0);
+                    sgf[lane] = sj < n ? static_cast<float>(gs[sj]) : 0.0f;
+                    __syncwarp();
+                    float u[T], v[T];
+#pragma unroll
+                    for (int q = 0; q < T; ++q) {
+                        u[q] = 0.0f;
+                        v[q] = 0.0f;
+                    }
+                    double rud = 0.0, rvd = 0.0;
+                    if (__all_sync(0xffffffffu, all_ok && s_count == 32)) {
+                        sym::react_tiles32_full<V, T>(f, t, tg, sf, sgf, u, v, rud, rvd);
+                    } else {
+#pragma unroll
+                        for (int q = 0; q < T; ++q) {
+                            float ru = 0.0f, rv = 0.0f;
+                            sym::react_tile32<V>(f, t[q], tg[q], t_ok[q], sf, sgf, s_count, u[q],
+                                                 v[q], ru, rv);
+                            rud += static_cast<double>(ru);
+                            rvd += static_cast<double>(rv);
+                        }
+                    }
+                    double2 r = reaction[jb * 32 + lane];
+                    r.x += rud;
+                    r.y += rvd;
+                    reaction[jb * 32 + lane] = r;
+#pragma unroll
+                    for (int q = 0; q < T; ++q) {
+                        ud[q] += static_cast<double>(u[q]);
+                        vd[q] += static_cast<double>(v[q]);
+                    }
+                }
+#pragma unroll
+                for (int q = 0; q < T; ++q) {
+                    const size_t ti = I * block_len + static_cast<size_t>(ib + q) * 32 + lane;
+                    if (t_ok[q]) {
+                        pu[J * stride + ti] = ud[q];
+                        pv[J * stride + ti] = vd[q];
+                    }
+                }
             }
-            if (diagonal) {
-                const double2 r = reaction[ib * 32 + lane];
-                ud += r.x;
-                vd += r.y;
-            }
-            if (t_ok) {
-                pu[J * stride + ti] = ud;
-                pv[J * stride + ti] = vd;
+        } else {
+            for (int ib = 0; ib < a; ++ib) {
+                const size_t t0 = I * block_len + static_cast<size_t>(ib) * 32;
+                const size_t ti = t0 + lane;
+                const bool t_ok = ti < n;
+                const float4 t = sym::split32(t_ok ? x[ti] : 0.0, t_ok ? y[ti] : 0.0);
+                const float tg = t_ok ? static_cast<float>(gs[ti]) : 0.0f;
+                double ud = 0.0, vd = 0.0;
+                for (int jb = diagonal ? ib : 0; jb < a; ++jb) {
+                    const size_t j0 = J * block_len + static_cast<size_t>(jb) * 32;
+                    const size_t sj = j0 + lane;
+                    const int s_count =
+                        j0 < n ? static_cast<int>(min(static_cast<size_t>(32), n - j0)) : 0;
+                    __syncwarp();  // the previous tile's reads of the buffer are done
+                    sf[lane] = sym::split32(sj < n ? x[sj] : 0.0, sj < n ? y[sj] : 0.0);
+                    sgf[lane] = sj < n ? static_cast<float>(gs[sj]) : 0.0f;
+                    __syncwarp();
+                    float u = 0.0f, v = 0.0f;
+                    if (diagonal && jb == ib) {
+                        sym::one_sided_tile32<V>(f, t, t_ok, sf, sgf, s_count, true, u, v);
+                    } else {
+                        float ru = 0.0f, rv = 0.0f;
+                        sym::react_tile32<V>(f, t, tg, t_ok, sf, sgf, s_count, u, v, ru, rv);
+                        double2 r = reaction[jb * 32 + lane];
+                        r.x += static_cast<double>(ru);
+                        r.y += static_cast<double>(rv);
+                        reaction[jb * 32 + lane] = r;
+                    }
+                    ud += static_cast<double>(u);
+                    vd += static_cast<double>(v);
+                }
+                if (diagonal) {
+                    const double2 r = reaction[ib * 32 + lane];
+                    ud += r.x;
+                    vd += r.y;
+                }
+                if (t_ok) {
+                    pu[J * stride + ti] = ud;
+                    pv[J * stride + ti] = vd;
+                }
             }
         }
         if (!diagonal) {
@@ -252,36 +322,59 @@ __global__ void __launch_bounds__(kThreads)
 constexpr int kPlaneTargets = 4;
 constexpr int kPlaneTargetsWide = 8;
 
-enum SymKernel : int { SYM_PERIODIC = 0, SYM_PERIODIC32 = 1, SYM_PLANE = 2, SYM_PLANE_WIDE = 3 };
+enum SymKernel : int {
+    SYM_PERIODIC = 0,
+    SYM_PERIODIC32 = 1,
+    SYM_PLANE = 2,
+    SYM_PLANE_WIDE = 3,
+    SYM_PLANE32 = 4,
+    SYM_PLANE32_WIDE = 5,
+    SYM_KERNELS = 6
+};
 
 int kernel_of(const SymmetricPlan &p) {
-    if (p.geometry == GEO_INFINITE)
-        return p.targets == kPlaneTargetsWide ? SYM_PLANE_WIDE : SYM_PLANE;
-    return p.precision == PV_PRECISION_FP32C ? SYM_PERIODIC32 : SYM_PERIODIC;
+    const bool fp32c = p.precision == PV_PRECISION_FP32C;
+    if (p.geometry == GEO_INFINITE) {
+        const bool wide = p.targets == kPlaneTargetsWide;
+        return fp32c ? (wide ? SYM_PLANE32_WIDE : SYM_PLANE32) : (wide ? SYM_PLANE_WIDE : SYM_PLANE);
+    }
+    return fp32c ? SYM_PERIODIC32 : SYM_PERIODIC;
+}
+
+template <typename K> int occupancy(K kernel, size_t smem) {
+    int blocks = 0;
+    const cudaError_t e =
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, kernel, kThreads, smem);
+    return e == cudaSuccess && blocks >= 1 ? blocks : 1;
 }
 
 int resident_ctas(int a, int kernel) {
-    static std::atomic<int> cached[4][17] = {};  // host threads may ask at once
-    if (a < 1 || a > 16 || kernel < 0 || kernel > 3)
+    static std::atomic<int> cached[SYM_KERNELS][17] = {};  // host threads may ask at once
+    if (a < 1 || a > 16 || kernel < 0 || kernel >= SYM_KERNELS)
         return 1;
     if (!cached[kernel][a].load(std::memory_order_relaxed)) {
-        int blocks = 0;
         const size_t smem = static_cast<size_t>(kThreads / 32) * a * 32 * sizeof(double2);
-        cudaError_t e;
-        if (kernel == SYM_PERIODIC32)
-            e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, periodic_symmetric32_kernel,
-                                                              kThreads, smem);
-        else if (kernel == SYM_PLANE)
-            e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-                &blocks, symmetric_kernel<sym::PlaneSym, kPlaneTargets>, kThreads, smem);
-        else if (kernel == SYM_PLANE_WIDE)
-            e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-                &blocks, symmetric_kernel<sym::PlaneSym, kPlaneTargetsWide>, kThreads, smem);
-        else
-            e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-                &blocks, symmetric_kernel<sym::PeriodicSym, 1>, kThreads, smem);
-        if (e != cudaSuccess || blocks < 1)
-            blocks = 1;
+        int blocks = 1;
+        switch (kernel) {
+        case SYM_PERIODIC32:
+            blocks = occupancy(symmetric32_kernel<f32::Periodic32, 1>, smem);
+            break;
+        case SYM_PLANE:
+            blocks = occupancy(symmetric_kernel<sym::PlaneSym, kPlaneTargets>, smem);
+            break;
+        case SYM_PLANE_WIDE:
+            blocks = occupancy(symmetric_kernel<sym::PlaneSym, kPlaneTargetsWide>, smem);
+            break;
+        case SYM_PLANE32:
+            blocks = occupancy(symmetric32_kernel<f32::Plane32, kPlaneTargets>, smem);
+            break;
+        case SYM_PLANE32_WIDE:
+            blocks = occupancy(symmetric32_kernel<f32::Plane32, kPlaneTargetsWide>, smem);
+            break;
+        default:
+            blocks = occupancy(symmetric_kernel<sym::PeriodicSym, 1>, smem);
+            break;
+        }
         cached[kernel][a].store(blocks, std::memory_order_relaxed);
     }
     return cached[kernel][a].load(std::memory_order_relaxed);
@@ -292,7 +385,7 @@ int resident_ctas(int a, int kernel) {
 SymmetricPlan plan_symmetric(size_t n, int sm_count, int precision, int geometry) {
     SymmetricPlan p{};
     const bool plane = geometry == GEO_INFINITE;
-    if (plane ? (precision != PV_PRECISION_FP64 || n < kSymmetricPlaneMinN)
+    if (plane ? n < (precision == PV_PRECISION_FP32C ? kSymmetricPlane32MinN : kSymmetricPlaneMinN)
               : (geometry != GEO_PERIODIC || n < kSymmetricMinN))
         return p;
     // the smallest block that keeps the partial rows within kSymmetricPartialBytes, or the largest
@@ -335,13 +428,19 @@ cudaError_t launch_symmetric(const double *x, const double *y, const double *gs,
     const dim3 grid(static_cast<unsigned>(p.grid)), block(kThreads);
     switch (kernel_of(p)) {
     case SYM_PERIODIC32:
-        return launch_pdl(periodic_symmetric32_kernel, grid, block, smem, stream, x, y, gs, n, p.a,
-                          items, p.items, counter, pu, pv, stride, g);
+        return launch_pdl(symmetric32_kernel<f32::Periodic32, 1>, grid, block, smem, stream, x, y,
+                          gs, n, p.a, items, p.items, counter, pu, pv, stride, g);
     case SYM_PLANE:
         return launch_pdl(symmetric_kernel<sym::PlaneSym, kPlaneTargets>, grid, block, smem,
                           stream, x, y, gs, n, p.a, items, p.items, counter, pu, pv, stride, g);
     case SYM_PLANE_WIDE:
         return launch_pdl(symmetric_kernel<sym::PlaneSym, kPlaneTargetsWide>, grid, block, smem,
+                          stream, x, y, gs, n, p.a, items, p.items, counter, pu, pv, stride, g);
+    case SYM_PLANE32:
+        return launch_pdl(symmetric32_kernel<f32::Plane32, kPlaneTargets>, grid, block, smem,
+                          stream, x, y, gs, n, p.a, items, p.items, counter, pu, pv, stride, g);
+    case SYM_PLANE32_WIDE:
+        return launch_pdl(symmetric32_kernel<f32::Plane32, kPlaneTargetsWide>, grid, block, smem,
                           stream, x, y, gs, n, p.a, items, p.items, counter, pu, pv, stride, g);
     default:
         return launch_pdl(symmetric_kernel<sym::PeriodicSym, 1>, grid, block, smem, stream, x, y,

@@ -138,8 +138,9 @@ __device__ __forceinline__ void one_sided_tile(const GeometryConsts &g, double t
 
 // FP32-compensated tiles: the 32 sources (hi/lo coordinates and FP32 circulation) sit in this
 // warp's shared buffer, read at index (lane + k) & 31; only their FP32 reactions rotate through
-// the lanes. The callers promote the FP32 sums of each tile into FP64.
-template <bool FULL>
+// the lanes. V: the pair kernel (f32::Periodic32, f32::Plane32). The callers promote the FP32
+// sums of each tile into FP64.
+template <class V, bool FULL>
 __device__ __forceinline__ void react_tile32_t(const f32::F32Geometry &f, const float4 t, float tg,
                                                bool t_ok, const float4 *sf, const float *sg,
                                                int s_count, float &u, float &v, float &ru,
@@ -150,7 +151,7 @@ __device__ __forceinline__ void react_tile32_t(const f32::F32Geometry &f, const 
         const int j = (lane + k) & 31;
         if (FULL || (t_ok && j < s_count)) {
             float ku, kv;
-            f32::periodic_values32(f, t, sf[j], ku, kv);
+            V::values(f, t, sf[j], ku, kv);
             const float g = sg[j];
             u = fmaf(-g, ku, u);
             v = fmaf(g, kv, v);
@@ -162,16 +163,63 @@ __device__ __forceinline__ void react_tile32_t(const f32::F32Geometry &f, const 
     }
 }
 
+template <class V = f32::Periodic32>
 __device__ __forceinline__ void react_tile32(const f32::F32Geometry &f, const float4 t, float tg,
                                              bool t_ok, const float4 *sf, const float *sg,
                                              int s_count, float &u, float &v, float &ru,
                                              float &rv) {
     if (__all_sync(0xffffffffu, t_ok && s_count == 32))
-        react_tile32_t<true>(f, t, tg, t_ok, sf, sg, s_count, u, v, ru, rv);
+        react_tile32_t<V, true>(f, t, tg, t_ok, sf, sg, s_count, u, v, ru, rv);
     else
-        react_tile32_t<false>(f, t, tg, t_ok, sf, sg, s_count, u, v, ru, rv);
+        react_tile32_t<V, false>(f, t, tg, t_ok, sf, sg, s_count, u, v, ru, rv);
 }
 
+// T targets per lane against the 32 sources of the buffer, every target and source present: each
+// step serves T pairs per lane, and the reactions' two shuffles are shared by them. A reaction
+// would sum 32T terms in FP32 over the tile; it is restarted every 8 steps instead (8T terms, as
+// many as the ordered FP32C kernel sums before promoting), and the four partials of a source,
+// left in the lanes 8, 16, 24 and 32 places on, are added in FP64 into rud, rvd.
+template <class V, int T>
+__device__ __forceinline__ void react_tiles32_full(const f32::F32Geometry &f, const float4 (&t)[T],
+                                                   const float (&tg)[T], const float4 *sf,
+                                                   const float *sg, float (&u)[T], float (&v)[T],
+                                                   double &rud, double &rvd) {
+    const int lane = threadIdx.x & 31, next = (lane + 1) & 31;
+    float pu[4], pv[4];
+#pragma unroll
+    for (int m = 0; m < 4; ++m) {
+        float ru = 0.0f, rv = 0.0f;
+#pragma unroll 2
+        for (int kk = 0; kk < 8; ++kk) {
+            const int j = (lane + 8 * m + kk) & 31;
+            const float4 s = sf[j];
+            const float g = sg[j];
+#pragma unroll
+            for (int q = 0; q < T; ++q) {
+                float ku, kv;
+                V::values(f, t[q], s, ku, kv);
+                u[q] = fmaf(-g, ku, u[q]);
+                v[q] = fmaf(g, kv, v[q]);
+                ru = fmaf(tg[q], ku, ru);
+                rv = fmaf(-tg[q], kv, rv);
+            }
+            ru = __shfl_sync(0xffffffffu, ru, next);
+            rv = __shfl_sync(0xffffffffu, rv, next);
+        }
+        pu[m] = ru;  // the partial of source (lane + 8 (m + 1)) & 31
+        pv[m] = rv;
+    }
+    rud = static_cast<double>(__shfl_sync(0xffffffffu, pu[0], (lane - 8) & 31));
+    rvd = static_cast<double>(__shfl_sync(0xffffffffu, pv[0], (lane - 8) & 31));
+    rud += static_cast<double>(__shfl_sync(0xffffffffu, pu[1], (lane - 16) & 31));
+    rvd += static_cast<double>(__shfl_sync(0xffffffffu, pv[1], (lane - 16) & 31));
+    rud += static_cast<double>(__shfl_sync(0xffffffffu, pu[2], (lane - 24) & 31));
+    rvd += static_cast<double>(__shfl_sync(0xffffffffu, pv[2], (lane - 24) & 31));
+    rud += static_cast<double>(pu[3]);
+    rvd += static_cast<double>(pv[3]);
+}
+
+template <class V = f32::Periodic32>
 __device__ __forceinline__ void one_sided_tile32(const f32::F32Geometry &f, const float4 t,
                                                  bool t_ok, const float4 *sf, const float *sg,
                                                  int s_count, bool same_block, float &u,
@@ -181,7 +229,7 @@ __device__ __forceinline__ void one_sided_tile32(const f32::F32Geometry &f, cons
         const int j = (lane + k) & 31;
         if (t_ok && j < s_count) {
             float ku, kv;
-            f32::periodic_values32(f, t, sf[j], ku, kv);
+            V::values(f, t, sf[j], ku, kv);
             u = fmaf(-sg[j], ku, u);
             v = fmaf(sg[j], kv, v);
         }

@@ -192,8 +192,36 @@ def test_small_plane_populations_use_the_ordered_kernel():
     assert not plane_kernel_with(x, y, g).statePlan()["symmetric"]
 
 
-def test_plane_fp32c_uses_the_ordered_kernel():
-    x, y, g = ics.infinite_plane(17000, 2)
+@pytest.mark.parametrize("n", [17000, 33000])
+def test_plane_fp32c_symmetric_against_the_fp64_oracle(port, n):
+    """The FP32-compensated plane once per unordered pair (4 targets per lane at 17000, 8 at
+    33000) against the FP64 ordered kernel: no worse than the ordered FP32C kernel on the same
+    state (max within 2x, rms within 1.5x, or the FP32C bounds 2e-6 / 2e-7 of smaller
+    populations), and at most 1e-5 anywhere; three ranges against the oracle."""
+    x, y, g = ics.infinite_plane(n, 23)
+    k = pv.InfinitePlaneKernel(0.0, precision=_lib.PRECISION_FP32C)
+    k.uploadDeviceState(pv.VortexSystem(x, y, g))
+    plan = k.statePlan()
+    assert plan["symmetric"] and plan["rows"] == (n + (255 if n >= 32768 else 127)) // (
+        256 if n >= 32768 else 128)
+    vel = k.evaluateDeviceState()
+    ref = pv.InfinitePlaneKernel(0.0).evaluate(x, y, g)
+    err = normalized_error(vel.x, vel.y, ref.x, ref.y)
+    ordered = k.evaluate(x, y, g)            # host arrays: the ordered FP32C kernel
+    err_o = normalized_error(ordered.x, ordered.y, ref.x, ref.y)
+    rms, rms_o = np.sqrt(np.mean(err ** 2)), np.sqrt(np.mean(err_o ** 2))
+    assert err.max() <= min(max(2.0 * err_o.max(), 2e-6), 1e-5)
+    assert rms <= min(max(1.5 * rms_o, 2e-7), 1e-6)
+    geo = Geometry("infinite")
+    for t0, t1 in ((0, 40), (n // 2, n // 2 + 40), (n - 40, n)):
+        u, v = port.evaluate_range(geo, x, y, g, t0, t1)
+        assert normalized_error(vel.x[t0:t1], vel.y[t0:t1], u, v).max() <= 1e-5
+    again = k.evaluateDeviceState()
+    assert np.array_equal(vel.x, again.x) and np.array_equal(vel.y, again.y)
+
+
+def test_small_plane_fp32c_uses_the_ordered_kernel():
+    x, y, g = ics.infinite_plane(16000, 2)
     k = pv.InfinitePlaneKernel(0.0, precision=_lib.PRECISION_FP32C)
     k.uploadDeviceState(pv.VortexSystem(x, y, g))
     assert not k.statePlan()["symmetric"]
