@@ -95,6 +95,7 @@ struct pv_context {
     cudaGraphExec_t attempt_graph = nullptr; // one DOPRI5 attempt with a valid FSAL derivative
     SymmetricPlan sym{};             // one evaluation per unordered pair (when planned)
     DeviceArray sym_items, sym_counter;
+    DeviceArray rk4_barrier;         // grid barrier of the cooperative RK4 steps (two words)
     int sym_items_blocks = 0;        // the block count the item table was built for
     DeviceArray inv_scratch, inv_out;
     DeviceArray cand;                // dipole candidates (3 doubles-worth each)
@@ -143,7 +144,7 @@ struct pv_context {
         for (DeviceArray *a : {&x, &y, &gamma, &gs, &p0x, &p0y, &p1x, &p1y, &pu, &pv, &inv_scratch,
                                &inv_out, &cand, &ex, &ey, &eg, &egs, &eu, &ev, &epu, &epv,
                                &removed_index, &fmt_stage, &fmt_len, &fmt_block, &fmt_out,
-                               &sym_items, &sym_counter})
+                               &sym_items, &sym_counter, &rk4_barrier})
             a->release();
         for (int s = 0; s < 7; ++s) {
             kx[s].release();
@@ -886,30 +887,67 @@ pv_status pv_evaluate_state(pv_context *ctx, double *u, double *v, size_t n) {
 
 namespace {
 // Enqueues one RK4 step (src/timestep.cpp:31-61) on the context stream.
-pv_status enqueue_rk4(pv_context *c, double dt) {
-    const double *px = c->x.p, *py = c->y.p;
+// Stage s of an RK4 step (src/timestep.cpp:31-61): evaluated at the state (s = 0) or at the
+// previous stage's position, writing the next position into the ping-pong buffers; stage 3
+// writes the combined state.
+StageArgs rk4_stage(pv_context *c, double dt, int s) {
+    static const double rows[3][3] = {{0.5}, {0.0, 0.5}, {0.0, 0.0, 1.0}};
     double *pos_x[2] = {c->p0x.p, c->p1x.p};
     double *pos_y[2] = {c->p0y.p, c->p1y.p};
-    static const double rows[3][3] = {{0.5}, {0.0, 0.5}, {0.0, 0.0, 1.0}};
+    StageArgs a = stage_base(c);
+    a.s = s;
+    a.ex = s == 0 ? c->x.p : pos_x[(s - 1) & 1];
+    a.ey = s == 0 ? c->y.p : pos_y[(s - 1) & 1];
+    a.dt = dt;
+    a.xt = pos_x[s & 1];
+    a.yt = pos_y[s & 1];
+    if (s < 3) {
+        a.mode = STAGE_POSITION;
+        a.ncoef = s + 1;
+        for (int j = 0; j <= s; ++j)
+            a.coef[j] = rows[s][j];
+    } else {
+        a.mode = STAGE_RK4_COMBINE;
+    }
+    return a;
+}
+
+// Whole RK4 steps in one cooperative launch: FP64, the ordered kernel's plan (no symmetric
+// rows), a small enough population, and no per-launch profiling.
+bool rk4_steps_apply(const pv_context *c) {
+    return !c->profiling && c->params.precision == PV_PRECISION_FP64 && !c->sym.enabled() &&
+           rk4_steps_eligible(c->n, c->plan.num_chunks);
+}
+
+pv_status enqueue_rk4_steps(pv_context *c, double dt, uint64_t steps) {
+    Rk4Steps p{};
+    for (int s = 0; s < 4; ++s)
+        p.stage[s] = rk4_stage(c, dt, s);
+    p.x = c->x.p;
+    p.y = c->y.p;
+    p.gs = c->gs.p;
+    p.n = c->n;
+    p.chunk = c->plan.chunk;
+    p.num_chunks = c->plan.num_chunks;
+    p.steps = steps;
+    if (!c->rk4_barrier.p) {
+        PV_CUDA(c, c->rk4_barrier.ensure(1));
+        PV_CUDA(c, cudaMemsetAsync(c->rk4_barrier.p, 0, 2 * sizeof(unsigned), c->stream));
+    }
+    p.barrier = reinterpret_cast<unsigned *>(c->rk4_barrier.p);
+    PV_CUDA(c, counted(c, PV_KERNEL_VELOCITY, 1,
+                       [&] { return launch_rk4_steps(p, c->sm_count, c->stream); }));
+    c->evaluations += 4 * steps;
+    return PV_OK;
+}
+
+pv_status enqueue_rk4(pv_context *c, double dt) {
+    const double *px = c->x.p, *py = c->y.p;
     pv_status st;
     for (int s = 0; s < 4; ++s) {
         if ((st = launch_eval(c, px, py)) != PV_OK)
             return st;
-        StageArgs a = stage_base(c);
-        a.s = s;
-        a.ex = px;
-        a.ey = py;
-        a.dt = dt;
-        a.xt = pos_x[s & 1];
-        a.yt = pos_y[s & 1];
-        if (s < 3) {
-            a.mode = STAGE_POSITION;
-            a.ncoef = s + 1;
-            for (int j = 0; j <= s; ++j)
-                a.coef[j] = rows[s][j];
-        } else {
-            a.mode = STAGE_RK4_COMBINE;
-        }
+        const StageArgs a = rk4_stage(c, dt, s);
         PV_CUDA(c, counted(c, PV_KERNEL_STAGE, 1, [&] { return launch_stage(a, c->stream, c->sm_count); }));
         px = a.xt;
         py = a.yt;
@@ -937,7 +975,7 @@ pv_status pv_rk4_step(pv_context *ctx, double dt) {
     DeviceGuard guard(ctx->device);
     if ((st = reset_control(ctx)) != PV_OK)
         return st;
-    if ((st = enqueue_rk4(ctx, dt)) != PV_OK)
+    if ((st = rk4_steps_apply(ctx) ? enqueue_rk4_steps(ctx, dt, 1) : enqueue_rk4(ctx, dt)) != PV_OK)
         return st;
     if ((st = read_control(ctx)) != PV_OK)
         return st;
@@ -959,7 +997,10 @@ pv_status pv_rk4_advance(pv_context *ctx, double dt, uint64_t steps) {
     DeviceGuard guard(ctx->device);
     if ((st = reset_control(ctx)) != PV_OK)
         return st;
-    if (ctx->profiling || steps < 4) {
+    if (rk4_steps_apply(ctx)) {
+        if ((st = enqueue_rk4_steps(ctx, dt, steps)) != PV_OK)
+            return st;
+    } else if (ctx->profiling || steps < 4) {
         for (uint64_t k = 0; k < steps; ++k)
             if ((st = enqueue_rk4(ctx, dt)) != PV_OK)
                 return st;

@@ -128,6 +128,23 @@ struct StageArgs {
 
 cudaError_t launch_stage(const StageArgs &a, cudaStream_t stream, int sm_count);
 
+// RK4 steps of a small FP64 population in one cooperative launch (pv_stepping.cu): the four
+// stages as enqueue_rk4 sets them up (stage[3].xt/yt: the combined state), bit for bit the same
+// results as launching them. barrier: two words, zero before the first launch, left with the
+// count at zero. Eligible up to kRk4StepsMaxN vortices with fewer than 32 chunks.
+struct Rk4Steps {
+    StageArgs stage[4];
+    double *x, *y;          // the state, updated after every step
+    const double *gs;       // scaled circulations
+    size_t n;
+    int chunk, num_chunks;  // the ordered kernel's source chunks
+    uint64_t steps;
+    unsigned *barrier;
+};
+constexpr size_t kRk4StepsMaxN = 2048;
+bool rk4_steps_eligible(size_t n, int num_chunks);
+cudaError_t launch_rk4_steps(const Rk4Steps &p, int sm_count, cudaStream_t stream);
+
 // Accept kernel: state <- xt (and, for DOPRI5, k0 <- k6 when the attempt was accepted).
 cudaError_t launch_accept(double *x, double *y, const double *xt, const double *yt, double *k0x,
                           double *k0y, const double *k6x, const double *k6y, size_t n, int dopri,

@@ -19,6 +19,8 @@
 // to the reference's (which x86-64 g++ computes without FMA contraction).
 #include "pv_internal.h"
 
+#include <algorithm>
+
 namespace pvb {
 
 namespace {
@@ -67,13 +69,15 @@ __device__ void dopri_control(DeviceControl *ctl) {
 
 // Everything a stage does for one target once its velocity (ku, kv) is summed: the slow path of
 // a non-finite sum, the stage velocity, and the stage position / RK4 combination / DOPRI5 error.
+// ex, ey: the positions the slow path recomputes from (a.ex, a.ey, or a copy of them).
 template <int MODE>
 __device__ __forceinline__ void finish_target(const StageArgs &a, size_t i, double ku, double kv,
-                                              double dt, double &local_max) {
+                                              double dt, double &local_max, const double *ex,
+                                              const double *ey) {
     if (a.reduce) {
         if (!isfinite(ku) || !isfinite(kv)) {
             const int verdict =
-                slow_target(a.g, a.ex, a.ey, a.gamma, a.n_src, a.t_offset + i, ku, kv);
+                slow_target(a.g, ex, ey, a.gamma, a.n_src, a.t_offset + i, ku, kv);
             if (verdict == ST_COINCIDENT || (verdict && !a.nonfinite_ok))
                 set_status(&a.ctl->status, verdict);
         }
@@ -184,7 +188,7 @@ __global__ void __launch_bounds__(256) stage_kernel(const StageArgs a) {
                     ku += s_u[g][lane];
                     kv += s_v[g][lane];
                 }
-                finish_target<MODE>(a, i, ku, kv, dt, local_max);
+                finish_target<MODE>(a, i, ku, kv, dt, local_max, a.ex, a.ey);
             }
             __syncthreads();
         }
@@ -203,7 +207,7 @@ __global__ void __launch_bounds__(256) stage_kernel(const StageArgs a) {
                 ku = a.kx[a.s][i];
                 kv = a.ky[a.s][i];
             }
-            finish_target<MODE>(a, i, ku, kv, dt, local_max);
+            finish_target<MODE>(a, i, ku, kv, dt, local_max, a.ex, a.ey);
         }
     }
 
@@ -280,6 +284,170 @@ cudaError_t launch_stage(const StageArgs &a, cudaStream_t stream, int sm_count) 
         return launch_stage_mode<STAGE_RK4_COMBINE>(a, stream, sm_count);
     case STAGE_DOPRI_ERROR:
         return launch_stage_mode<STAGE_DOPRI_ERROR>(a, stream, sm_count);
+    default:
+        return cudaErrorInvalidValue;
+    }
+}
+
+// ---------------------------------------------------------------------------------------------
+// RK4 steps of a small population in one cooperative launch. Below N ~ 2000 a step's nine
+// launches take longer to schedule than to run, so one CTA per SM keeps the whole step loop: each
+// CTA owns a range of targets, and a grid barrier separates the four evaluations of a step.
+//
+// The results are bit for bit those of the launch sequence (enqueue_rk4): a target's velocity is
+// summed chunk by chunk (the ordered kernel's chunks, sources in index order, pair<true> with the
+// self flag) and the chunk sums are added in chunk order from 0.0, as the stage kernel does with
+// fewer than kWideRows chunks; finish_target then runs unchanged. The previous step's combined
+// state (stage 3's output) is the next step's evaluation point and is copied into the state target
+// by target in the phase that reads it, so a step costs four barriers.
+
+// Grid barrier over the CTAs of a cooperative launch: count arrivals, the last arrival opens the
+// next generation. A wait that does not end within the spin limit sets ST_TIMEOUT and returns
+// false; the other CTAs then time out at their next barrier.
+constexpr uint32_t kGridSpinLimit = 1u << 24;
+__device__ bool grid_barrier(unsigned *bar, int *status) {
+    __shared__ int ok;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        volatile unsigned *generation = bar + 1;
+        const unsigned gen = *generation;
+        __threadfence();
+        ok = 1;
+        if (atomicAdd(bar, 1u) == gridDim.x - 1) {
+            atomicExch(bar, 0u);
+            __threadfence();
+            atomicAdd(bar + 1, 1u);
+        } else {
+            uint32_t it = 0;
+            while (*generation == gen) {
+                if (++it > kGridSpinLimit) {
+                    set_status(status, ST_TIMEOUT);
+                    ok = 0;
+                    break;
+                }
+                __nanosleep(64);
+            }
+        }
+        __threadfence();
+    }
+    __syncthreads();
+    return ok != 0;
+}
+
+template <class Pair>
+__global__ void __launch_bounds__(256) rk4_steps_kernel(const Rk4Steps p) {
+    extern __shared__ double smem[];
+    const size_t n = p.n;
+    const int nc = p.num_chunks;
+    const size_t per_cta = (n + gridDim.x - 1) / gridDim.x;
+    const size_t t0 = static_cast<size_t>(blockIdx.x) * per_cta;
+    const size_t t1 = t0 < n ? min(t0 + per_cta, n) : t0;
+    const int mine = static_cast<int>(t1 - t0);
+    double *sx = smem, *sy = smem + n, *sg = smem + 2 * n;
+    double *qu = smem + 3 * n, *qv = qu + per_cta * nc;
+    int *status = &p.stage[0].ctl->status;
+    for (size_t j = threadIdx.x; j < n; j += blockDim.x)
+        sg[j] = p.gs[j];
+    double local_max = 0.0;
+    for (uint64_t step = 0; step < p.steps; ++step) {
+#pragma unroll
+        for (int s = 0; s < 4; ++s) {
+            const StageArgs &a = p.stage[s];
+            // evaluation point: the state, or for a step's first stage after the first step the
+            // previous step's combination (not yet copied into the state)
+            const bool carried = s == 0 && step > 0;
+            const double *px = carried ? p.stage[3].xt : a.ex;
+            const double *py = carried ? p.stage[3].yt : a.ey;
+            for (size_t j = threadIdx.x; j < n; j += blockDim.x) {
+                sx[j] = __ldcg(px + j);
+                sy[j] = __ldcg(py + j);
+            }
+            __syncthreads();
+            for (int w = threadIdx.x; w < mine * nc; w += blockDim.x) {
+                const int li = w % mine, c = w / mine;
+                const size_t i = t0 + li;
+                const size_t j0 = static_cast<size_t>(c) * p.chunk;
+                const size_t j1 = min(j0 + static_cast<size_t>(p.chunk), n);
+                const double tx = sx[i], ty = sy[i];
+                double u = 0.0, v = 0.0;
+                for (size_t j = j0; j < j1; ++j)
+                    Pair::template pair<true>(a.g, tx, ty, sx[j], sy[j], sg[j], i == j, u, v);
+                qu[li * nc + c] = u;
+                qv[li * nc + c] = v;
+            }
+            __syncthreads();
+            for (int li = threadIdx.x; li < mine; li += blockDim.x) {
+                const size_t i = t0 + li;
+                if (carried) {  // the accept of the previous step
+                    p.x[i] = px[i];
+                    p.y[i] = py[i];
+                }
+                double ku = 0.0, kv = 0.0;
+                for (int c = 0; c < nc; ++c) {
+                    ku += qu[li * nc + c];
+                    kv += qv[li * nc + c];
+                }
+                // the slow path recomputes from this phase's positions, held in shared memory
+                if (s < 3)
+                    finish_target<STAGE_POSITION>(a, i, ku, kv, a.dt, local_max, sx, sy);
+                else
+                    finish_target<STAGE_RK4_COMBINE>(a, i, ku, kv, a.dt, local_max, sx, sy);
+            }
+            if (!grid_barrier(p.barrier, status))
+                return;
+            if (*reinterpret_cast<volatile int *>(status) != 0)
+                return;  // every CTA reads the same word after the barrier
+        }
+    }
+    for (int li = threadIdx.x; li < mine; li += blockDim.x) {  // the last step's accept
+        const size_t i = t0 + li;
+        p.x[i] = __ldcg(p.stage[3].xt + i);
+        p.y[i] = __ldcg(p.stage[3].yt + i);
+    }
+}
+
+size_t rk4_steps_smem(size_t n, int num_chunks, int grid) {
+    const size_t per_cta = (n + grid - 1) / grid;
+    return (3 * n + 2 * per_cta * static_cast<size_t>(num_chunks)) * sizeof(double);
+}
+
+bool rk4_steps_eligible(size_t n, int num_chunks) {
+    return n >= 1 && n <= kRk4StepsMaxN && num_chunks >= 1 && num_chunks < kWideRows;
+}
+
+template <class Pair>
+cudaError_t launch_rk4_steps_t(const Rk4Steps &p, int grid, cudaStream_t stream) {
+    const size_t smem = rk4_steps_smem(p.n, p.num_chunks, grid);
+    cudaError_t e = cudaFuncSetAttribute(rk4_steps_kernel<Pair>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         static_cast<int>(smem));
+    if (e != cudaSuccess)
+        return e;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(static_cast<unsigned>(grid));
+    cfg.blockDim = dim3(256);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = stream;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeCooperative;  // every CTA resident, or no launch at all
+    attr[0].val.cooperative = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, rk4_steps_kernel<Pair>, p);
+}
+
+cudaError_t launch_rk4_steps(const Rk4Steps &p, int sm_count, cudaStream_t stream) {
+    if (!rk4_steps_eligible(p.n, p.num_chunks) || p.steps == 0 || !p.barrier)
+        return cudaErrorInvalidValue;
+    const int grid = static_cast<int>(
+        std::min<size_t>(static_cast<size_t>(sm_count > 0 ? sm_count : 148), p.n));
+    switch (p.stage[0].g.geometry) {
+    case GEO_INFINITE:
+        return launch_rk4_steps_t<InfinitePair>(p, grid, stream);
+    case GEO_PERIODIC:
+        return launch_rk4_steps_t<PeriodicPair>(p, grid, stream);
+    case GEO_DISK:
+        return launch_rk4_steps_t<DiskPair>(p, grid, stream);
     default:
         return cudaErrorInvalidValue;
     }

@@ -202,3 +202,58 @@ def test_dopri_graph_replay_equals_launches_and_profiling():
     assert r0 == r1 and np.array_equal(x0, x1) and np.array_equal(y0, y1)
     launches, timed, ms = st1["velocity"]
     assert launches == timed and ms > 0  # every replayed launch was timed by its graph events
+
+
+@pytest.mark.parametrize("name", sorted(GEOS))
+@pytest.mark.parametrize("n", [300, 1024, 2048])
+def test_rk4_cooperative_steps_equal_the_launch_sequence(name, n):
+    """Small FP64 populations take whole RK4 steps in one cooperative launch; with per-launch
+    profiling on, the same steps run as the launch sequence. Both give the same state bit for
+    bit, through rk4Advance and through single steps, or stop with the same error (a disk vortex
+    of a close pair can leave the disk) at the same state."""
+    geo = GEOS[name]
+    x, y, g = state(name, n, 70 + n)
+    ks = []
+    for profiling in (False, True):
+        k = make_kernel(geo)
+        k.uploadDeviceState(pv.VortexSystem(x, y, g))
+        k.setProfiling(profiling)
+        k.resetKernelStats()
+        error = None
+        try:
+            k.rk4Advance(5e-4, 7)
+            for _ in range(3):
+                k.deviceRk4Step(5e-4)
+        except ValueError as exc:
+            error = str(exc)
+        out = pv.VortexSystem(x.copy(), y.copy(), g)
+        k.downloadDeviceState(out)
+        ks.append((k, out, error))
+    (fast, a, ea), (_, b, eb) = ks
+    assert ea == eb
+    assert np.array_equal(a.x, b.x) and np.array_equal(a.y, b.y)
+    if ea is None:
+        assert fast.evaluationCount == 40
+        if n == 1024:  # one launch for the 7 steps and one per single step
+            assert fast.kernelStats()["velocity"][0] == 4
+
+
+def test_rk4_cooperative_failure_keeps_the_last_state(port):
+    """A disk vortex pushed through the wall inside rk4Advance: the reference's error, and the
+    state after the last good step, as with the launch sequence."""
+    geo = GEOS["disk"]
+    x = np.array([0.9999, -0.2])
+    y = np.array([0.0, 0.0])
+    g = np.array([1.0, 50.0])
+    outs = []
+    for profiling in (False, True):
+        k = make_kernel(geo)
+        k.uploadDeviceState(pv.VortexSystem(x, y, g))
+        k.setProfiling(profiling)
+        with pytest.raises(ValueError, match="vortex lies on or outside the disk"):
+            k.rk4Advance(1e-2, 50)
+        out = pv.VortexSystem(x.copy(), y.copy(), g)
+        k.downloadDeviceState(out)
+        outs.append(out)
+    assert np.array_equal(outs[0].x, outs[1].x) and np.array_equal(outs[0].y, outs[1].y)
+    assert np.all(outs[0].x ** 2 + outs[0].y ** 2 < 1.0)
