@@ -638,7 +638,7 @@ def run_other_configs() -> dict:
                   "linear_impulse_y": inv1.linearImpulseY - inv0.linearImpulseY,
                   "angular_impulse": inv1.angularImpulse - inv0.angularImpulse,
                   "hamiltonian": inv1.hamiltonian - inv0.hamiltonian},
-        "note": "the 100 steps are one CUDA graph of a step replayed (pv_rk4_advance)"}
+        "note": "the 100 steps are one cooperative launch (pv_rk4_advance, N <= 2048)"}
     x, y, g = ics.workload_state("disk_rk4_n16384")
     forms = {}
     vel = {}

@@ -325,7 +325,7 @@ __device__ bool grid_barrier(unsigned *bar, int *status) {
                     ok = 0;
                     break;
                 }
-                __nanosleep(64);
+                __nanosleep(16);
             }
         }
         __threadfence();
@@ -370,6 +370,9 @@ __global__ void __launch_bounds__(256) rk4_steps_kernel(const Rk4Steps p) {
                 const size_t j1 = min(j0 + static_cast<size_t>(p.chunk), n);
                 const double tx = sx[i], ty = sy[i];
                 double u = 0.0, v = 0.0;
+                // unrolled so that the independent work of several sources overlaps; the sums
+                // still take the sources in index order
+#pragma unroll 4
                 for (size_t j = j0; j < j1; ++j)
                     Pair::template pair<true>(a.g, tx, ty, sx[j], sy[j], sg[j], i == j, u, v);
                 qu[li * nc + c] = u;
