@@ -95,7 +95,7 @@ struct pv_context {
     cudaGraphExec_t attempt_graph = nullptr; // one DOPRI5 attempt with a valid FSAL derivative
     SymmetricPlan sym{};             // one evaluation per unordered pair (when planned)
     DeviceArray sym_items, sym_counter;
-    DeviceArray rk4_barrier;         // grid barrier of the cooperative RK4 steps (two words)
+    DeviceArray rk4_barrier;         // arrival counter of the cooperative RK4 steps' grid barrier
     int sym_items_blocks = 0;        // the block count the item table was built for
     DeviceArray inv_scratch, inv_out;
     DeviceArray cand;                // dipole candidates (3 doubles-worth each)
@@ -930,11 +930,9 @@ pv_status enqueue_rk4_steps(pv_context *c, double dt, uint64_t steps) {
     p.chunk = c->plan.chunk;
     p.num_chunks = c->plan.num_chunks;
     p.steps = steps;
-    if (!c->rk4_barrier.p) {
-        PV_CUDA(c, c->rk4_barrier.ensure(1));
-        PV_CUDA(c, cudaMemsetAsync(c->rk4_barrier.p, 0, 2 * sizeof(unsigned), c->stream));
-    }
-    p.barrier = reinterpret_cast<unsigned *>(c->rk4_barrier.p);
+    PV_CUDA(c, c->rk4_barrier.ensure(1));
+    PV_CUDA(c, cudaMemsetAsync(c->rk4_barrier.p, 0, sizeof(unsigned long long), c->stream));
+    p.barrier = reinterpret_cast<unsigned long long *>(c->rk4_barrier.p);
     PV_CUDA(c, counted(c, PV_KERNEL_VELOCITY, 1,
                        [&] { return launch_rk4_steps(p, c->sm_count, c->stream); }));
     c->evaluations += 4 * steps;

@@ -130,8 +130,8 @@ cudaError_t launch_stage(const StageArgs &a, cudaStream_t stream, int sm_count);
 
 // RK4 steps of a small FP64 population in one cooperative launch (pv_stepping.cu): the four
 // stages as enqueue_rk4 sets them up (stage[3].xt/yt: the combined state), bit for bit the same
-// results as launching them. barrier: two words, zero before the first launch, left with the
-// count at zero. Eligible up to kRk4StepsMaxN vortices with fewer than 32 chunks.
+// results as launching them. barrier: the grid barrier's arrival counter, zero at every
+// launch. Eligible up to kRk4StepsMaxN vortices with fewer than 32 chunks.
 struct Rk4Steps {
     StageArgs stage[4];
     double *x, *y;          // the state, updated after every step
@@ -139,7 +139,7 @@ struct Rk4Steps {
     size_t n;
     int chunk, num_chunks;  // the ordered kernel's source chunks
     uint64_t steps;
-    unsigned *barrier;
+    unsigned long long *barrier;
 };
 constexpr size_t kRk4StepsMaxN = 2048;
 bool rk4_steps_eligible(size_t n, int num_chunks);

@@ -301,34 +301,34 @@ cudaError_t launch_stage(const StageArgs &a, cudaStream_t stream, int sm_count) 
 // state (stage 3's output) is the next step's evaluation point and is copied into the state target
 // by target in the phase that reads it, so a step costs four barriers.
 
-// Grid barrier over the CTAs of a cooperative launch: count arrivals, the last arrival opens the
-// next generation. A wait that does not end within the spin limit sets ST_TIMEOUT and returns
-// false; the other CTAs then time out at their next barrier.
+// Grid barrier over the CTAs of a cooperative launch. The arrival counter starts at zero (the
+// host clears it before the launch) and only grows: the r-th barrier is open once it reaches
+// r * gridDim.x. One fence and one atomic per CTA, then polling with an acquire load. A wait
+// that does not end within the spin limit sets ST_TIMEOUT and returns false; the other CTAs
+// then time out at their next barrier.
 constexpr uint32_t kGridSpinLimit = 1u << 24;
-__device__ bool grid_barrier(unsigned *bar, int *status) {
+__device__ bool grid_barrier(unsigned long long *arrivals, unsigned long long open_at,
+                             int *status) {
     __shared__ int ok;
     __syncthreads();
     if (threadIdx.x == 0) {
-        volatile unsigned *generation = bar + 1;
-        const unsigned gen = *generation;
-        __threadfence();
+        __threadfence();  // this CTA's writes, ordered by the __syncthreads, before its arrival
+        atomicAdd(arrivals, 1ull);
         ok = 1;
-        if (atomicAdd(bar, 1u) == gridDim.x - 1) {
-            atomicExch(bar, 0u);
-            __threadfence();
-            atomicAdd(bar + 1, 1u);
-        } else {
-            uint32_t it = 0;
-            while (*generation == gen) {
-                if (++it > kGridSpinLimit) {
-                    set_status(status, ST_TIMEOUT);
-                    ok = 0;
-                    break;
-                }
-                __nanosleep(16);
+        uint32_t it = 0;
+        for (;;) {
+            unsigned long long now;
+            asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(now) : "l"(arrivals) : "memory");
+            if (now >= open_at)
+                break;
+            if (++it > kGridSpinLimit) {
+                set_status(status, ST_TIMEOUT);
+                ok = 0;
+                break;
             }
+            if (it > 64)
+                __nanosleep(32);
         }
-        __threadfence();
     }
     __syncthreads();
     return ok != 0;
@@ -349,6 +349,7 @@ __global__ void __launch_bounds__(256) rk4_steps_kernel(const Rk4Steps p) {
     for (size_t j = threadIdx.x; j < n; j += blockDim.x)
         sg[j] = p.gs[j];
     double local_max = 0.0;
+    unsigned long long open_at = 0;
     for (uint64_t step = 0; step < p.steps; ++step) {
 #pragma unroll
         for (int s = 0; s < 4; ++s) {
@@ -358,6 +359,7 @@ __global__ void __launch_bounds__(256) rk4_steps_kernel(const Rk4Steps p) {
             const bool carried = s == 0 && step > 0;
             const double *px = carried ? p.stage[3].xt : a.ex;
             const double *py = carried ? p.stage[3].yt : a.ey;
+#pragma unroll 8  // the loads of several iterations in flight at once
             for (size_t j = threadIdx.x; j < n; j += blockDim.x) {
                 sx[j] = __ldcg(px + j);
                 sy[j] = __ldcg(py + j);
@@ -396,7 +398,8 @@ __global__ void __launch_bounds__(256) rk4_steps_kernel(const Rk4Steps p) {
                 else
                     finish_target<STAGE_RK4_COMBINE>(a, i, ku, kv, a.dt, local_max, sx, sy);
             }
-            if (!grid_barrier(p.barrier, status))
+            open_at += gridDim.x;
+            if (!grid_barrier(p.barrier, open_at, status))
                 return;
             if (*reinterpret_cast<volatile int *>(status) != 0)
                 return;  // every CTA reads the same word after the barrier
