@@ -14,7 +14,8 @@ With --gpus N (launched one process per GPU) every rank runs its own independent
 
 --impl reference times the reference's own CPU implementation (the unmodified PointVortex code
 compiled from its sources into oracle/_ref) on the same workload and metric, with all host
-threads, on a bounded sample of targets per step.
+threads: its own DOPRI5 steps and dipole events, timed for as many of the K steps as fit a
+bounded wall-clock budget. That arm never imports the package (no libpvb200.so is mapped).
 """
 from __future__ import annotations
 
@@ -61,6 +62,18 @@ FLOPS_PER_UNORDERED_PAIR_PLANE_SYMMETRIC = 16
 # one ncu capture (dram__bytes_read.sum 174.8 KB, dram__bytes_write.sum 0 B, with ncu's cache
 # flush before the launch): the sources are read once, the partial rows stay in L2.
 TRAFFIC_BYTES_PER_LAUNCH = 174848
+
+
+def load_ics():
+    """The seeded IC generator (pointvortex_b200/ics.py, plain numpy), loaded from its file. The
+    reference arm, the CPU baselines and the reference CUDA leg use it this way so that they never
+    import the package, whose import maps libpvb200.so."""
+    import importlib.util
+    spec = importlib.util.spec_from_file_location(
+        "pvb200_ics_standalone", os.path.join(ROOT, "pointvortex_b200", "ics.py"))
+    module = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(module)
+    return module
 
 
 def rank_info():
@@ -327,7 +340,7 @@ def cpu_baseline(seconds: float = 10.0):
     """The reference's CPU/OpenMP periodic kernel on a bounded sample of targets of the same
     state, all host threads."""
     from oracle.pyoracle import Geometry, Oracle
-    from pointvortex_b200 import ics
+    ics = load_ics()
     try:
         ref = Oracle("reference")
         kind = "reference"
@@ -350,12 +363,25 @@ def cpu_baseline(seconds: float = 10.0):
             f"state against all {N} sources, {sec:.1f} s"}
 
 
+# Wall-clock budget of the reference arm's timed steps: the arm stops timing after the step that
+# crosses it (the metric is a rate, so fewer steps change its sample, not its meaning).
+REFERENCE_TIMED_BUDGET_S = 150.0
+REFERENCE_WARMUP_BUDGET_S = 60.0
+
+
 def run_reference(args):
+    """The reference's own CPU path of the same workload, all host threads: DOPRI5 steps of
+    RungeKuttaIntegrator::dopri5Step (src/timestep.cpp:62-120, FSAL kept between steps) over
+    PeriodicBoxKernel (src/compute.cpp:203-256), each followed by DipoleManager::process
+    (src/dipole.cpp:42-127, removal at the workload's threshold) and the FSAL invalidation the
+    driver makes after events (src/main.cpp:329-333). Unmodified reference code compiled into
+    oracle/_ref (the port when it is absent); nothing of this repository's CUDA library is
+    loaded."""
     rank, world, _ = rank_info()
     if rank != 0:
         return None
     from oracle.pyoracle import Geometry, Oracle
-    from pointvortex_b200 import ics
+    ics = load_ics()
     try:
         ref = Oracle("reference")
         kind = "reference"
@@ -363,32 +389,64 @@ def run_reference(args):
         ref = Oracle("port")
         kind = "port"
     x, y, g = ics.periodic_box(N, SEED, LENGTH)
-    geo = Geometry("periodic", box_length_x=LENGTH, box_length_y=LENGTH, image_layers=LAYERS)
+    geo = Geometry("periodic", box_length_x=LENGTH, box_length_y=LENGTH, image_layers=LAYERS,
+                   absolute_tolerance=ATOL, relative_tolerance=RTOL, minimum_time_step=DTMIN,
+                   maximum_time_step=DTMAX, dipole_removal=True,
+                   dipole_removal_distance=DIPOLE_THRESHOLD, random_seed=SEED)
     cores = ref.max_threads()
     ref.set_threads(cores)
+    state = {"x": x, "y": y, "g": g, "dt": DT0, "fsal": False,
+             "stepper": ref.stepper(geo, N), "n": N}
+
+    def step():
+        """One accepted DOPRI5 step + dipole events; returns the pair-interactions evaluated."""
+        n = state["n"]
+        nx, ny, res = state["stepper"].dopri5_step(state["x"], state["y"], state["g"], state["dt"])
+        evals = (0 if state["fsal"] else 1) + 6 * (int(res[3]) + 1)
+        state["fsal"] = True
+        state["dt"] = float(res[1])
+        if kind == "reference":
+            events, nx, ny, ng = ref.dipole_process(geo, nx, ny, state["g"])
+        else:
+            events, ng = 0, state["g"]
+        if events:
+            state["stepper"] = ref.stepper(geo, nx.size)  # the driver invalidates FSAL
+            state["fsal"] = False
+            state["g"], state["n"] = ng, nx.size
+        state["x"], state["y"] = nx, ny
+        return evals * n * (n - 1)
+
     t0 = time.perf_counter()
-    ref.evaluate_range(geo, x, y, g, 0, 8)
-    per_target = max(time.perf_counter() - t0, 1e-5) / 8
-    budget = 150.0 / max(args.steps + args.warmup, 1)    # whole run within a few minutes
-    targets = int(min(N, max(1, budget / per_target)))
-    for _ in range(args.warmup):
-        ref.evaluate_range(geo, x, y, g, 0, targets)
+    warm = 0
+    for _ in range(max(args.warmup, 1)):  # the first step also takes the start-up rejections
+        step()
+        warm += 1
+        if time.perf_counter() - t0 > REFERENCE_WARMUP_BUDGET_S:
+            break
+    pairs, timed = 0.0, 0
     t0 = time.perf_counter()
     for _ in range(args.steps):
-        ref.evaluate_range(geo, x, y, g, 0, targets)
+        pairs += step()
+        timed += 1
+        if time.perf_counter() - t0 > REFERENCE_TIMED_BUDGET_S:
+            break
     sec = time.perf_counter() - t0
-    value = args.steps * targets * (N - 1) / sec
-    sample = (f"each step: velocity of targets [0, {targets}) of the N={N} periodic state "
-              f"against all {N} sources (the reference's PeriodicBoxKernel::evaluateRange)")
+    value = pairs / sec
+    sample = (f"{timed} accepted DOPRI5 steps (of {args.steps} requested; {warm} warm-up) of the "
+              f"N={N} periodic workload, each with the dipole events: the reference's "
+              f"RungeKuttaIntegrator::dopri5Step over PeriodicBoxKernel and its DipoleManager, "
+              f"N(N-1) pairs per evaluation")
     return {"metric": METRIC, "value": value, "unit": "pair-interactions/s", "n_gpus": world,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": sec * 1e3 / args.steps,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": sec * 1e3 / timed,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic (seeded uniform positions, balanced +-1 circulations)",
             "impl": "reference",
             "config": {"workload": WORKLOAD, "geometry": "periodic", "n_vortices": N,
-                       "image_layers": LAYERS},
+                       "box_length": "2pi", "image_layers": LAYERS, "integrator": "dopri5",
+                       "rtol": RTOL, "atol": ATOL, "dipole_threshold": DIPOLE_THRESHOLD,
+                       "step": "one accepted DOPRI5 step + dipole scan"},
             "cpu_baseline": {"value": value, "unit": "pair-interactions/s", "cores": cores,
-                             "kind": kind, "sample": sample},
+                             "kind": kind, "sample": sample, "steps_timed": timed},
             "e2e": {"value": value, "unit": "pair-interactions/s", "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0}}
 
@@ -442,7 +500,7 @@ def run_reference_cuda(evals: int = 3, steps: int = 3) -> dict:
     round trip after every evaluation. Runs in its own process."""
     import ctypes
     from oracle.pyoracle import REF_CUDA_LIB, _Params
-    from pointvortex_b200 import ics
+    ics = load_ics()
     lib = ctypes.CDLL(REF_CUDA_LIB)
     D = ctypes.POINTER(ctypes.c_double)
     lib.pvref_stepper_create.restype = ctypes.c_void_p

@@ -354,6 +354,14 @@ pv_status pv_context_stream(const pv_context *ctx, void **stream);
  * pv_evaluate_range). pointvortex_b200/autotune.py fills it by timing the candidates. */
 pv_status pv_set_tuning(int geometry, int precision, int log2_n, int per_thread);
 pv_status pv_get_tuning(int geometry, int precision, int log2_n, int *per_thread);
+/* Polls of the context's bounded device waits before they give up with the runtime error "a bounded
+ * device wait timed out": copy_polls for a velocity tile's bulk copies (default 2^22), barrier_polls
+ * for a grid barrier of the cooperative RK4 steps (default 2^24); a negative value restores the
+ * default, 0 gives up without polling. A wait that gives up leaves the device state at the last
+ * completed step (a velocity tile first waits, with the default bound, for its copies in flight; a
+ * grid barrier is broken for every CTA at once). Only the tests of these exits shorten them. No
+ * reference counterpart (the reference CUDA backend has no device-side waits). */
+pv_status pv_set_wait_limits(pv_context *ctx, int64_t copy_polls, int64_t barrier_polls);
 /* Bracket every launch of the context with CUDA events recorded on its own stream. */
 pv_status pv_set_profiling(pv_context *ctx, int enabled);
 /* Synchronises the context stream and returns the counters accumulated since the last reset. */

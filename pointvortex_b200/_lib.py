@@ -173,6 +173,7 @@ SIGNATURES = {
     "pv_set_tuning": (_ST, [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int]),
     "pv_get_tuning": (_ST, [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_int)]),
     "pv_set_profiling": (_ST, [_CTX, ctypes.c_int]),
+    "pv_set_wait_limits": (_ST, [_CTX, ctypes.c_int64, ctypes.c_int64]),
     "pv_get_kernel_stats": (_ST, [_CTX, ctypes.POINTER(PvKernelStats)]),
     "pv_reset_kernel_stats": (_ST, [_CTX]),
 }

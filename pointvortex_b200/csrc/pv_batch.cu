@@ -184,6 +184,8 @@ __device__ __forceinline__ void run_item(const GeometryConsts &g, const double *
         const int st = k & 1;
         const bool ok = mbar_wait_bounded(&bars[st], (k >> 1) & 1, timeout_status);
         if (__syncthreads_or(!ok)) {
+            if (tid == 0)  // the copies of tiles k and k + 1 may still be in flight
+                mbar_drain(bars, k, t + 1 < ntiles);
             timed_out = true;
             return;
         }
@@ -392,6 +394,8 @@ __device__ __forceinline__ void run_item32(const GeometryConsts &g, const double
         const int st = k & 1;
         const bool ok = mbar_wait_bounded(&bars[st], (k >> 1) & 1, timeout_status);
         if (__syncthreads_or(!ok)) {
+            if (tid == 0)  // the copies of tiles k and k + 1 may still be in flight
+                mbar_drain(bars, k, t + 1 < ntiles);
             timed_out = true;
             return;
         }

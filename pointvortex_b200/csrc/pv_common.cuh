@@ -112,13 +112,26 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity) {
 // Bounded wait: gives up after `limit` polls (each try_wait may itself suspend the thread for a
 // hardware-chosen interval), reports ST_TIMEOUT and returns false. A bulk copy from valid global
 // memory always completes, so the bound only turns an impossible hang into an error status.
+// limit = 0 gives up without polling (the tests of the timeout exits use it).
 constexpr uint32_t kWaitLimit = 1u << 22;
-__device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, uint32_t parity, int *status) {
-    for (uint32_t it = 0; it < kWaitLimit; ++it)
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, uint32_t parity, int *status,
+                                                  uint32_t limit = kWaitLimit) {
+    for (uint32_t it = 0; it < limit; ++it)
         if (mbar_try_wait(bar, parity))
             return true;
     set_status(status, ST_TIMEOUT);
     return false;
+}
+
+// After a bounded wait gave up at tile k of a two-stage ring (tile k on stage k & 1, phase parity
+// (k >> 1) & 1), waits for the bulk copies still in flight -- tile k's and, when it was issued,
+// tile k + 1's -- so that none lands in shared memory after the CTA has exited. Run by the thread
+// that issued them, before it returns. The wait is bounded again, with the default limit.
+__device__ __forceinline__ void mbar_drain(uint64_t *bars, uint32_t k, bool next_issued) {
+    const uint32_t end = k + (next_issued ? 2u : 1u);
+    for (uint32_t q = k; q < end; ++q)
+        for (uint32_t it = 0; it < kWaitLimit && !mbar_try_wait(&bars[q & 1], (q >> 1) & 1); ++it) {
+        }
 }
 
 // ---------------------------------------------------------------------------------------------

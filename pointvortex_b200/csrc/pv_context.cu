@@ -121,6 +121,10 @@ struct pv_context {
     // text output (pv_format_*): row slots, row lengths, block offsets, the packed frame
     DeviceArray fmt_stage, fmt_len, fmt_block, fmt_out;
 
+    // polls of the bounded device waits (pv_set_wait_limits): tile copies, grid barrier
+    uint32_t wait_limit = kWaitLimit;
+    uint32_t spin_limit = kGridSpinLimit;
+
     // launch accounting and optional per-launch CUDA-event timing (pv_set_profiling)
     bool profiling = false;
     uint64_t launches[PV_KERNEL_KINDS] = {};
@@ -446,6 +450,7 @@ pv_status launch_eval(pv_context *c, const double *px, const double *py) {
     a.num_chunks = c->plan.num_chunks;
     a.status = &c->ctl->status;
     a.g = c->gc;
+    a.wait_limit = c->wait_limit;
     PV_CUDA(c, counted(c, PV_KERNEL_VELOCITY, 1, [&] {
                 return c->params.precision == PV_PRECISION_FP32C
                            ? launch_velocity_fp32c(a, c->plan, c->stream)
@@ -501,7 +506,9 @@ std::vector<const void *> attempt_key(const pv_context *c) {
                                    c->p1x.p, c->p1y.p, c->pu.p, c->pv.p, c->sym_items.p,
                                    c->sym_counter.p, c->ctl, c->cand.p,
                                    reinterpret_cast<const void *>(static_cast<uintptr_t>(
-                                       c->dipole_configured && c->dipole.removal ? 1 : 0))};
+                                       c->dipole_configured && c->dipole.removal ? 1 : 0)),
+                                   reinterpret_cast<const void *>(
+                                       static_cast<uintptr_t>(c->wait_limit))};
     uint64_t bits;
     std::memcpy(&bits, &c->dipole.distance, sizeof bits);
     k.push_back(reinterpret_cast<const void *>(static_cast<uintptr_t>(bits)));
@@ -595,6 +602,7 @@ pv_status evaluate_host(pv_context *c, const double *x, const double *y, const d
     a.num_chunks = plan.num_chunks;
     a.status = &c->ctl->status;
     a.g = c->gc;
+    a.wait_limit = c->wait_limit;
     PV_CUDA(c, counted(c, PV_KERNEL_VELOCITY, 1, [&] {
                 return c->params.precision == PV_PRECISION_FP32C
                            ? launch_velocity_fp32c(a, plan, c->stream)
@@ -930,6 +938,7 @@ pv_status enqueue_rk4_steps(pv_context *c, double dt, uint64_t steps) {
     p.chunk = c->plan.chunk;
     p.num_chunks = c->plan.num_chunks;
     p.steps = steps;
+    p.spin_limit = c->spin_limit;
     PV_CUDA(c, c->rk4_barrier.ensure(1));
     PV_CUDA(c, cudaMemsetAsync(c->rk4_barrier.p, 0, sizeof(unsigned long long), c->stream));
     p.barrier = reinterpret_cast<unsigned long long *>(c->rk4_barrier.p);
@@ -1731,6 +1740,17 @@ pv_status pv_context_stream(const pv_context *ctx, void **stream) {
     if (!ctx || !stream)
         return PV_ERROR_INVALID_ARGUMENT;
     *stream = static_cast<void *>(ctx->stream);
+    return PV_OK;
+}
+
+pv_status pv_set_wait_limits(pv_context *ctx, int64_t copy_polls, int64_t barrier_polls) {
+    if (!ctx)
+        return PV_ERROR_INVALID_ARGUMENT;
+    if (copy_polls > static_cast<int64_t>(UINT32_MAX) ||
+        barrier_polls > static_cast<int64_t>(UINT32_MAX))
+        return fail(ctx, PV_ERROR_INVALID_ARGUMENT, "wait limit out of range");
+    ctx->wait_limit = copy_polls < 0 ? kWaitLimit : static_cast<uint32_t>(copy_polls);
+    ctx->spin_limit = barrier_polls < 0 ? kGridSpinLimit : static_cast<uint32_t>(barrier_polls);
     return PV_OK;
 }
 

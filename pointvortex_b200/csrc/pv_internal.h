@@ -46,6 +46,7 @@ struct EvalArgs {
     int num_chunks;
     int *status;
     GeometryConsts g;
+    uint32_t wait_limit = kWaitLimit;  // polls of a bounded tile wait (pv_set_wait_limits)
 };
 
 struct EvalPlan {
@@ -128,6 +129,9 @@ struct StageArgs {
 
 cudaError_t launch_stage(const StageArgs &a, cudaStream_t stream, int sm_count);
 
+// Polls a grid barrier of the cooperative RK4 steps waits before it gives up (ST_TIMEOUT).
+constexpr uint32_t kGridSpinLimit = 1u << 24;
+
 // RK4 steps of a small FP64 population in one cooperative launch (pv_stepping.cu): the four
 // stages as enqueue_rk4 sets them up (stage[3].xt/yt: the combined state), bit for bit the same
 // results as launching them. barrier: the grid barrier's arrival counter, zero at every
@@ -140,6 +144,7 @@ struct Rk4Steps {
     int chunk, num_chunks;  // the ordered kernel's source chunks
     uint64_t steps;
     unsigned long long *barrier;
+    uint32_t spin_limit = kGridSpinLimit;  // polls of a grid-barrier wait (pv_set_wait_limits)
 };
 constexpr size_t kRk4StepsMaxN = 2048;
 bool rk4_steps_eligible(size_t n, int num_chunks);

@@ -17,7 +17,9 @@
 // In host code the array's name is only a host-side stand-in for the symbol, not a device
 // address: the first call on each device (with that device current) asks the runtime for the
 // array's device address with cudaGetSymbolAddress and caches it. Make that first call on a
-// device before any stream capture begins.
+// device before any stream capture begins. The cache is keyed by device ordinal and assumes the
+// runtime's primary context of that device for the life of the process: after cudaDeviceReset,
+// or with another context current, the cached address is not valid.
 #include "pvb200.h"
 #include "pv_internal.h"
 
@@ -71,18 +73,28 @@ pv_status scratch_for_device(int device, double **out) {
     return PV_OK;
 }
 
-// One block, fixed order: scaled circulations, the finiteness / disk checks of
-// validateVortexArrays and validateDiskPositions, and the periodic zero-net-circulation check of
-// validatePeriodicCirculation (src/vortex.h:7-14; src/compute.cpp:31-48).
+// Status of a periodic population whose circulations do not sum to zero. Set together with
+// status2 = 1, so that the velocity and reduction kernels (which return at once on a non-zero
+// status) leave u and v untouched; map_status reports it as the reference's invalid_argument.
+constexpr int kStatusNotNeutral = 100;
+constexpr int kNeutralTile = 2048;  // circulations staged in shared memory per pass
+
+// One block: scaled circulations and the input checks of the reference, in the reference's order
+// (src/compute.cpp:203-211 for the box): finiteness of every value (validateVortexArrays,
+// src/vortex.h:7-14), then the box's zero net circulation (validatePeriodicCirculation,
+// src/compute.cpp:31-38) or the disk's containment (validateDiskPositions, src/compute.cpp:41-48).
+// The net circulation and the sum of |Gamma| are added by one thread in index order, as the
+// reference adds them, so that a population near the 1e-12 threshold gets the same verdict here
+// as from the reference and from pv_evaluate; the block stages the circulations in shared memory
+// for it.
 __global__ void __launch_bounds__(1024)
     prepare_kernel(const double *x, const double *y, const double *gamma, size_t n,
                    GeometryConsts g, double *scaled, DeviceControl *ctl) {
-    __shared__ double s_total[32], s_abs[32];
+    __shared__ double s_gamma[kNeutralTile];
     __shared__ int s_bad;
     if (threadIdx.x == 0)
         s_bad = 0;
     __syncthreads();
-    double total = 0.0, absolute = 0.0;
     int bad = 0;
     for (size_t i = threadIdx.x; i < n; i += blockDim.x) {
         const double xi = x[i], yi = y[i], gi = gamma[i];
@@ -92,37 +104,41 @@ __global__ void __launch_bounds__(1024)
                  __dadd_rn(__dmul_rn(xi, xi), __dmul_rn(yi, yi)) >= g.radius2)
             bad = max(bad, 1);
         scaled[i] = scaled_circulation(g, gi);
-        total += gi;
-        absolute += fabs(gi);
     }
     if (bad)
         atomicMax(&s_bad, bad);
-    for (int off = 16; off > 0; off >>= 1) {
-        total += __shfl_down_sync(0xffffffffu, total, off);
-        absolute += __shfl_down_sync(0xffffffffu, absolute, off);
-    }
-    if ((threadIdx.x & 31) == 0) {
-        s_total[threadIdx.x >> 5] = total;
-        s_abs[threadIdx.x >> 5] = absolute;
-    }
     __syncthreads();
-    if (threadIdx.x == 0) {
-        double t = 0.0, a = 0.0;
-        for (int w = 0; w < static_cast<int>(blockDim.x >> 5); ++w) {
-            t += s_total[w];
-            a += s_abs[w];
-        }
-        if (s_bad == 2)
+    if (s_bad == 2) {
+        if (threadIdx.x == 0)
             set_status(&ctl->status, ST_NONFINITE_POSITION);
-        else if (g.geometry == GEO_PERIODIC && fabs(t) > 1e-12 * fmax(1.0, a))
-            ctl->status2 = 1; // periodic neutrality violated (invalid_argument)
-        else if (s_bad == 1)
-            set_status(&ctl->status, ST_OUTSIDE_DISK);
+        return;
     }
+    if (g.geometry == GEO_PERIODIC) {
+        double total = 0.0, absolute = 0.0;  // meaningful in thread 0 only
+        for (size_t base = 0; base < n; base += kNeutralTile) {
+            const size_t len = min(static_cast<size_t>(kNeutralTile), n - base);
+            for (size_t k = threadIdx.x; k < len; k += blockDim.x)
+                s_gamma[k] = gamma[base + k];
+            __syncthreads();
+            if (threadIdx.x == 0)
+                for (size_t k = 0; k < len; ++k) {
+                    total += s_gamma[k];
+                    absolute += fabs(s_gamma[k]);
+                }
+            __syncthreads();
+        }
+        if (threadIdx.x == 0 && fabs(total) > 1e-12 * fmax(1.0, absolute)) {
+            ctl->status2 = 1;
+            set_status(&ctl->status, kStatusNotNeutral);
+        }
+        return;
+    }
+    if (threadIdx.x == 0 && s_bad == 1)
+        set_status(&ctl->status, ST_OUTSIDE_DISK);
 }
 
 pv_status map_status(const DeviceControl &c, int geometry) {
-    if (c.status2 == 1 && c.status == 0)
+    if (c.status2 == 1)  // set only for finite data, and no later kernel ran
         return noalloc_fail(PV_ERROR_INVALID_ARGUMENT,
                             "periodic box requires zero total circulation");
     switch (c.status) {
@@ -140,6 +156,8 @@ pv_status map_status(const DeviceControl &c, int geometry) {
     case ST_NONFINITE_VELOCITY:
         return noalloc_fail(PV_ERROR_RUNTIME,
                             "non-finite velocity; check scales and close encounters");
+    case ST_TIMEOUT:
+        return noalloc_fail(PV_ERROR_RUNTIME, "a bounded device wait timed out");
     default:
         return noalloc_fail(PV_ERROR_RUNTIME, "device reported status " + std::to_string(c.status));
     }

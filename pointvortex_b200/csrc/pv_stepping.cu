@@ -303,32 +303,47 @@ cudaError_t launch_stage(const StageArgs &a, cudaStream_t stream, int sm_count) 
 
 // Grid barrier over the CTAs of a cooperative launch. The arrival counter starts at zero (the
 // host clears it before the launch) and only grows: the r-th barrier is open once it reaches
-// r * gridDim.x. One fence and one atomic per CTA, then polling with an acquire load. A wait
-// that does not end within the spin limit sets ST_TIMEOUT and returns false; the other CTAs
-// then time out at their next barrier.
-constexpr uint32_t kGridSpinLimit = 1u << 24;
+// r * gridDim.x. One fence and one atomic per CTA, then polling with an acquire load.
+//
+// A wait that outlasts `limit` polls breaks the barrier instead of walking away from it: a
+// compare-and-swap sets kBarrierBroken in the counter, and succeeds only if the counter has not
+// moved since it was read. Every CTA therefore agrees on each barrier: either it opened (the last
+// arrival came before the swap) and all pass it, or it is broken and none does -- later arrivals
+// and pollers see the flag and return. The breaker sets ST_TIMEOUT. Since the state is written
+// only in phases that follow an open barrier, a timeout leaves it at the last completed step.
+constexpr unsigned long long kBarrierBroken = 1ull << 62;
 __device__ bool grid_barrier(unsigned long long *arrivals, unsigned long long open_at,
-                             int *status) {
+                             int *status, uint32_t limit) {
     __shared__ int ok;
     __syncthreads();
     if (threadIdx.x == 0) {
         __threadfence();  // this CTA's writes, ordered by the __syncthreads, before its arrival
-        atomicAdd(arrivals, 1ull);
+        unsigned long long now = atomicAdd(arrivals, 1ull) + 1ull;
         ok = 1;
         uint32_t it = 0;
         for (;;) {
-            unsigned long long now;
-            asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(now) : "l"(arrivals) : "memory");
-            if (now >= open_at)
-                break;
-            if (++it > kGridSpinLimit) {
-                set_status(status, ST_TIMEOUT);
+            if (now & kBarrierBroken) {
                 ok = 0;
                 break;
             }
+            if (now >= open_at)
+                break;
+            if (it >= limit) {
+                const unsigned long long seen = atomicCAS(arrivals, now, now | kBarrierBroken);
+                if (seen == now) {
+                    set_status(status, ST_TIMEOUT);
+                    ok = 0;
+                    break;
+                }
+                now = seen;  // another CTA arrived (or broke it) meanwhile: look again
+                continue;
+            }
+            ++it;
             if (it > 64)
                 __nanosleep(32);
+            asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(now) : "l"(arrivals) : "memory");
         }
+        __threadfence();  // the other CTAs' writes before their arrivals are visible from here
     }
     __syncthreads();
     return ok != 0;
@@ -399,10 +414,11 @@ __global__ void __launch_bounds__(256) rk4_steps_kernel(const Rk4Steps p) {
                     finish_target<STAGE_RK4_COMBINE>(a, i, ku, kv, a.dt, local_max, sx, sy);
             }
             open_at += gridDim.x;
-            if (!grid_barrier(p.barrier, open_at, status))
+            if (!grid_barrier(p.barrier, open_at, status, p.spin_limit))
                 return;
+            // every CTA reads the same word after an open barrier: errors are set before arrival
             if (*reinterpret_cast<volatile int *>(status) != 0)
-                return;  // every CTA reads the same word after the barrier
+                return;
         }
     }
     for (int li = threadIdx.x; li < mine; li += blockDim.x) {  // the last step's accept

@@ -97,13 +97,14 @@ __global__ void __launch_bounds__(B) velocity_kernel(const EvalArgs a) {
     }
     __syncthreads();
 
-    bool timed_out = false;
     for (int t = 0; t < ntiles; ++t) {
         const int st = t & 1;
-        const bool ok = mbar_wait_bounded(&bars[st], static_cast<uint32_t>((t >> 1) & 1), a.status);
+        const bool ok = mbar_wait_bounded(&bars[st], static_cast<uint32_t>((t >> 1) & 1), a.status,
+                                          a.wait_limit);
         if (__syncthreads_or(!ok)) {
-            timed_out = true;
-            break;
+            if (tid == 0)  // the copies of tiles t and t + 1 may still be in flight
+                mbar_drain(bars, static_cast<uint32_t>(t), t + 1 < ntiles);
+            return;
         }
         const size_t j0 = src0 + static_cast<size_t>(t) * kTile;
         const int cnt = static_cast<int>(min(static_cast<size_t>(kTile), src1 - j0));
@@ -133,16 +134,6 @@ __global__ void __launch_bounds__(B) velocity_kernel(const EvalArgs a) {
         __syncthreads();
         if (tid == 0 && t + 2 < ntiles)
             issue(t + 2);
-    }
-    if (timed_out) {
-        // Give copies still in flight a bounded chance to land before shared memory is released.
-        if (tid == 0)
-            for (int s = 0; s < 2; ++s)
-                for (uint32_t it = 0; it < 1024 && !mbar_try_wait(&bars[s], 0) &&
-                                      !mbar_try_wait(&bars[s], 1);
-                     ++it) {
-                }
-        return;
     }
 
     const size_t base = static_cast<size_t>(chunk) * a.stride - a.t_begin;

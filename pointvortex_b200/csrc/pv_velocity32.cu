@@ -110,9 +110,13 @@ __global__ void __launch_bounds__(B) velocity32_kernel(const EvalArgs a) {
 
     for (int t = 0; t < ntiles; ++t) {
         const int st = t & 1;
-        const bool ok = mbar_wait_bounded(&bars[st], static_cast<uint32_t>((t >> 1) & 1), a.status);
-        if (__syncthreads_or(!ok))
+        const bool ok = mbar_wait_bounded(&bars[st], static_cast<uint32_t>((t >> 1) & 1), a.status,
+                                          a.wait_limit);
+        if (__syncthreads_or(!ok)) {
+            if (tid == 0)  // the copies of tiles t and t + 1 may still be in flight
+                mbar_drain(bars, static_cast<uint32_t>(t), t + 1 < ntiles);
             return;
+        }
         const size_t j0 = src0 + static_cast<size_t>(t) * kTile32;
         const int cnt = static_cast<int>(min(static_cast<size_t>(kTile32), src1 - j0));
         // split the tile into double-float FP32 coordinates once per CTA

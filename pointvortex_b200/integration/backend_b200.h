@@ -1,5 +1,6 @@
 // backend_b200.h — the B200 backend's hooks beyond src/backend.h, for a driver patched to keep
-// the population on the GPU (the patch is shown in INTEGRATION.md).
+// the population on the GPU: device dipole events and the GPU trajectory and checkpoint writers
+// (src/main.cpp:327-337 is the loop such a driver changes).
 #pragma once
 
 #include "backend.h"

@@ -351,6 +351,12 @@ class VelocityKernel:
         """Bracket every kernel launch with CUDA events on the context's stream."""
         self._check(lib.pv_set_profiling(self._ctx, int(bool(enabled))))
 
+    def setWaitLimits(self, copy_polls: int = -1, barrier_polls: int = -1) -> None:
+        """Polls of the bounded device waits before they give up (pv_set_wait_limits): the tile
+        copies of a velocity launch and the grid barrier of the cooperative RK4 steps; -1 keeps
+        the default, 0 gives up without polling."""
+        self._check(lib.pv_set_wait_limits(self._ctx, int(copy_polls), int(barrier_polls)))
+
     def kernelStats(self) -> dict:
         """{kind: (launches, timed launches, summed milliseconds)} since the last reset."""
         st = _lib.PvKernelStats()

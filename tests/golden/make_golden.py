@@ -148,10 +148,13 @@ def output_fixtures(ref: Oracle) -> None:
 
 def main() -> int:
     ap = argparse.ArgumentParser()
-    ap.add_argument("--reference", default="/root/reference")
+    ap.add_argument("--reference", default=os.environ.get("PV_REFERENCE_DIR"),
+                    help="the reference checkout (default: $PV_REFERENCE_DIR)")
     ap.add_argument("--only", choices=["dipole_events", "output"], default=None,
                     help="regenerate one fixture family only")
     args = ap.parse_args()
+    if not args.reference:
+        ap.error("give --reference <dir> or set PV_REFERENCE_DIR")
     subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle"), "ref",
                     f"REF={args.reference}"], check=True)
     ref = Oracle("reference")
