@@ -579,7 +579,7 @@ def solve_batch(specs, budget: int, precision: str, device: int = 0):
         info = b.info(sid)
         b.result(sid)
         evals = 6 * (info.acceptedSteps + info.rejectedSteps) + 1
-        out.append((info.state, float(evals) * n * (n - 1)))
+        out.append((info, float(evals) * n * (n - 1)))
     elapsed = time.perf_counter() - t0
     b.close()
     return out, attempts, elapsed
@@ -591,15 +591,25 @@ def run_ensemble(n_sims: int = 512, budget: int = 10, seed: int = 7,
     workloads are chaotic, so unbudgeted work per simulation is unbounded)."""
     specs = ensemble_specs(n_sims, seed)
     results, attempts, elapsed = solve_batch(specs, budget, precision)
-    finished = {}
-    for state, _ in results:
-        finished[state] = finished.get(state, 0) + 1
+    finished, reasons = {}, {}
+    projected = {}
+    for (info, _), (geo, n, _) in zip(results, specs):
+        finished[info.state] = finished.get(info.state, 0) + 1
+        key = f"{geo}:{info.reason}"
+        reasons[key] = reasons.get(key, 0) + 1
+        if info.state == "budget" and info.time > 0:
+            # accepted steps this simulation would need to reach t_end at its average step so far
+            projected.setdefault(geo, []).append(info.acceptedSteps * 0.5 / info.time)
     pairs = sum(p for _, p in results)
     return {"simulations": n_sims, "vortices": sum(n for _, n, _ in specs), "step_budget": budget,
-            "attempts": attempts, "seconds": elapsed, "solves_per_s": n_sims / elapsed,
+            "attempts": attempts, "seconds": elapsed, "budgeted_solves_per_s": n_sims / elapsed,
             "pair_interactions_per_s": pairs / elapsed, "states": finished,
+            "stop_reasons": dict(sorted(reasons.items())),
+            "projected_steps_to_t_end_median": {g: float(np.median(v)) for g, v in projected.items()},
             "dtype": "f64" if precision == "fp64" else "f32 compensated (f64 state and control)",
-            "note": "one arena, lock-step DOPRI5 attempts, CUDA-graph replay per attempt"}
+            "note": "one arena, lock-step DOPRI5 attempts, CUDA-graph replay per attempt; a "
+                    "'budgeted solve' is a simulation that stopped (done, budget or failure), "
+                    "not one that reached t_end"}
 
 
 def run_ensemble_sharded(rank: int, world: int, device: int, n_sims: int = 512, budget: int = 10,
@@ -620,7 +630,7 @@ def run_ensemble_sharded(rank: int, world: int, device: int, n_sims: int = 512, 
             timing["error"] = str(exc)[:200]
             return []
         timing["seconds"] = elapsed
-        return [(i, r) for (i, _), r in zip(mine, results)]
+        return [(i, (info.reason, pairs)) for (i, _), (info, pairs) in zip(mine, results)]
 
     dist.barrier()
     merged = run_sharded(specs, lambda s: simulation_cost(s[0], s[1]), run_local, rank, world,
@@ -632,8 +642,12 @@ def run_ensemble_sharded(rank: int, world: int, device: int, n_sims: int = 512, 
     if errors or any(m is None for m in merged):
         return {"error": (errors or ["a rank returned no results"])[0]}
     pairs = sum(p for _, p in merged)
+    reasons = {}
+    for reason, _ in merged:
+        reasons[reason] = reasons.get(reason, 0) + 1
     return {"simulations": n_sims, "ranks": world, "seconds": seconds,
-            "solves_per_s": n_sims / seconds, "pair_interactions_per_s": pairs / seconds,
+            "budgeted_solves_per_s": n_sims / seconds, "pair_interactions_per_s": pairs / seconds,
+            "stop_reasons": reasons,
             "note": "replicas: one batch engine per GPU, cost-balanced partition, results "
                     "gathered once"}
 
@@ -660,6 +674,29 @@ def run_serving(budget: int = 10) -> dict:
     base["rate_per_s"] = 100.0
     out["one_request_per_launch_fp64"] = base
     return out
+
+
+def reference_rk4_drift(x, y, g, steps: int = 100, dt: float = 1e-3) -> dict:
+    """The invariants' drift of the reference's own CPU run of the same RK4 case
+    (RungeKuttaIntegrator::rk4Step, src/timestep.cpp:31-61; computeInvariants,
+    src/compute.cpp:134-163), printed beside the GPU's: H and L are not conserved by RK4 at this
+    step, so their drift is compared in size, not value."""
+    from oracle.pyoracle import Geometry, Oracle
+    try:
+        ref = Oracle("reference")
+    except FileNotFoundError:
+        return {"unavailable": "oracle/_ref was not built"}
+    ref.set_threads(ref.max_threads())
+    geo = Geometry("infinite")
+    inv0 = ref.invariants(geo, x, y, g)
+    st = ref.stepper(geo, x.size)
+    cx, cy = x.copy(), y.copy()
+    for _ in range(steps):
+        cx, cy = st.rk4_step(cx, cy, g, dt)
+    d = ref.invariants(geo, cx, cy, g) - inv0
+    return {"circulation": float(d[0]), "linear_impulse_x": float(d[1]),
+            "linear_impulse_y": float(d[2]), "angular_impulse": float(d[3]),
+            "hamiltonian": float(d[4]), "kind": "reference CPU (oracle/_ref)"}
 
 
 def run_other_configs() -> dict:
@@ -697,6 +734,7 @@ def run_other_configs() -> dict:
                   "angular_impulse": inv1.angularImpulse - inv0.angularImpulse,
                   "hamiltonian": inv1.hamiltonian - inv0.hamiltonian},
         "note": "the 100 steps are one cooperative launch (pv_rk4_advance, N <= 2048)"}
+    out["infinite_rk4_n1024"]["reference_drift"] = reference_rk4_drift(x, y, g)
     x, y, g = ics.workload_state("disk_rk4_n16384")
     forms = {}
     vel = {}
@@ -723,6 +761,57 @@ def run_other_configs() -> dict:
     forms["fp32c_vs_fp64_error"] = {"max": float(err.max()), "rms": float(np.sqrt(np.mean(err ** 2)))}
     forms["speedup"] = forms["fp32c"]["pair_interactions_per_s"] / forms["fp64"]["pair_interactions_per_s"]
     out["disk_n16384"] = forms
+    return out
+
+
+def run_fp32c_curve(reps: int = 10) -> dict:
+    """Error and speed of the FP32-compensated form against its near-field radius, on the periodic
+    workload state (N = 4096, symmetric kernel) and the disk workload state (N = 16384, Gaussian
+    circulations, ordered kernel): per radius (in units of the mean spacing; 0 = no near field) the
+    per-vortex error against the FP64 kernel (itself within 1e-12 of the oracle) and the time per
+    evaluation, next to the FP64 kernel's."""
+    import torch
+    import pointvortex_b200 as pv
+    from pointvortex_b200 import ics
+    out = {}
+    cases = [("periodic_n4096", lambda p: pv.PeriodicBoxKernel(LENGTH, LENGTH, LAYERS, precision=p),
+              ics.workload_state("periodic_dopri5_n4096"), LENGTH / np.sqrt(4096)),
+             ("disk_n16384", lambda p: pv.DiskKernel(1.0, precision=p),
+              ics.workload_state("disk_rk4_n16384"), np.sqrt(np.pi / 16384))]
+
+    def timed(k):
+        k.evaluateDeviceState()
+        k.setProfiling(True)
+        k.resetKernelStats()
+        for _ in range(reps):
+            f = k.evaluateDeviceState()
+        st = k.kernelStats()
+        k.setProfiling(False)
+        ms = (st["velocity"][2] + st["stage"][2]) / max(st["stage"][1], 1)
+        return f, ms
+
+    for name, make, (x, y, g), spacing in cases:
+        k64 = make(0)
+        k64.uploadDeviceState(pv.VortexSystem(x, y, g))
+        ref, ms64 = timed(k64)
+        mag = np.hypot(ref.x, ref.y)
+        scale = np.maximum(mag, np.sqrt(np.mean(mag * mag)))
+        rows = []
+        k32 = make(1)
+        k32.uploadDeviceState(pv.VortexSystem(x, y, g))
+        for units in (0.0, 0.5, 1.0, 2.0, 4.0, 8.0):
+            k32.setNearField(units * spacing)
+            f, ms = timed(k32)
+            err = np.hypot(f.x - ref.x, f.y - ref.y) / scale
+            rows.append({"radius_spacings": units, "radius": units * spacing,
+                         "max": float(err.max()), "rms": float(np.sqrt(np.mean(err ** 2))),
+                         "ms_per_evaluation": ms, "speedup_vs_fp64": ms64 / ms})
+        k32.setNearField(-1.0)
+        out[name] = {"fp64_ms_per_evaluation": ms64, "default_radius": k32.nearField,
+                     "curve": rows, "note": "evaluation = velocity launches + reduction stage"}
+        k32.close()
+        k64.close()
+    torch.cuda.synchronize()
     return out
 
 
@@ -834,6 +923,8 @@ def main(argv=None):
                     help="print the per-kernel summary of an ncu launch list and exit")
     ap.add_argument("--no-peak-probe", action="store_true",
                     help="report the roofline against the last measured FP64 peak")
+    ap.add_argument("--fp32c-curve", action="store_true",
+                    help="print the FP32C error and speed against the near-field radius and exit")
     args = ap.parse_args(argv)
     rank, world, _ = rank_info()
     if args.summarize_launches:
@@ -841,6 +932,9 @@ def main(argv=None):
         return 0
     if args.reference_cuda:
         print(json.dumps(run_reference_cuda()), flush=True)
+        return 0
+    if args.fp32c_curve:
+        print(json.dumps(run_fp32c_curve()), flush=True)
         return 0
     if args.kernel_case:
         print(json.dumps(run_kernel_case(args.kernel_case, args.evals, args.precision,
@@ -873,6 +967,10 @@ def main(argv=None):
             result["other_configs"] = run_other_configs()
         except Exception as exc:
             result["other_configs"] = {"error": str(exc)[:200]}
+        try:
+            result["fp32c_near_field"] = run_fp32c_curve()
+        except Exception as exc:
+            result["fp32c_near_field"] = {"error": str(exc)[:200]}
         try:
             out = run_output()
             inputs = out.pop("inputs")

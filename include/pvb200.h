@@ -270,6 +270,13 @@ typedef struct pv_batch_solve {
 #define PV_SIM_FAILED 3  /* stopped with an error: see status (device status code) */
 #define PV_SIM_BUDGET 4  /* stopped at its step budget before t_end */
 
+/* Which condition stopped a simulation whose status is the adaptive integrator's failure (the
+ * reference throws the same runtime_error for each: src/timestep.cpp:116-117, src/main.cpp:314). */
+#define PV_FAILURE_NONE 0
+#define PV_FAILURE_REJECTION_CAP 1   /* more than 32 rejections in one step */
+#define PV_FAILURE_DT_FLOOR 2        /* rejected at dt <= minimum time step */
+#define PV_FAILURE_NO_TIME_ADVANCE 3 /* t + dt == t: the step cannot advance the time */
+
 typedef struct pv_batch_sim_info {
     int state;                  /* PV_SIM_* */
     int status;                 /* device status code when failed, 0 otherwise */
@@ -278,6 +285,7 @@ typedef struct pv_batch_sim_info {
     uint64_t accepted_steps;
     uint64_t rejected_steps;
     uint32_t population;
+    int failure;                /* PV_FAILURE_* when status is the integrator's failure */
 } pv_batch_sim_info;
 
 typedef struct pv_batch_totals {
@@ -354,6 +362,15 @@ pv_status pv_context_stream(const pv_context *ctx, void **stream);
  * pv_evaluate_range). pointvortex_b200/autotune.py fills it by timing the candidates. */
 pv_status pv_set_tuning(int geometry, int precision, int log2_n, int per_thread);
 pv_status pv_get_tuning(int geometry, int precision, int log2_n, int *per_thread);
+/* Near-field radius of the FP32-compensated form (precision PV_PRECISION_FP32C): periodic pairs
+ * closer than it (minimum image) and disk wall images closer than it to their target are left out
+ * of the FP32 sums and evaluated in FP64. radius < 0 selects the default for the population (twice
+ * the mean spacing of N uniform vortices), 0 turns the near field off. Applies to the device state
+ * at once and to later evaluations; the plane and FP64 contexts ignore it. No reference
+ * counterpart (the reference evaluates in FP64 only). */
+pv_status pv_set_near_field(pv_context *ctx, double radius);
+/* The near-field radius in use for the device state (0 when there is none). */
+pv_status pv_get_near_field(const pv_context *ctx, double *radius);
 /* Polls of the context's bounded device waits before they give up with the runtime error "a bounded
  * device wait timed out": copy_polls for a velocity tile's bulk copies (default 2^22), barrier_polls
  * for a grid barrier of the cooperative RK4 steps (default 2^24); a negative value restores the

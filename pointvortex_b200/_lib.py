@@ -93,7 +93,8 @@ class PvBatchSolve(ctypes.Structure):
 class PvBatchSimInfo(ctypes.Structure):
     _fields_ = [("state", ctypes.c_int), ("status", ctypes.c_int), ("time", ctypes.c_double),
                 ("suggested_time_step", ctypes.c_double), ("accepted_steps", ctypes.c_uint64),
-                ("rejected_steps", ctypes.c_uint64), ("population", ctypes.c_uint32)]
+                ("rejected_steps", ctypes.c_uint64), ("population", ctypes.c_uint32),
+                ("failure", ctypes.c_int)]
 
 
 class PvBatchTotals(ctypes.Structure):
@@ -174,6 +175,8 @@ SIGNATURES = {
     "pv_get_tuning": (_ST, [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_int)]),
     "pv_set_profiling": (_ST, [_CTX, ctypes.c_int]),
     "pv_set_wait_limits": (_ST, [_CTX, ctypes.c_int64, ctypes.c_int64]),
+    "pv_set_near_field": (_ST, [_CTX, ctypes.c_double]),
+    "pv_get_near_field": (_ST, [_CTX, _D]),
     "pv_get_kernel_stats": (_ST, [_CTX, ctypes.POINTER(PvKernelStats)]),
     "pv_reset_kernel_stats": (_ST, [_CTX]),
 }

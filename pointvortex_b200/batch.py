@@ -23,6 +23,13 @@ class CapacityError(RuntimeError):
     """Admission refused: no free slot or no room in the batch arena."""
 
 
+# Why a failed simulation stopped: the device status code (and, for the integrator's failure, which
+# of its conditions), named after the reference's checks.
+_STATUS_REASONS = {2: "outside_disk", 3: "nonfinite_position", 4: "nonfinite_error_estimate",
+                   5: "nonfinite_velocity", 6: "coincident", 10: "timeout"}
+_INTEGRATOR_FAILURES = {1: "rejection_cap", 2: "dt_floor", 3: "no_time_advance"}
+
+
 @dataclass
 class SimInfo:
     state: str
@@ -32,6 +39,19 @@ class SimInfo:
     acceptedSteps: int
     rejectedSteps: int
     population: int
+    failure: int = 0
+
+    @property
+    def reason(self) -> str:
+        """"done", "budget", "running", or the failure: rejection_cap (more than 32 rejections
+        in one step), dt_floor (rejected at the minimum step), no_time_advance (src/timestep.cpp:
+        116-117, src/main.cpp:314-315), outside_disk (src/compute.cpp:41-48), coincident,
+        nonfinite_velocity, nonfinite_position, nonfinite_error_estimate, timeout."""
+        if self.state != "failed":
+            return self.state
+        if self.status == 1:
+            return _INTEGRATOR_FAILURES.get(self.failure, "integrator")
+        return _STATUS_REASONS.get(self.status, f"status_{self.status}")
 
 
 PRECISIONS = {"fp64": _lib.PRECISION_FP64, "fp32c": _lib.PRECISION_FP32C}
@@ -105,7 +125,8 @@ class Batch:
         i = _lib.PvBatchSimInfo()
         self._check(lib.pv_batch_info(self._b, sid, ctypes.byref(i)))
         return SimInfo(STATES.get(i.state, "free"), i.status, i.time, i.suggested_time_step,
-                       int(i.accepted_steps), int(i.rejected_steps), int(i.population))
+                       int(i.accepted_steps), int(i.rejected_steps), int(i.population),
+                       int(i.failure))
 
     def result(self, sid: int):
         n = self.info(sid).population

@@ -19,7 +19,7 @@ CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libpvb200.so")
 OBJ_DIR = os.path.join(HERE, "_build")
 SOURCES = ["pv_velocity.cu", "pv_velocity32.cu", "pv_stepping.cu", "pv_invariants.cu", "pv_dipole.cu", "pv_context.cu",
-           "pv_noalloc.cu", "pv_batch.cu", "pv_output.cu", "pv_symmetric.cu"]
+           "pv_noalloc.cu", "pv_batch.cu", "pv_output.cu", "pv_symmetric.cu", "pv_near.cu"]
 HEADERS = ["pv_common.cuh", "pv_geometry.cuh", "pv_format.cuh", "pv_pair32.cuh", "pv_symmetric.cuh",
            "pv_internal.h"]
 NVCC_FLAGS = [

@@ -73,7 +73,7 @@ struct SimControl {
     int accepted;
     int fsal;
     unsigned rejected;
-    unsigned pad0;
+    int failure;                   // PV_FAILURE_* of a ST_DOPRI_FAILED stop
     unsigned long long err_bits;
     unsigned long long steps;
     unsigned long long max_steps;
@@ -301,11 +301,12 @@ __device__ __forceinline__ void run_symmetric_item32(const GeometryConsts &g, co
         sg[lane] = sj < n ? static_cast<float>(sgs[sj]) : 0.0f;
         __syncwarp();
         float u = 0.0f, v = 0.0f;
+        const sym::NearTile no_near{{nullptr, nullptr}, ti, j0};  // ensembles: no near field
         if (diagonal) {
-            sym::one_sided_tile32(f, t, t_ok, sf, sg, s_count, q == w, u, v);
+            sym::one_sided_tile32(f, t, t_ok, sf, sg, s_count, q == w, u, v, no_near);
         } else {
             float ru = 0.0f, rv = 0.0f;
-            sym::react_tile32(f, t, tg, t_ok, sf, sg, s_count, u, v, ru, rv);
+            sym::react_tile32(f, t, tg, t_ok, sf, sg, s_count, u, v, ru, rv, no_near);
             red_u[w * kBlock + q * 32 + lane] = static_cast<double>(ru);
             red_v[w * kBlock + q * 32 + lane] = static_cast<double>(rv);
         }
@@ -340,7 +341,7 @@ __device__ __forceinline__ void run_item32(const GeometryConsts &g, const double
                                            size_t src1, size_t blk0, size_t blk1, double *pu,
                                            double *pv, size_t out0, double (*s_x)[kTileB],
                                            double (*s_y)[kTileB], double (*s_g)[kTileB],
-                                           float4 *s_f, float *s_gf, uint64_t *bars,
+                                           float4 *s_f, float4 *s_fi, float *s_gf, uint64_t *bars,
                                            uint32_t &seq, int *timeout_status, bool &timed_out) {
     const int tid = threadIdx.x;
     const f32::F32Geometry f = f32::make_f32(g);
@@ -403,9 +404,9 @@ __device__ __forceinline__ void run_item32(const GeometryConsts &g, const double
         const int cnt = static_cast<int>(min(static_cast<size_t>(kTileB), src1 - j0));
         for (int j = tid; j < cnt; j += kBlock) {
             const double xj = s_x[st][j], yj = s_y[st][j];
-            const float xh = static_cast<float>(xj), yh = static_cast<float>(yj);
-            s_f[j] = make_float4(xh, yh, static_cast<float>(xj - static_cast<double>(xh)),
-                                 static_cast<float>(yj - static_cast<double>(yh)));
+            s_f[j] = f32::split_position(xj, yj);
+            if (GEO == GEO_DISK)
+                s_fi[j] = f32::image_position(g, xj, yj);
             s_gf[j] = static_cast<float>(s_g[st][j]);
         }
         __syncthreads();
@@ -416,21 +417,21 @@ __device__ __forceinline__ void run_item32(const GeometryConsts &g, const double
 #pragma unroll 1
                 for (int j = jb; j < je; ++j) {
                     const float4 sf = s_f[j];
+                    const float4 si = GEO == GEO_DISK ? s_fi[j] : sf;
                     const float gf = s_gf[j];
 #pragma unroll
-                    for (int q = 0; q < T; ++q)
-                        f32::pair32<GEO, true>(f, g, tg[q], sf, gf, s_x[st][j], s_y[st][j],
-                                               s_g[st][j], ti[q] == j0 + j, u[q], v[q], ud[q], vd[q]);
+                    for (int q = 0; q < T; ++q)  // ensembles: no near field (nothing is listed)
+                        f32::pair32<GEO, true>(f, tg[q], sf, si, gf, ti[q] == j0 + j, u[q], v[q]);
                 }
             } else {
 #pragma unroll 2
                 for (int j = jb; j < je; ++j) {
                     const float4 sf = s_f[j];
+                    const float4 si = GEO == GEO_DISK ? s_fi[j] : sf;
                     const float gf = s_gf[j];
 #pragma unroll
                     for (int q = 0; q < T; ++q)
-                        f32::pair32<GEO, false>(f, g, tg[q], sf, gf, s_x[st][j], s_y[st][j],
-                                                s_g[st][j], false, u[q], v[q], ud[q], vd[q]);
+                        f32::pair32<GEO, false>(f, tg[q], sf, si, gf, false, u[q], v[q]);
                 }
             }
 #pragma unroll
@@ -473,6 +474,7 @@ __global__ void __launch_bounds__(kBlock) batch_velocity_kernel(const VelocityBa
     __shared__ alignas(128) double s_y[2][kTileB];
     __shared__ alignas(128) double s_g[2][kTileB];
     __shared__ alignas(16) float4 s_f[PREC == PV_PRECISION_FP32C ? kTileB : 1];
+    __shared__ alignas(16) float4 s_fi[PREC == PV_PRECISION_FP32C ? kTileB : 1];  // disk images
     __shared__ float s_gf[PREC == PV_PRECISION_FP32C ? kTileB : 1];
     __shared__ alignas(8) uint64_t bars[2];
     __shared__ GeometryConsts s_geo;
@@ -532,17 +534,17 @@ __global__ void __launch_bounds__(kBlock) batch_velocity_kernel(const VelocityBa
             switch (s_geo.geometry) {
             case GEO_INFINITE:
                 run_item32<GEO_INFINITE, 4>(s_geo, px, py, sgs, src0, src1, blk0, blk1, pu, pv,
-                                            out0, s_x, s_y, s_g, s_f, s_gf, bars, seq,
+                                            out0, s_x, s_y, s_g, s_f, s_fi, s_gf, bars, seq,
                                             a.timeout_status, timed_out);
                 break;
             case GEO_PERIODIC:
                 run_item32<GEO_PERIODIC, 1>(s_geo, px, py, sgs, src0, src1, blk0, blk1, pu, pv,
-                                            out0, s_x, s_y, s_g, s_f, s_gf, bars, seq,
+                                            out0, s_x, s_y, s_g, s_f, s_fi, s_gf, bars, seq,
                                             a.timeout_status, timed_out);
                 break;
             default:
                 run_item32<GEO_DISK, 2>(s_geo, px, py, sgs, src0, src1, blk0, blk1, pu, pv, out0,
-                                        s_x, s_y, s_g, s_f, s_gf, bars, seq, a.timeout_status,
+                                        s_x, s_y, s_g, s_f, s_fi, s_gf, bars, seq, a.timeout_status,
                                         timed_out);
                 break;
             }
@@ -744,14 +746,18 @@ __global__ void batch_control_kernel(SimControl *ctl, unsigned n_sims) {
             c.state = SIM_BUDGET;
         } else {
             c.dt_attempt = min_r(c.dt, c.t_end - c.t);
-            if (!(c.t + c.dt_attempt > c.t))
-                c.status = ST_DOPRI_FAILED, c.state = SIM_FAILED;
+            if (!(c.t + c.dt_attempt > c.t))  // src/main.cpp:314-315
+                c.status = ST_DOPRI_FAILED, c.state = SIM_FAILED,
+                c.failure = PV_FAILURE_NO_TIME_ADVANCE;
         }
     } else {
         ++c.rejections_total;
-        if (dt <= c.dtmin || ++c.rejected > 32u) {
+        // src/timestep.cpp:116-117: the floor is tested first, as there
+        const bool floor = dt <= c.dtmin;
+        if (floor || ++c.rejected > 32u) {
             c.status = ST_DOPRI_FAILED;
             c.state = SIM_FAILED;
+            c.failure = floor ? PV_FAILURE_DT_FLOOR : PV_FAILURE_REJECTION_CAP;
         } else {
             c.dt_attempt = max_r(c.dtmin, min_r(suggested, __dmul_rn(dt, 0.9)));
         }
@@ -1300,6 +1306,7 @@ pv_status pv_batch_info(pv_batch *b, uint32_t id, pv_batch_sim_info *info) {
     info->accepted_steps = c.steps;
     info->rejected_steps = c.rejections_total;
     info->population = b->descs[id].n;
+    info->failure = c.status == ST_DOPRI_FAILED ? c.failure : PV_FAILURE_NONE;
     return PV_OK;
 }
 

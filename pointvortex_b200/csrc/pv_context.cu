@@ -121,6 +121,11 @@ struct pv_context {
     // text output (pv_format_*): row slots, row lengths, block offsets, the packed frame
     DeviceArray fmt_stage, fmt_len, fmt_block, fmt_out;
 
+    // FP32C near field (pv_set_near_field): the lists of pairs left to the FP64 pass, and the
+    // radius (< 0: the default for the population, 0: none)
+    DeviceArray near_count, near_slot;
+    double near_radius = -1.0;
+
     // polls of the bounded device waits (pv_set_wait_limits): tile copies, grid barrier
     uint32_t wait_limit = kWaitLimit;
     uint32_t spin_limit = kGridSpinLimit;
@@ -148,7 +153,7 @@ struct pv_context {
         for (DeviceArray *a : {&x, &y, &gamma, &gs, &p0x, &p0y, &p1x, &p1y, &pu, &pv, &inv_scratch,
                                &inv_out, &cand, &ex, &ey, &eg, &egs, &eu, &ev, &epu, &epv,
                                &removed_index, &fmt_stage, &fmt_len, &fmt_block, &fmt_out,
-                               &sym_items, &sym_counter, &rk4_barrier})
+                               &sym_items, &sym_counter, &rk4_barrier, &near_count, &near_slot})
             a->release();
         for (int s = 0; s < 7; ++s) {
             kx[s].release();
@@ -421,16 +426,62 @@ std::vector<double> scaled(const GeometryConsts &g, const double *gamma, size_t 
     return out;
 }
 
+// The FP32-compensated form's near field: periodic pairs and disk wall images closer than the
+// radius are evaluated in FP64 (pv_near.cu). The plane has none.
+bool near_field_used(const pv_context *c) {
+    return c->params.precision == PV_PRECISION_FP32C &&
+           (c->gc.geometry == GEO_PERIODIC || c->gc.geometry == GEO_DISK);
+}
+
+double near_radius_for(const pv_context *c, size_t n) {
+    return c->near_radius < 0.0 ? default_near_radius(c->gc, n) : c->near_radius;
+}
+
+// Lists for n targets; the counts start at zero (the FP64 pass leaves them zero).
+pv_status ensure_near_lists(pv_context *c, size_t n) {
+    const double *before = c->near_count.p;
+    PV_CUDA(c, c->near_count.ensure((n + 1) / 2));
+    if (c->near_count.p != before)
+        PV_CUDA(c, cudaMemsetAsync(c->near_count.p, 0, c->near_count.cap * sizeof(double),
+                                   c->stream));
+    PV_CUDA(c, c->near_slot.ensure(n * static_cast<size_t>(f32::kNearSlots) / 2));
+    return PV_OK;
+}
+
+f32::NearLists near_lists(const pv_context *c) {
+    return {reinterpret_cast<unsigned *>(c->near_count.p),
+            reinterpret_cast<unsigned *>(c->near_slot.p)};
+}
+
 // Velocity of the state positions (px, py) into k_s via partials + stage kernel.
 pv_status launch_eval(pv_context *c, const double *px, const double *py) {
+    const bool near = near_field_used(c);
+    const f32::NearLists lists = near ? near_lists(c) : f32::NearLists{nullptr, nullptr};
+    NearPass np{};
+    np.lists = lists;
+    np.x = px;
+    np.y = py;
+    np.gs = c->gs.p;
+    np.n = c->n;
+    np.t_begin = 0;
+    np.t_end = c->n;
+    np.stride = padded(c->n);
+    np.g = c->gc;
     if (c->sym.enabled()) {
         PV_CUDA(c, counted(c, PV_KERNEL_VELOCITY, 1, [&] {
                     return launch_symmetric(
                         px, py, c->gs.p, c->n, c->sym,
                         reinterpret_cast<const unsigned *>(c->sym_items.p),
-                        reinterpret_cast<unsigned *>(c->sym_counter.p), c->pu.p, c->pv.p,
-                        padded(c->n), c->gc, c->stream);
+                        reinterpret_cast<unsigned *>(c->sym_counter.p),
+                        reinterpret_cast<double2 *>(c->pu.p), padded(c->n), c->gc, lists,
+                        c->stream);
                 }));
+        if (near) {
+            np.pr = reinterpret_cast<double2 *>(c->pu.p);
+            np.rows = c->sym.blocks;
+            PV_CUDA(c, counted(c, PV_KERNEL_VELOCITY, 1,
+                               [&] { return launch_near_field(np, c->stream); }));
+        }
         ++c->evaluations;
         return PV_OK;
     }
@@ -451,11 +502,18 @@ pv_status launch_eval(pv_context *c, const double *px, const double *py) {
     a.status = &c->ctl->status;
     a.g = c->gc;
     a.wait_limit = c->wait_limit;
+    a.near = lists;
     PV_CUDA(c, counted(c, PV_KERNEL_VELOCITY, 1, [&] {
                 return c->params.precision == PV_PRECISION_FP32C
                            ? launch_velocity_fp32c(a, c->plan, c->stream)
                            : launch_velocity(a, c->plan, c->stream);
             }));
+    if (near) {
+        np.pu = c->pu.p;
+        np.pv = c->pv.p;
+        np.rows = c->plan.num_chunks;
+        PV_CUDA(c, counted(c, PV_KERNEL_VELOCITY, 1, [&] { return launch_near_field(np, c->stream); }));
+    }
     ++c->evaluations;
     return PV_OK;
 }
@@ -466,8 +524,12 @@ StageArgs stage_base(pv_context *c) {
     s.reduce = 1;
     s.num_chunks = c->sym.enabled() ? c->sym.blocks : c->plan.num_chunks;
     s.stride = padded(c->n);
-    s.pu = c->pu.p;
-    s.pv = c->pv.p;
+    if (c->sym.enabled()) {  // interleaved (u, v) rows in pu's room
+        s.pr = reinterpret_cast<const double2 *>(c->pu.p);
+    } else {
+        s.pu = c->pu.p;
+        s.pv = c->pv.p;
+    }
     for (int j = 0; j < 7; ++j) {
         s.kx[j] = c->kx[j].p;
         s.ky[j] = c->ky[j].p;
@@ -508,7 +570,11 @@ std::vector<const void *> attempt_key(const pv_context *c) {
                                    reinterpret_cast<const void *>(static_cast<uintptr_t>(
                                        c->dipole_configured && c->dipole.removal ? 1 : 0)),
                                    reinterpret_cast<const void *>(
-                                       static_cast<uintptr_t>(c->wait_limit))};
+                                       static_cast<uintptr_t>(c->wait_limit)),
+                                   c->near_count.p, c->near_slot.p};
+    uint64_t near_bits;
+    std::memcpy(&near_bits, &c->gc.near2, sizeof near_bits);
+    k.push_back(reinterpret_cast<const void *>(static_cast<uintptr_t>(near_bits)));
     uint64_t bits;
     std::memcpy(&bits, &c->dipole.distance, sizeof bits);
     k.push_back(reinterpret_cast<const void *>(static_cast<uintptr_t>(bits)));
@@ -529,11 +595,19 @@ pv_status ensure_state_capacity(pv_context *c, size_t n) {
     }
     c->plan = plan_evaluation(c->gc.geometry, n, n, c->sm_count, 0, c->params.precision);
     c->sym = plan_symmetric(n, c->sm_count, c->params.precision, c->gc.geometry);
+    if (near_field_used(c)) {
+        const double r = near_radius_for(c, n);
+        c->gc.near2 = r * r;
+        pv_status st = ensure_near_lists(c, n);
+        if (st != PV_OK)
+            return st;
+    }
     const size_t rows = c->sym.enabled() ? static_cast<size_t>(c->sym.blocks)
                                          : static_cast<size_t>(c->plan.num_chunks);
     const size_t partial = rows * np;
-    PV_CUDA(c, c->pu.ensure(partial));
-    PV_CUDA(c, c->pv.ensure(partial));
+    // the symmetric kernels' rows hold (u, v) pairs in pu's room; the chunk partials use both
+    PV_CUDA(c, c->pu.ensure(c->sym.enabled() ? 2 * partial : partial));
+    PV_CUDA(c, c->pv.ensure(c->sym.enabled() ? 1 : partial));
     if (c->sym.enabled() && c->sym_items_blocks != c->sym.blocks) {
         std::vector<unsigned> items(c->sym.items);
         symmetric_items(c->sym, items.data());
@@ -603,11 +677,35 @@ pv_status evaluate_host(pv_context *c, const double *x, const double *y, const d
     a.status = &c->ctl->status;
     a.g = c->gc;
     a.wait_limit = c->wait_limit;
+    const bool near = near_field_used(c);
+    if (near) {
+        const double r = near_radius_for(c, n);
+        a.g.near2 = r * r;
+        if ((st = ensure_near_lists(c, n)) != PV_OK)
+            return st;
+        a.near = near_lists(c);
+    }
     PV_CUDA(c, counted(c, PV_KERNEL_VELOCITY, 1, [&] {
                 return c->params.precision == PV_PRECISION_FP32C
                            ? launch_velocity_fp32c(a, plan, c->stream)
                            : launch_velocity(a, plan, c->stream);
             }));
+    if (near) {
+        NearPass np{};
+        np.lists = a.near;
+        np.x = c->ex.p;
+        np.y = c->ey.p;
+        np.gs = c->egs.p;
+        np.n = n;
+        np.t_begin = begin;
+        np.t_end = end;
+        np.pu = c->epu.p;
+        np.pv = c->epv.p;
+        np.stride = stride;
+        np.rows = plan.num_chunks;
+        np.g = a.g;
+        PV_CUDA(c, counted(c, PV_KERNEL_VELOCITY, 1, [&] { return launch_near_field(np, c->stream); }));
+    }
     StageArgs s{};
     s.n = nt;
     s.mode = STAGE_REDUCE_ONLY;
@@ -1205,7 +1303,7 @@ pv_status pv_dopri5_step(pv_context *ctx, double dt, double absolute_tolerance,
             for (const auto &t : ctx->graph_timers)
                 ctx->pending.push_back(t);
             ctx->evaluations += 6;
-            ctx->launches[PV_KERNEL_VELOCITY] += 6;
+            ctx->launches[PV_KERNEL_VELOCITY] += near_field_used(ctx) ? 12 : 6;
             ctx->launches[PV_KERNEL_STAGE] += 7;
             ctx->launches[PV_KERNEL_ACCEPT] += 1;
             if (prescan)
@@ -1740,6 +1838,31 @@ pv_status pv_context_stream(const pv_context *ctx, void **stream) {
     if (!ctx || !stream)
         return PV_ERROR_INVALID_ARGUMENT;
     *stream = static_cast<void *>(ctx->stream);
+    return PV_OK;
+}
+
+pv_status pv_set_near_field(pv_context *ctx, double radius) {
+    if (!ctx)
+        return PV_ERROR_INVALID_ARGUMENT;
+    if (std::isnan(radius) || std::isinf(radius))
+        return fail(ctx, PV_ERROR_INVALID_ARGUMENT, "near-field radius must be finite");
+    ctx->near_radius = radius < 0.0 ? -1.0 : radius;
+    if (ctx->state_valid && near_field_used(ctx)) {
+        DeviceGuard guard(ctx->device);
+        const double r = near_radius_for(ctx, ctx->n);
+        ctx->gc.near2 = r * r;
+        const pv_status st = ensure_near_lists(ctx, ctx->n);
+        if (st != PV_OK)
+            return st;
+        PV_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    }
+    return PV_OK;
+}
+
+pv_status pv_get_near_field(const pv_context *ctx, double *radius) {
+    if (!ctx || !radius)
+        return PV_ERROR_INVALID_ARGUMENT;
+    *radius = near_field_used(ctx) ? std::sqrt(ctx->gc.near2) : 0.0;
     return PV_OK;
 }
 

@@ -43,6 +43,8 @@ struct GeometryConsts {
                             // |x^ -+ shift6| <= 40 with its rounding, as thresholds on x^)
     // disk
     double radius, radius2, inv_radius, inv_radius2;
+    // FP32-compensated form: near-field radius squared (0: none), pv_pair32.cuh
+    double near2;
 };
 
 // Scaled circulation stored per source, chosen so that each pair needs one multiply by it:
@@ -91,6 +93,12 @@ struct DiskPair {
             c = 0.0;
         u = fma(-c, dy, u);
         v = fma(c, dx, v);
+        image(g, tx, ty, sx, sy, sg, u, v);
+    }
+    // The image term alone (every j, j == i included).
+    __device__ __forceinline__ static void image(const GeometryConsts &g, double tx, double ty,
+                                                 double sx, double sy, double sg, double &u,
+                                                 double &v) {
         const double px = tx * g.inv_radius2, py = ty * g.inv_radius2;
         const double a = fma(-px, sx, fma(-py, sy, 1.0));
         const double b = fma(py, sx, -px * sy);

@@ -8,6 +8,7 @@
 #include <string>
 
 #include "pv_geometry.cuh"
+#include "pv_pair32.cuh"
 
 namespace pvb {
 
@@ -47,6 +48,7 @@ struct EvalArgs {
     int *status;
     GeometryConsts g;
     uint32_t wait_limit = kWaitLimit;  // polls of a bounded tile wait (pv_set_wait_limits)
+    f32::NearLists near = {nullptr, nullptr};  // FP32C near-field lists (indexed by target)
 };
 
 struct EvalPlan {
@@ -69,7 +71,7 @@ cudaError_t launch_velocity_fp32c(const EvalArgs &a, const EvalPlan &p, cudaStre
 
 // The periodic box and the infinite plane (FP64, FP32C) evaluated once per unordered pair
 // (pv_symmetric.cu) for a whole population (targets = sources). Partial rows: `blocks` rows of
-// the same layout as the chunk partials.
+// `stride` (u, v) pairs, row r of vortex i at rows[r * stride + i].
 struct SymmetricPlan {
     int a = 0;           // 32-vortex sub-blocks per block; 0: not used
     int blocks = 0;      // partial rows
@@ -89,10 +91,32 @@ constexpr size_t kSymmetricPartialBytesMax = static_cast<size_t>(4) << 30;  // b
 SymmetricPlan plan_symmetric(size_t n, int sm_count, int precision, int geometry);
 void symmetric_items(const SymmetricPlan &p, unsigned *out);  // p.items packed (I << 16) | J
 // counter: two words, zero before the first launch; each launch leaves them zero again.
+// near: the near-field lists of the FP32C periodic kernel (pv_pair32.cuh; count == nullptr:
+// none); the other kernels ignore it.
 cudaError_t launch_symmetric(const double *x, const double *y, const double *gs, size_t n,
                              const SymmetricPlan &p, const unsigned *items, unsigned *counter,
-                             double *pu, double *pv, size_t stride, const GeometryConsts &g,
-                             cudaStream_t stream);
+                             double2 *rows, size_t stride, const GeometryConsts &g,
+                             const f32::NearLists &near, cudaStream_t stream);
+
+// ---- FP32C near field (pv_near.cu) -----------------------------------------------------------
+// The FP64 pass over the pairs an FP32 evaluation listed (f32::NearLists): their exact terms are
+// added into the last partial row, and every list count is reset. Targets [t_begin, t_end) of n
+// sources; the partial entry of target i in row r is r * stride + (i - t_begin), in pr
+// (interleaved rows of the symmetric kernels) or pu/pv (chunk partials).
+struct NearPass {
+    f32::NearLists lists;
+    const double *x, *y, *gs;  // the evaluated positions and the scaled circulations
+    size_t n;
+    size_t t_begin, t_end;
+    double *pu, *pv;
+    double2 *pr;
+    size_t stride;
+    int rows;
+    GeometryConsts g;
+};
+cudaError_t launch_near_field(const NearPass &a, cudaStream_t stream);
+// The default near-field radius of the FP32C form for n vortices (0: the geometry has none).
+double default_near_radius(const GeometryConsts &g, size_t n);
 
 // ---- stage kernels (reduction, stage positions, RK4 combine, DOPRI5 error and control) ------
 enum StageMode : int {
@@ -108,7 +132,8 @@ struct StageArgs {
     int reduce;                     // 1: reduce partials into k_s; 0: k_s already final
     int num_chunks;
     size_t stride;
-    const double *pu, *pv;
+    const double *pu, *pv;          // chunk partials, u and v apart
+    const double2 *pr;              // or (non-null) interleaved (u, v) rows of the symmetric kernels
     int s;                          // index of the stage being produced (k_s)
     double *kx[7], *ky[7];          // stage velocity fields
     const double *ex, *ey;          // positions the stage was evaluated at (slow path)

@@ -1,10 +1,19 @@
-// pv_pair32.cuh — FP32-compensated pair terms, shared by the single-simulation kernel
-// (pv_velocity32.cu) and the batched ensembles (pv_batch.cu).
+// pv_pair32.cuh — FP32-compensated pair terms, shared by the single-simulation kernels
+// (pv_velocity32.cu, pv_symmetric.cu) and the batched ensembles (pv_batch.cu).
 //
 // Coordinates enter as double-float pairs (hi = fp32(x), lo = fp32(x - hi)), so a displacement
 // (t_hi - s_hi) + (t_lo - s_lo) keeps ~2^-24 relative accuracy at every separation. The periodic
-// series and the direct Biot-Savart term run on the FP32 pipe; the disk image term falls back to
-// FP64 where 1 - t.s/R^2 < 1/8. Callers promote FP32 partial sums into FP64 every kFlush sources.
+// series, the direct Biot-Savart term and the disk's wall image run on the FP32 pipe. The wall
+// image of a source s is the circle theorem's vortex -Gamma at s* = R^2 s / |s|^2 (the
+// reference's image term, src/compute.cpp:314-333, is exactly its velocity), so it is evaluated
+// as a direct term from s*, whose displacement is as accurate as any other: no cancellation
+// near the wall.
+//
+// Near field: an FP32 term carries ~1e-7 of its own size, so the few pairs whose terms are large
+// set the error of a sum. Pairs closer than the near-field radius -- the periodic pair at its
+// minimum-image distance, the disk image at its distance to the target -- are left out of the FP32
+// sum and listed (near_append) for the FP64 pass of pv_near.cu, which adds their exact FP64 terms
+// in index order. Callers promote FP32 partial sums into FP64 every kFlush sources.
 #pragma once
 
 #include "pv_common.cuh"
@@ -14,6 +23,23 @@ namespace pvb {
 namespace f32 {
 
 constexpr int kFlush = 64; // sources summed in FP32 before promotion to FP64
+
+// Near-field lists: per target, up to kNearSlots listed sources (a source index, with kNearImage
+// set for the disk's wall image of that source). count[t] may exceed kNearSlots: the FP64 pass
+// then evaluates the whole target in FP64. count == nullptr: nothing is listed.
+constexpr int kNearSlots = 32;
+constexpr unsigned kNearImage = 0x80000000u;
+struct NearLists {
+    unsigned *count;  // [n] zero before an evaluation; the FP64 pass leaves it zero again
+    unsigned *slot;   // [n][kNearSlots]
+};
+
+__device__ __forceinline__ void near_append(const NearLists &lists, size_t target,
+                                            unsigned entry) {
+    const unsigned k = atomicAdd(lists.count + target, 1u);
+    if (k < kNearSlots)
+        lists.slot[target * kNearSlots + k] = entry;
+}
 
 __device__ __forceinline__ float rcp_approx_f32(float x) {
     float r;
@@ -28,6 +54,7 @@ struct F32Geometry { // the FP32 constants of one evaluation
     float k1, k2, k6, shift6;
     int m_exact, has6;
     float inv_radius2;
+    float near2;       // near-field radius squared (0: no near field)
 };
 
 __device__ __forceinline__ F32Geometry make_f32(const GeometryConsts &g) {
@@ -49,7 +76,26 @@ __device__ __forceinline__ F32Geometry make_f32(const GeometryConsts &g) {
     f.m_exact = g.m_exact;
     f.has6 = g.has6;
     f.inv_radius2 = static_cast<float>(g.inv_radius2);
+    f.near2 = static_cast<float>(g.near2);
     return f;
+}
+
+// (x_hi, y_hi, x_lo, y_lo) of a double position.
+__device__ __forceinline__ float4 split_position(double x, double y) {
+    const float xh = static_cast<float>(x), yh = static_cast<float>(y);
+    return make_float4(xh, yh, static_cast<float>(x - static_cast<double>(xh)),
+                       static_cast<float>(y - static_cast<double>(yh)));
+}
+
+// The wall image of a disk source at (x, y): the vortex -Gamma at R^2 (x, y) / (x^2 + y^2), as
+// double-float coordinates. A source at the centre has its image at infinity and contributes 0
+// in the reference; a far finite point (FP32 squares stay finite) gives a term below 1e-15.
+__device__ __forceinline__ float4 image_position(const GeometryConsts &g, double x, double y) {
+    const double r2 = fma(x, x, y * y);
+    if (!(r2 > 1e-30 * g.radius2))
+        return make_float4(1e15f, 0.0f, 0.0f, 0.0f);
+    const double k = __ddiv_rn(g.radius2, r2);
+    return split_position(k * x, k * y);
 }
 
 // sinh, cosh, sin, cos of t (|t| <= pi/2), the FP32 truncation of the shared series in
@@ -74,10 +120,11 @@ __device__ __forceinline__ void shcs_f32(float t, float &sh, float &ch, float &s
     c = fmaf(-t2, o0, e0);
 }
 
-// Half of x^ = (2 pi/L) remainder(dx, L) in FP32 from a double-float displacement.
-__device__ __forceinline__ float half_angle_f32(const F32Geometry &f, float dx) {
+// Half of x^ = (2 pi/L) remainder(dx, L) in FP32 from a double-float displacement; r receives the
+// minimum-image displacement remainder(dx, L).
+__device__ __forceinline__ float half_angle_f32(const F32Geometry &f, float dx, float &r) {
     const float n = rintf(dx * f.inv_l);
-    const float r = fmaf(-n, f.l_lo, fmaf(-n, f.l_hi, dx));
+    r = fmaf(-n, f.l_lo, fmaf(-n, f.l_hi, dx));
     return f.half_wave * r;
 }
 
@@ -118,11 +165,15 @@ struct Target32 {
 // u -= g_s ku, v += g_s kv. t and s are (x_hi, y_hi, x_lo, y_lo). Exchanging target and source
 // negates the displacement exactly, and every quantity below is an exactly odd or even function
 // of it, so ku and kv are exactly odd: the symmetric kernels use one evaluation for both.
-__device__ __forceinline__ void periodic_values32(const F32Geometry &f, const float4 t,
+// Returns true for a near pair (minimum-image distance below the near-field radius, the same
+// verdict from either side): its terms are then 0 here and come from the FP64 pass.
+__device__ __forceinline__ bool periodic_values32(const F32Geometry &f, const float4 t,
                                                   const float4 s, float &ku, float &kv) {
     const float dx = (t.x - s.x) + (t.z - s.z);
     const float dy = (t.y - s.y) + (t.w - s.w);
-    const float hx = half_angle_f32(f, dx), hy = half_angle_f32(f, dy);
+    float rx, ry;
+    const float hx = half_angle_f32(f, dx, rx), hy = half_angle_f32(f, dy, ry);
+    const bool near = fmaf(rx, rx, ry * ry) < f.near2;
     float shx, chx, snx, csx, shy, chy, sny, csy;
     shcs_f32(hx, shx, chx, snx, csx);
     shcs_f32(hy, shy, chy, sny, csy);
@@ -130,17 +181,19 @@ __device__ __forceinline__ void periodic_values32(const F32Geometry &f, const fl
     const float cos_x = fmaf(-2.0f * snx, snx, 1.0f), cos_y = fmaf(-2.0f * sny, sny, 1.0f);
     const float sin_x = 2.0f * snx * csx, sin_y = 2.0f * sny * csy;
     const float sinh_x = 2.0f * shx * chx, sinh_y = 2.0f * shy * chy;
-    const float d0u = 2.0f * fmaf(shx, shx, sny * sny);
-    const float d0v = 2.0f * fmaf(shy, shy, snx * snx);
+    const float d0u = near ? 1.0f : 2.0f * fmaf(shx, shx, sny * sny);
+    const float d0v = near ? 1.0f : 2.0f * fmaf(shy, shy, snx * snx);
     float nu, du, ru, nv, dv, rv;
     image_sum_f32(f, hx, cosh_x, sinh_x, cos_y, nu, du, ru);
     image_sum_f32(f, hy, cosh_y, sinh_y, cos_x, nv, dv, rv);
-    ku = sin_y * fmaf(d0u, fmaf(du, ru, nu), du) * rcp_approx_f32(d0u * du);
-    kv = sin_x * fmaf(d0v, fmaf(dv, rv, nv), dv) * rcp_approx_f32(d0v * dv);
+    ku = near ? 0.0f : sin_y * fmaf(d0u, fmaf(du, ru, nu), du) * rcp_approx_f32(d0u * du);
+    kv = near ? 0.0f : sin_x * fmaf(d0v, fmaf(dv, rv, nv), dv) * rcp_approx_f32(d0v * dv);
+    return near;
 }
 
 // The plane's kernel values in FP32: K = (dy, dx) / (r^2 + eps^2) from the double-float
-// displacement. Exactly odd under exchanging target and source, as periodic_values32.
+// displacement. Exactly odd under exchanging target and source, as periodic_values32. The plane
+// has no near field.
 __device__ __forceinline__ void plane_values32(const F32Geometry &f, const float4 t,
                                                const float4 s, float &ku, float &kv) {
     const float dx = (t.x - s.x) + (t.z - s.z);
@@ -150,29 +203,38 @@ __device__ __forceinline__ void plane_values32(const F32Geometry &f, const float
     kv = dx * inv;
 }
 
-// The pair kernels of the FP32 symmetric tiles (circulations enter unscaled).
+// The pair kernels of the FP32 symmetric tiles (circulations enter unscaled). values() returns
+// true for a near pair (terms 0, listed for the FP64 pass); kNear: the kernel has a near field.
 struct Periodic32 {
-    __device__ __forceinline__ static void values(const F32Geometry &f, const float4 t,
+    static constexpr bool kNear = true;
+    __device__ __forceinline__ static bool values(const F32Geometry &f, const float4 t,
                                                   const float4 s, float &ku, float &kv) {
-        periodic_values32(f, t, s, ku, kv);
+        return periodic_values32(f, t, s, ku, kv);
     }
 };
 struct Plane32 {
-    __device__ __forceinline__ static void values(const F32Geometry &f, const float4 t,
+    static constexpr bool kNear = false;
+    __device__ __forceinline__ static bool values(const F32Geometry &f, const float4 t,
                                                   const float4 s, float &ku, float &kv) {
         plane_values32(f, t, s, ku, kv);
+        return false;
     }
 };
 
+// One ordered pair in FP32: t the target, s the source (x_hi, y_hi, x_lo, y_lo), si the source's
+// wall image (disk only), sgf its scaled circulation. CHECK/self: the self pair (diagonal tiles)
+// has no direct term; the disk keeps its self image, as the reference does. Returns true when the
+// pair (periodic box) or the source's wall image (disk) is in the near field: that term is then
+// left out here and the caller lists the pair for the FP64 pass.
 template <int GEO, bool CHECK>
-__device__ __forceinline__ void pair32(const F32Geometry &f, const GeometryConsts &g,
-                                       const Target32 &t, const float4 s, float sgf, double sxd,
-                                       double syd, double sgd, bool self, float &u, float &v,
-                                       double &ud, double &vd) {
+__device__ __forceinline__ bool pair32(const F32Geometry &f, const Target32 &t, const float4 s,
+                                       const float4 si, float sgf, bool self, float &u, float &v) {
     const float dx = (t.xh - s.x) + (t.xl - s.z);
     const float dy = (t.yh - s.y) + (t.yl - s.w);
     if (GEO == GEO_PERIODIC) {
-        const float hx = half_angle_f32(f, dx), hy = half_angle_f32(f, dy);
+        float rx, ry;
+        const float hx = half_angle_f32(f, dx, rx), hy = half_angle_f32(f, dy, ry);
+        const bool near = fmaf(rx, rx, ry * ry) < f.near2 && !(CHECK && self);
         float shx, chx, snx, csx, shy, chy, sny, csy;
         shcs_f32(hx, shx, chx, snx, csx);
         shcs_f32(hy, shy, chy, sny, csy);
@@ -180,25 +242,19 @@ __device__ __forceinline__ void pair32(const F32Geometry &f, const GeometryConst
         const float cos_x = fmaf(-2.0f * snx, snx, 1.0f), cos_y = fmaf(-2.0f * sny, sny, 1.0f);
         const float sin_x = 2.0f * snx * csx, sin_y = 2.0f * sny * csy;
         const float sinh_x = 2.0f * shx * chx, sinh_y = 2.0f * shy * chy;
-        float d0u = 2.0f * fmaf(shx, shx, sny * sny);
-        float d0v = 2.0f * fmaf(shy, shy, snx * snx);
-        if (CHECK && self) {
-            d0u = 1.0f;
-            d0v = 1.0f;
-        }
+        const bool skip = near || (CHECK && self);
+        const float d0u = skip ? 1.0f : 2.0f * fmaf(shx, shx, sny * sny);
+        const float d0v = skip ? 1.0f : 2.0f * fmaf(shy, shy, snx * snx);
         float nu, du, ru, nv, dv, rv;
         image_sum_f32(f, hx, cosh_x, sinh_x, cos_y, nu, du, ru);
         image_sum_f32(f, hy, cosh_y, sinh_y, cos_x, nv, dv, rv);
         const float numer_u = fmaf(d0u, fmaf(du, ru, nu), du);
         const float numer_v = fmaf(d0v, fmaf(dv, rv, nv), dv);
-        float cu = sgf * sin_y * numer_u, cv = sgf * sin_x * numer_v;
-        if (CHECK && self) {
-            cu = 0.0f;
-            cv = 0.0f;
-        }
+        const float cu = skip ? 0.0f : sgf * sin_y * numer_u;
+        const float cv = skip ? 0.0f : sgf * sin_x * numer_v;
         u = fmaf(-cu, rcp_approx_f32(d0u * du), u);
         v = fmaf(cv, rcp_approx_f32(d0v * dv), v);
-        return;
+        return near;
     }
     // direct Biot–Savart term (plane, and the disk's j != i term)
     const float r2 = fmaf(dx, dx, fmaf(dy, dy, GEO == GEO_INFINITE ? f.eps2 : 0.0f));
@@ -207,24 +263,17 @@ __device__ __forceinline__ void pair32(const F32Geometry &f, const GeometryConst
         c = 0.0f;
     u = fmaf(-c, dy, u);
     v = fmaf(c, dx, v);
-    if (GEO == GEO_DISK) {
-        const float px = (t.xh + t.xl) * f.inv_radius2, py = (t.yh + t.yl) * f.inv_radius2;
-        const float sx = s.x + s.z, sy = s.y + s.w;
-        const float a = fmaf(-px, sx, fmaf(-py, sy, 1.0f));
-        if (a >= 0.125f) {
-            const float b = fmaf(py, sx, -px * sy);
-            const float ci = (sgf * f.inv_radius2) * rcp_approx_f32(fmaf(a, a, b * b));
-            u = fmaf(ci, fmaf(b, sx, -a * sy), u);
-            v = fmaf(ci, fmaf(a, sx, b * sy), v);
-        } else { // near the wall: the FP64 image term of DiskPair
-            const double pxd = t.x * g.inv_radius2, pyd = t.y * g.inv_radius2;
-            const double ad = fma(-pxd, sxd, fma(-pyd, syd, 1.0));
-            const double bd = fma(pyd, sxd, -pxd * syd);
-            const double cid = (sgd * g.inv_radius2) * rcp_refined(fma(ad, ad, bd * bd));
-            ud = fma(cid, fma(bd, sxd, -ad * syd), ud);
-            vd = fma(cid, fma(ad, sxd, bd * syd), vd);
-        }
+    if (GEO == GEO_DISK) {  // the wall image: the vortex -Gamma at si
+        const float ix = (t.xh - si.x) + (t.xl - si.z);
+        const float iy = (t.yh - si.y) + (t.yl - si.w);
+        const float ri2 = fmaf(ix, ix, iy * iy);
+        const bool near = ri2 < f.near2;
+        const float ci = near ? 0.0f : sgf * rcp_approx_f32(ri2);
+        u = fmaf(ci, iy, u);
+        v = fmaf(-ci, ix, v);
+        return near;
     }
+    return false;
 }
 
 }  // namespace f32

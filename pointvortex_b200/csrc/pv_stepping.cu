@@ -174,11 +174,35 @@ __global__ void __launch_bounds__(256) stage_kernel(const StageArgs a) {
              base += static_cast<size_t>(gridDim.x) * kWideTargets) {
             const size_t i = base + lane;
             double su = 0.0, sv = 0.0;
-            if (i < a.n)
+            if (i < a.n && a.pr) {
+                // interleaved rows: one 16-byte load per row, eight rows in flight per thread
+                // before they are added (in row order, so the sum does not depend on timing)
+                const double2 *col = a.pr + i;
+                const size_t step = static_cast<size_t>(kWideGroups) * a.stride;
+                int c = group;
+                for (; c + 7 * kWideGroups < a.num_chunks; c += 8 * kWideGroups) {
+                    double2 r[8];
+                    const double2 *p = col + static_cast<size_t>(c) * a.stride;
+#pragma unroll
+                    for (int q = 0; q < 8; ++q)
+                        r[q] = __ldcg(p + q * step);
+#pragma unroll
+                    for (int q = 0; q < 8; ++q) {
+                        su += r[q].x;
+                        sv += r[q].y;
+                    }
+                }
+                for (; c < a.num_chunks; c += kWideGroups) {
+                    const double2 r = __ldcg(col + static_cast<size_t>(c) * a.stride);
+                    su += r.x;
+                    sv += r.y;
+                }
+            } else if (i < a.n) {
                 for (int c = group; c < a.num_chunks; c += kWideGroups) {
                     su += a.pu[static_cast<size_t>(c) * a.stride + i];
                     sv += a.pv[static_cast<size_t>(c) * a.stride + i];
                 }
+            }
             s_u[group][lane] = su;
             s_v[group][lane] = sv;
             __syncthreads();
@@ -200,8 +224,14 @@ __global__ void __launch_bounds__(256) stage_kernel(const StageArgs a) {
                 ku = 0.0;
                 kv = 0.0;
                 for (int c = 0; c < a.num_chunks; ++c) {
-                    ku += a.pu[static_cast<size_t>(c) * a.stride + i];
-                    kv += a.pv[static_cast<size_t>(c) * a.stride + i];
+                    if (a.pr) {
+                        const double2 r = a.pr[static_cast<size_t>(c) * a.stride + i];
+                        ku += r.x;
+                        kv += r.y;
+                    } else {
+                        ku += a.pu[static_cast<size_t>(c) * a.stride + i];
+                        kv += a.pv[static_cast<size_t>(c) * a.stride + i];
+                    }
                 }
             } else {
                 ku = a.kx[a.s][i];

@@ -19,9 +19,10 @@
 //     self pair skipped, as in the reference);
 //   * the plane's pair term is cheap next to the five shuffles of a rotation step, so off the
 //     diagonal each lane holds 4 or 8 targets against the rotating sources;
-//   * partial sums go to rows of a [blocks][N] array: vortices of block I receive row J from item
-//     (I, J), vortices of block J receive row I, and each (row, vortex) is written exactly once,
-//     so the stage kernel's fixed-order sum over rows keeps results deterministic.
+//   * partial sums go to rows of a [blocks][N] array of (u, v) pairs (one 16-byte store per entry):
+//     vortices of block I receive row J from item (I, J), vortices of block J receive row I, and
+//     each (row, vortex) is written exactly once, so the stage kernel's fixed-order sum over rows
+//     keeps results deterministic.
 #include "pvb200.h"
 #include "pv_internal.h"
 #include "pv_symmetric.cuh"
@@ -57,8 +58,7 @@ __global__ void __launch_bounds__(kThreads)
     symmetric_kernel(const double *__restrict__ x, const double *__restrict__ y,
                      const double *__restrict__ gs, size_t n, int a,
                      const unsigned *__restrict__ items, unsigned n_items, unsigned *counter,
-                     double *__restrict__ pu, double *__restrict__ pv, size_t stride,
-                     GeometryConsts g) {
+                     double2 *__restrict__ pr, size_t stride, GeometryConsts g) {
     extern __shared__ double2 reaction_smem[];
     pdl_enter();
     const int lane = threadIdx.x & 31;
@@ -111,8 +111,7 @@ __global__ void __launch_bounds__(kThreads)
                 for (int t = 0; t < T; ++t) {
                     const size_t ti = I * block_len + static_cast<size_t>(ib + t) * 32 + lane;
                     if (t_ok[t]) {
-                        pu[J * stride + ti] = u[t];
-                        pv[J * stride + ti] = v[t];
+                        pr[J * stride + ti] = make_double2(u[t], v[t]);
                     }
                 }
             }
@@ -142,8 +141,7 @@ __global__ void __launch_bounds__(kThreads)
                     v += r.y;
                 }
                 if (t_ok) {
-                    pu[J * stride + ti] = u;
-                    pv[J * stride + ti] = v;
+                    pr[J * stride + ti] = make_double2(u, v);
                 }
             }
         }
@@ -151,9 +149,7 @@ __global__ void __launch_bounds__(kThreads)
             for (int jb = 0; jb < a; ++jb) {
                 const size_t sj = J * block_len + static_cast<size_t>(jb) * 32 + lane;
                 if (sj < n) {
-                    const double2 r = reaction[jb * 32 + lane];
-                    pu[I * stride + sj] = r.x;
-                    pv[I * stride + sj] = r.y;
+                    pr[I * stride + sj] = reaction[jb * 32 + lane];
                 }
             }
         }
@@ -172,8 +168,8 @@ __global__ void __launch_bounds__(kThreads)
     symmetric32_kernel(const double *__restrict__ x, const double *__restrict__ y,
                        const double *__restrict__ gs, size_t n, int a,
                        const unsigned *__restrict__ items, unsigned n_items, unsigned *counter,
-                       double *__restrict__ pu, double *__restrict__ pv, size_t stride,
-                       GeometryConsts g) {
+                       double2 *__restrict__ pr, size_t stride, GeometryConsts g,
+                       f32::NearLists near) {
     extern __shared__ double2 reaction_smem[];
     __shared__ float4 src_f[kThreads];
     __shared__ float src_g[kThreads];
@@ -234,8 +230,9 @@ __global__ void __launch_bounds__(kThreads)
 #pragma unroll
                         for (int q = 0; q < T; ++q) {
                             float ru = 0.0f, rv = 0.0f;
+                            const size_t tq = I * block_len + static_cast<size_t>(ib + q) * 32 + lane;
                             sym::react_tile32<V>(f, t[q], tg[q], t_ok[q], sf, sgf, s_count, u[q],
-                                                 v[q], ru, rv);
+                                                 v[q], ru, rv, sym::NearTile{near, tq, j0});
                             rud += static_cast<double>(ru);
                             rvd += static_cast<double>(rv);
                         }
@@ -254,8 +251,7 @@ __global__ void __launch_bounds__(kThreads)
                 for (int q = 0; q < T; ++q) {
                     const size_t ti = I * block_len + static_cast<size_t>(ib + q) * 32 + lane;
                     if (t_ok[q]) {
-                        pu[J * stride + ti] = ud[q];
-                        pv[J * stride + ti] = vd[q];
+                        pr[J * stride + ti] = make_double2(ud[q], vd[q]);
                     }
                 }
             }
@@ -277,11 +273,12 @@ __global__ void __launch_bounds__(kThreads)
                     sgf[lane] = sj < n ? static_cast<float>(gs[sj]) : 0.0f;
                     __syncwarp();
                     float u = 0.0f, v = 0.0f;
+                    const sym::NearTile nt{near, ti, j0};
                     if (diagonal && jb == ib) {
-                        sym::one_sided_tile32<V>(f, t, t_ok, sf, sgf, s_count, true, u, v);
+                        sym::one_sided_tile32<V>(f, t, t_ok, sf, sgf, s_count, true, u, v, nt);
                     } else {
                         float ru = 0.0f, rv = 0.0f;
-                        sym::react_tile32<V>(f, t, tg, t_ok, sf, sgf, s_count, u, v, ru, rv);
+                        sym::react_tile32<V>(f, t, tg, t_ok, sf, sgf, s_count, u, v, ru, rv, nt);
                         double2 r = reaction[jb * 32 + lane];
                         r.x += static_cast<double>(ru);
                         r.y += static_cast<double>(rv);
@@ -296,8 +293,7 @@ __global__ void __launch_bounds__(kThreads)
                     vd += r.y;
                 }
                 if (t_ok) {
-                    pu[J * stride + ti] = ud;
-                    pv[J * stride + ti] = vd;
+                    pr[J * stride + ti] = make_double2(ud, vd);
                 }
             }
         }
@@ -305,9 +301,7 @@ __global__ void __launch_bounds__(kThreads)
             for (int jb = 0; jb < a; ++jb) {
                 const size_t sj = J * block_len + static_cast<size_t>(jb) * 32 + lane;
                 if (sj < n) {
-                    const double2 r = reaction[jb * 32 + lane];
-                    pu[I * stride + sj] = r.x;
-                    pv[I * stride + sj] = r.y;
+                    pr[I * stride + sj] = reaction[jb * 32 + lane];
                 }
             }
         }
@@ -422,29 +416,31 @@ void symmetric_items(const SymmetricPlan &p, unsigned *out) {
 
 cudaError_t launch_symmetric(const double *x, const double *y, const double *gs, size_t n,
                              const SymmetricPlan &p, const unsigned *items, unsigned *counter,
-                             double *pu, double *pv, size_t stride, const GeometryConsts &g,
-                             cudaStream_t stream) {
+                             double2 *rows, size_t stride, const GeometryConsts &g,
+                             const f32::NearLists &near, cudaStream_t stream) {
     const size_t smem = static_cast<size_t>(kThreads / 32) * p.a * 32 * sizeof(double2);
     const dim3 grid(static_cast<unsigned>(p.grid)), block(kThreads);
     switch (kernel_of(p)) {
     case SYM_PERIODIC32:
         return launch_pdl(symmetric32_kernel<f32::Periodic32, 1>, grid, block, smem, stream, x, y,
-                          gs, n, p.a, items, p.items, counter, pu, pv, stride, g);
+                          gs, n, p.a, items, p.items, counter, rows, stride, g, near);
     case SYM_PLANE:
         return launch_pdl(symmetric_kernel<sym::PlaneSym, kPlaneTargets>, grid, block, smem,
-                          stream, x, y, gs, n, p.a, items, p.items, counter, pu, pv, stride, g);
+                          stream, x, y, gs, n, p.a, items, p.items, counter, rows, stride, g);
     case SYM_PLANE_WIDE:
         return launch_pdl(symmetric_kernel<sym::PlaneSym, kPlaneTargetsWide>, grid, block, smem,
-                          stream, x, y, gs, n, p.a, items, p.items, counter, pu, pv, stride, g);
+                          stream, x, y, gs, n, p.a, items, p.items, counter, rows, stride, g);
     case SYM_PLANE32:
         return launch_pdl(symmetric32_kernel<f32::Plane32, kPlaneTargets>, grid, block, smem,
-                          stream, x, y, gs, n, p.a, items, p.items, counter, pu, pv, stride, g);
+                          stream, x, y, gs, n, p.a, items, p.items, counter, rows, stride, g,
+                          near);
     case SYM_PLANE32_WIDE:
         return launch_pdl(symmetric32_kernel<f32::Plane32, kPlaneTargetsWide>, grid, block, smem,
-                          stream, x, y, gs, n, p.a, items, p.items, counter, pu, pv, stride, g);
+                          stream, x, y, gs, n, p.a, items, p.items, counter, rows, stride, g,
+                          near);
     default:
         return launch_pdl(symmetric_kernel<sym::PeriodicSym, 1>, grid, block, smem, stream, x, y,
-                          gs, n, p.a, items, p.items, counter, pu, pv, stride, g);
+                          gs, n, p.a, items, p.items, counter, rows, stride, g);
     }
 }
 

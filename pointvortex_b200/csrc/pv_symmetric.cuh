@@ -140,18 +140,37 @@ __device__ __forceinline__ void one_sided_tile(const GeometryConsts &g, double t
 // warp's shared buffer, read at index (lane + k) & 31; only their FP32 reactions rotate through
 // the lanes. V: the pair kernel (f32::Periodic32, f32::Plane32). The callers promote the FP32
 // sums of each tile into FP64.
+//
+// Near pairs (V::kNear kernels) contribute 0 here and are listed for the FP64 pass, in both
+// directions, under the lane's target `ti` and the tile's source j0 + j.
+struct NearTile {
+    f32::NearLists lists;  // lists.count == nullptr: no near field
+    size_t ti;             // this lane's target
+    size_t j0;             // the tile's first source
+};
+
+template <class V>
+__device__ __forceinline__ void list_near_pair(const NearTile &nt, int j, bool both) {
+    if (V::kNear && nt.lists.count) {
+        f32::near_append(nt.lists, nt.ti, static_cast<unsigned>(nt.j0 + j));
+        if (both)
+            f32::near_append(nt.lists, nt.j0 + j, static_cast<unsigned>(nt.ti));
+    }
+}
+
 template <class V, bool FULL>
 __device__ __forceinline__ void react_tile32_t(const f32::F32Geometry &f, const float4 t, float tg,
                                                bool t_ok, const float4 *sf, const float *sg,
                                                int s_count, float &u, float &v, float &ru,
-                                               float &rv) {
+                                               float &rv, const NearTile &nt) {
     const int lane = threadIdx.x & 31, next = (lane + 1) & 31;
 #pragma unroll 2
     for (int k = 0; k < 32; ++k) {
         const int j = (lane + k) & 31;
         if (FULL || (t_ok && j < s_count)) {
             float ku, kv;
-            V::values(f, t, sf[j], ku, kv);
+            if (V::values(f, t, sf[j], ku, kv))
+                list_near_pair<V>(nt, j, true);
             const float g = sg[j];
             u = fmaf(-g, ku, u);
             v = fmaf(g, kv, v);
@@ -167,15 +186,16 @@ template <class V = f32::Periodic32>
 __device__ __forceinline__ void react_tile32(const f32::F32Geometry &f, const float4 t, float tg,
                                              bool t_ok, const float4 *sf, const float *sg,
                                              int s_count, float &u, float &v, float &ru,
-                                             float &rv) {
+                                             float &rv, const NearTile &nt) {
     if (__all_sync(0xffffffffu, t_ok && s_count == 32))
-        react_tile32_t<V, true>(f, t, tg, t_ok, sf, sg, s_count, u, v, ru, rv);
+        react_tile32_t<V, true>(f, t, tg, t_ok, sf, sg, s_count, u, v, ru, rv, nt);
     else
-        react_tile32_t<V, false>(f, t, tg, t_ok, sf, sg, s_count, u, v, ru, rv);
+        react_tile32_t<V, false>(f, t, tg, t_ok, sf, sg, s_count, u, v, ru, rv, nt);
 }
 
 // T targets per lane against the 32 sources of the buffer, every target and source present: each
-// step serves T pairs per lane, and the reactions' two shuffles are shared by them. A reaction
+// step serves T pairs per lane, and the reactions' two shuffles are shared by them. Only for pair
+// kernels without a near field (the plane): a near verdict is not acted on here. A reaction
 // would sum 32T terms in FP32 over the tile; it is restarted every 8 steps instead (8T terms, as
 // many as the ordered FP32C kernel sums before promoting), and the four partials of a source,
 // left in the lanes 8, 16, 24 and 32 places on, are added in FP64 into rud, rvd.
@@ -223,13 +243,14 @@ template <class V = f32::Periodic32>
 __device__ __forceinline__ void one_sided_tile32(const f32::F32Geometry &f, const float4 t,
                                                  bool t_ok, const float4 *sf, const float *sg,
                                                  int s_count, bool same_block, float &u,
-                                                 float &v) {
+                                                 float &v, const NearTile &nt) {
     const int lane = threadIdx.x & 31;
     for (int k = same_block ? 1 : 0; k < 32; ++k) {
         const int j = (lane + k) & 31;
         if (t_ok && j < s_count) {
             float ku, kv;
-            V::values(f, t, sf[j], ku, kv);
+            if (V::values(f, t, sf[j], ku, kv))  // the other side lists its own pair
+                list_near_pair<V>(nt, j, false);
             u = fmaf(-sg[j], ku, u);
             v = fmaf(sg[j], kv, v);
         }
@@ -237,11 +258,7 @@ __device__ __forceinline__ void one_sided_tile32(const f32::F32Geometry &f, cons
 }
 
 // (x_hi, y_hi, x_lo, y_lo) of a double position.
-__device__ __forceinline__ float4 split32(double x, double y) {
-    const float xh = static_cast<float>(x), yh = static_cast<float>(y);
-    return make_float4(xh, yh, static_cast<float>(x - static_cast<double>(xh)),
-                       static_cast<float>(y - static_cast<double>(yh)));
-}
+__device__ __forceinline__ float4 split32(double x, double y) { return f32::split_position(x, y); }
 
 }  // namespace sym
 }  // namespace pvb

@@ -1,22 +1,26 @@
 // pv_velocity32.cu — the FP32-compensated precision form of the velocity evaluation.
 //
 // Same tiling, TMA staging, chunk partials and slow path as pv_velocity.cu; the pair terms are
-// evaluated on the FP32 pipe (128 lanes/clk/SM on B200, twice the FP64 pipe) with three
+// evaluated on the FP32 pipe (128 lanes/clk/SM on B200, twice the FP64 pipe) with these
 // compensations:
 //
 //   * coordinates as double-float pairs: every staged source and every target is split into
 //     hi = fp32(x), lo = fp32(x - hi), and a displacement is (t_hi - s_hi) + (t_lo - s_lo). The
 //     first difference is exact when the coordinates are close (Sterbenz) and carries the relative
 //     error of one rounding otherwise, so dx keeps ~2^-24 relative accuracy at every separation,
-//     which absolute FP32 coordinates cannot (their rounding is relative to |x|, not |dx|);
+//     which absolute FP32 coordinates cannot (their rounding is relative to |x|, not |dx|). This
+//     is what coordinates relative to a tile centre would buy, without sorting the vortices into
+//     compact tiles;
 //   * FP32 partial sums over 64 sources are promoted into FP64 accumulators, so the summation error
 //     does not grow with N;
-//   * the disk image term falls back to FP64 where 1 - t.s/R^2 < 1/8 (target and source near the
-//     wall and aligned), where the FP32 form would cancel. The periodic m = 0 denominator
-//     2 (sinh^2(x^/2) + sin^2(y^/2)) and every m != 0 term have no cancellation, so the periodic
-//     series stays in FP32 throughout.
+//   * the disk's wall image of each source is staged as a position (the vortex -Gamma at
+//     R^2 s/|s|^2, computed in FP64 once per CTA and tile), so the image term is a direct term
+//     from an accurately known point instead of the cancelling 1 - t.s/R^2 form;
+//   * near field: the periodic pairs closer than the near-field radius (minimum image) and the
+//     disk images closer than it to their target are left out of the FP32 sums and listed for the
+//     FP64 pass (pv_near.cu), which adds their exact terms.
 //
-// What remains is the FP32 rounding of each pair term (a few ulp, ~1e-7 relative); the velocity
+// What remains is the FP32 rounding of each far term (a few ulp, ~1e-7 of the term); the velocity
 // error against the FP64 oracle is that, summed over sources (reported by the parity tests).
 #include "pv_internal.h"
 #include "pv_pair32.cuh"
@@ -35,6 +39,7 @@ __global__ void __launch_bounds__(B) velocity32_kernel(const EvalArgs a) {
     __shared__ alignas(128) double s_y[2][kTile32];
     __shared__ alignas(128) double s_g[2][kTile32];
     __shared__ alignas(16) float4 s_f[kTile32];
+    __shared__ alignas(16) float4 s_fi[GEO == GEO_DISK ? kTile32 : 1];  // wall images (disk)
     __shared__ float s_gf[kTile32];
     __shared__ alignas(8) uint64_t bars[2];
     __shared__ int s_status;
@@ -119,37 +124,44 @@ __global__ void __launch_bounds__(B) velocity32_kernel(const EvalArgs a) {
         }
         const size_t j0 = src0 + static_cast<size_t>(t) * kTile32;
         const int cnt = static_cast<int>(min(static_cast<size_t>(kTile32), src1 - j0));
-        // split the tile into double-float FP32 coordinates once per CTA
+        // split the tile into double-float FP32 coordinates (and, in the disk, the sources' wall
+        // images) once per CTA
         for (int j = tid; j < cnt; j += B) {
             const double xj = s_x[st][j], yj = s_y[st][j];
-            const float xh = static_cast<float>(xj), yh = static_cast<float>(yj);
-            s_f[j] = make_float4(xh, yh, static_cast<float>(xj - static_cast<double>(xh)),
-                                 static_cast<float>(yj - static_cast<double>(yh)));
+            s_f[j] = split_position(xj, yj);
+            if (GEO == GEO_DISK)
+                s_fi[j] = image_position(a.g, xj, yj);
             s_gf[j] = static_cast<float>(s_g[st][j]);
         }
         __syncthreads();
         const bool diagonal = j0 < blk1 && blk0 < j0 + cnt;
+        // a near pair (or wall image) is left to the FP64 pass: list it under its target
+        const unsigned flag = GEO == GEO_DISK ? kNearImage : 0u;
         for (int jb = 0; jb < cnt; jb += kFlush) {
             const int je = min(cnt, jb + kFlush);
             if (diagonal) {
 #pragma unroll 1
                 for (int j = jb; j < je; ++j) {
                     const float4 sf = s_f[j];
+                    const float4 si = GEO == GEO_DISK ? s_fi[j] : sf;
                     const float gf = s_gf[j];
 #pragma unroll
                     for (int k = 0; k < T; ++k)
-                        pair32<GEO, true>(f, a.g, tg[k], sf, gf, s_x[st][j], s_y[st][j], s_g[st][j],
-                                          ti[k] == j0 + j, u[k], v[k], ud[k], vd[k]);
+                        if (pair32<GEO, true>(f, tg[k], sf, si, gf, ti[k] == j0 + j, u[k], v[k]) &&
+                            a.near.count && ti[k] < blk1)
+                            near_append(a.near, ti[k], static_cast<unsigned>(j0 + j) | flag);
                 }
             } else {
 #pragma unroll 2
                 for (int j = jb; j < je; ++j) {
                     const float4 sf = s_f[j];
+                    const float4 si = GEO == GEO_DISK ? s_fi[j] : sf;
                     const float gf = s_gf[j];
 #pragma unroll
                     for (int k = 0; k < T; ++k)
-                        pair32<GEO, false>(f, a.g, tg[k], sf, gf, s_x[st][j], s_y[st][j],
-                                           s_g[st][j], false, u[k], v[k], ud[k], vd[k]);
+                        if (pair32<GEO, false>(f, tg[k], sf, si, gf, false, u[k], v[k]) &&
+                            a.near.count && ti[k] < blk1)
+                            near_append(a.near, ti[k], static_cast<unsigned>(j0 + j) | flag);
                 }
             }
 #pragma unroll

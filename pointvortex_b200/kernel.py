@@ -351,6 +351,17 @@ class VelocityKernel:
         """Bracket every kernel launch with CUDA events on the context's stream."""
         self._check(lib.pv_set_profiling(self._ctx, int(bool(enabled))))
 
+    def setNearField(self, radius: float = -1.0) -> None:
+        """Near-field radius of the FP32-compensated form (pv_set_near_field): periodic pairs and
+        disk wall images closer than it are evaluated in FP64; -1 the default, 0 none."""
+        self._check(lib.pv_set_near_field(self._ctx, float(radius)))
+
+    @property
+    def nearField(self) -> float:
+        r = ctypes.c_double(0.0)
+        self._check(lib.pv_get_near_field(self._ctx, ctypes.byref(r)))
+        return float(r.value)
+
     def setWaitLimits(self, copy_polls: int = -1, barrier_polls: int = -1) -> None:
         """Polls of the bounded device waits before they give up (pv_set_wait_limits): the tile
         copies of a velocity launch and the grid barrier of the cooperative RK4 steps; -1 keeps

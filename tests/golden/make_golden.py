@@ -105,6 +105,35 @@ def dipole_event_fixtures(ref: Oracle) -> None:
         save(f"dipole_events_{boundary}_{mode}.npz", **out)
 
 
+# The timed periodic workload: N = 4096 in the 2 pi box, M = 8, DOPRI5 rtol 1e-9 / atol 1e-12 from
+# dt = 1e-3, close-dipole removal at 1e-3 after every accepted step.
+DOPRI_WORKLOAD = dict(boundary="periodic", box_length_x=2 * np.pi, box_length_y=2 * np.pi,
+                      image_layers=8, absolute_tolerance=1e-12, relative_tolerance=1e-9,
+                      minimum_time_step=1e-12, maximum_time_step=0.1, dipole_removal=True,
+                      dipole_removal_distance=1e-3)
+
+
+def dopri_workload_fixture(ref: Oracle) -> None:
+    """Two accepted DOPRI5 steps of the timed periodic workload by the reference's own
+    RungeKuttaIntegrator (FSAL kept between them, src/timestep.cpp:62-120), each followed by
+    its DipoleManager::process (src/dipole.cpp:42-127): the states, the step results (accepted
+    dt, suggested dt, error, rejections) and the event counts."""
+    x, y, g = ics.workload_state("periodic_dopri5_n4096")
+    geo = Geometry(**DOPRI_WORKLOAD)
+    st = ref.stepper(geo, x.size)
+    out = {"x0": x, "y0": y, "g": g, "dt0": np.array([1e-3])}
+    dt = 1e-3
+    for k in (1, 2):
+        x, y, r = st.dopri5_step(x, y, g, dt)
+        events, x, y, g2 = ref.dipole_process(geo, x, y, g)
+        if events:
+            raise RuntimeError("the fixture assumes no dipole events in its first steps")
+        out.update({f"x{k}": x, f"y{k}": y, f"r{k}": r, f"events{k}": np.array([events])})
+        dt = r[1]
+        print(f"step {k}: {r}", flush=True)
+    save("workload_periodic_dopri5_n4096_steps.npz", **out)
+
+
 def output_inputs():
     """Inputs of the writer fixtures: a periodic state with velocities, with awkward values
     (negative zero, integers, powers of ten, subnormals, huge and tiny magnitudes) mixed in."""
@@ -150,7 +179,7 @@ def main() -> int:
     ap = argparse.ArgumentParser()
     ap.add_argument("--reference", default=os.environ.get("PV_REFERENCE_DIR"),
                     help="the reference checkout (default: $PV_REFERENCE_DIR)")
-    ap.add_argument("--only", choices=["dipole_events", "output"], default=None,
+    ap.add_argument("--only", choices=["dipole_events", "output", "dopri_workload"], default=None,
                     help="regenerate one fixture family only")
     args = ap.parse_args()
     if not args.reference:
@@ -164,6 +193,9 @@ def main() -> int:
         return 0
     if args.only == "output":
         output_fixtures(ref)
+        return 0
+    if args.only == "dopri_workload":
+        dopri_workload_fixture(ref)
         return 0
 
     # small cases, all three geometries (+ the core-radius plane)
@@ -231,6 +263,7 @@ def main() -> int:
              threshold=np.array([geo.dipole_removal_distance]))
     dipole_event_fixtures(ref)
     output_fixtures(ref)
+    dopri_workload_fixture(ref)
     print(f"done in {time.time() - t0:.1f} s")
     _ = rng
     return 0

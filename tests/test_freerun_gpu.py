@@ -12,7 +12,8 @@ a factor 10 for where the first differences land. Measured on this state (refere
 understates both, because the fastest vortices (tight pairs, speeds ~1e4) amplify a rounding
 difference the most. Invariants that the
 dynamics conserve exactly (circulation, linear impulse) must be conserved as tightly as the
-reference conserves them; the Hamiltonian and angular impulse drift are compared in size."""
+reference conserves them; the Hamiltonian and angular impulse drifts may not exceed the envelope
+of the reference's own runs."""
 import numpy as np
 import pytest
 
@@ -75,6 +76,19 @@ def test_free_run_divergence_no_worse_than_reference_self_divergence(reference):
                         inv_gpu.angularImpulse, inv_gpu.hamiltonian])
     drift_cpu = np.abs(inv_cpu - inv0)
     drift_gpu = np.abs(gpu_arr - inv0)
-    print("drift cpu", drift_cpu, "drift gpu", drift_gpu)
+    # the reference's own runs from the 1-ulp state and with reversed summation
+    drift_ulp = np.abs(reference.invariants(geo, *perturbed[100], g)
+                       - reference.invariants(geo, xp, yp, g))
+    drift_rev = np.abs(reference.invariants(geo, *reordered[100], g) - inv0)
+    envelope = np.max([drift_cpu, drift_ulp, drift_rev], axis=0)
+    print("drift cpu", drift_cpu, "1-ulp", drift_ulp, "reversed", drift_rev, "gpu", drift_gpu)
     assert drift_gpu[0] <= 1e-12
     assert drift_gpu[1] <= max(10 * drift_cpu[1], 1e-12) and drift_gpu[2] <= max(10 * drift_cpu[2], 1e-12)
+    # The Hamiltonian and the angular impulse are conserved by the flow but not by RK4 at this
+    # step: a few tight pairs are under-resolved, and how much H and L drift depends on the
+    # chaotic details. Over the reference's own runs from this state (1-ulp perturbations, reversed
+    # summation) |dH| spans 14.1-17.8 and |dL| 0.003-0.024. The GPU's drift may not be larger
+    # than the envelope of the three reference runs made here, with a factor 1.5 for H and 3 for
+    # L (whose spread between runs is relatively wider).
+    assert drift_gpu[4] <= 1.5 * envelope[4], (drift_gpu[4], envelope[4])
+    assert drift_gpu[3] <= 3.0 * envelope[3], (drift_gpu[3], envelope[3])
