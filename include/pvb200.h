@@ -221,6 +221,9 @@ typedef struct pv_plan_info {
     int rows;
     int targets_per_thread; /* ordered kernel */
     int chunk;              /* ordered kernel: sources per work item */
+    int symmetric_min_ctas; /* symmetric form: the kernel built for this many CTAs per SM (0: default) */
+    int symmetric_targets;  /* symmetric form: targets per lane off the diagonal */
+    uint32_t split_items;   /* symmetric form: items two warps may share at the end of the queue */
 } pv_plan_info;
 pv_status pv_state_plan(const pv_context *ctx, pv_plan_info *info);
 
@@ -362,6 +365,15 @@ pv_status pv_context_stream(const pv_context *ctx, void **stream);
  * pv_evaluate_range). pointvortex_b200/autotune.py fills it by timing the candidates. */
 pv_status pv_set_tuning(int geometry, int precision, int log2_n, int per_thread);
 pv_status pv_get_tuning(int geometry, int precision, int log2_n, int *per_thread);
+/* Autotuner table of the once-per-unordered-pair form (periodic box and plane), by geometry,
+ * precision and floor(log2 N): mode 0 restores the built-in plan, 1 selects the ordered kernel,
+ * 2 the symmetric form; min_ctas (periodic FP64: 7 or 8, else 0) selects the kernel built for that
+ * many resident CTAs per SM; targets (plane: 4 or 8, else 0) the targets per lane. Process-wide;
+ * read when a context plans its device state (pv_upload_state). No reference counterpart. */
+pv_status pv_set_symmetric_tuning(int geometry, int precision, int log2_n, int mode, int min_ctas,
+                                  int targets);
+pv_status pv_get_symmetric_tuning(int geometry, int precision, int log2_n, int *mode,
+                                  int *min_ctas, int *targets);
 /* Near-field radius of the FP32-compensated form (precision PV_PRECISION_FP32C): periodic pairs
  * closer than it (minimum image) and disk wall images closer than it to their target are left out
  * of the FP32 sums and evaluated in FP64. radius < 0 selects the default for the population (twice

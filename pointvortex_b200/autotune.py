@@ -1,7 +1,14 @@
-"""Autotuner of the velocity plan: for every geometry, precision and N bucket (floor(log2 N)) it
-times the tiled kernel with 1, 2 and 4 targets per thread on a seeded state of that size and keeps
-the fastest in the library's tuning table (pv_set_tuning). Results are cached as JSON; the package
-loads `tuning.json` next to this file when it exists.
+"""Autotuner of the velocity plans, per geometry, precision and N bucket (floor(log2 N)), on a
+seeded state of that size, keeping the fastest in the library's tables:
+
+* the ordered-pair kernel: 1, 2 or 4 targets per thread (pv_set_tuning);
+* the once-per-unordered-pair form of the periodic box and the plane (pv_set_symmetric_tuning):
+  the ordered kernel or the symmetric form, and for the symmetric form the occupancy it is built
+  for (periodic FP64: the default, 7 or 8 CTAs per SM) or the targets per lane (plane: 4 or 8).
+  A candidate is timed as a whole evaluation of the device state: velocity launches and the
+  reduction of their partial rows.
+
+Results are cached as JSON; the package loads `tuning.json` next to this file when it exists.
 
     python -m pointvortex_b200.autotune [--out path] [--min-log2 6] [--max-log2 16]
 """
@@ -32,6 +39,20 @@ def get_entry(geometry: int, precision: int, log2_n: int) -> int:
     return out.value
 
 
+def set_symmetric_entry(geometry: int, precision: int, log2_n: int, mode: int, min_ctas: int = 0,
+                        targets: int = 0) -> None:
+    rc = lib.pv_set_symmetric_tuning(geometry, precision, log2_n, mode, min_ctas, targets)
+    if rc != _lib.PV_OK:
+        raise ValueError(lib.pv_last_error(None).decode())
+
+
+def get_symmetric_entry(geometry: int, precision: int, log2_n: int) -> tuple:
+    m, c, t = ctypes.c_int(0), ctypes.c_int(0), ctypes.c_int(0)
+    lib.pv_get_symmetric_tuning(geometry, precision, log2_n, ctypes.byref(m), ctypes.byref(c),
+                                ctypes.byref(t))
+    return m.value, c.value, t.value
+
+
 def load(path: str = DEFAULT_PATH) -> int:
     """Applies a cached table; returns the number of entries."""
     if not os.path.exists(path):
@@ -40,7 +61,10 @@ def load(path: str = DEFAULT_PATH) -> int:
         table = json.load(f)
     for e in table.get("entries", []):
         set_entry(GEOMETRIES[e["geometry"]], PRECISIONS[e["precision"]], e["log2_n"], e["per_thread"])
-    return len(table.get("entries", []))
+    for e in table.get("symmetric", []):
+        set_symmetric_entry(GEOMETRIES[e["geometry"]], PRECISIONS[e["precision"]], e["log2_n"],
+                            e["mode"], e.get("min_ctas", 0), e.get("targets", 0))
+    return len(table.get("entries", [])) + len(table.get("symmetric", []))
 
 
 def _time_plan(geometry: str, precision: int, n: int, per_thread: int, evals: int) -> float:
@@ -66,6 +90,52 @@ def _time_plan(geometry: str, precision: int, n: int, per_thread: int, evals: in
     return ms / max(timed, 1)
 
 
+def _time_evaluation(geometry: str, precision: int, n: int, evals: int) -> float:
+    """ms per evaluation of the device state (velocity launches + reduction), current tables."""
+    from .kernel import InfinitePlaneKernel, PeriodicBoxKernel, VortexSystem
+    if geometry == "infinite":
+        k = InfinitePlaneKernel(0.0, precision=precision)
+        x, y, g = ics.infinite_plane(n, 1)
+    else:
+        k = PeriodicBoxKernel(6.283185307179586, 6.283185307179586, 8, precision=precision)
+        x, y, g = ics.periodic_box(n + n % 2, 1)
+    k.uploadDeviceState(VortexSystem(x, y, g))
+    k.evaluateDeviceState()
+    k.setProfiling(True)
+    k.resetKernelStats()
+    for _ in range(evals):
+        k.evaluateDeviceState()
+    st = k.kernelStats()
+    k.close()
+    return (st["velocity"][2] + st["stage"][2]) / max(st["stage"][1], 1)
+
+
+# candidates of the symmetric-form table: (mode, min_ctas, targets)
+SYMMETRIC_CANDIDATES = {
+    ("periodic", "fp64"): [(1, 0, 0), (2, 0, 0), (2, 7, 0), (2, 8, 0)],
+    ("periodic", "fp32c"): [(1, 0, 0), (2, 0, 0)],
+    ("infinite", "fp64"): [(1, 0, 0), (2, 0, 4), (2, 0, 8)],
+    ("infinite", "fp32c"): [(1, 0, 0), (2, 0, 4), (2, 0, 8)],
+}
+
+
+def tune_symmetric(log2_range=range(11, 17), evals: int = 3) -> list:
+    entries = []
+    for (geo, prec), cands in SYMMETRIC_CANDIDATES.items():
+        for b in log2_range:
+            n = 1 << b
+            times = {}
+            for cand in cands:
+                set_symmetric_entry(GEOMETRIES[geo], PRECISIONS[prec], b, *cand)
+                times[cand] = _time_evaluation(geo, PRECISIONS[prec], n, evals)
+            best = min(times, key=times.get)
+            set_symmetric_entry(GEOMETRIES[geo], PRECISIONS[prec], b, *best)
+            entries.append({"geometry": geo, "precision": prec, "log2_n": b, "mode": best[0],
+                            "min_ctas": best[1], "targets": best[2],
+                            "ms": {"/".join(map(str, c)): v for c, v in times.items()}})
+    return entries
+
+
 def tune(geometries=("infinite", "periodic", "disk"), precisions=("fp64", "fp32c"),
          log2_range=range(6, 17), evals: int = 3) -> dict:
     entries = []
@@ -78,7 +148,8 @@ def tune(geometries=("infinite", "periodic", "disk"), precisions=("fp64", "fp32c
                 set_entry(GEOMETRIES[geo], PRECISIONS[prec], b, best)
                 entries.append({"geometry": geo, "precision": prec, "log2_n": b, "per_thread": best,
                                 "ms": {str(k): v for k, v in times.items()}})
-    return {"entries": entries}
+    symmetric = tune_symmetric(range(max(11, log2_range.start), log2_range.stop), evals)
+    return {"entries": entries, "symmetric": symmetric}
 
 
 def main(argv=None) -> int:

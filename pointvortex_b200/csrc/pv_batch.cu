@@ -1197,8 +1197,12 @@ pv_status pv_batch_add(pv_batch *b, const pv_params *params, const double *x, co
     const size_t pad = round_up(n, kAlign);
     const size_t chunk = chunk_for(n);
     // periodic populations from kSymmetricMinN up: once per unordered pair, one partial row
-    // per 128-block (a function of n only, so the choice never depends on the batch)
-    const bool symmetric = g.geometry == GEO_PERIODIC && n >= kSymmetricMinN;
+    // per 128-block. The autotuner's table of the symmetric form (pv_set_symmetric_tuning) may
+    // choose otherwise for the population's size; either way the choice is a function of the
+    // simulation's own n, geometry and precision, never of the batch.
+    const int tuned = symmetric_tuning_lookup(g.geometry, params->precision, n) & 15;
+    const bool symmetric = g.geometry == GEO_PERIODIC && n >= 128 &&
+                           (tuned == 2 || (tuned == 0 && n >= kSymmetricMinN));
     const unsigned chunks = symmetric ? symmetric_rows(static_cast<unsigned>(n))
                                       : static_cast<unsigned>((n + chunk - 1) / chunk);
     size_t off = 0, poff = 0;

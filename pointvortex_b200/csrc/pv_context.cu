@@ -95,6 +95,7 @@ struct pv_context {
     cudaGraphExec_t attempt_graph = nullptr; // one DOPRI5 attempt with a valid FSAL derivative
     SymmetricPlan sym{};             // one evaluation per unordered pair (when planned)
     DeviceArray sym_items, sym_counter;
+    DeviceArray sym_split, sym_flags;  // the join of the split items (scratch, flags)
     DeviceArray rk4_barrier;         // arrival counter of the cooperative RK4 steps' grid barrier
     int sym_items_blocks = 0;        // the block count the item table was built for
     DeviceArray inv_scratch, inv_out;
@@ -153,7 +154,8 @@ struct pv_context {
         for (DeviceArray *a : {&x, &y, &gamma, &gs, &p0x, &p0y, &p1x, &p1y, &pu, &pv, &inv_scratch,
                                &inv_out, &cand, &ex, &ey, &eg, &egs, &eu, &ev, &epu, &epv,
                                &removed_index, &fmt_stage, &fmt_len, &fmt_block, &fmt_out,
-                               &sym_items, &sym_counter, &rk4_barrier, &near_count, &near_slot})
+                               &sym_items, &sym_counter, &rk4_barrier, &near_count, &near_slot,
+                               &sym_split, &sym_flags})
             a->release();
         for (int s = 0; s < 7; ++s) {
             kx[s].release();
@@ -331,6 +333,7 @@ pv_status make_consts(const pv_params &p, GeometryConsts &g, std::string &messag
         g.half_lx = 0.5 * lx;
         g.half_ly = 0.5 * ly;
         g.wave = 2.0 * kPi / lx;
+        g.half_wave = 0.5 * g.wave;
         g.scale = 0.5 / lx;
         g.m_exact = std::min(p.image_layers, 2);
         g.has6 = p.image_layers >= 6 ? 1 : 0;
@@ -367,6 +370,8 @@ pv_status make_consts(const pv_params &p, GeometryConsts &g, std::string &messag
             hi = std::nextafter(hi, -1e300);
         g.lo6 = lo;
         g.hi6 = hi;
+        g.lo6h = 0.5 * lo;
+        g.hi6h = 0.5 * hi;
         return PV_OK;
     }
     if (p.geometry == PV_GEOMETRY_DISK) {
@@ -474,6 +479,8 @@ pv_status launch_eval(pv_context *c, const double *px, const double *py) {
                         reinterpret_cast<const unsigned *>(c->sym_items.p),
                         reinterpret_cast<unsigned *>(c->sym_counter.p),
                         reinterpret_cast<double2 *>(c->pu.p), padded(c->n), c->gc, lists,
+                        c->sym.split ? reinterpret_cast<double2 *>(c->sym_split.p) : nullptr,
+                        c->sym.split ? reinterpret_cast<unsigned *>(c->sym_flags.p) : nullptr,
                         c->stream);
                 }));
         if (near) {
@@ -571,7 +578,8 @@ std::vector<const void *> attempt_key(const pv_context *c) {
                                        c->dipole_configured && c->dipole.removal ? 1 : 0)),
                                    reinterpret_cast<const void *>(
                                        static_cast<uintptr_t>(c->wait_limit)),
-                                   c->near_count.p, c->near_slot.p};
+                                   c->near_count.p, c->near_slot.p, c->sym_split.p,
+                                   c->sym_flags.p};
     uint64_t near_bits;
     std::memcpy(&near_bits, &c->gc.near2, sizeof near_bits);
     k.push_back(reinterpret_cast<const void *>(static_cast<uintptr_t>(near_bits)));
@@ -614,6 +622,12 @@ pv_status ensure_state_capacity(pv_context *c, size_t n) {
         PV_CUDA(c, c->sym_items.ensure((items.size() + 1) / 2));
         PV_CUDA(c, c->sym_counter.ensure(1));
         PV_CUDA(c, cudaMemsetAsync(c->sym_counter.p, 0, 2 * sizeof(unsigned), c->stream));
+        if (c->sym.split) {
+            PV_CUDA(c, c->sym_split.ensure(static_cast<size_t>(c->sym.split) * 256));
+            PV_CUDA(c, c->sym_flags.ensure((c->sym.split + 1) / 2));
+            PV_CUDA(c, cudaMemsetAsync(c->sym_flags.p, 0, c->sym_flags.cap * sizeof(double),
+                                       c->stream));
+        }
         PV_CUDA(c, cudaMemcpyAsync(c->sym_items.p, items.data(), items.size() * sizeof(unsigned),
                                    cudaMemcpyHostToDevice, c->stream));
         PV_CUDA(c, cudaStreamSynchronize(c->stream));
@@ -1802,6 +1816,9 @@ pv_status pv_state_plan(const pv_context *ctx, pv_plan_info *info) {
     info->rows = ctx->sym.enabled() ? ctx->sym.blocks : ctx->plan.num_chunks;
     info->targets_per_thread = ctx->plan.per_thread;
     info->chunk = ctx->plan.chunk;
+    info->symmetric_min_ctas = ctx->sym.enabled() ? ctx->sym.min_ctas : 0;
+    info->symmetric_targets = ctx->sym.enabled() ? ctx->sym.targets : 0;
+    info->split_items = ctx->sym.enabled() ? ctx->sym.split : 0u;
     return PV_OK;
 }
 
@@ -1824,6 +1841,26 @@ pv_status pv_set_tuning(int geometry, int precision, int log2_n, int per_thread)
         g_create_error = "invalid tuning entry";
         return PV_ERROR_INVALID_ARGUMENT;
     }
+    return PV_OK;
+}
+
+pv_status pv_set_symmetric_tuning(int geometry, int precision, int log2_n, int mode, int min_ctas,
+                                  int targets) {
+    if (!symmetric_tuning_store(geometry, precision, log2_n, mode, min_ctas, targets)) {
+        g_create_error = "invalid symmetric tuning entry";
+        return PV_ERROR_INVALID_ARGUMENT;
+    }
+    return PV_OK;
+}
+
+pv_status pv_get_symmetric_tuning(int geometry, int precision, int log2_n, int *mode,
+                                  int *min_ctas, int *targets) {
+    if (!mode || !min_ctas || !targets || log2_n < 0 || log2_n >= 40)
+        return PV_ERROR_INVALID_ARGUMENT;
+    const int packed = symmetric_tuning_lookup(geometry, precision, size_t(1) << log2_n);
+    *mode = packed & 15;
+    *min_ctas = (packed >> 4) & 15;
+    *targets = (packed >> 8) & 15;
     return PV_OK;
 }
 

@@ -30,6 +30,7 @@ struct GeometryConsts {
     double inv_lx, inv_ly;  // 1/L
     double half_lx, half_ly;
     double wave;            // 2 pi / Lx
+    double half_wave;       // pi / Lx (exactly wave / 2)
     double scale;           // 0.5 / Lx
     int m_exact;            // image pairs m = +-1..m_exact summed exactly (min(M, 2))
     int has6;               // images m = +-6 kept when within the |shift| <= 40 window (M >= 6)
@@ -41,6 +42,7 @@ struct GeometryConsts {
     double shift6;          // (2 pi) * 6, rounded as the reference rounds it
     double lo6, hi6;        // m = +6 kept iff x^ >= lo6, m = -6 iff x^ <= hi6 (the reference's
                             // |x^ -+ shift6| <= 40 with its rounding, as thresholds on x^)
+    double lo6h, hi6h;      // the same thresholds on x^/2 (exactly lo6/2, hi6/2)
     // disk
     double radius, radius2, inv_radius, inv_radius2;
     // FP32-compensated form: near-field radius squared (0: none), pv_pair32.cuh
@@ -128,30 +130,33 @@ struct DiskPair {
 //   * |m| >= 7 always has |shift| > 40 and is dropped, as in the reference.
 // sinh, cosh, sin and cos of x^/2 and y^/2 come from one shared series (|x^/2| <= pi/2).
 struct PeriodicPair {
-    // Images m != 0 of one axis as num/den + rest.
-    __device__ __forceinline__ static void image_sum(const GeometryConsts &g, double hat, double ch,
-                                                     double sh, double c, double &num, double &den,
-                                                     double &rest) {
+    // Images m != 0 of one axis as num/den + rest. half_hat = x^/2 (the m = +-6 window test).
+    // The first image pair starts the fraction as itself (num = pair_num, den = pair_den: what
+    // adding it to 0/1 would give, exactly).
+    __device__ __forceinline__ static void image_sum(const GeometryConsts &g, double half_hat,
+                                                     double ch, double sh, double c, double &num,
+                                                     double &den, double &rest) {
         const double ch2 = ch * ch;
         const double p = fma(c, c, ch2);   // C^2 + c^2
         const double q = -2.0 * c * ch;    // -2 c C
         const double m2c = -2.0 * c;
         num = 0.0;
         den = 1.0;
-#pragma unroll
-        for (int m = 1; m <= 2; ++m) {
-            if (m <= g.m_exact) {
-                const double pair_num = fma(ch, g.two_cosh_m[m], m2c);
-                const double pair_den = fma(q, g.cosh_m[m], p + g.sinh2_m[m]);
-                num = fma(pair_num, den, num * pair_den);
-                den *= pair_den;
-            }
+        if (g.m_exact >= 1) {
+            num = fma(ch, g.two_cosh_m[1], m2c);
+            den = fma(q, g.cosh_m[1], p + g.sinh2_m[1]);
+        }
+        if (g.m_exact >= 2) {
+            const double pair_num = fma(ch, g.two_cosh_m[2], m2c);
+            const double pair_den = fma(q, g.cosh_m[2], p + g.sinh2_m[2]);
+            num = fma(pair_num, den, num * pair_den);
+            den *= pair_den;
         }
         const double ch2x = fma(2.0, ch2, -1.0); // cosh 2x^
         rest = fma(ch, g.k1, c * ch2x * g.k2);
         if (g.has6) {
-            const bool plus = hat >= g.lo6;
-            const bool minus = hat <= g.hi6;
+            const bool plus = half_hat >= g.lo6h;
+            const bool minus = half_hat <= g.hi6h;
             const double e = (plus ? ch + sh : 0.0) + (minus ? ch - sh : 0.0);
             rest = fma(g.k6, e, rest);
         }
@@ -167,11 +172,12 @@ struct PeriodicPair {
     __device__ __forceinline__ static void terms(const GeometryConsts &g, double tx, double ty,
                                                  double sx, double sy, double &au, double &bu,
                                                  double &av, double &bv) {
-        const double xh = g.wave * exact_remainder(tx - sx, g.lx, g.inv_lx, g.half_lx);
-        const double yh = g.wave * exact_remainder(ty - sy, g.ly, g.inv_ly, g.half_ly);
+        // x^/2 and y^/2: pi/L times the remainder is exactly half of (2 pi/L) times it
+        const double hx = g.half_wave * exact_remainder(tx - sx, g.lx, g.inv_lx, g.half_lx);
+        const double hy = g.half_wave * exact_remainder(ty - sy, g.ly, g.inv_ly, g.half_ly);
         double shx, chx, snx, csx, shy, chy, sny, csy;
-        sinh_cosh_sin_cos(0.5 * xh, shx, chx, snx, csx);
-        sinh_cosh_sin_cos(0.5 * yh, shy, chy, sny, csy);
+        sinh_cosh_sin_cos(hx, shx, chx, snx, csx);
+        sinh_cosh_sin_cos(hy, shy, chy, sny, csy);
         const double cosh_x = fma(2.0 * shx, shx, 1.0); // cosh x^ = 1 + 2 sinh^2(x^/2)
         const double cosh_y = fma(2.0 * shy, shy, 1.0);
         const double cos_x = fma(-2.0 * snx, snx, 1.0); // cos x^ = 1 - 2 sin^2(x^/2)
@@ -183,8 +189,8 @@ struct PeriodicPair {
         const double d0u = 2.0 * fma(shx, shx, sny * sny);
         const double d0v = 2.0 * fma(shy, shy, snx * snx);
         double nu, du, ru, nv, dv, rv;
-        image_sum(g, xh, cosh_x, sinh_x, cos_y, nu, du, ru);
-        image_sum(g, yh, cosh_y, sinh_y, cos_x, nv, dv, rv);
+        image_sum(g, hx, cosh_x, sinh_x, cos_y, nu, du, ru);
+        image_sum(g, hy, cosh_y, sinh_y, cos_x, nv, dv, rv);
         // 1/d0 + num/den + rest = (den + d0 (num + den rest)) / (d0 den)
         au = sin_y * fma(d0u, fma(du, ru, nu), du);
         av = sin_x * fma(d0v, fma(dv, rv, nv), dv);

@@ -51,26 +51,86 @@ __device__ __forceinline__ void release_queue(unsigned *counter) {
     }
 }
 
+// One half of a split item (I, J), I < J, blocks of 32: the rotation steps [16 h, 16 h + 16) of
+// its tile, so that two warps can share the item at the end of the queue. Each half leaves its
+// target and reaction sums in the item's scratch slot; the half that finishes second adds the two
+// in fixed order (half 0 + half 1) and writes the item's partial-row entries, then clears the
+// flag for the next launch. The partial sums do not depend on which half finished first.
+template <class P>
+__device__ __forceinline__ void half_item(const double *__restrict__ x,
+                                          const double *__restrict__ y,
+                                          const double *__restrict__ gs, size_t n, unsigned I,
+                                          unsigned J, unsigned h, double2 *scratch,
+                                          unsigned *flag, double2 *__restrict__ pr, size_t stride,
+                                          const GeometryConsts &g) {
+    const int lane = threadIdx.x & 31;
+    const size_t ti = static_cast<size_t>(I) * 32 + lane;  // I < J: block I is full
+    const int home = (lane + 16 * static_cast<int>(h)) & 31;  // this lane's first source
+    const size_t sj = static_cast<size_t>(J) * 32 + home;
+    const int s_ok = sj < n ? 1 : 0;
+    const double tx = x[ti], ty = y[ti], tg = P::kScale * gs[ti];
+    const double sx = s_ok ? x[sj] : 0.0, sy = s_ok ? y[sj] : 0.0;
+    const double sg = s_ok ? P::kScale * gs[sj] : 0.0;
+    double u = 0.0, v = 0.0, ru = 0.0, rv = 0.0;
+    sym::react_tile<P, 16>(g, tx, ty, tg, true, sx, sy, sg, s_ok, u, v, ru, rv);
+    // after 16 rotations the lane holds the reaction of source (home + 16) & 31
+    const int rs = (home + 16) & 31;
+    double2 *mine = scratch + h * 64;
+    __stcg(mine + lane, make_double2(u, v));
+    __stcg(mine + 32 + rs, make_double2(ru, rv));
+    __threadfence();
+    __syncwarp();
+    unsigned first = 0;
+    if (lane == 0)
+        first = atomicAdd(flag, 1u);
+    first = __shfl_sync(0xffffffffu, first, 0);
+    if (first == 0)
+        return;  // the other half adds the two
+    __threadfence();
+    const double2 ta = __ldcg(scratch + lane), tb = __ldcg(scratch + 64 + lane);
+    pr[static_cast<size_t>(J) * stride + ti] = make_double2(ta.x + tb.x, ta.y + tb.y);
+    const size_t sh = static_cast<size_t>(J) * 32 + lane;
+    if (sh < n) {
+        const double2 ra = __ldcg(scratch + 32 + lane), rb = __ldcg(scratch + 96 + lane);
+        pr[static_cast<size_t>(I) * stride + sh] = make_double2(ra.x + rb.x, ra.y + rb.y);
+    }
+    if (lane == 0)
+        *flag = 0u;
+}
+
 // P: the pair kernel (sym::PeriodicSym, sym::PlaneSym). T: targets per lane in the items off the
 // diagonal (a multiple of T sub-blocks per block); diagonal items hold one target per lane.
-template <class P, int T>
-__global__ void __launch_bounds__(kThreads)
+// Tickets [0, n_whole) are whole items; with blocks of 32 the last n_split items may be taken as
+// two halves each (tickets n_whole + 2 q + h), which shortens the end of the queue.
+// MINB: resident CTAs per SM the register allocation must allow (1: the compiler's choice; the
+// periodic kernel is also built for 7 and 8, fewer registers for more warps to hide latency).
+template <class P, int T, int MINB = 1>
+__global__ void __launch_bounds__(kThreads, MINB)
     symmetric_kernel(const double *__restrict__ x, const double *__restrict__ y,
                      const double *__restrict__ gs, size_t n, int a,
-                     const unsigned *__restrict__ items, unsigned n_items, unsigned *counter,
-                     double2 *__restrict__ pr, size_t stride, GeometryConsts g) {
+                     const unsigned *__restrict__ items, unsigned n_whole, unsigned n_split,
+                     unsigned *counter, double2 *__restrict__ pr, size_t stride, GeometryConsts g,
+                     double2 *split_scratch, unsigned *split_flags) {
     extern __shared__ double2 reaction_smem[];
     pdl_enter();
     const int lane = threadIdx.x & 31;
     double2 *reaction = reaction_smem + (threadIdx.x >> 5) * a * 32;  // this warp's sources
     const size_t block_len = static_cast<size_t>(32) * a;
+    const unsigned n_tickets = n_whole + 2 * n_split;
     for (;;) {
         unsigned item = 0;
         if (lane == 0)
             item = atomicAdd(counter, 1u);
         item = __shfl_sync(0xffffffffu, item, 0);
-        if (item >= n_items)
+        if (item >= n_tickets)
             break;
+        if (item >= n_whole) {
+            const unsigned q = (item - n_whole) >> 1, h = (item - n_whole) & 1u;
+            const unsigned packed = items[n_whole + q];
+            half_item<P>(x, y, gs, n, packed >> 16, packed & 0xffffu, h, split_scratch + q * 128,
+                         split_flags + q, pr, stride, g);
+            continue;
+        }
         const unsigned packed = items[item];
         const unsigned I = packed >> 16, J = packed & 0xffffu;
         const bool diagonal = I == J;
@@ -323,7 +383,9 @@ enum SymKernel : int {
     SYM_PLANE_WIDE = 3,
     SYM_PLANE32 = 4,
     SYM_PLANE32_WIDE = 5,
-    SYM_KERNELS = 6
+    SYM_PERIODIC_7 = 6,   // the periodic FP64 kernel built for 7 resident CTAs per SM
+    SYM_PERIODIC_8 = 7,   // ... and for 8
+    SYM_KERNELS = 8
 };
 
 int kernel_of(const SymmetricPlan &p) {
@@ -332,8 +394,15 @@ int kernel_of(const SymmetricPlan &p) {
         const bool wide = p.targets == kPlaneTargetsWide;
         return fp32c ? (wide ? SYM_PLANE32_WIDE : SYM_PLANE32) : (wide ? SYM_PLANE_WIDE : SYM_PLANE);
     }
-    return fp32c ? SYM_PERIODIC32 : SYM_PERIODIC;
+    if (fp32c)
+        return SYM_PERIODIC32;
+    return p.min_ctas == 8 ? SYM_PERIODIC_8 : (p.min_ctas == 7 ? SYM_PERIODIC_7 : SYM_PERIODIC);
 }
+
+// Autotuner table of the symmetric form (pv_set_symmetric_tuning), by geometry (0 plane,
+// 1 periodic), precision and floor(log2 N): 0 = the built-in plan; otherwise
+// mode | (min_ctas << 4) | (targets << 8) with mode 1 = the ordered kernel, 2 = the symmetric form.
+std::atomic<int> g_sym_tuning[2][2][40] = {};
 
 template <typename K> int occupancy(K kernel, size_t smem) {
     int blocks = 0;
@@ -365,6 +434,12 @@ int resident_ctas(int a, int kernel) {
         case SYM_PLANE32_WIDE:
             blocks = occupancy(symmetric32_kernel<f32::Plane32, kPlaneTargetsWide>, smem);
             break;
+        case SYM_PERIODIC_7:
+            blocks = occupancy(symmetric_kernel<sym::PeriodicSym, 1, 7>, smem);
+            break;
+        case SYM_PERIODIC_8:
+            blocks = occupancy(symmetric_kernel<sym::PeriodicSym, 1, 8>, smem);
+            break;
         default:
             blocks = occupancy(symmetric_kernel<sym::PeriodicSym, 1>, smem);
             break;
@@ -376,17 +451,59 @@ int resident_ctas(int a, int kernel) {
 
 }  // namespace
 
+int symmetric_tuning_lookup(int geometry, int precision, size_t n) {
+    if ((geometry != GEO_INFINITE && geometry != GEO_PERIODIC) || precision < 0 || precision > 1 ||
+        n == 0)
+        return 0;
+    int bucket = 0;
+    while ((size_t(2) << bucket) <= n && bucket < 39)
+        ++bucket;
+    return g_sym_tuning[geometry == GEO_PERIODIC ? 1 : 0][precision][bucket].load(
+        std::memory_order_relaxed);
+}
+
+bool symmetric_tuning_store(int geometry, int precision, int log2_n, int mode, int min_ctas,
+                            int targets) {
+    if ((geometry != GEO_INFINITE && geometry != GEO_PERIODIC) || precision < 0 || precision > 1 ||
+        log2_n < 0 || log2_n >= 40 || mode < 0 || mode > 2)
+        return false;
+    if (min_ctas != 0 && !(geometry == GEO_PERIODIC && precision == PV_PRECISION_FP64 &&
+                           (min_ctas == 7 || min_ctas == 8)))
+        return false;
+    if (targets != 0 && !(geometry == GEO_INFINITE && (targets == kPlaneTargets ||
+                                                      targets == kPlaneTargetsWide)))
+        return false;
+    const int packed = mode == 0 ? 0 : (mode | (min_ctas << 4) | (targets << 8));
+    g_sym_tuning[geometry == GEO_PERIODIC ? 1 : 0][precision][log2_n].store(
+        packed, std::memory_order_relaxed);
+    return true;
+}
+
 SymmetricPlan plan_symmetric(size_t n, int sm_count, int precision, int geometry) {
     SymmetricPlan p{};
     const bool plane = geometry == GEO_INFINITE;
-    if (plane ? n < (precision == PV_PRECISION_FP32C ? kSymmetricPlane32MinN : kSymmetricPlaneMinN)
-              : (geometry != GEO_PERIODIC || n < kSymmetricMinN))
+    if (!plane && geometry != GEO_PERIODIC)
+        return p;
+    // the measured table overrides the built-in choice of form, occupancy and targets per lane
+    const int tuned = symmetric_tuning_lookup(geometry, precision, n);
+    const int mode = tuned & 15, tuned_ctas = (tuned >> 4) & 15, tuned_targets = (tuned >> 8) & 15;
+    if (mode == 1)
+        return p;
+    const size_t min_n = plane ? (precision == PV_PRECISION_FP32C ? kSymmetricPlane32MinN
+                                                                  : kSymmetricPlaneMinN)
+                               : kSymmetricMinN;
+    if (mode != 2 && n < min_n)
+        return p;
+    if (n < 64)
         return p;
     // the smallest block that keeps the partial rows within kSymmetricPartialBytes, or the largest
     // block up to kSymmetricPartialBytesMax (N ~ 3.7e5); beyond that the ordered kernel runs. The
     // plane's blocks hold at least as many sub-blocks as a lane holds targets.
     const int targets =
-        plane ? (n >= kSymmetricPlaneWideN ? kPlaneTargetsWide : kPlaneTargets) : 1;
+        plane ? (tuned_targets ? tuned_targets
+                               : (n >= kSymmetricPlaneWideN ? kPlaneTargetsWide : kPlaneTargets))
+              : 1;
+    p.min_ctas = tuned_ctas;
     const size_t np = (n + 255) & ~static_cast<size_t>(255);
     for (int a = targets; a <= 16; a *= 2) {
         const size_t blocks = (n + 32 * static_cast<size_t>(a) - 1) / (32 * static_cast<size_t>(a));
@@ -395,12 +512,19 @@ SymmetricPlan plan_symmetric(size_t n, int sm_count, int precision, int geometry
         const size_t bytes = blocks * np * 2 * sizeof(double);
         if (bytes <= kSymmetricPartialBytes || (a == 16 && bytes <= kSymmetricPartialBytesMax)) {
             p.a = a;
+            p.min_ctas = tuned_ctas;
             p.blocks = static_cast<int>(blocks);
             p.items = static_cast<unsigned>(blocks * (blocks + 1) / 2);
             p.precision = precision;
             p.geometry = geometry;
             p.targets = targets;
             p.grid = std::max(sm_count, 1) * resident_ctas(a, kernel_of(p));
+            // FP64, blocks of 32, one target per lane: the last wave's worth of items (one per
+            // warp) may be split in halves between two warps
+            if (a == 1 && targets == 1 && precision == PV_PRECISION_FP64) {
+                const unsigned off_diagonal = p.items - static_cast<unsigned>(blocks);
+                p.split = std::min(off_diagonal, static_cast<unsigned>(p.grid) * (kThreads / 32));
+            }
             return p;
         }
     }
@@ -408,16 +532,22 @@ SymmetricPlan plan_symmetric(size_t n, int sm_count, int precision, int geometry
 }
 
 void symmetric_items(const SymmetricPlan &p, unsigned *out) {
+    // the diagonal items (evaluated one-sided, never split) first, then I < J row by row
     size_t k = 0;
     for (unsigned i = 0; i < static_cast<unsigned>(p.blocks); ++i)
-        for (unsigned j = i; j < static_cast<unsigned>(p.blocks); ++j)
+        out[k++] = (i << 16) | i;
+    for (unsigned i = 0; i < static_cast<unsigned>(p.blocks); ++i)
+        for (unsigned j = i + 1; j < static_cast<unsigned>(p.blocks); ++j)
             out[k++] = (i << 16) | j;
 }
 
 cudaError_t launch_symmetric(const double *x, const double *y, const double *gs, size_t n,
                              const SymmetricPlan &p, const unsigned *items, unsigned *counter,
                              double2 *rows, size_t stride, const GeometryConsts &g,
-                             const f32::NearLists &near, cudaStream_t stream) {
+                             const f32::NearLists &near, double2 *split_scratch,
+                             unsigned *split_flags, cudaStream_t stream) {
+    const unsigned n_split = split_scratch && split_flags ? p.split : 0u;
+    const unsigned n_whole = p.items - n_split;
     const size_t smem = static_cast<size_t>(kThreads / 32) * p.a * 32 * sizeof(double2);
     const dim3 grid(static_cast<unsigned>(p.grid)), block(kThreads);
     switch (kernel_of(p)) {
@@ -426,10 +556,12 @@ cudaError_t launch_symmetric(const double *x, const double *y, const double *gs,
                           gs, n, p.a, items, p.items, counter, rows, stride, g, near);
     case SYM_PLANE:
         return launch_pdl(symmetric_kernel<sym::PlaneSym, kPlaneTargets>, grid, block, smem,
-                          stream, x, y, gs, n, p.a, items, p.items, counter, rows, stride, g);
+                          stream, x, y, gs, n, p.a, items, n_whole, n_split, counter, rows, stride, g,
+                          split_scratch, split_flags);
     case SYM_PLANE_WIDE:
         return launch_pdl(symmetric_kernel<sym::PlaneSym, kPlaneTargetsWide>, grid, block, smem,
-                          stream, x, y, gs, n, p.a, items, p.items, counter, rows, stride, g);
+                          stream, x, y, gs, n, p.a, items, n_whole, n_split, counter, rows, stride, g,
+                          split_scratch, split_flags);
     case SYM_PLANE32:
         return launch_pdl(symmetric32_kernel<f32::Plane32, kPlaneTargets>, grid, block, smem,
                           stream, x, y, gs, n, p.a, items, p.items, counter, rows, stride, g,
@@ -438,9 +570,18 @@ cudaError_t launch_symmetric(const double *x, const double *y, const double *gs,
         return launch_pdl(symmetric32_kernel<f32::Plane32, kPlaneTargetsWide>, grid, block, smem,
                           stream, x, y, gs, n, p.a, items, p.items, counter, rows, stride, g,
                           near);
+    case SYM_PERIODIC_7:
+        return launch_pdl(symmetric_kernel<sym::PeriodicSym, 1, 7>, grid, block, smem, stream, x, y,
+                          gs, n, p.a, items, n_whole, n_split, counter, rows, stride, g,
+                          split_scratch, split_flags);
+    case SYM_PERIODIC_8:
+        return launch_pdl(symmetric_kernel<sym::PeriodicSym, 1, 8>, grid, block, smem, stream, x, y,
+                          gs, n, p.a, items, n_whole, n_split, counter, rows, stride, g,
+                          split_scratch, split_flags);
     default:
         return launch_pdl(symmetric_kernel<sym::PeriodicSym, 1>, grid, block, smem, stream, x, y,
-                          gs, n, p.a, items, p.items, counter, rows, stride, g);
+                          gs, n, p.a, items, n_whole, n_split, counter, rows, stride, g,
+                          split_scratch, split_flags);
     }
 }
 

@@ -330,7 +330,9 @@ class VelocityKernel:
         info = _lib.PvPlanInfo()
         self._check(lib.pv_state_plan(self._ctx, ctypes.byref(info)))
         return {"symmetric": bool(info.symmetric), "rows": info.rows,
-                "targets_per_thread": info.targets_per_thread, "chunk": info.chunk}
+                "targets_per_thread": info.targets_per_thread, "chunk": info.chunk,
+                "symmetric_min_ctas": info.symmetric_min_ctas,
+                "symmetric_targets": info.symmetric_targets, "split_items": info.split_items}
 
     @property
     def evaluationCount(self) -> int:

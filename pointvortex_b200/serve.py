@@ -9,7 +9,10 @@ callback (streamed), and their room freed. Latency is measured from arrival to r
 In a lock-step attempt every simulation advances once, so a batch moves at the pace of its most
 expensive member. With policy "split" the server also admits by estimated work: cheap requests
 (one evaluation at most `split_work` plane-pair units) go to their own batch, which takes several
-attempts for each attempt of the batch holding the expensive ones.
+attempts for each attempt of the batch holding the expensive ones. Both are batches -- the
+expensive requests share their launches too -- each driven by its own host thread on its own CUDA
+stream, so their kernels overlap on the GPU. Within a lane, waiting requests are admitted
+shortest estimated work first (order="sjf") or in arrival order (order="fifo").
 
 `one_at_a_time()` is the comparison loop: the same requests, FIFO, each solved alone with the
 single-simulation context API (one simulation per launch, plain FP64).
@@ -92,12 +95,12 @@ def poisson_stream(n_requests: int, rate: float, seed: int, n_min: int = 32, n_m
 
 
 class _Lane:
-    """One batch with its own FIFO queue of arrived requests."""
+    """One batch with its own queue of arrived requests."""
 
     def __init__(self, capacity_vortices: int, max_slots: int, device: int, attempts: int):
         self.batch = Batch(capacity_vortices, max_slots, device)
         self.attempts = attempts
-        self.ready: list = []            # (arrival, rid, request), arrival order
+        self.ready: list = []            # (arrival, rid, request), in admission order
         self.running: dict[int, tuple] = {}
 
     def admit(self, server: "Server", now: float) -> int:
@@ -217,26 +220,37 @@ class _ContextLane:
 
 
 class Server:
-    """Continuous batching. policy "fifo": one batch, requests admitted in arrival order.
-    policy "split" (admission by estimated work): requests whose evaluation costs at most
-    `split_work` plane-pair units go to the batch, which takes `small_attempts` attempts per
-    call; the expensive ones, each of which fills the GPU alone, are solved one at a time on
-    single-simulation contexts (`attempts_per_tick` steps per call). Two host threads drive the
-    two on their own streams, so cheap requests are never held to the pace of an expensive one.
-    Within each the order is FIFO."""
+    """Continuous batching. policy "fifo": one batch. policy "split" (admission by estimated
+    work): requests whose evaluation costs at most `split_work` plane-pair units go to a cheap
+    batch, which takes `small_attempts` attempts per call; the expensive ones go to a second
+    batch (`attempts_per_tick` attempts per call), where they share launches with each other. Two
+    host threads drive the two batches on their own streams, so cheap requests are never held to
+    the pace of an expensive one and the two batches' kernels overlap. policy "split_context":
+    the expensive requests are instead solved one at a time on single-simulation contexts.
+    order: "sjf" admits a lane's waiting requests shortest estimated work first, "fifo" in
+    arrival order (a request that does not fit blocks the ones behind it)."""
 
     def __init__(self, capacity_vortices: int, max_slots: int, attempts_per_tick: int = 4,
                  device: int = 0, keep_states: bool = False, policy: str = "fifo",
-                 split_work: float = 2.0 ** 26, small_attempts: int = 16):
-        if policy not in ("fifo", "split"):
-            raise ValueError("policy must be fifo or split")
+                 split_work: float = 2.0 ** 26, small_attempts: int = 16, order: str = "fifo",
+                 expensive_fraction: float = 0.75):
+        if policy not in ("fifo", "split", "split_context"):
+            raise ValueError("policy must be fifo, split or split_context")
+        if order not in ("fifo", "sjf"):
+            raise ValueError("order must be fifo or sjf")
         self.policy = policy
+        self.order = order
         self.keep_states = keep_states
         self.split_work = split_work
         self.arrivals: list = []         # (arrival, rid, request) min-heap
         self.completions: list[Completion] = []
         if policy == "fifo":
             self.lanes = [_Lane(capacity_vortices, max_slots, device, attempts_per_tick)]
+        elif policy == "split":
+            # the arena (the HBM budget) is shared out: most room to the expensive requests
+            big = int(capacity_vortices * expensive_fraction)
+            self.lanes = [_Lane(capacity_vortices - big, max_slots, device, small_attempts),
+                          _Lane(big, max(max_slots // 4, 1), device, attempts_per_tick)]
         else:
             self.lanes = [_Lane(capacity_vortices, max_slots, device, small_attempts),
                           _ContextLane(device, attempts_per_tick)]
@@ -254,10 +268,18 @@ class Server:
         return self.lanes[0]
 
     def _route(self, now: float) -> None:
-        """Moves the requests that have arrived into their lane's ready list (arrival order)."""
+        """Moves the requests that have arrived into their lane's ready list (arrival order, or
+        shortest estimated work first with order "sjf")."""
+        touched = set()
         while self.arrivals and self.arrivals[0][0] <= now:
             item = heapq.heappop(self.arrivals)
-            self._lane_of(item[2]).ready.append(item)
+            lane = self._lane_of(item[2])
+            lane.ready.append(item)
+            touched.add(id(lane))
+        if self.order == "sjf":
+            for lane in self.lanes:
+                if id(lane) in touched:
+                    lane.ready.sort(key=lambda it: (work(it[2]), it[0], it[1]))
 
     def _admit_lane(self, lane: _Lane, now: float) -> int:
         admitted = 0
@@ -311,7 +333,7 @@ class Server:
         total = len(requests)
         if total == 0:
             pass
-        elif self.policy == "split":
+        elif self.policy in ("split", "split_context"):
             self._serve_threads(total, on_complete, clock, start)
         else:
             lane = self.lanes[0]

@@ -65,3 +65,30 @@ def test_parameter_validation_precedes_device_access():
     for make, message in cases:
         with pytest.raises(ValueError, match=message):
             make()
+
+
+def test_symmetric_tuning_table_round_trip_and_validation():
+    """The symmetric-form table (pv_set_symmetric_tuning) stores what it accepts, rejects entries
+    the planner cannot honour, and mode 0 restores the built-in plan. Host-only: no device."""
+    from pointvortex_b200 import autotune
+    periodic, plane, fp64, fp32c = 1, 0, 0, 1
+    saved = [autotune.get_symmetric_entry(periodic, fp64, 12),
+             autotune.get_symmetric_entry(plane, fp32c, 15)]
+    try:
+        autotune.set_symmetric_entry(periodic, fp64, 12, 2, 8, 0)
+        assert autotune.get_symmetric_entry(periodic, fp64, 12) == (2, 8, 0)
+        autotune.set_symmetric_entry(plane, fp32c, 15, 2, 0, 8)
+        assert autotune.get_symmetric_entry(plane, fp32c, 15) == (2, 0, 8)
+        autotune.set_symmetric_entry(periodic, fp64, 12, 1)
+        assert autotune.get_symmetric_entry(periodic, fp64, 12) == (1, 0, 0)
+        for bad in [(2, fp64, 12, 2, 0, 0),        # the disk has no symmetric form
+                    (periodic, fp32c, 12, 2, 8, 0),  # occupancy variants: periodic FP64 only
+                    (plane, fp64, 15, 2, 0, 3),      # plane targets: 4 or 8
+                    (periodic, fp64, 12, 3, 0, 0)]:  # modes 0..2
+            with pytest.raises(ValueError):
+                autotune.set_symmetric_entry(*bad)
+        autotune.set_symmetric_entry(periodic, fp64, 12, 0)
+        assert autotune.get_symmetric_entry(periodic, fp64, 12) == (0, 0, 0)
+    finally:
+        autotune.set_symmetric_entry(periodic, fp64, 12, *saved[0])
+        autotune.set_symmetric_entry(plane, fp32c, 15, *saved[1])

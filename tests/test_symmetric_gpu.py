@@ -225,3 +225,28 @@ def test_small_plane_fp32c_uses_the_ordered_kernel():
     k = pv.InfinitePlaneKernel(0.0, precision=_lib.PRECISION_FP32C)
     k.uploadDeviceState(pv.VortexSystem(x, y, g))
     assert not k.statePlan()["symmetric"]
+
+
+def test_tuning_table_changes_the_plan_and_keeps_parity(port):
+    """An entry of the symmetric-form table changes the plan the context chooses (pv_state_plan):
+    the ordered kernel instead of the symmetric form, or the periodic kernel built for 7 or 8 CTAs
+    per SM; every choice stays within the parity tolerance of the oracle."""
+    from pointvortex_b200 import autotune
+    x, y, g = ics.periodic_box(4096, 91, 2.0)
+    geo = Geometry("periodic", box_length_x=2.0, box_length_y=2.0)
+    ur, vr = port.evaluate(geo, x, y, g)
+    seen = []
+    saved = autotune.get_symmetric_entry(1, 0, 12)
+    try:
+        for entry in [(1,), (2, 7), (2, 8), (0,)]:
+            autotune.set_symmetric_entry(1, 0, 12, *entry)
+            k = pv.PeriodicBoxKernel(2.0, 2.0, 8)
+            k.uploadDeviceState(pv.VortexSystem(x, y, g))
+            plan = k.statePlan()
+            seen.append((plan["symmetric"], plan["symmetric_min_ctas"]))
+            f = k.evaluateDeviceState()
+            assert normalized_error(f.x, f.y, ur, vr).max() <= 1e-12, entry
+            k.close()
+    finally:
+        autotune.set_symmetric_entry(1, 0, 12, *saved)
+    assert seen == [(False, 0), (True, 7), (True, 8), (True, 0)]
