@@ -61,17 +61,38 @@ def alone_on_a_context(req: Request):
     return solver.state, solver.steps, solver.positions()
 
 
-def test_split_policy_results_equal_alone_results():
-    """Admission by estimated work (cheap requests batched, expensive ones on single-simulation
-    contexts, two threads) changes when a request runs, never what it computes."""
-    from pointvortex_b200.serve import _ContextLane
+def _serve_split(policy: str, order: str):
     reqs = poisson_stream(16, rate=400.0, seed=11, n_min=32, n_max=3000, t_end_range=(0.01, 0.02),
                           rtols=(1e-6, 1e-9), max_steps=30)
     server = Server(capacity_vortices=20000, max_slots=8, attempts_per_tick=2, keep_states=True,
-                    policy="split", split_work=2.0 ** 18, small_attempts=4)
+                    policy=policy, split_work=2.0 ** 18, small_attempts=4, order=order)
     summary = server.serve(reqs)
     server.close()
-    assert summary["requests"] == len(reqs) and summary["policy"] == "split"
+    assert summary["requests"] == len(reqs) and summary["policy"] == policy
+    return reqs, server
+
+
+def test_split_policy_results_equal_alone_results():
+    """Admission by estimated work (cheap and expensive requests in two batches, two threads and
+    streams, shortest estimated work first) changes when a request runs, never what it computes:
+    every result equals the request solved alone in a batch of its own."""
+    reqs, server = _serve_split("split", "sjf")
+    by_id = {c.rid: c for c in server.completions}
+    expensive = 0
+    for req in reqs:
+        c = by_id[req.rid]
+        expensive += server._lane_of(req) is server.lanes[1]
+        info, (x, y) = alone(req)
+        assert c.state == info.state and c.accepted_steps == info.acceptedSteps, req
+        assert np.array_equal(c.x, x) and np.array_equal(c.y, y), req
+        assert c.pairs > 0
+    assert 0 < expensive < len(reqs)
+
+
+def test_split_context_policy_results_equal_alone_results():
+    """The variant with the expensive requests on single-simulation contexts, one at a time."""
+    from pointvortex_b200.serve import _ContextLane
+    reqs, server = _serve_split("split_context", "fifo")
     by_id = {c.rid: c for c in server.completions}
     on_contexts = 0
     for req in reqs:
