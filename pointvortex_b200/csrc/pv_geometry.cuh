@@ -97,6 +97,15 @@ struct DiskPair {
         v = fma(c, dx, v);
         image(g, tx, ty, sx, sy, sg, u, v);
     }
+    // The direct term alone (j != i).
+    __device__ __forceinline__ static void direct(double tx, double ty, double sx, double sy,
+                                                  double sg, double &u, double &v) {
+        const double dx = tx - sx;
+        const double dy = ty - sy;
+        const double c = sg * rcp_refined(fma(dx, dx, dy * dy));
+        u = fma(-c, dy, u);
+        v = fma(c, dx, v);
+    }
     // The image term alone (every j, j == i included).
     __device__ __forceinline__ static void image(const GeometryConsts &g, double tx, double ty,
                                                  double sx, double sy, double sg, double &u,

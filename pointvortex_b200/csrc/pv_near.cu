@@ -1,8 +1,9 @@
 // pv_near.cu — the FP64 near-field pass of the FP32-compensated form.
 //
 // The FP32 kernels (pv_velocity32.cu, pv_symmetric.cu) leave out of their sums the pairs whose
-// terms are large -- periodic pairs closer than the near-field radius at their minimum image, and
-// disk wall images closer than it to their target -- and list them per target (pv_pair32.cuh).
+// terms are large -- periodic pairs closer than the near-field radius at their minimum image, disk
+// pairs closer than it, and disk wall images closer than it to their target -- and list them per
+// target (pv_pair32.cuh).
 // This pass, one thread per target, evaluates the listed terms with the FP64 pair functions of the
 // plain kernels (pv_geometry.cuh: the reference's truncated Weiss-McWilliams series,
 // src/compute.cpp:203-256, and its disk image term, src/compute.cpp:314-333), in increasing source
@@ -78,8 +79,10 @@ __global__ void __launch_bounds__(256) near_field_kernel(const NearPass a) {
         const size_t j = e[k] >> 1;
         if (e[k] & 1u)
             DiskPair::image(a.g, tx, ty, a.x[j], a.y[j], a.gs[j], du, dv);
-        else
+        else if (a.g.geometry == GEO_PERIODIC)
             PeriodicPair::pair<false>(a.g, tx, ty, a.x[j], a.y[j], a.gs[j], false, du, dv);
+        else
+            DiskPair::direct(tx, ty, a.x[j], a.y[j], a.gs[j], du, dv);
     }
     if (a.pr) {
         double2 r = a.pr[last];

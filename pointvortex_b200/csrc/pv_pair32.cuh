@@ -10,10 +10,11 @@
 // near the wall.
 //
 // Near field: an FP32 term carries ~1e-7 of its own size, so the few pairs whose terms are large
-// set the error of a sum. Pairs closer than the near-field radius -- the periodic pair at its
-// minimum-image distance, the disk image at its distance to the target -- are left out of the FP32
-// sum and listed (near_append) for the FP64 pass of pv_near.cu, which adds their exact FP64 terms
-// in index order. Callers promote FP32 partial sums into FP64 every kFlush sources.
+// set the error of a sum. Terms closer than the near-field radius -- the periodic pair at its
+// minimum-image distance, the disk's direct pair, and the disk image at its distance to the
+// target -- are left out of the FP32 sum and listed (near_append) for the FP64 pass of pv_near.cu,
+// which adds their exact FP64 terms in index order. The plane has no near field. Callers promote
+// FP32 partial sums into FP64 every kFlush sources.
 #pragma once
 
 #include "pv_common.cuh"
@@ -221,14 +222,19 @@ struct Plane32 {
     }
 };
 
+// Near-field verdicts of pair32: the pair's own term (periodic box, disk direct term) and the
+// source's wall image (disk), each left out of the FP32 sum when set.
+constexpr int kNearPair = 1;
+constexpr int kNearWall = 2;
+
 // One ordered pair in FP32: t the target, s the source (x_hi, y_hi, x_lo, y_lo), si the source's
 // wall image (disk only), sgf its scaled circulation. CHECK/self: the self pair (diagonal tiles)
-// has no direct term; the disk keeps its self image, as the reference does. Returns true when the
-// pair (periodic box) or the source's wall image (disk) is in the near field: that term is then
-// left out here and the caller lists the pair for the FP64 pass.
+// has no direct term; the disk keeps its self image, as the reference does. Returns which of the
+// pair's terms are in the near field (kNearPair, kNearWall): those are left out here and the
+// caller lists them for the FP64 pass. The plane has no near field.
 template <int GEO, bool CHECK>
-__device__ __forceinline__ bool pair32(const F32Geometry &f, const Target32 &t, const float4 s,
-                                       const float4 si, float sgf, bool self, float &u, float &v) {
+__device__ __forceinline__ int pair32(const F32Geometry &f, const Target32 &t, const float4 s,
+                                      const float4 si, float sgf, bool self, float &u, float &v) {
     const float dx = (t.xh - s.x) + (t.xl - s.z);
     const float dy = (t.yh - s.y) + (t.yl - s.w);
     if (GEO == GEO_PERIODIC) {
@@ -254,11 +260,17 @@ __device__ __forceinline__ bool pair32(const F32Geometry &f, const Target32 &t, 
         const float cv = skip ? 0.0f : sgf * sin_x * numer_v;
         u = fmaf(-cu, rcp_approx_f32(d0u * du), u);
         v = fmaf(cv, rcp_approx_f32(d0v * dv), v);
-        return near;
+        return near ? kNearPair : 0;
     }
     // direct Biot–Savart term (plane, and the disk's j != i term)
     const float r2 = fmaf(dx, dx, fmaf(dy, dy, GEO == GEO_INFINITE ? f.eps2 : 0.0f));
     float c = sgf * rcp_approx_f32(r2);
+    bool near = false;
+    if (GEO == GEO_DISK) {
+        near = r2 < f.near2 && !(CHECK && self);
+        if (near)
+            c = 0.0f;
+    }
     if (CHECK && self)
         c = 0.0f;
     u = fmaf(-c, dy, u);
@@ -267,13 +279,22 @@ __device__ __forceinline__ bool pair32(const F32Geometry &f, const Target32 &t, 
         const float ix = (t.xh - si.x) + (t.xl - si.z);
         const float iy = (t.yh - si.y) + (t.yl - si.w);
         const float ri2 = fmaf(ix, ix, iy * iy);
-        const bool near = ri2 < f.near2;
-        const float ci = near ? 0.0f : sgf * rcp_approx_f32(ri2);
+        const bool near_wall = ri2 < f.near2;
+        const float ci = near_wall ? 0.0f : sgf * rcp_approx_f32(ri2);
         u = fmaf(ci, iy, u);
         v = fmaf(-ci, ix, v);
-        return near;
+        return (near ? kNearPair : 0) | (near_wall ? kNearWall : 0);
     }
-    return false;
+    return 0;
+}
+
+// Lists the near terms a pair32 verdict left out, under target ti and source j.
+__device__ __forceinline__ void list_near(const NearLists &lists, int verdict, size_t ti,
+                                          unsigned j) {
+    if (verdict & kNearPair)
+        near_append(lists, ti, j);
+    if (verdict & kNearWall)
+        near_append(lists, ti, j | kNearImage);
 }
 
 }  // namespace f32

@@ -16,9 +16,9 @@
 //   * the disk's wall image of each source is staged as a position (the vortex -Gamma at
 //     R^2 s/|s|^2, computed in FP64 once per CTA and tile), so the image term is a direct term
 //     from an accurately known point instead of the cancelling 1 - t.s/R^2 form;
-//   * near field: the periodic pairs closer than the near-field radius (minimum image) and the
-//     disk images closer than it to their target are left out of the FP32 sums and listed for the
-//     FP64 pass (pv_near.cu), which adds their exact terms.
+//   * near field: the periodic pairs closer than the near-field radius (minimum image), the disk's
+//     direct pairs closer than it and the disk images closer than it to their target are left out
+//     of the FP32 sums and listed for the FP64 pass (pv_near.cu), which adds their exact terms.
 //
 // What remains is the FP32 rounding of each far term (a few ulp, ~1e-7 of the term); the velocity
 // error against the FP64 oracle is that, summed over sources (reported by the parity tests).
@@ -135,8 +135,7 @@ __global__ void __launch_bounds__(B) velocity32_kernel(const EvalArgs a) {
         }
         __syncthreads();
         const bool diagonal = j0 < blk1 && blk0 < j0 + cnt;
-        // a near pair (or wall image) is left to the FP64 pass: list it under its target
-        const unsigned flag = GEO == GEO_DISK ? kNearImage : 0u;
+        // near terms are left to the FP64 pass: listed under their target
         for (int jb = 0; jb < cnt; jb += kFlush) {
             const int je = min(cnt, jb + kFlush);
             if (diagonal) {
@@ -146,10 +145,12 @@ __global__ void __launch_bounds__(B) velocity32_kernel(const EvalArgs a) {
                     const float4 si = GEO == GEO_DISK ? s_fi[j] : sf;
                     const float gf = s_gf[j];
 #pragma unroll
-                    for (int k = 0; k < T; ++k)
-                        if (pair32<GEO, true>(f, tg[k], sf, si, gf, ti[k] == j0 + j, u[k], v[k]) &&
-                            a.near.count && ti[k] < blk1)
-                            near_append(a.near, ti[k], static_cast<unsigned>(j0 + j) | flag);
+                    for (int k = 0; k < T; ++k) {
+                        const int near =
+                            pair32<GEO, true>(f, tg[k], sf, si, gf, ti[k] == j0 + j, u[k], v[k]);
+                        if (near && a.near.count && ti[k] < blk1)
+                            list_near(a.near, near, ti[k], static_cast<unsigned>(j0 + j));
+                    }
                 }
             } else {
 #pragma unroll 2
@@ -158,10 +159,11 @@ __global__ void __launch_bounds__(B) velocity32_kernel(const EvalArgs a) {
                     const float4 si = GEO == GEO_DISK ? s_fi[j] : sf;
                     const float gf = s_gf[j];
 #pragma unroll
-                    for (int k = 0; k < T; ++k)
-                        if (pair32<GEO, false>(f, tg[k], sf, si, gf, false, u[k], v[k]) &&
-                            a.near.count && ti[k] < blk1)
-                            near_append(a.near, ti[k], static_cast<unsigned>(j0 + j) | flag);
+                    for (int k = 0; k < T; ++k) {
+                        const int near = pair32<GEO, false>(f, tg[k], sf, si, gf, false, u[k], v[k]);
+                        if (near && a.near.count && ti[k] < blk1)
+                            list_near(a.near, near, ti[k], static_cast<unsigned>(j0 + j));
+                    }
                 }
             }
 #pragma unroll

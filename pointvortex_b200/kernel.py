@@ -354,8 +354,9 @@ class VelocityKernel:
         self._check(lib.pv_set_profiling(self._ctx, int(bool(enabled))))
 
     def setNearField(self, radius: float = -1.0) -> None:
-        """Near-field radius of the FP32-compensated form (pv_set_near_field): periodic pairs and
-        disk wall images closer than it are evaluated in FP64; -1 the default, 0 none."""
+        """Near-field radius of the FP32-compensated form (pv_set_near_field): periodic pairs,
+        disk pairs and disk wall images closer than it are evaluated in FP64; -1 the default, 0
+        none."""
         self._check(lib.pv_set_near_field(self._ctx, float(radius)))
 
     @property
