@@ -223,7 +223,6 @@ typedef struct pv_plan_info {
     int chunk;              /* ordered kernel: sources per work item */
     int symmetric_min_ctas; /* symmetric form: the kernel built for this many CTAs per SM (0: default) */
     int symmetric_targets;  /* symmetric form: targets per lane off the diagonal */
-    uint32_t split_items;   /* symmetric form: items two warps may share at the end of the queue */
 } pv_plan_info;
 pv_status pv_state_plan(const pv_context *ctx, pv_plan_info *info);
 

@@ -68,8 +68,7 @@ REINJECTION = {"none": 0, "independent": 1, "paired": 2}
 class PvPlanInfo(ctypes.Structure):
     _fields_ = [("symmetric", ctypes.c_int), ("rows", ctypes.c_int),
                 ("targets_per_thread", ctypes.c_int), ("chunk", ctypes.c_int),
-                ("symmetric_min_ctas", ctypes.c_int), ("symmetric_targets", ctypes.c_int),
-                ("split_items", ctypes.c_uint32)]
+                ("symmetric_min_ctas", ctypes.c_int), ("symmetric_targets", ctypes.c_int)]
 
 
 TRAJECTORY_ROW_MAX = 192   # PV_TRAJECTORY_ROW_MAX

@@ -95,7 +95,6 @@ struct pv_context {
     cudaGraphExec_t attempt_graph = nullptr; // one DOPRI5 attempt with a valid FSAL derivative
     SymmetricPlan sym{};             // one evaluation per unordered pair (when planned)
     DeviceArray sym_items, sym_counter;
-    DeviceArray sym_split, sym_flags;  // the join of the split items (scratch, flags)
     DeviceArray rk4_barrier;         // arrival counter of the cooperative RK4 steps' grid barrier
     int sym_items_blocks = 0;        // the block count the item table was built for
     DeviceArray inv_scratch, inv_out;
@@ -154,8 +153,7 @@ struct pv_context {
         for (DeviceArray *a : {&x, &y, &gamma, &gs, &p0x, &p0y, &p1x, &p1y, &pu, &pv, &inv_scratch,
                                &inv_out, &cand, &ex, &ey, &eg, &egs, &eu, &ev, &epu, &epv,
                                &removed_index, &fmt_stage, &fmt_len, &fmt_block, &fmt_out,
-                               &sym_items, &sym_counter, &rk4_barrier, &near_count, &near_slot,
-                               &sym_split, &sym_flags})
+                               &sym_items, &sym_counter, &rk4_barrier, &near_count, &near_slot})
             a->release();
         for (int s = 0; s < 7; ++s) {
             kx[s].release();
@@ -479,8 +477,6 @@ pv_status launch_eval(pv_context *c, const double *px, const double *py) {
                         reinterpret_cast<const unsigned *>(c->sym_items.p),
                         reinterpret_cast<unsigned *>(c->sym_counter.p),
                         reinterpret_cast<double2 *>(c->pu.p), padded(c->n), c->gc, lists,
-                        c->sym.split ? reinterpret_cast<double2 *>(c->sym_split.p) : nullptr,
-                        c->sym.split ? reinterpret_cast<unsigned *>(c->sym_flags.p) : nullptr,
                         c->stream);
                 }));
         if (near) {
@@ -578,8 +574,7 @@ std::vector<const void *> attempt_key(const pv_context *c) {
                                        c->dipole_configured && c->dipole.removal ? 1 : 0)),
                                    reinterpret_cast<const void *>(
                                        static_cast<uintptr_t>(c->wait_limit)),
-                                   c->near_count.p, c->near_slot.p, c->sym_split.p,
-                                   c->sym_flags.p};
+                                   c->near_count.p, c->near_slot.p};
     uint64_t near_bits;
     std::memcpy(&near_bits, &c->gc.near2, sizeof near_bits);
     k.push_back(reinterpret_cast<const void *>(static_cast<uintptr_t>(near_bits)));
@@ -622,12 +617,6 @@ pv_status ensure_state_capacity(pv_context *c, size_t n) {
         PV_CUDA(c, c->sym_items.ensure((items.size() + 1) / 2));
         PV_CUDA(c, c->sym_counter.ensure(1));
         PV_CUDA(c, cudaMemsetAsync(c->sym_counter.p, 0, 2 * sizeof(unsigned), c->stream));
-        if (c->sym.split) {
-            PV_CUDA(c, c->sym_split.ensure(static_cast<size_t>(c->sym.split) * 256));
-            PV_CUDA(c, c->sym_flags.ensure((c->sym.split + 1) / 2));
-            PV_CUDA(c, cudaMemsetAsync(c->sym_flags.p, 0, c->sym_flags.cap * sizeof(double),
-                                       c->stream));
-        }
         PV_CUDA(c, cudaMemcpyAsync(c->sym_items.p, items.data(), items.size() * sizeof(unsigned),
                                    cudaMemcpyHostToDevice, c->stream));
         PV_CUDA(c, cudaStreamSynchronize(c->stream));
@@ -1818,7 +1807,6 @@ pv_status pv_state_plan(const pv_context *ctx, pv_plan_info *info) {
     info->chunk = ctx->plan.chunk;
     info->symmetric_min_ctas = ctx->sym.enabled() ? ctx->sym.min_ctas : 0;
     info->symmetric_targets = ctx->sym.enabled() ? ctx->sym.targets : 0;
-    info->split_items = ctx->sym.enabled() ? ctx->sym.split : 0u;
     return PV_OK;
 }
 

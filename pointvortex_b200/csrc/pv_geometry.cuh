@@ -140,8 +140,6 @@ struct DiskPair {
 // sinh, cosh, sin and cos of x^/2 and y^/2 come from one shared series (|x^/2| <= pi/2).
 struct PeriodicPair {
     // Images m != 0 of one axis as num/den + rest. half_hat = x^/2 (the m = +-6 window test).
-    // The first image pair starts the fraction as itself (num = pair_num, den = pair_den: what
-    // adding it to 0/1 would give, exactly).
     __device__ __forceinline__ static void image_sum(const GeometryConsts &g, double half_hat,
                                                      double ch, double sh, double c, double &num,
                                                      double &den, double &rest) {
@@ -151,15 +149,14 @@ struct PeriodicPair {
         const double m2c = -2.0 * c;
         num = 0.0;
         den = 1.0;
-        if (g.m_exact >= 1) {
-            num = fma(ch, g.two_cosh_m[1], m2c);
-            den = fma(q, g.cosh_m[1], p + g.sinh2_m[1]);
-        }
-        if (g.m_exact >= 2) {
-            const double pair_num = fma(ch, g.two_cosh_m[2], m2c);
-            const double pair_den = fma(q, g.cosh_m[2], p + g.sinh2_m[2]);
-            num = fma(pair_num, den, num * pair_den);
-            den *= pair_den;
+#pragma unroll
+        for (int m = 1; m <= 2; ++m) {
+            if (m <= g.m_exact) {
+                const double pair_num = fma(ch, g.two_cosh_m[m], m2c);
+                const double pair_den = fma(q, g.cosh_m[m], p + g.sinh2_m[m]);
+                num = fma(pair_num, den, num * pair_den);
+                den *= pair_den;
+            }
         }
         const double ch2x = fma(2.0, ch2, -1.0); // cosh 2x^
         rest = fma(ch, g.k1, c * ch2x * g.k2);

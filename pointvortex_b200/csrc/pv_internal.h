@@ -80,7 +80,6 @@ struct SymmetricPlan {
     int precision = 0;   // PV_PRECISION_FP64 or PV_PRECISION_FP32C
     int geometry = 0;    // GEO_PERIODIC or GEO_INFINITE
     int targets = 1;     // targets per lane off the diagonal (the plane: 4 or 8)
-    unsigned split = 0;  // items at the end of the queue that two warps may share (halves)
     int min_ctas = 0;    // periodic FP64: the kernel built for 7 or 8 CTAs per SM (0: default)
     bool enabled() const { return a > 0; }
 };
@@ -100,13 +99,10 @@ void symmetric_items(const SymmetricPlan &p, unsigned *out);
 // counter: two words, zero before the first launch; each launch leaves them zero again.
 // near: the near-field lists of the FP32C periodic kernel (pv_pair32.cuh; count == nullptr:
 // none); the other kernels ignore it.
-// split_scratch (128 double2 per split item) and split_flags (zero before the first launch; every
-// launch leaves them zero): the join of the split items (p.split); null: no item is split.
 cudaError_t launch_symmetric(const double *x, const double *y, const double *gs, size_t n,
                              const SymmetricPlan &p, const unsigned *items, unsigned *counter,
                              double2 *rows, size_t stride, const GeometryConsts &g,
-                             const f32::NearLists &near, double2 *split_scratch,
-                             unsigned *split_flags, cudaStream_t stream);
+                             const f32::NearLists &near, cudaStream_t stream);
 
 // ---- FP32C near field (pv_near.cu) -----------------------------------------------------------
 // The FP64 pass over the pairs an FP32 evaluation listed (f32::NearLists): their exact terms are

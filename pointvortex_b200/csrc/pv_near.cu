@@ -4,11 +4,12 @@
 // terms are large -- periodic pairs closer than the near-field radius at their minimum image, disk
 // pairs closer than it, and disk wall images closer than it to their target -- and list them per
 // target (pv_pair32.cuh).
-// This pass, one thread per target, evaluates the listed terms with the FP64 pair functions of the
+// This pass, one warp per target, evaluates the listed terms with the FP64 pair functions of the
 // plain kernels (pv_geometry.cuh: the reference's truncated Weiss-McWilliams series,
-// src/compute.cpp:203-256, and its disk image term, src/compute.cpp:314-333), in increasing source
-// order, and adds their sum to the target's entry of the evaluation's last partial row, which the
-// stage kernel then reduces with the others in fixed order: results stay deterministic.
+// src/compute.cpp:203-256, its direct term and its disk image term, src/compute.cpp:286-336),
+// sorted by source, adds them in a fixed tree, and adds that sum to the target's entry of the
+// evaluation's last partial row, which the stage kernel then reduces with the others in fixed
+// order: results stay deterministic.
 //
 // A target with more listed pairs than its slots hold is evaluated whole in FP64 instead (every
 // source, the same pair functions): its partial rows are replaced by that one sum.
@@ -23,28 +24,49 @@ namespace pvb {
 
 namespace {
 
-__global__ void __launch_bounds__(256) near_field_kernel(const NearPass a) {
+constexpr int kNearWarps = 8;  // targets per CTA: one warp each
+
+// Sum of a warp's values in a fixed tree (lane 0 receives it): the same order on every run.
+__device__ __forceinline__ double warp_sum(double v) {
+    for (int off = 16; off > 0; off >>= 1)
+        v += __shfl_down_sync(0xffffffffu, v, off);
+    return v;
+}
+
+// One warp per target. The listed entries (at most 32: one per lane) are sorted across the warp
+// (a bitonic network over the lanes), each lane evaluates one in FP64, and the warp adds the terms
+// in a fixed tree; so the sum does not depend on the order in which the FP32 kernel listed them.
+__global__ void __launch_bounds__(kNearWarps * 32) near_field_kernel(const NearPass a) {
     pdl_enter();
-    const size_t i = a.t_begin + blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x;
+    const int lane = threadIdx.x & 31;
+    const size_t i = a.t_begin + static_cast<size_t>(blockIdx.x) * kNearWarps + (threadIdx.x >> 5);
     if (i >= a.t_end)
-        return;
-    const unsigned count = a.lists.count[i];
+        return;  // the whole warp
+    unsigned count = 0;
+    if (lane == 0) {
+        count = a.lists.count[i];
+        if (count)
+            a.lists.count[i] = 0u;
+    }
+    count = __shfl_sync(0xffffffffu, count, 0);
     if (count == 0)
         return;
-    a.lists.count[i] = 0u;
     const double tx = a.x[i], ty = a.y[i];
     const size_t local = i - a.t_begin;
     const size_t last = static_cast<size_t>(a.rows - 1) * a.stride + local;
     double du = 0.0, dv = 0.0;
     if (count > static_cast<unsigned>(f32::kNearSlots)) {
-        // overflow: the whole target in FP64, in source order; its FP32 rows are dropped
-        for (size_t j = 0; j < a.n; ++j) {
+        // overflow: the whole target in FP64, the lanes striding over the sources; its FP32 rows
+        // are dropped
+        for (size_t j = lane; j < a.n; j += 32) {
             if (a.g.geometry == GEO_PERIODIC)
                 PeriodicPair::pair<true>(a.g, tx, ty, a.x[j], a.y[j], a.gs[j], j == i, du, dv);
             else
                 DiskPair::pair<true>(a.g, tx, ty, a.x[j], a.y[j], a.gs[j], j == i, du, dv);
         }
-        for (int r = 0; r + 1 < a.rows; ++r) {
+        du = warp_sum(du);
+        dv = warp_sum(dv);
+        for (int r = lane; r + 1 < a.rows; r += 32) {
             const size_t e = static_cast<size_t>(r) * a.stride + local;
             if (a.pr) {
                 a.pr[e] = make_double2(0.0, 0.0);
@@ -53,45 +75,49 @@ __global__ void __launch_bounds__(256) near_field_kernel(const NearPass a) {
                 a.pv[e] = 0.0;
             }
         }
-        if (a.pr) {
-            a.pr[last] = make_double2(du, dv);
-        } else {
-            a.pu[last] = du;
-            a.pv[last] = dv;
+        if (lane == 0) {
+            if (a.pr) {
+                a.pr[last] = make_double2(du, dv);
+            } else {
+                a.pu[last] = du;
+                a.pv[last] = dv;
+            }
         }
         return;
     }
-    // the listed sources in increasing order (insertion sort of at most kNearSlots entries; a
-    // source's image sorts after the source itself)
-    unsigned e[f32::kNearSlots];
-    const unsigned *slot = a.lists.slot + i * f32::kNearSlots;
-    for (unsigned k = 0; k < count; ++k) {
-        const unsigned v = slot[k];
-        const unsigned key = (v & ~f32::kNearImage) * 2u + (v >> 31);
-        unsigned m = k;
-        while (m > 0 && e[m - 1] > key) {
-            e[m] = e[m - 1];
-            --m;
-        }
-        e[m] = key;
+    // the listed entries in increasing (source, image) order across the lanes; a source's image
+    // sorts after the source itself, empty lanes last
+    unsigned key = 0xffffffffu;
+    if (lane < static_cast<int>(count)) {
+        const unsigned v = a.lists.slot[i * f32::kNearSlots + lane];
+        key = (v & ~f32::kNearImage) * 2u + (v >> 31);
     }
-    for (unsigned k = 0; k < count; ++k) {
-        const size_t j = e[k] >> 1;
-        if (e[k] & 1u)
+    for (int k = 2; k <= 32; k <<= 1)
+        for (int j = k >> 1; j > 0; j >>= 1) {
+            const unsigned other = __shfl_xor_sync(0xffffffffu, key, j);
+            key = (((lane & j) == 0) == ((lane & k) == 0)) ? min(key, other) : max(key, other);
+        }
+    if (key != 0xffffffffu) {
+        const size_t j = key >> 1;
+        if (key & 1u)
             DiskPair::image(a.g, tx, ty, a.x[j], a.y[j], a.gs[j], du, dv);
         else if (a.g.geometry == GEO_PERIODIC)
             PeriodicPair::pair<false>(a.g, tx, ty, a.x[j], a.y[j], a.gs[j], false, du, dv);
         else
             DiskPair::direct(tx, ty, a.x[j], a.y[j], a.gs[j], du, dv);
     }
-    if (a.pr) {
-        double2 r = a.pr[last];
-        r.x += du;
-        r.y += dv;
-        a.pr[last] = r;
-    } else {
-        a.pu[last] += du;
-        a.pv[last] += dv;
+    du = warp_sum(du);
+    dv = warp_sum(dv);
+    if (lane == 0) {
+        if (a.pr) {
+            double2 r = a.pr[last];
+            r.x += du;
+            r.y += dv;
+            a.pr[last] = r;
+        } else {
+            a.pu[last] += du;
+            a.pv[last] += dv;
+        }
     }
 }
 
@@ -101,8 +127,8 @@ cudaError_t launch_near_field(const NearPass &a, cudaStream_t stream) {
     if (a.t_end <= a.t_begin || !a.lists.count || a.rows < 1)
         return cudaSuccess;
     const size_t targets = a.t_end - a.t_begin;
-    const unsigned grid = static_cast<unsigned>((targets + 255) / 256);
-    return launch_pdl(near_field_kernel, dim3(grid), dim3(256), 0, stream, a);
+    const unsigned grid = static_cast<unsigned>((targets + kNearWarps - 1) / kNearWarps);
+    return launch_pdl(near_field_kernel, dim3(grid), dim3(kNearWarps * 32), 0, stream, a);
 }
 
 double default_near_radius(const GeometryConsts &g, size_t n) {

@@ -51,86 +51,28 @@ __device__ __forceinline__ void release_queue(unsigned *counter) {
     }
 }
 
-// One half of a split item (I, J), I < J, blocks of 32: the rotation steps [16 h, 16 h + 16) of
-// its tile, so that two warps can share the item at the end of the queue. Each half leaves its
-// target and reaction sums in the item's scratch slot; the half that finishes second adds the two
-// in fixed order (half 0 + half 1) and writes the item's partial-row entries, then clears the
-// flag for the next launch. The partial sums do not depend on which half finished first.
-template <class P>
-__device__ __forceinline__ void half_item(const double *__restrict__ x,
-                                          const double *__restrict__ y,
-                                          const double *__restrict__ gs, size_t n, unsigned I,
-                                          unsigned J, unsigned h, double2 *scratch,
-                                          unsigned *flag, double2 *__restrict__ pr, size_t stride,
-                                          const GeometryConsts &g) {
-    const int lane = threadIdx.x & 31;
-    const size_t ti = static_cast<size_t>(I) * 32 + lane;  // I < J: block I is full
-    const int home = (lane + 16 * static_cast<int>(h)) & 31;  // this lane's first source
-    const size_t sj = static_cast<size_t>(J) * 32 + home;
-    const int s_ok = sj < n ? 1 : 0;
-    const double tx = x[ti], ty = y[ti], tg = P::kScale * gs[ti];
-    const double sx = s_ok ? x[sj] : 0.0, sy = s_ok ? y[sj] : 0.0;
-    const double sg = s_ok ? P::kScale * gs[sj] : 0.0;
-    double u = 0.0, v = 0.0, ru = 0.0, rv = 0.0;
-    sym::react_tile<P, 16>(g, tx, ty, tg, true, sx, sy, sg, s_ok, u, v, ru, rv);
-    // after 16 rotations the lane holds the reaction of source (home + 16) & 31
-    const int rs = (home + 16) & 31;
-    double2 *mine = scratch + h * 64;
-    __stcg(mine + lane, make_double2(u, v));
-    __stcg(mine + 32 + rs, make_double2(ru, rv));
-    __threadfence();
-    __syncwarp();
-    unsigned first = 0;
-    if (lane == 0)
-        first = atomicAdd(flag, 1u);
-    first = __shfl_sync(0xffffffffu, first, 0);
-    if (first == 0)
-        return;  // the other half adds the two
-    __threadfence();
-    const double2 ta = __ldcg(scratch + lane), tb = __ldcg(scratch + 64 + lane);
-    pr[static_cast<size_t>(J) * stride + ti] = make_double2(ta.x + tb.x, ta.y + tb.y);
-    const size_t sh = static_cast<size_t>(J) * 32 + lane;
-    if (sh < n) {
-        const double2 ra = __ldcg(scratch + 32 + lane), rb = __ldcg(scratch + 96 + lane);
-        pr[static_cast<size_t>(I) * stride + sh] = make_double2(ra.x + rb.x, ra.y + rb.y);
-    }
-    if (lane == 0)
-        *flag = 0u;
-}
-
 // P: the pair kernel (sym::PeriodicSym, sym::PlaneSym). T: targets per lane in the items off the
 // diagonal (a multiple of T sub-blocks per block); diagonal items hold one target per lane.
-// Tickets [0, n_whole) are whole items; with blocks of 32 the last n_split items may be taken as
-// two halves each (tickets n_whole + 2 q + h), which shortens the end of the queue.
-// MINB: resident CTAs per SM the register allocation must allow (1: the compiler's choice; the
-// periodic kernel is also built for 7 and 8, fewer registers for more warps to hide latency).
-template <class P, int T, int MINB = 1>
+// MINB: resident CTAs per SM the register allocation must allow (0: the compiler's own choice;
+// the periodic kernel is also built for 7 and 8, fewer registers for more warps to hide latency).
+template <class P, int T, int MINB = 0>
 __global__ void __launch_bounds__(kThreads, MINB)
     symmetric_kernel(const double *__restrict__ x, const double *__restrict__ y,
                      const double *__restrict__ gs, size_t n, int a,
-                     const unsigned *__restrict__ items, unsigned n_whole, unsigned n_split,
-                     unsigned *counter, double2 *__restrict__ pr, size_t stride, GeometryConsts g,
-                     double2 *split_scratch, unsigned *split_flags) {
+                     const unsigned *__restrict__ items, unsigned n_items, unsigned *counter,
+                     double2 *__restrict__ pr, size_t stride, GeometryConsts g) {
     extern __shared__ double2 reaction_smem[];
     pdl_enter();
     const int lane = threadIdx.x & 31;
     double2 *reaction = reaction_smem + (threadIdx.x >> 5) * a * 32;  // this warp's sources
     const size_t block_len = static_cast<size_t>(32) * a;
-    const unsigned n_tickets = n_whole + 2 * n_split;
     for (;;) {
         unsigned item = 0;
         if (lane == 0)
             item = atomicAdd(counter, 1u);
         item = __shfl_sync(0xffffffffu, item, 0);
-        if (item >= n_tickets)
+        if (item >= n_items)
             break;
-        if (item >= n_whole) {
-            const unsigned q = (item - n_whole) >> 1, h = (item - n_whole) & 1u;
-            const unsigned packed = items[n_whole + q];
-            half_item<P>(x, y, gs, n, packed >> 16, packed & 0xffffu, h, split_scratch + q * 128,
-                         split_flags + q, pr, stride, g);
-            continue;
-        }
         const unsigned packed = items[item];
         const unsigned I = packed >> 16, J = packed & 0xffffu;
         const bool diagonal = I == J;
@@ -519,12 +461,6 @@ SymmetricPlan plan_symmetric(size_t n, int sm_count, int precision, int geometry
             p.geometry = geometry;
             p.targets = targets;
             p.grid = std::max(sm_count, 1) * resident_ctas(a, kernel_of(p));
-            // FP64, blocks of 32, one target per lane: the last wave's worth of items (one per
-            // warp) may be split in halves between two warps
-            if (a == 1 && targets == 1 && precision == PV_PRECISION_FP64) {
-                const unsigned off_diagonal = p.items - static_cast<unsigned>(blocks);
-                p.split = std::min(off_diagonal, static_cast<unsigned>(p.grid) * (kThreads / 32));
-            }
             return p;
         }
     }
@@ -532,7 +468,7 @@ SymmetricPlan plan_symmetric(size_t n, int sm_count, int precision, int geometry
 }
 
 void symmetric_items(const SymmetricPlan &p, unsigned *out) {
-    // the diagonal items (evaluated one-sided, never split) first, then I < J row by row
+    // the diagonal items (evaluated one-sided) first, then I < J row by row
     size_t k = 0;
     for (unsigned i = 0; i < static_cast<unsigned>(p.blocks); ++i)
         out[k++] = (i << 16) | i;
@@ -544,10 +480,7 @@ void symmetric_items(const SymmetricPlan &p, unsigned *out) {
 cudaError_t launch_symmetric(const double *x, const double *y, const double *gs, size_t n,
                              const SymmetricPlan &p, const unsigned *items, unsigned *counter,
                              double2 *rows, size_t stride, const GeometryConsts &g,
-                             const f32::NearLists &near, double2 *split_scratch,
-                             unsigned *split_flags, cudaStream_t stream) {
-    const unsigned n_split = split_scratch && split_flags ? p.split : 0u;
-    const unsigned n_whole = p.items - n_split;
+                             const f32::NearLists &near, cudaStream_t stream) {
     const size_t smem = static_cast<size_t>(kThreads / 32) * p.a * 32 * sizeof(double2);
     const dim3 grid(static_cast<unsigned>(p.grid)), block(kThreads);
     switch (kernel_of(p)) {
@@ -556,12 +489,10 @@ cudaError_t launch_symmetric(const double *x, const double *y, const double *gs,
                           gs, n, p.a, items, p.items, counter, rows, stride, g, near);
     case SYM_PLANE:
         return launch_pdl(symmetric_kernel<sym::PlaneSym, kPlaneTargets>, grid, block, smem,
-                          stream, x, y, gs, n, p.a, items, n_whole, n_split, counter, rows, stride, g,
-                          split_scratch, split_flags);
+                          stream, x, y, gs, n, p.a, items, p.items, counter, rows, stride, g);
     case SYM_PLANE_WIDE:
         return launch_pdl(symmetric_kernel<sym::PlaneSym, kPlaneTargetsWide>, grid, block, smem,
-                          stream, x, y, gs, n, p.a, items, n_whole, n_split, counter, rows, stride, g,
-                          split_scratch, split_flags);
+                          stream, x, y, gs, n, p.a, items, p.items, counter, rows, stride, g);
     case SYM_PLANE32:
         return launch_pdl(symmetric32_kernel<f32::Plane32, kPlaneTargets>, grid, block, smem,
                           stream, x, y, gs, n, p.a, items, p.items, counter, rows, stride, g,
@@ -572,16 +503,13 @@ cudaError_t launch_symmetric(const double *x, const double *y, const double *gs,
                           near);
     case SYM_PERIODIC_7:
         return launch_pdl(symmetric_kernel<sym::PeriodicSym, 1, 7>, grid, block, smem, stream, x, y,
-                          gs, n, p.a, items, n_whole, n_split, counter, rows, stride, g,
-                          split_scratch, split_flags);
+                          gs, n, p.a, items, p.items, counter, rows, stride, g);
     case SYM_PERIODIC_8:
         return launch_pdl(symmetric_kernel<sym::PeriodicSym, 1, 8>, grid, block, smem, stream, x, y,
-                          gs, n, p.a, items, n_whole, n_split, counter, rows, stride, g,
-                          split_scratch, split_flags);
+                          gs, n, p.a, items, p.items, counter, rows, stride, g);
     default:
         return launch_pdl(symmetric_kernel<sym::PeriodicSym, 1>, grid, block, smem, stream, x, y,
-                          gs, n, p.a, items, n_whole, n_split, counter, rows, stride, g,
-                          split_scratch, split_flags);
+                          gs, n, p.a, items, p.items, counter, rows, stride, g);
     }
 }
 

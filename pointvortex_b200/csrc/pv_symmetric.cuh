@@ -48,17 +48,16 @@ struct PlaneSym {
 };
 
 // Targets (tx, ty, tg) against the sources held in the lanes (sx, sy, sg and their reactions
-// ru, rv); adds the targets' sums to u, v and the sources' to ru, rv. After STEPS = 32 rotations
-// the sources are back at home; after 16 (half a tile) each is 16 lanes on.
+// ru, rv); adds the targets' sums to u, v and the sources' to ru, rv. Sources end at home.
 // FULL: all 32 targets and sources exist (every tile but the last block's), no predicates.
-template <class P, bool FULL, int STEPS = 32>
+template <class P, bool FULL>
 __device__ __forceinline__ void react_tile_t(const GeometryConsts &g, double tx, double ty,
                                              double tg, bool t_ok, double sx, double sy,
                                              double sg, int s_ok, double &u, double &v,
                                              double &ru, double &rv) {
     const int next = (threadIdx.x + 1) & 31;
 #pragma unroll 2
-    for (int k = 0; k < STEPS; ++k) {
+    for (int k = 0; k < 32; ++k) {
         if (FULL || (t_ok && s_ok)) {
             double ku, kv;
             P::values(g, tx, ty, sx, sy, ku, kv);
@@ -77,15 +76,15 @@ __device__ __forceinline__ void react_tile_t(const GeometryConsts &g, double tx,
     }
 }
 
-template <class P = PeriodicSym, int STEPS = 32>
+template <class P = PeriodicSym>
 __device__ __forceinline__ void react_tile(const GeometryConsts &g, double tx, double ty,
                                            double tg, bool t_ok, double sx, double sy, double sg,
                                            int s_ok, double &u, double &v, double &ru,
                                            double &rv) {
     if (__all_sync(0xffffffffu, t_ok && s_ok))
-        react_tile_t<P, true, STEPS>(g, tx, ty, tg, t_ok, sx, sy, sg, s_ok, u, v, ru, rv);
+        react_tile_t<P, true>(g, tx, ty, tg, t_ok, sx, sy, sg, s_ok, u, v, ru, rv);
     else
-        react_tile_t<P, false, STEPS>(g, tx, ty, tg, t_ok, sx, sy, sg, s_ok, u, v, ru, rv);
+        react_tile_t<P, false>(g, tx, ty, tg, t_ok, sx, sy, sg, s_ok, u, v, ru, rv);
 }
 
 // T targets per lane (T sub-blocks of targets) against one sub-block of 32 sources, every target

@@ -332,7 +332,7 @@ class VelocityKernel:
         return {"symmetric": bool(info.symmetric), "rows": info.rows,
                 "targets_per_thread": info.targets_per_thread, "chunk": info.chunk,
                 "symmetric_min_ctas": info.symmetric_min_ctas,
-                "symmetric_targets": info.symmetric_targets, "split_items": info.split_items}
+                "symmetric_targets": info.symmetric_targets}
 
     @property
     def evaluationCount(self) -> int:

@@ -263,7 +263,7 @@ class Server:
         heapq.heappush(self.arrivals, (req.arrival, req.rid, req))
 
     def _lane_of(self, req: Request):
-        if self.policy == "split" and work(req) > self.split_work:
+        if self.policy in ("split", "split_context") and work(req) > self.split_work:
             return self.lanes[1]
         return self.lanes[0]
 
