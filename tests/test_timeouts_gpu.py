@@ -13,7 +13,7 @@ import numpy as np
 import pytest
 
 import pointvortex_b200 as pv
-from conftest import normalized_error, position_error
+from conftest import normalized_error, position_error  # noqa: F401
 from oracle.pyoracle import Geometry
 from pointvortex_b200 import ics
 
@@ -58,8 +58,30 @@ def test_velocity_timeout_inside_a_step_leaves_the_state(port):
     k.setWaitLimits()
     k.deviceRk4Step(1e-3)
     sx, sy = download(k, x.size, g)
+    # the same step on a context whose waits never ran out: bit for bit
+    fresh = pv.InfinitePlaneKernel(0.0)
+    fresh.uploadDeviceState(pv.VortexSystem(x, y, g))
+    fresh.deviceRk4Step(1e-3)
+    fx, fy = download(fresh, x.size, g)
+    assert np.array_equal(sx, fx) and np.array_equal(sy, fy)
+    # and the reference's step, within the teacher-forced tolerance (1e-12 dt max|u|)
+    u, v = port.evaluate(Geometry("infinite"), x, y, g)
     rx, ry = port.stepper(Geometry("infinite"), x.size).rk4_step(x, y, g, 1e-3)
-    assert position_error(sx, sy, rx, ry) <= 1e-13
+    tol = 1e-12 * 1e-3 * float(np.hypot(u, v).max())
+    assert float(np.max(np.hypot(sx - rx, sy - ry))) <= tol
+
+
+def plain_steps(x, y, g, steps):
+    """The states after 1..steps RK4 steps (dt 1e-3) on a context whose waits keep their
+    defaults."""
+    k = pv.InfinitePlaneKernel(0.0)
+    k.uploadDeviceState(pv.VortexSystem(x, y, g))
+    out = [(x.copy(), y.copy())]
+    for _ in range(steps):
+        k.deviceRk4Step(1e-3)
+        out.append(download(k, x.size, g))
+    k.close()
+    return out
 
 
 def test_cooperative_barrier_timeout_is_agreed(port):
@@ -67,8 +89,11 @@ def test_cooperative_barrier_timeout_is_agreed(port):
     geo = Geometry("infinite")
     x, y, g = ics.infinite_plane(1024, 33)
     k = pv.InfinitePlaneKernel(0.0)
-    ref = port.stepper(geo, x.size)
-    rx, ry = ref.rk4_step(x, y, g, 1e-3)
+    rx, ry = plain_steps(x, y, g, 1)[1]
+    u, v = port.evaluate(geo, x, y, g)
+    ox, oy = port.stepper(geo, x.size).rk4_step(x, y, g, 1e-3)
+    # the undisturbed GPU step against the reference's: the teacher-forced tolerance
+    assert float(np.max(np.hypot(rx - ox, ry - oy))) <= 1e-12 * 1e-3 * float(np.hypot(u, v).max())
     timeouts = 0
     for _ in range(8):
         k.uploadDeviceState(pv.VortexSystem(x, y, g))
@@ -80,26 +105,22 @@ def test_cooperative_barrier_timeout_is_agreed(port):
             timeouts += 1
             sx, sy = download(k, x.size, g)
             assert np.array_equal(sx, x) and np.array_equal(sy, y)
-        else:  # every CTA arrived before any gave up: an ordinary step
+        else:  # every CTA arrived before any gave up: an ordinary step, bit for bit
             sx, sy = download(k, x.size, g)
-            assert position_error(sx, sy, rx, ry) <= 1e-13
+            assert np.array_equal(sx, rx) and np.array_equal(sy, ry)
     # a barrier that gives up at once breaks unless all 148 CTAs arrive within the same instant
     assert timeouts >= 1
     k.setWaitLimits()
     k.uploadDeviceState(pv.VortexSystem(x, y, g))
     k.deviceRk4Step(1e-3)
     sx, sy = download(k, x.size, g)
-    assert position_error(sx, sy, rx, ry) <= 1e-13
+    assert np.array_equal(sx, rx) and np.array_equal(sy, ry)
 
 
 def test_cooperative_advance_timeout_stops_at_a_whole_step(port):
-    geo = Geometry("infinite")
     x, y, g = ics.infinite_plane(1024, 34)
     steps = 4
-    ref = port.stepper(geo, x.size)
-    states = [(x, y)]
-    for _ in range(steps):
-        states.append(ref.rk4_step(*states[-1], g, 1e-3))
+    states = plain_steps(x, y, g, steps)  # the cooperative launch is bit for bit the same
     k = pv.InfinitePlaneKernel(0.0)
     for _ in range(4):
         k.uploadDeviceState(pv.VortexSystem(x, y, g))
@@ -111,9 +132,11 @@ def test_cooperative_advance_timeout_stops_at_a_whole_step(port):
             assert TIMEOUT in str(exc)
             done = None
         sx, sy = download(k, x.size, g)
-        errors = [position_error(sx, sy, a, b) for a, b in states]
-        best = int(np.argmin(errors))
-        assert errors[best] <= 1e-12, errors  # the state is that of a whole number of steps
+        # the state is that of a whole number of steps, bit for bit
+        matches = [i for i, (a, b) in enumerate(states)
+                   if np.array_equal(sx, a) and np.array_equal(sy, b)]
+        assert len(matches) == 1, [position_error(sx, sy, a, b) for a, b in states]
+        best = matches[0]
         if done is not None:
             assert best == steps
         else:
