@@ -347,7 +347,8 @@ pv_status pv_evaluate_device_noalloc(const pv_params *params, const double *x, c
 #define PV_KERNEL_INVARIANTS 3 /* moments, Hamiltonian tiles, final sum */
 #define PV_KERNEL_DIPOLE 4     /* close-dipole candidate scan and survivor compaction */
 #define PV_KERNEL_OUTPUT 5     /* text formatting of trajectory / checkpoint rows */
-#define PV_KERNEL_KINDS 6
+#define PV_KERNEL_NEAR 6       /* FP32C: the FP64 pass over the near-field pairs */
+#define PV_KERNEL_KINDS 7
 
 typedef struct pv_kernel_stats {
     uint64_t launches[PV_KERNEL_KINDS];       /* kernels launched by this context */

@@ -104,7 +104,7 @@ class PvBatchTotals(ctypes.Structure):
                 ("occupied_slots", ctypes.c_uint32)]
 
 
-KERNEL_KINDS = ("velocity", "stage", "accept", "invariants", "dipole", "output")
+KERNEL_KINDS = ("velocity", "stage", "accept", "invariants", "dipole", "output", "near")
 
 
 class PvKernelStats(ctypes.Structure):

@@ -107,7 +107,7 @@ def _time_evaluation(geometry: str, precision: int, n: int, evals: int) -> float
         k.evaluateDeviceState()
     st = k.kernelStats()
     k.close()
-    return (st["velocity"][2] + st["stage"][2]) / max(st["stage"][1], 1)
+    return (st["velocity"][2] + st["near"][2] + st["stage"][2]) / max(st["stage"][1], 1)
 
 
 # candidates of the symmetric-form table: (mode, min_ctas, targets)

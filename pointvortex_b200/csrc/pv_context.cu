@@ -482,7 +482,7 @@ pv_status launch_eval(pv_context *c, const double *px, const double *py) {
         if (near) {
             np.pr = reinterpret_cast<double2 *>(c->pu.p);
             np.rows = c->sym.blocks;
-            PV_CUDA(c, counted(c, PV_KERNEL_VELOCITY, 1,
+            PV_CUDA(c, counted(c, PV_KERNEL_NEAR, 1,
                                [&] { return launch_near_field(np, c->stream); }));
         }
         ++c->evaluations;
@@ -515,7 +515,7 @@ pv_status launch_eval(pv_context *c, const double *px, const double *py) {
         np.pu = c->pu.p;
         np.pv = c->pv.p;
         np.rows = c->plan.num_chunks;
-        PV_CUDA(c, counted(c, PV_KERNEL_VELOCITY, 1, [&] { return launch_near_field(np, c->stream); }));
+        PV_CUDA(c, counted(c, PV_KERNEL_NEAR, 1, [&] { return launch_near_field(np, c->stream); }));
     }
     ++c->evaluations;
     return PV_OK;
@@ -707,7 +707,7 @@ pv_status evaluate_host(pv_context *c, const double *x, const double *y, const d
         np.stride = stride;
         np.rows = plan.num_chunks;
         np.g = a.g;
-        PV_CUDA(c, counted(c, PV_KERNEL_VELOCITY, 1, [&] { return launch_near_field(np, c->stream); }));
+        PV_CUDA(c, counted(c, PV_KERNEL_NEAR, 1, [&] { return launch_near_field(np, c->stream); }));
     }
     StageArgs s{};
     s.n = nt;
@@ -1306,7 +1306,9 @@ pv_status pv_dopri5_step(pv_context *ctx, double dt, double absolute_tolerance,
             for (const auto &t : ctx->graph_timers)
                 ctx->pending.push_back(t);
             ctx->evaluations += 6;
-            ctx->launches[PV_KERNEL_VELOCITY] += near_field_used(ctx) ? 12 : 6;
+            ctx->launches[PV_KERNEL_VELOCITY] += 6;
+            if (near_field_used(ctx))
+                ctx->launches[PV_KERNEL_NEAR] += 6;
             ctx->launches[PV_KERNEL_STAGE] += 7;
             ctx->launches[PV_KERNEL_ACCEPT] += 1;
             if (prescan)
