@@ -420,8 +420,11 @@ __device__ __forceinline__ void run_item32(const GeometryConsts &g, const double
                     const float4 si = GEO == GEO_DISK ? s_fi[j] : sf;
                     const float gf = s_gf[j];
 #pragma unroll
-                    for (int q = 0; q < T; ++q)  // ensembles: no near field (nothing is listed)
-                        f32::pair32<GEO, true>(f, tg[q], sf, si, gf, ti[q] == j0 + j, u[q], v[q]);
+                    for (int q = 0; q < T; ++q) {  // ensembles: no near field (nothing is listed)
+                        bool np, nw;
+                        f32::pair32<GEO, true>(f, tg[q], sf, si, gf, ti[q] == j0 + j, u[q], v[q], np,
+                                               nw);
+                    }
                 }
             } else {
 #pragma unroll 2
@@ -430,8 +433,10 @@ __device__ __forceinline__ void run_item32(const GeometryConsts &g, const double
                     const float4 si = GEO == GEO_DISK ? s_fi[j] : sf;
                     const float gf = s_gf[j];
 #pragma unroll
-                    for (int q = 0; q < T; ++q)
-                        f32::pair32<GEO, false>(f, tg[q], sf, si, gf, false, u[q], v[q]);
+                    for (int q = 0; q < T; ++q) {
+                        bool np, nw;
+                        f32::pair32<GEO, false>(f, tg[q], sf, si, gf, false, u[q], v[q], np, nw);
+                    }
                 }
             }
 #pragma unroll

@@ -222,19 +222,19 @@ struct Plane32 {
     }
 };
 
-// Near-field verdicts of pair32: the pair's own term (periodic box, disk direct term) and the
-// source's wall image (disk), each left out of the FP32 sum when set.
-constexpr int kNearPair = 1;
-constexpr int kNearWall = 2;
-
 // One ordered pair in FP32: t the target, s the source (x_hi, y_hi, x_lo, y_lo), si the source's
 // wall image (disk only), sgf its scaled circulation. CHECK/self: the self pair (diagonal tiles)
-// has no direct term; the disk keeps its self image, as the reference does. Returns which of the
-// pair's terms are in the near field (kNearPair, kNearWall): those are left out here and the
-// caller lists them for the FP64 pass. The plane has no near field.
+// has no direct term; the disk keeps its self image, as the reference does. near_pair (the
+// pair's own term: periodic box, disk direct term) and near_wall (the source's wall image, disk)
+// tell which terms are in the near field: those are left out here, and the caller lists them for
+// the FP64 pass. Returns near_pair || near_wall (one test in the caller's common path). The plane
+// has no near field.
 template <int GEO, bool CHECK>
-__device__ __forceinline__ int pair32(const F32Geometry &f, const Target32 &t, const float4 s,
-                                      const float4 si, float sgf, bool self, float &u, float &v) {
+__device__ __forceinline__ bool pair32(const F32Geometry &f, const Target32 &t, const float4 s,
+                                       const float4 si, float sgf, bool self, float &u, float &v,
+                                       bool &near_pair, bool &near_wall) {
+    near_pair = false;
+    near_wall = false;
     const float dx = (t.xh - s.x) + (t.xl - s.z);
     const float dy = (t.yh - s.y) + (t.yl - s.w);
     if (GEO == GEO_PERIODIC) {
@@ -260,16 +260,15 @@ __device__ __forceinline__ int pair32(const F32Geometry &f, const Target32 &t, c
         const float cv = skip ? 0.0f : sgf * sin_x * numer_v;
         u = fmaf(-cu, rcp_approx_f32(d0u * du), u);
         v = fmaf(cv, rcp_approx_f32(d0v * dv), v);
-        return near ? kNearPair : 0;
+        near_pair = near;
+        return near;
     }
     // direct Biot–Savart term (plane, and the disk's j != i term)
     const float r2 = fmaf(dx, dx, fmaf(dy, dy, GEO == GEO_INFINITE ? f.eps2 : 0.0f));
     float c = sgf * rcp_approx_f32(r2);
-    bool near = false;
     if (GEO == GEO_DISK) {
-        near = r2 < f.near2 && !(CHECK && self);
-        if (near)
-            c = 0.0f;
+        near_pair = r2 < f.near2 && !(CHECK && self);
+        c = near_pair ? 0.0f : c;
     }
     if (CHECK && self)
         c = 0.0f;
@@ -279,21 +278,21 @@ __device__ __forceinline__ int pair32(const F32Geometry &f, const Target32 &t, c
         const float ix = (t.xh - si.x) + (t.xl - si.z);
         const float iy = (t.yh - si.y) + (t.yl - si.w);
         const float ri2 = fmaf(ix, ix, iy * iy);
-        const bool near_wall = ri2 < f.near2;
+        near_wall = ri2 < f.near2;
         const float ci = near_wall ? 0.0f : sgf * rcp_approx_f32(ri2);
         u = fmaf(ci, iy, u);
         v = fmaf(-ci, ix, v);
-        return (near ? kNearPair : 0) | (near_wall ? kNearWall : 0);
+        return near_pair || near_wall;
     }
-    return 0;
+    return false;
 }
 
-// Lists the near terms a pair32 verdict left out, under target ti and source j.
-__device__ __forceinline__ void list_near(const NearLists &lists, int verdict, size_t ti,
-                                          unsigned j) {
-    if (verdict & kNearPair)
+// Lists the near terms pair32 left out, under target ti and source j.
+__device__ __forceinline__ void list_near(const NearLists &lists, bool near_pair, bool near_wall,
+                                          size_t ti, unsigned j) {
+    if (near_pair)
         near_append(lists, ti, j);
-    if (verdict & kNearWall)
+    if (near_wall)
         near_append(lists, ti, j | kNearImage);
 }
 

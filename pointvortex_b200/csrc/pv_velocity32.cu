@@ -146,10 +146,11 @@ __global__ void __launch_bounds__(B) velocity32_kernel(const EvalArgs a) {
                     const float gf = s_gf[j];
 #pragma unroll
                     for (int k = 0; k < T; ++k) {
-                        const int near =
-                            pair32<GEO, true>(f, tg[k], sf, si, gf, ti[k] == j0 + j, u[k], v[k]);
-                        if (near && a.near.count && ti[k] < blk1)
-                            list_near(a.near, near, ti[k], static_cast<unsigned>(j0 + j));
+                        bool np, nw;
+                        if (pair32<GEO, true>(f, tg[k], sf, si, gf, ti[k] == j0 + j, u[k], v[k], np,
+                                              nw) &&
+                            a.near.count && ti[k] < blk1)
+                            list_near(a.near, np, nw, ti[k], static_cast<unsigned>(j0 + j));
                     }
                 }
             } else {
@@ -160,9 +161,10 @@ __global__ void __launch_bounds__(B) velocity32_kernel(const EvalArgs a) {
                     const float gf = s_gf[j];
 #pragma unroll
                     for (int k = 0; k < T; ++k) {
-                        const int near = pair32<GEO, false>(f, tg[k], sf, si, gf, false, u[k], v[k]);
-                        if (near && a.near.count && ti[k] < blk1)
-                            list_near(a.near, near, ti[k], static_cast<unsigned>(j0 + j));
+                        bool np, nw;
+                        if (pair32<GEO, false>(f, tg[k], sf, si, gf, false, u[k], v[k], np, nw) &&
+                            a.near.count && ti[k] < blk1)
+                            list_near(a.near, np, nw, ti[k], static_cast<unsigned>(j0 + j));
                     }
                 }
             }
