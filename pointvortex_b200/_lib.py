@@ -109,9 +109,9 @@ KERNEL_KINDS = ("velocity", "stage", "accept", "invariants", "dipole", "output",
 
 class PvKernelStats(ctypes.Structure):
     _fields_ = [
-        ("launches", ctypes.c_uint64 * 6),
-        ("timed_launches", ctypes.c_uint64 * 6),
-        ("milliseconds", ctypes.c_double * 6),
+        ("launches", ctypes.c_uint64 * len(KERNEL_KINDS)),
+        ("timed_launches", ctypes.c_uint64 * len(KERNEL_KINDS)),
+        ("milliseconds", ctypes.c_double * len(KERNEL_KINDS)),
     ]
 
 

@@ -168,16 +168,52 @@ __device__ __forceinline__ double exact_remainder(double a, double L, double inv
 // grouped by powers t^(4k+r) so that the hyperbolic and circular functions share every term:
 //   sinh t = t (E1 + t^2 O1),  sin t = t (E1 - t^2 O1),  cosh t = E0 + t^2 O0,  cos t = E0 - t^2 O0
 // with E1 = sum_k w^k/(4k+1)!, O1 = sum_k w^k/(4k+3)!, E0 = sum_k w^k/(4k)!, O0 = sum_k w^k/(4k+2)!,
-// w = t^4 in [0, (pi/2)^4]. Each of the four is the Taylor polynomial of one degree more,
-// economized by Lanczos' method (its top term traded for the shifted Chebyshev polynomial of that
-// degree on [0, (pi/2)^4], computed in exact rational arithmetic): E1 and E0 keep five
-// coefficients, O1 and O0 four. Relative error of the polynomials over the interval: E1 3.2e-19,
-// E0 6.7e-18, O1 5.3e-16, O0 3.4e-15; of the functions (double evaluation against 30-digit
-// references): sinh, sin below 6e-16, cosh below 1.7e-15, cos below 4.1e-15 absolute. Horner in w.
-// Every output keeps its exact parity in t (odd: t times a polynomial in w; even: a polynomial in
-// w and t^2), which the once-per-unordered-pair kernels rely on.
+// w = t^4 in [0, (pi/2)^4]. Horner in w. Every output keeps its exact parity in t (odd: t times a
+// polynomial in w; even: a polynomial in w and t^2), which the once-per-unordered-pair kernels rely
+// on.
+//
+// sinh_cosh_sin_cos: the Taylor polynomials, truncated after the w^5 (E) and w^4 (O) terms; the
+// first omitted term is below 2e-17 relative. The Hamiltonian uses it: its periodic image product
+// adds up to 2M + 1 = 129 factors whose logarithms accumulate the series' error.
 __device__ __forceinline__ void sinh_cosh_sin_cos(double t, double &sh, double &ch, double &s,
                                                   double &c) {
+    const double t2 = t * t, w = t2 * t2;
+    double e1 = fma(w, 1.9572941063391263e-20, 2.8114572543455206e-15); // 1/21!, 1/17!
+    e1 = fma(w, e1, 1.6059043836821613e-10);                             // 1/13!
+    e1 = fma(w, e1, 2.7557319223985893e-06);                             // 1/9!
+    e1 = fma(w, e1, 0.008333333333333333);                             // 1/5!
+    e1 = fma(w, e1, 1.0);
+    double o1 = fma(w, 8.22063524662433e-18, 7.647163731819816e-13); // 1/19!, 1/15!
+    o1 = fma(w, o1, 2.505210838544172e-08);                             // 1/11!
+    o1 = fma(w, o1, 0.0001984126984126984);                             // 1/7!
+    o1 = fma(w, o1, 0.16666666666666666);                             // 1/3!
+    double e0 = fma(w, 4.110317623312165e-19, 4.779477332387385e-14); // 1/20!, 1/16!
+    e0 = fma(w, e0, 2.08767569878681e-09);                             // 1/12!
+    e0 = fma(w, e0, 2.48015873015873e-05);                             // 1/8!
+    e0 = fma(w, e0, 0.041666666666666664);                             // 1/4!
+    e0 = fma(w, e0, 1.0);
+    double o0 = fma(w, 1.5619206968586225e-16, 1.1470745597729725e-11); // 1/18!, 1/14!
+    o0 = fma(w, o0, 2.755731922398589e-07);                             // 1/10!
+    o0 = fma(w, o0, 0.001388888888888889);                             // 1/6!
+    o0 = fma(w, o0, 0.5);                                                // 1/2!
+    const double t3 = t * t2, te1 = t * e1;
+    sh = fma(t3, o1, te1);
+    s = fma(-t3, o1, te1);
+    ch = fma(t2, o0, e0);
+    c = fma(-t2, o0, e0);
+}
+
+// sinh_cosh_sin_cos_economized: one coefficient fewer per polynomial, for the velocity's pair
+// terms. Each of the four is the Taylor polynomial of one degree more economized by Lanczos'
+// method (its top term traded for the shifted Chebyshev polynomial of that degree on
+// [0, (pi/2)^4], computed in exact rational arithmetic): E1 and E0 keep five coefficients, O1 and
+// O0 four. Relative error of the polynomials over the interval: E1 3.2e-19, E0 6.7e-18, O1
+// 5.3e-16, O0 3.4e-15; of the functions (double evaluation against 30-digit references): sinh,
+// sin below 6e-16 relative, cosh below 1.7e-15 relative, cos below 4.1e-15 absolute. In a pair
+// term cos(t) only scales sin(x^) = 2 sin(t) cos(t), a factor of the term, so the term's error
+// stays at the 1e-15 level, three orders below the parity tolerance.
+__device__ __forceinline__ void sinh_cosh_sin_cos_economized(double t, double &sh, double &ch,
+                                                             double &s, double &c) {
     const double t2 = t * t, w = t2 * t2;
     double e1 = fma(w, 2.8117551578451845e-15, 1.6059043678126643e-10);
     e1 = fma(w, e1, 2.7557319224020396e-06);

@@ -182,8 +182,8 @@ struct PeriodicPair {
         const double hx = g.half_wave * exact_remainder(tx - sx, g.lx, g.inv_lx, g.half_lx);
         const double hy = g.half_wave * exact_remainder(ty - sy, g.ly, g.inv_ly, g.half_ly);
         double shx, chx, snx, csx, shy, chy, sny, csy;
-        sinh_cosh_sin_cos(hx, shx, chx, snx, csx);
-        sinh_cosh_sin_cos(hy, shy, chy, sny, csy);
+        sinh_cosh_sin_cos_economized(hx, shx, chx, snx, csx);
+        sinh_cosh_sin_cos_economized(hy, shy, chy, sny, csy);
         const double cosh_x = fma(2.0 * shx, shx, 1.0); // cosh x^ = 1 + 2 sinh^2(x^/2)
         const double cosh_y = fma(2.0 * shy, shy, 1.0);
         const double cos_x = fma(-2.0 * snx, snx, 1.0); // cos x^ = 1 - 2 sin^2(x^/2)

@@ -92,3 +92,12 @@ def test_symmetric_tuning_table_round_trip_and_validation():
     finally:
         autotune.set_symmetric_entry(periodic, fp64, 12, *saved[0])
         autotune.set_symmetric_entry(plane, fp32c, 15, *saved[1])
+
+
+def test_kernel_stats_struct_matches_the_header():
+    """The ctypes mirror of pv_kernel_stats holds PV_KERNEL_KINDS entries per array."""
+    from pointvortex_b200 import _lib
+    text = open(HEADER).read()
+    kinds = int(re.search(r"#define PV_KERNEL_KINDS (\d+)", text).group(1))
+    assert len(_lib.KERNEL_KINDS) == kinds
+    assert ctypes.sizeof(_lib.PvKernelStats) == kinds * 3 * 8
