@@ -793,8 +793,8 @@ def run_other_configs() -> dict:
 
 def run_fp32c_curve(reps: int = 10) -> dict:
     """Error and speed of the FP32-compensated form against its near-field radius, on the periodic
-    workload state (N = 4096, symmetric kernel) and the disk workload state (N = 16384, Gaussian
-    circulations, ordered kernel): per radius (in units of the mean spacing; 0 = no near field) the
+    workload state (N = 4096, symmetric kernel), a periodic state of N = 16384, and the disk
+    workload state (N = 16384, Gaussian circulations, ordered kernel): per radius (in units of the mean spacing; 0 = no near field) the
     per-vortex error against the FP64 kernel (itself within 1e-12 of the oracle) and the time per
     evaluation, next to the FP64 kernel's."""
     import torch
@@ -803,6 +803,8 @@ def run_fp32c_curve(reps: int = 10) -> dict:
     out = {}
     cases = [("periodic_n4096", lambda p: pv.PeriodicBoxKernel(LENGTH, LENGTH, LAYERS, precision=p),
               ics.workload_state("periodic_dopri5_n4096"), LENGTH / np.sqrt(4096)),
+             ("periodic_n16384", lambda p: pv.PeriodicBoxKernel(LENGTH, LENGTH, LAYERS, precision=p),
+              ics.periodic_box(16384, 20240104, LENGTH), LENGTH / np.sqrt(16384)),
              ("disk_n16384", lambda p: pv.DiskKernel(1.0, precision=p),
               ics.workload_state("disk_rk4_n16384"), np.sqrt(np.pi / 16384))]
 

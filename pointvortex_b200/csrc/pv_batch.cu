@@ -984,7 +984,10 @@ pv_status launch_velocity_stage(pv_batch *b, int stage, int only_without_fsal, i
         a.items = b->d_items;
         a.n_items = b->n_items;
         a.counter = b->d_counters + 2 * counter;
-        const unsigned grid = static_cast<unsigned>(std::max(1, b->sm_count * b->resident));
+        // a persistent grid of one wave, or fewer CTAs than that when the queue is short (a
+        // small ensemble: CTAs that would only find the queue empty cost launch time)
+        const unsigned grid = static_cast<unsigned>(
+            std::max(1u, std::min(static_cast<unsigned>(b->sm_count * b->resident), b->n_items)));
         batch_velocity_kernel<PV_PRECISION_FP64><<<grid, kBlock, 0, b->stream>>>(a);
         PVB_CUDA(b, cudaGetLastError());
     }
@@ -992,7 +995,8 @@ pv_status launch_velocity_stage(pv_batch *b, int stage, int only_without_fsal, i
         a.items = b->d_items + b->n_items;
         a.n_items = b->n_items32;
         a.counter = b->d_counters + 2 * counter + 1;
-        const unsigned grid = static_cast<unsigned>(std::max(1, b->sm_count * b->resident32));
+        const unsigned grid = static_cast<unsigned>(std::max(
+            1u, std::min(static_cast<unsigned>(b->sm_count * b->resident32), b->n_items32)));
         batch_velocity_kernel<PV_PRECISION_FP32C><<<grid, kBlock, 0, b->stream>>>(a);
         PVB_CUDA(b, cudaGetLastError());
     }
