@@ -830,6 +830,10 @@ struct pv_batch {
     uint64_t attempts = 0, evaluations_pairs = 0;
     cudaGraphExec_t attempt_graph = nullptr; // one captured attempt for the current tables
     bool use_graph = true;
+    // attempts launched directly since the tables last changed: the attempt is captured as a
+    // graph only once they have stayed the same for kCaptureAfter attempts, so that a stream of
+    // admissions and retirements does not pay a capture and an instantiation for each change
+    unsigned unchanged_attempts = 0;
 
     ~pv_batch() {
         if (attempt_graph)
@@ -1032,6 +1036,9 @@ pv_status enqueue_attempt(pv_batch *b) {
     PVB_CUDA(b, cudaGetLastError());
     return PV_OK;
 }
+
+// Attempts with unchanged tables after which the attempt is captured as a graph.
+constexpr unsigned kCaptureAfter = 8;
 
 // Captures one attempt (17 nodes for the current work queue and slice table) as a CUDA graph, so
 // that each further attempt is one graph launch.
@@ -1276,15 +1283,22 @@ pv_status pv_batch_advance(pv_batch *b, uint32_t attempts, uint32_t *running) {
         if (b->tables_dirty) {
             if ((st = rebuild_tables(b)) != PV_OK)
                 return st;
-            if ((st = capture_attempt(b)) != PV_OK)
-                return st;
+            if (b->attempt_graph) {
+                cudaGraphExecDestroy(b->attempt_graph);
+                b->attempt_graph = nullptr;
+            }
+            b->unchanged_attempts = 0;
         }
         if (b->n_items + b->n_items32 == 0)
             break;
+        if (!b->attempt_graph && b->unchanged_attempts >= kCaptureAfter &&
+            (st = capture_attempt(b)) != PV_OK)
+            return st;
         if (b->attempt_graph)
             PVB_CUDA(b, cudaGraphLaunch(b->attempt_graph, b->stream));
         else if ((st = enqueue_attempt(b)) != PV_OK)
             return st;
+        ++b->unchanged_attempts;
         ++b->attempts;
     }
     PVB_CUDA(b, cudaMemcpyAsync(b->h_ctl, b->d_ctl, b->max_sims * sizeof(SimControl),
