@@ -146,11 +146,10 @@ __device__ __forceinline__ void finish_target(const StageArgs &a, size_t i, doub
 }
 
 // WIDE: many partial rows (the symmetric kernel's). A block then covers kWideTargets targets with
-// 256 / kWideTargets row groups (eight consecutive targets: each row group reads one 128-byte line
-// of interleaved rows): thread (group, t) sums rows group, group + groups, ...
+// 256 / kWideTargets row groups: thread (group, t) sums rows group, group + groups, ...
 // (coalesced over the targets), and the threads of group 0 add the group sums in fixed order.
 // Otherwise one thread per target sums its rows in order.
-constexpr int kWideTargets = 8;
+constexpr int kWideTargets = 16;
 constexpr int kWideGroups = 256 / kWideTargets;
 
 template <int MODE, bool WIDE>
@@ -176,19 +175,19 @@ __global__ void __launch_bounds__(256) stage_kernel(const StageArgs a) {
             const size_t i = base + lane;
             double su = 0.0, sv = 0.0;
             if (i < a.n && a.pr) {
-                // interleaved rows: one 16-byte load per row, four rows in flight per thread
+                // interleaved rows: one 16-byte load per row, eight rows in flight per thread
                 // before they are added (in row order, so the sum does not depend on timing)
                 const double2 *col = a.pr + i;
                 const size_t step = static_cast<size_t>(kWideGroups) * a.stride;
                 int c = group;
-                for (; c + 3 * kWideGroups < a.num_chunks; c += 4 * kWideGroups) {
-                    double2 r[4];
+                for (; c + 7 * kWideGroups < a.num_chunks; c += 8 * kWideGroups) {
+                    double2 r[8];
                     const double2 *p = col + static_cast<size_t>(c) * a.stride;
 #pragma unroll
-                    for (int q = 0; q < 4; ++q)
+                    for (int q = 0; q < 8; ++q)
                         r[q] = __ldcg(p + q * step);
 #pragma unroll
-                    for (int q = 0; q < 4; ++q) {
+                    for (int q = 0; q < 8; ++q) {
                         su += r[q].x;
                         sv += r[q].y;
                     }
