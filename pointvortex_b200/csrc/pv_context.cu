@@ -366,6 +366,10 @@ pv_status make_consts(const pv_params &p, GeometryConsts &g, std::string &messag
             hi = std::nextafter(hi, 1e300);
         while (!(std::fabs(hi + s6) <= 40.0))
             hi = std::nextafter(hi, -1e300);
+        if (hi != -lo) { // rounding is symmetric, so the windows are; the kernels rely on it
+            message = "internal error: asymmetric m = 6 image window";
+            return PV_ERROR_RUNTIME;
+        }
         g.lo6 = lo;
         g.hi6 = hi;
         g.lo6h = 0.5 * lo;

@@ -145,26 +145,30 @@ struct PeriodicPair {
                                                      double &den, double &rest) {
         const double ch2 = ch * ch;
         const double p = fma(c, c, ch2);   // C^2 + c^2
-        const double q = -2.0 * c * ch;    // -2 c C
         const double m2c = -2.0 * c;
+        const double q = m2c * ch;         // -2 c C
+        // m = 1 starts the fraction, m = 2 joins it: num/den = pn1/pd1 + pn2/pd2
         num = 0.0;
         den = 1.0;
-#pragma unroll
-        for (int m = 1; m <= 2; ++m) {
-            if (m <= g.m_exact) {
-                const double pair_num = fma(ch, g.two_cosh_m[m], m2c);
-                const double pair_den = fma(q, g.cosh_m[m], p + g.sinh2_m[m]);
-                num = fma(pair_num, den, num * pair_den);
-                den *= pair_den;
-            }
+        if (g.m_exact >= 1) {
+            num = fma(ch, g.two_cosh_m[1], m2c);
+            den = fma(q, g.cosh_m[1], p + g.sinh2_m[1]);
         }
-        const double ch2x = fma(2.0, ch2, -1.0); // cosh 2x^
-        rest = fma(ch, g.k1, c * ch2x * g.k2);
+        if (g.m_exact >= 2) {
+            const double pair_num = fma(ch, g.two_cosh_m[2], m2c);
+            const double pair_den = fma(q, g.cosh_m[2], p + g.sinh2_m[2]);
+            num = fma(pair_num, den, num * pair_den);
+            den *= pair_den;
+        }
+        // m = 3..5: 2u C + 2u^2 c cosh 2x^ summed over u = sech(2 pi m), with
+        // k2 cosh 2x^ = k2 (2 C^2 - 1) as one fma
+        rest = fma(ch, g.k1, c * fma(2.0 * g.k2, ch2, -g.k2));
         if (g.has6) {
-            const bool plus = half_hat >= g.lo6h;
-            const bool minus = half_hat <= g.hi6h;
-            const double e = (plus ? ch + sh : 0.0) + (minus ? ch - sh : 0.0);
-            rest = fma(g.k6, e, rest);
+            // the windows x^ >= lo6 (m = +6) and x^ <= hi6 (m = -6), with lo6 = -hi6 < 0: both
+            // hold for |x^| <= hi6, giving (C + S) + (C - S) = 2C; beyond, only the one on x^'s
+            // side, giving C + |S|. Even in x^ like the two terms.
+            const double add = fabs(half_hat) <= g.hi6h ? ch : fabs(sh);
+            rest = fma(g.k6, ch + add, rest);
         }
     }
 
@@ -184,16 +188,19 @@ struct PeriodicPair {
         double shx, chx, snx, csx, shy, chy, sny, csy;
         sinh_cosh_sin_cos_economized(hx, shx, chx, snx, csx);
         sinh_cosh_sin_cos_economized(hy, shy, chy, sny, csy);
-        const double cosh_x = fma(2.0 * shx, shx, 1.0); // cosh x^ = 1 + 2 sinh^2(x^/2)
-        const double cosh_y = fma(2.0 * shy, shy, 1.0);
-        const double cos_x = fma(-2.0 * snx, snx, 1.0); // cos x^ = 1 - 2 sin^2(x^/2)
-        const double cos_y = fma(-2.0 * sny, sny, 1.0);
+        const double tshx = 2.0 * shx, tshy = 2.0 * shy;    // scaling by 2 is exact
+        const double nsnx = -2.0 * snx, nsny = -2.0 * sny;
+        const double cosh_x = fma(tshx, shx, 1.0); // cosh x^ = 1 + 2 sinh^2(x^/2)
+        const double cosh_y = fma(tshy, shy, 1.0);
+        const double cos_x = fma(nsnx, snx, 1.0);  // cos x^ = 1 - 2 sin^2(x^/2)
+        const double cos_y = fma(nsny, sny, 1.0);
         const double sin_x = HALF_SINE ? snx * csx : 2.0 * snx * csx; // sin x^ (or half)
         const double sin_y = HALF_SINE ? sny * csy : 2.0 * sny * csy;
-        const double sinh_x = 2.0 * shx * chx;          // sinh x^
-        const double sinh_y = 2.0 * shy * chy;
-        const double d0u = 2.0 * fma(shx, shx, sny * sny);
-        const double d0v = 2.0 * fma(shy, shy, snx * snx);
+        const double sinh_x = tshx * chx;          // sinh x^
+        const double sinh_y = tshy * chy;
+        // 2 (sinh^2(x^/2) + sin^2(y^/2)) with the factor 2 inside: the same rounding, bit for bit
+        const double d0u = fma(tshx, shx, -(nsny * sny));
+        const double d0v = fma(tshy, shy, -(nsnx * snx));
         double nu, du, ru, nv, dv, rv;
         image_sum(g, hx, cosh_x, sinh_x, cos_y, nu, du, ru);
         image_sum(g, hy, cosh_y, sinh_y, cos_x, nv, dv, rv);

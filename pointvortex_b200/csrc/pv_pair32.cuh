@@ -52,8 +52,8 @@ struct F32Geometry { // the FP32 constants of one evaluation
     float eps2;
     float l_hi, l_lo, inv_l, half_wave;
     float two_cosh_m[3], cosh_m[3], sinh2_m[3];
-    float k1, k2, k6, shift6;
-    int m_exact, has6;
+    float k1, k2;
+    int m_exact;
     float inv_radius2;
     float near2;       // near-field radius squared (0: no near field)
 };
@@ -72,10 +72,7 @@ __device__ __forceinline__ F32Geometry make_f32(const GeometryConsts &g) {
     }
     f.k1 = static_cast<float>(g.k1);
     f.k2 = static_cast<float>(g.k2);
-    f.k6 = static_cast<float>(g.k6);
-    f.shift6 = static_cast<float>(0.5 * g.shift6);
     f.m_exact = g.m_exact;
-    f.has6 = g.has6;
     f.inv_radius2 = static_cast<float>(g.inv_radius2);
     f.near2 = static_cast<float>(g.near2);
     return f;
@@ -129,32 +126,28 @@ __device__ __forceinline__ float half_angle_f32(const F32Geometry &f, float dx, 
     return f.half_wave * r;
 }
 
-__device__ __forceinline__ void image_sum_f32(const F32Geometry &f, float half_hat, float ch,
-                                              float sh, float c, float &num, float &den,
-                                              float &rest) {
+// Images m != 0 of one axis in FP32, as PeriodicPair::image_sum. The m = +-6 images are left
+// out: their term is at most 2 exp(-12 pi) cosh(pi) ~ 1e-15 of the m = 0 term, eight orders below
+// FP32 resolution.
+__device__ __forceinline__ void image_sum_f32(const F32Geometry &f, float ch, float c, float &num,
+                                              float &den, float &rest) {
     const float ch2 = ch * ch;
     const float p = fmaf(c, c, ch2);
-    const float q = -2.0f * c * ch;
     const float m2c = -2.0f * c;
+    const float q = m2c * ch;
     num = 0.0f;
     den = 1.0f;
-#pragma unroll
-    for (int m = 1; m <= 2; ++m) {
-        if (m <= f.m_exact) {
-            const float pn = fmaf(ch, f.two_cosh_m[m], m2c);
-            const float pd = fmaf(q, f.cosh_m[m], p + f.sinh2_m[m]);
-            num = fmaf(pn, den, num * pd);
-            den *= pd;
-        }
+    if (f.m_exact >= 1) {
+        num = fmaf(ch, f.two_cosh_m[1], m2c);
+        den = fmaf(q, f.cosh_m[1], p + f.sinh2_m[1]);
     }
-    const float ch2x = fmaf(2.0f, ch2, -1.0f);
-    rest = fmaf(ch, f.k1, c * ch2x * f.k2);
-    if (f.has6) { // |x^ -+ 12 pi| <= 40  <=>  |x^/2 -+ 6 pi| <= 20
-        const bool plus = fabsf(half_hat - f.shift6) <= 20.0f;
-        const bool minus = fabsf(half_hat + f.shift6) <= 20.0f;
-        const float e = (plus ? ch + sh : 0.0f) + (minus ? ch - sh : 0.0f);
-        rest = fmaf(f.k6, e, rest);
+    if (f.m_exact >= 2) {
+        const float pn = fmaf(ch, f.two_cosh_m[2], m2c);
+        const float pd = fmaf(q, f.cosh_m[2], p + f.sinh2_m[2]);
+        num = fmaf(pn, den, num * pd);
+        den *= pd;
     }
+    rest = fmaf(ch, f.k1, c * fmaf(2.0f * f.k2, ch2, -f.k2));
 }
 
 struct Target32 {
@@ -178,15 +171,15 @@ __device__ __forceinline__ bool periodic_values32(const F32Geometry &f, const fl
     float shx, chx, snx, csx, shy, chy, sny, csy;
     shcs_f32(hx, shx, chx, snx, csx);
     shcs_f32(hy, shy, chy, sny, csy);
-    const float cosh_x = fmaf(2.0f * shx, shx, 1.0f), cosh_y = fmaf(2.0f * shy, shy, 1.0f);
-    const float cos_x = fmaf(-2.0f * snx, snx, 1.0f), cos_y = fmaf(-2.0f * sny, sny, 1.0f);
+    const float tshx = 2.0f * shx, tshy = 2.0f * shy, nsnx = -2.0f * snx, nsny = -2.0f * sny;
+    const float cosh_x = fmaf(tshx, shx, 1.0f), cosh_y = fmaf(tshy, shy, 1.0f);
+    const float cos_x = fmaf(nsnx, snx, 1.0f), cos_y = fmaf(nsny, sny, 1.0f);
     const float sin_x = 2.0f * snx * csx, sin_y = 2.0f * sny * csy;
-    const float sinh_x = 2.0f * shx * chx, sinh_y = 2.0f * shy * chy;
-    const float d0u = near ? 1.0f : 2.0f * fmaf(shx, shx, sny * sny);
-    const float d0v = near ? 1.0f : 2.0f * fmaf(shy, shy, snx * snx);
+    const float d0u = near ? 1.0f : fmaf(tshx, shx, -(nsny * sny)); // 2 (sh_x^2 + sn_y^2)
+    const float d0v = near ? 1.0f : fmaf(tshy, shy, -(nsnx * snx));
     float nu, du, ru, nv, dv, rv;
-    image_sum_f32(f, hx, cosh_x, sinh_x, cos_y, nu, du, ru);
-    image_sum_f32(f, hy, cosh_y, sinh_y, cos_x, nv, dv, rv);
+    image_sum_f32(f, cosh_x, cos_y, nu, du, ru);
+    image_sum_f32(f, cosh_y, cos_x, nv, dv, rv);
     ku = near ? 0.0f : sin_y * fmaf(d0u, fmaf(du, ru, nu), du) * rcp_approx_f32(d0u * du);
     kv = near ? 0.0f : sin_x * fmaf(d0v, fmaf(dv, rv, nv), dv) * rcp_approx_f32(d0v * dv);
     return near;
@@ -244,16 +237,16 @@ __device__ __forceinline__ bool pair32(const F32Geometry &f, const Target32 &t, 
         float shx, chx, snx, csx, shy, chy, sny, csy;
         shcs_f32(hx, shx, chx, snx, csx);
         shcs_f32(hy, shy, chy, sny, csy);
-        const float cosh_x = fmaf(2.0f * shx, shx, 1.0f), cosh_y = fmaf(2.0f * shy, shy, 1.0f);
-        const float cos_x = fmaf(-2.0f * snx, snx, 1.0f), cos_y = fmaf(-2.0f * sny, sny, 1.0f);
+        const float tshx = 2.0f * shx, tshy = 2.0f * shy, nsnx = -2.0f * snx, nsny = -2.0f * sny;
+        const float cosh_x = fmaf(tshx, shx, 1.0f), cosh_y = fmaf(tshy, shy, 1.0f);
+        const float cos_x = fmaf(nsnx, snx, 1.0f), cos_y = fmaf(nsny, sny, 1.0f);
         const float sin_x = 2.0f * snx * csx, sin_y = 2.0f * sny * csy;
-        const float sinh_x = 2.0f * shx * chx, sinh_y = 2.0f * shy * chy;
         const bool skip = near || (CHECK && self);
-        const float d0u = skip ? 1.0f : 2.0f * fmaf(shx, shx, sny * sny);
-        const float d0v = skip ? 1.0f : 2.0f * fmaf(shy, shy, snx * snx);
+        const float d0u = skip ? 1.0f : fmaf(tshx, shx, -(nsny * sny)); // 2 (sh_x^2 + sn_y^2)
+        const float d0v = skip ? 1.0f : fmaf(tshy, shy, -(nsnx * snx));
         float nu, du, ru, nv, dv, rv;
-        image_sum_f32(f, hx, cosh_x, sinh_x, cos_y, nu, du, ru);
-        image_sum_f32(f, hy, cosh_y, sinh_y, cos_x, nv, dv, rv);
+        image_sum_f32(f, cosh_x, cos_y, nu, du, ru);
+        image_sum_f32(f, cosh_y, cos_x, nv, dv, rv);
         const float numer_u = fmaf(d0u, fmaf(du, ru, nu), du);
         const float numer_v = fmaf(d0v, fmaf(dv, rv, nv), dv);
         const float cu = skip ? 0.0f : sgf * sin_y * numer_u;
