@@ -68,6 +68,8 @@ bool tuning_store(int geometry, int precision, int log2_n, int per_thread);
 cudaError_t launch_velocity(const EvalArgs &a, const EvalPlan &p, cudaStream_t stream);
 // The FP32-compensated precision form (pv_velocity32.cu): same arguments, same partial layout.
 cudaError_t launch_velocity_fp32c(const EvalArgs &a, const EvalPlan &p, cudaStream_t stream);
+// Resident CTAs per SM of the FP32-compensated ordered kernel (the planner's wave arithmetic).
+int resident_fp32c(int geometry, int per_thread);
 
 // The periodic box and the infinite plane (FP64, FP32C) evaluated once per unordered pair
 // (pv_symmetric.cu) for a whole population (targets = sources). Partial rows: `blocks` rows of

@@ -280,6 +280,93 @@ __device__ __forceinline__ bool pair32(const F32Geometry &f, const Target32 &t, 
     return false;
 }
 
+// The disk's pair with both of its terms in one set of f32x2 instructions (FADD2, FMUL2, FFMA2:
+// two FP32 lanes per register pair and per issue on sm_100). Lane 0 is the direct term, lane 1
+// the source's wall image. The sources are staged packed and with the signs arranged so that no
+// negation is issued per pair:
+//   px = (-s.xh, -si.xh, -s.xl, -si.xl), py = (s.yh, si.yh, s.yl, si.yl), g2 = (gf, -gf),
+// and the target is (xh, xh), (xl, xl), (-yh, -yh), (-yl, -yl). Then dx = t - s and
+// dyn = s_y - t_y = -dy exactly (IEEE negation commutes with rounding), so the updates
+// u += c dyn, v += c dx are the scalar form's u -= c dy, v += c dx bit for bit, per term; the two
+// terms accumulate in separate lanes. A near term gets rcp(inf) = 0.
+struct DiskTarget2 {
+    float2 xh, xl, nyh, nyl;
+};
+
+__device__ __forceinline__ DiskTarget2 disk_target2(const Target32 &t) {
+    return {make_float2(t.xh, t.xh), make_float2(t.xl, t.xl), make_float2(-t.yh, -t.yh),
+            make_float2(-t.yl, -t.yl)};
+}
+
+__device__ __forceinline__ void disk_pack_source(const float4 sf, const float4 si, float gf,
+                                                 float4 &px, float4 &py, float2 &g2) {
+    px = make_float4(-sf.x, -si.x, -sf.z, -si.z);
+    py = make_float4(sf.y, si.y, sf.w, si.w);
+    g2 = make_float2(gf, -gf);
+}
+
+// The scalar form's source operands of pair32 from the packed ones (exact).
+__device__ __forceinline__ void disk_unpack_source(const float4 px, const float4 py, float4 &sf,
+                                                   float4 &si) {
+    sf = make_float4(-px.x, py.x, -px.z, py.z);
+    si = make_float4(-px.y, py.y, -px.w, py.w);
+}
+
+__device__ __forceinline__ float2 disk_r2_x2(const DiskTarget2 &t, const float4 px,
+                                             const float4 py, float2 &dx, float2 &dyn) {
+    dx = __fadd2_rn(__fadd2_rn(t.xh, make_float2(px.x, px.y)),
+                    __fadd2_rn(t.xl, make_float2(px.z, px.w)));
+    dyn = __fadd2_rn(__fadd2_rn(make_float2(py.x, py.y), t.nyh),
+                     __fadd2_rn(make_float2(py.z, py.w), t.nyl));
+    return __ffma2_rn(dx, dx, __fmul2_rn(dyn, dyn));
+}
+
+// closest: the smallest squared distance of either term met so far, for the caller's near-field
+// listing after a block of sources (disk_list_near_x2), so that the pair loop has no branch.
+__device__ __forceinline__ void disk_pair_x2(const F32Geometry &f, const DiskTarget2 &t,
+                                             const float4 px, const float4 py, const float2 g2,
+                                             float2 &u2, float2 &v2, float &closest) {
+    float2 dx, dyn;
+    const float2 r2 = disk_r2_x2(t, px, py, dx, dyn);
+    const float inf = __int_as_float(0x7f800000);
+    const float2 c = __fmul2_rn(g2, make_float2(rcp_approx_f32(r2.x < f.near2 ? inf : r2.x),
+                                                rcp_approx_f32(r2.y < f.near2 ? inf : r2.y)));
+    u2 = __ffma2_rn(c, dyn, u2);
+    v2 = __ffma2_rn(c, dx, v2);
+    closest = fminf(closest, fminf(r2.x, r2.y));
+}
+
+// Lists the near terms that disk_pair_x2 left out among the staged sources [jb, je) (source
+// index j0 + j), for every lane whose `flagged` is set, the whole warp at a time: the flagged
+// target is broadcast and each lane recomputes the squared distances (the same operations, so
+// the same verdicts) of every 32nd source. Near terms are rare (a dozen per target at the default
+// radius), so this runs for few blocks; all 32 lanes must be present.
+__device__ __forceinline__ void disk_list_near_x2(const F32Geometry &f, const NearLists &lists,
+                                                  const DiskTarget2 &t, size_t ti, bool flagged,
+                                                  const float4 *spx, const float4 *spy, int jb,
+                                                  int je, size_t j0) {
+    unsigned todo = __ballot_sync(0xffffffffu, flagged);
+    const int lane = threadIdx.x & 31;
+    while (todo) {
+        const int l = __ffs(todo) - 1;
+        todo &= todo - 1;
+        DiskTarget2 tl;
+        tl.xh.x = tl.xh.y = __shfl_sync(0xffffffffu, t.xh.x, l);
+        tl.xl.x = tl.xl.y = __shfl_sync(0xffffffffu, t.xl.x, l);
+        tl.nyh.x = tl.nyh.y = __shfl_sync(0xffffffffu, t.nyh.x, l);
+        tl.nyl.x = tl.nyl.y = __shfl_sync(0xffffffffu, t.nyl.x, l);
+        const size_t target = __shfl_sync(0xffffffffu, ti, l);
+        for (int j = jb + lane; j < je; j += 32) {
+            float2 dx, dyn;
+            const float2 r2 = disk_r2_x2(tl, spx[j], spy[j], dx, dyn);
+            if (r2.x < f.near2)
+                near_append(lists, target, static_cast<unsigned>(j0 + j));
+            if (r2.y < f.near2)
+                near_append(lists, target, static_cast<unsigned>(j0 + j) | kNearImage);
+        }
+    }
+}
+
 // Lists the near terms pair32 left out, under target ti and source j.
 __device__ __forceinline__ void list_near(const NearLists &lists, bool near_pair, bool near_wall,
                                           size_t ti, unsigned j) {

@@ -229,6 +229,8 @@ EvalPlan plan_evaluation(int geometry, size_t n_targets, size_t n_sources, int s
     if (per_thread_override == 1 || per_thread_override == 2 || per_thread_override == 4)
         p.per_thread = per_thread_override;
     const auto resident_of = [&](int t) {
+        if (precision == 1)
+            return resident_fp32c(geometry, t);
         return geometry == GEO_INFINITE   ? resident_for<InfinitePair>(t)
                : geometry == GEO_PERIODIC ? resident_for<PeriodicPair>(t)
                                           : resident_for<DiskPair>(t);

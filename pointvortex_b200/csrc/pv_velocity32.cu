@@ -26,6 +26,7 @@
 #include "pv_pair32.cuh"
 
 #include <algorithm>
+#include <atomic>
 
 namespace pvb {
 
@@ -38,9 +39,12 @@ __global__ void __launch_bounds__(B) velocity32_kernel(const EvalArgs a) {
     __shared__ alignas(128) double s_x[2][kTile32];
     __shared__ alignas(128) double s_y[2][kTile32];
     __shared__ alignas(128) double s_g[2][kTile32];
+    // plane, periodic: s_f = (xh, yh, xl, yl), s_gf. Disk: each source packed with its wall image
+    // for the f32x2 pair (disk_pair_x2): s_f = px, s_fi = py, s_g2 = (gf, -gf).
     __shared__ alignas(16) float4 s_f[kTile32];
-    __shared__ alignas(16) float4 s_fi[GEO == GEO_DISK ? kTile32 : 1];  // wall images (disk)
-    __shared__ float s_gf[kTile32];
+    __shared__ alignas(16) float4 s_fi[GEO == GEO_DISK ? kTile32 : 1];
+    __shared__ float s_gf[GEO == GEO_DISK ? 1 : kTile32];
+    __shared__ alignas(8) float2 s_g2[GEO == GEO_DISK ? kTile32 : 1];
     __shared__ alignas(8) uint64_t bars[2];
     __shared__ int s_status;
 
@@ -77,6 +81,15 @@ __global__ void __launch_bounds__(B) velocity32_kernel(const EvalArgs a) {
         tg[k].yl = static_cast<float>(tg[k].y - static_cast<double>(tg[k].yh));
         u[k] = v[k] = 0.0f;
         ud[k] = vd[k] = 0.0;
+    }
+    DiskTarget2 t2[GEO == GEO_DISK ? T : 1];
+    float2 u2[GEO == GEO_DISK ? T : 1], v2[GEO == GEO_DISK ? T : 1];
+    if (GEO == GEO_DISK) {
+#pragma unroll
+        for (int k = 0; k < T; ++k) {
+            t2[k] = disk_target2(tg[k]);
+            u2[k] = v2[k] = make_float2(0.0f, 0.0f);
+        }
     }
 
     const int ntiles = src1 > src0 ? static_cast<int>((src1 - src0 + kTile32 - 1) / kTile32) : 0;
@@ -128,10 +141,13 @@ __global__ void __launch_bounds__(B) velocity32_kernel(const EvalArgs a) {
         // images) once per CTA
         for (int j = tid; j < cnt; j += B) {
             const double xj = s_x[st][j], yj = s_y[st][j];
-            s_f[j] = split_position(xj, yj);
-            if (GEO == GEO_DISK)
-                s_fi[j] = image_position(a.g, xj, yj);
-            s_gf[j] = static_cast<float>(s_g[st][j]);
+            if (GEO == GEO_DISK) {
+                disk_pack_source(split_position(xj, yj), image_position(a.g, xj, yj),
+                                 static_cast<float>(s_g[st][j]), s_f[j], s_fi[j], s_g2[j]);
+            } else {
+                s_f[j] = split_position(xj, yj);
+                s_gf[j] = static_cast<float>(s_g[st][j]);
+            }
         }
         __syncthreads();
         const bool diagonal = j0 < blk1 && blk0 < j0 + cnt;
@@ -141,9 +157,14 @@ __global__ void __launch_bounds__(B) velocity32_kernel(const EvalArgs a) {
             if (diagonal) {
 #pragma unroll 1
                 for (int j = jb; j < je; ++j) {
-                    const float4 sf = s_f[j];
-                    const float4 si = GEO == GEO_DISK ? s_fi[j] : sf;
-                    const float gf = s_gf[j];
+                    float4 sf = s_f[j], si = sf;
+                    float gf;
+                    if (GEO == GEO_DISK) {
+                        disk_unpack_source(sf, s_fi[j], sf, si);
+                        gf = s_g2[j].x;
+                    } else {
+                        gf = s_gf[j];
+                    }
 #pragma unroll
                     for (int k = 0; k < T; ++k) {
                         bool np, nw;
@@ -153,16 +174,35 @@ __global__ void __launch_bounds__(B) velocity32_kernel(const EvalArgs a) {
                             list_near(a.near, np, nw, ti[k], static_cast<unsigned>(j0 + j));
                     }
                 }
+            } else if (GEO == GEO_DISK) {
+                float closest[T];
+#pragma unroll
+                for (int k = 0; k < T; ++k)
+                    closest[k] = __int_as_float(0x7f800000);
+#pragma unroll 4
+                for (int j = jb; j < je; ++j) {
+                    const float4 px = s_f[j], py = s_fi[j];
+                    const float2 g2 = s_g2[j];
+#pragma unroll
+                    for (int k = 0; k < T; ++k)
+                        disk_pair_x2(f, t2[k], px, py, g2, u2[k], v2[k], closest[k]);
+                }
+                if (a.near.count) {
+#pragma unroll
+                    for (int k = 0; k < T; ++k)
+                        disk_list_near_x2(f, a.near, t2[k], ti[k],
+                                          closest[k] < f.near2 && ti[k] < blk1, s_f, s_fi, jb, je,
+                                          j0);
+                }
             } else {
 #pragma unroll 2
                 for (int j = jb; j < je; ++j) {
                     const float4 sf = s_f[j];
-                    const float4 si = GEO == GEO_DISK ? s_fi[j] : sf;
                     const float gf = s_gf[j];
 #pragma unroll
                     for (int k = 0; k < T; ++k) {
                         bool np, nw;
-                        if (pair32<GEO, false>(f, tg[k], sf, si, gf, false, u[k], v[k], np, nw) &&
+                        if (pair32<GEO, false>(f, tg[k], sf, sf, gf, false, u[k], v[k], np, nw) &&
                             a.near.count && ti[k] < blk1)
                             list_near(a.near, np, nw, ti[k], static_cast<unsigned>(j0 + j));
                     }
@@ -173,6 +213,13 @@ __global__ void __launch_bounds__(B) velocity32_kernel(const EvalArgs a) {
                 ud[k] += static_cast<double>(u[k]);
                 vd[k] += static_cast<double>(v[k]);
                 u[k] = v[k] = 0.0f;
+                if (GEO == GEO_DISK) { // the direct and the image lanes, in that order
+                    ud[k] += static_cast<double>(u2[k].x);
+                    ud[k] += static_cast<double>(u2[k].y);
+                    vd[k] += static_cast<double>(v2[k].x);
+                    vd[k] += static_cast<double>(v2[k].y);
+                    u2[k] = v2[k] = make_float2(0.0f, 0.0f);
+                }
             }
         }
         __syncthreads();
@@ -186,6 +233,24 @@ __global__ void __launch_bounds__(B) velocity32_kernel(const EvalArgs a) {
             a.pu[base + ti[k]] = ud[k];
             a.pv[base + ti[k]] = vd[k];
         }
+}
+
+template <int GEO, int T> int resident32() {
+    static std::atomic<int> cached{0};  // host threads may plan at once
+    if (!cached.load(std::memory_order_relaxed)) {
+        int blocks = 0;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, velocity32_kernel<GEO, 128, T>,
+                                                          128, 0) != cudaSuccess ||
+            blocks < 1)
+            blocks = 1;
+        cached.store(blocks, std::memory_order_relaxed);
+    }
+    return cached.load(std::memory_order_relaxed);
+}
+
+template <int GEO> int resident32_t(int per_thread) {
+    return per_thread == 1 ? resident32<GEO, 1>()
+                           : (per_thread == 2 ? resident32<GEO, 2>() : resident32<GEO, 4>());
 }
 
 template <int GEO, int T> cudaError_t launch32_t(const EvalArgs &a, const EvalPlan &p, cudaStream_t s) {
@@ -206,6 +271,12 @@ template <int GEO> cudaError_t launch32_geo(const EvalArgs &a, const EvalPlan &p
     }
 }
 } // namespace
+
+int resident_fp32c(int geometry, int per_thread) {
+    return geometry == GEO_INFINITE   ? resident32_t<GEO_INFINITE>(per_thread)
+           : geometry == GEO_PERIODIC ? resident32_t<GEO_PERIODIC>(per_thread)
+                                      : resident32_t<GEO_DISK>(per_thread);
+}
 
 cudaError_t launch_velocity_fp32c(const EvalArgs &a, const EvalPlan &p, cudaStream_t stream) {
     if (a.t_end <= a.t_begin)
