@@ -36,22 +36,23 @@ __device__ __forceinline__ double warp_sum(double v) {
 // One warp per target. The listed entries (at most 32: one per lane) are sorted across the warp
 // (a bitonic network over the lanes), each lane evaluates one in FP64, and the warp adds the terms
 // in a fixed tree; so the sum does not depend on the order in which the FP32 kernel listed them.
-__global__ void __launch_bounds__(kNearWarps * 32) near_field_kernel(const NearPass a) {
+// Four CTAs per SM (at most 64 registers): a population's targets are then one wave, and each
+// warp's chain of dependent loads (list count and slots, the listed sources, the partial row)
+// overlaps the others'. The count, the slots and the target are loaded together.
+__global__ void __launch_bounds__(kNearWarps * 32, 4) near_field_kernel(const NearPass a) {
     pdl_enter();
     const int lane = threadIdx.x & 31;
     const size_t i = a.t_begin + static_cast<size_t>(blockIdx.x) * kNearWarps + (threadIdx.x >> 5);
     if (i >= a.t_end)
         return;  // the whole warp
-    unsigned count = 0;
-    if (lane == 0) {
-        count = a.lists.count[i];
-        if (count)
-            a.lists.count[i] = 0u;
-    }
-    count = __shfl_sync(0xffffffffu, count, 0);
+    const unsigned count = a.lists.count[i];
+    const unsigned listed = a.lists.slot[i * f32::kNearSlots + lane];  // meaningful below count
+    const double tx = a.x[i], ty = a.y[i];
     if (count == 0)
         return;
-    const double tx = a.x[i], ty = a.y[i];
+    __syncwarp();
+    if (lane == 0)
+        a.lists.count[i] = 0u;
     const size_t local = i - a.t_begin;
     const size_t last = static_cast<size_t>(a.rows - 1) * a.stride + local;
     double du = 0.0, dv = 0.0;
@@ -88,10 +89,8 @@ __global__ void __launch_bounds__(kNearWarps * 32) near_field_kernel(const NearP
     // the listed entries in increasing (source, image) order across the lanes; a source's image
     // sorts after the source itself, empty lanes last
     unsigned key = 0xffffffffu;
-    if (lane < static_cast<int>(count)) {
-        const unsigned v = a.lists.slot[i * f32::kNearSlots + lane];
-        key = (v & ~f32::kNearImage) * 2u + (v >> 31);
-    }
+    if (lane < static_cast<int>(count))
+        key = (listed & ~f32::kNearImage) * 2u + (listed >> 31);
     for (int k = 2; k <= 32; k <<= 1)
         for (int j = k >> 1; j > 0; j >>= 1) {
             const unsigned other = __shfl_xor_sync(0xffffffffu, key, j);

@@ -96,58 +96,89 @@ __device__ __forceinline__ float4 image_position(const GeometryConsts &g, double
     return split_position(k * x, k * y);
 }
 
-// sinh, cosh, sin, cos of t (|t| <= pi/2), the FP32 truncation of the shared series in
-// pv_common.cuh (first omitted term below 1e-8 relative).
-__device__ __forceinline__ void shcs_f32(float t, float &sh, float &ch, float &s, float &c) {
-    const float t2 = t * t, w = t2 * t2;
-    float e1 = fmaf(w, 1.6059043836821613e-10f, 2.7557319223985893e-06f); // 1/13!, 1/9!
-    e1 = fmaf(w, e1, 8.333333333333333e-03f);
-    e1 = fmaf(w, e1, 1.0f);
-    float o1 = fmaf(w, 2.505210838544172e-08f, 1.984126984126984e-04f); // 1/11!, 1/7!
-    o1 = fmaf(w, o1, 1.6666666666666666e-01f);
-    float e0 = fmaf(w, 2.08767569878681e-09f, 2.48015873015873e-05f); // 1/12!, 1/8!
-    e0 = fmaf(w, e0, 4.1666666666666664e-02f);
-    e0 = fmaf(w, e0, 1.0f);
-    float o0 = fmaf(w, 1.1470745597729725e-11f, 2.755731922398589e-07f); // 1/14!, 1/10!
-    o0 = fmaf(w, o0, 1.388888888888889e-03f);
-    o0 = fmaf(w, o0, 0.5f);
-    const float t3 = t * t2, te1 = t * e1;
-    sh = fmaf(t3, o1, te1);
-    s = fmaf(-t3, o1, te1);
-    ch = fmaf(t2, o0, e0);
-    c = fmaf(-t2, o0, e0);
+// Two FP32 lanes per instruction (FADD2, FMUL2, FFMA2 on sm_100): the periodic pair's x and y
+// axes, or the disk's direct and image terms, run side by side. Each lane is rounded exactly as
+// the scalar instruction would round it.
+__device__ __forceinline__ float2 splat2(float a) { return make_float2(a, a); }
+__device__ __forceinline__ float2 add2(float2 a, float2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ float2 mul2(float2 a, float2 b) { return __fmul2_rn(a, b); }
+__device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
+__device__ __forceinline__ float2 swap2(float2 a) { return make_float2(a.y, a.x); }
+
+// sinh, sin and cos of t (|t| <= pi/2) for both lanes, the FP32 truncation of the shared series in
+// pv_common.cuh (first omitted term below 1e-8 relative; cosh t is not needed in FP32).
+__device__ __forceinline__ void sh_sn_cs_x2(float2 t, float2 &sh, float2 &sn, float2 &cs) {
+    const float2 m1 = splat2(-1.0f);
+    const float2 t2 = mul2(t, t), w = mul2(t2, t2);
+    float2 e1 = fma2(w, splat2(1.6059043836821613e-10f), splat2(2.7557319223985893e-06f)); // 1/13!, 1/9!
+    e1 = fma2(w, e1, splat2(8.333333333333333e-03f));
+    e1 = fma2(w, e1, splat2(1.0f));
+    float2 o1 = fma2(w, splat2(2.505210838544172e-08f), splat2(1.984126984126984e-04f)); // 1/11!, 1/7!
+    o1 = fma2(w, o1, splat2(1.6666666666666666e-01f));
+    float2 e0 = fma2(w, splat2(2.08767569878681e-09f), splat2(2.48015873015873e-05f)); // 1/12!, 1/8!
+    e0 = fma2(w, e0, splat2(4.1666666666666664e-02f));
+    e0 = fma2(w, e0, splat2(1.0f));
+    float2 o0 = fma2(w, splat2(1.1470745597729725e-11f), splat2(2.755731922398589e-07f)); // 1/14!, 1/10!
+    o0 = fma2(w, o0, splat2(1.388888888888889e-03f));
+    o0 = fma2(w, o0, splat2(0.5f));
+    const float2 t3 = mul2(t, t2), te1 = mul2(t, e1);
+    sh = fma2(t3, o1, te1);
+    sn = fma2(mul2(t3, m1), o1, te1);
+    cs = fma2(mul2(t2, m1), o0, e0);
 }
 
-// Half of x^ = (2 pi/L) remainder(dx, L) in FP32 from a double-float displacement; r receives the
-// minimum-image displacement remainder(dx, L).
-__device__ __forceinline__ float half_angle_f32(const F32Geometry &f, float dx, float &r) {
-    const float n = rintf(dx * f.inv_l);
-    r = fmaf(-n, f.l_lo, fmaf(-n, f.l_hi, dx));
-    return f.half_wave * r;
-}
-
-// Images m != 0 of one axis in FP32, as PeriodicPair::image_sum. The m = +-6 images are left
-// out: their term is at most 2 exp(-12 pi) cosh(pi) ~ 1e-15 of the m = 0 term, eight orders below
-// FP32 resolution.
-__device__ __forceinline__ void image_sum_f32(const F32Geometry &f, float ch, float c, float &num,
-                                              float &den, float &rest) {
-    const float ch2 = ch * ch;
-    const float p = fmaf(c, c, ch2);
-    const float m2c = -2.0f * c;
-    const float q = m2c * ch;
-    num = 0.0f;
-    den = 1.0f;
+// The periodic pair's core in FP32, both axes at once (lane 0: the target's u term, lane 1: its v
+// term). th/tl and sh/sl are the (x, y) hi and lo parts of target and source. Returns the near
+// verdict (minimum-image distance below the near-field radius); a2 = (sin y^ N_u, sin x^ N_v)
+// and b2 = (d0_u den_u, d0_v den_v): the terms are a2 / b2. skip (near or the self pair) sets
+// d0 = 1 so that b2 stays finite; the caller discards those terms.
+__device__ __forceinline__ bool periodic_core_x2(const F32Geometry &f, float2 th, float2 tl,
+                                                 float2 sh, float2 sl, bool self, float2 &a2,
+                                                 float2 &b2) {
+    const float2 m1 = splat2(-1.0f);
+    // (dx, dy) = (t_hi - s_hi) + (t_lo - s_lo); fma(s, -1, t) is t - s exactly
+    const float2 d = add2(fma2(sh, m1, th), fma2(sl, m1, tl));
+    // half of x^ = (2 pi/L) remainder(dx, L) from the double-float displacement
+    const float2 q = mul2(d, splat2(f.inv_l));
+    const float2 n = make_float2(rintf(q.x), rintf(q.y));
+    const float2 r = fma2(n, splat2(-f.l_lo), fma2(n, splat2(-f.l_hi), d));
+    const float2 h = mul2(splat2(f.half_wave), r);
+    const bool near = fmaf(r.x, r.x, r.y * r.y) < f.near2 && !self;
+    float2 shh, snh, csh;
+    sh_sn_cs_x2(h, shh, snh, csh);
+    const float2 tsh = mul2(splat2(2.0f), shh), tsn = mul2(splat2(2.0f), snh);
+    const float2 cosh_ = fma2(tsh, shh, splat2(1.0f));                  // cosh x^ = 1 + 2 sinh^2
+    const float2 cos_ = fma2(mul2(splat2(-2.0f), snh), snh, splat2(1.0f)); // cos x^ = 1 - 2 sin^2
+    const float2 sin_ = mul2(tsn, csh);                                  // sin x^ = 2 sin cos
+    // d0 = (2 (sh_x^2 + sn_y^2), 2 (sh_y^2 + sn_x^2))
+    float2 d0 = fma2(tsh, shh, swap2(mul2(tsn, snh)));
+    if (near || self)
+        d0 = splat2(1.0f);
+    // the images m != 0 of each lane's axis, as PeriodicPair::image_sum; C = cosh of the lane's
+    // axis, c = cos of the other. The m = +-6 images are left out: their term is at most
+    // 2 exp(-12 pi) cosh(pi) ~ 1e-15 of the m = 0 term, eight orders below FP32 resolution.
+    const float2 C = cosh_, c = swap2(cos_);
+    const float2 ch2 = mul2(C, C);
+    const float2 p = fma2(c, c, ch2);
+    const float2 m2c = mul2(splat2(-2.0f), c);
+    const float2 qq = mul2(m2c, C);
+    float2 num = splat2(0.0f), den = splat2(1.0f);
     if (f.m_exact >= 1) {
-        num = fmaf(ch, f.two_cosh_m[1], m2c);
-        den = fmaf(q, f.cosh_m[1], p + f.sinh2_m[1]);
+        num = fma2(C, splat2(f.two_cosh_m[1]), m2c);
+        den = fma2(qq, splat2(f.cosh_m[1]), add2(p, splat2(f.sinh2_m[1])));
     }
     if (f.m_exact >= 2) {
-        const float pn = fmaf(ch, f.two_cosh_m[2], m2c);
-        const float pd = fmaf(q, f.cosh_m[2], p + f.sinh2_m[2]);
-        num = fmaf(pn, den, num * pd);
-        den *= pd;
+        const float2 pn = fma2(C, splat2(f.two_cosh_m[2]), m2c);
+        const float2 pd = fma2(qq, splat2(f.cosh_m[2]), add2(p, splat2(f.sinh2_m[2])));
+        num = fma2(pn, den, mul2(num, pd));
+        den = mul2(den, pd);
     }
-    rest = fmaf(ch, f.k1, c * fmaf(2.0f * f.k2, ch2, -f.k2));
+    const float2 rest =
+        fma2(C, splat2(f.k1), mul2(c, fma2(splat2(2.0f * f.k2), ch2, splat2(-f.k2))));
+    // 1/d0 + num/den + rest = (den + d0 (num + den rest)) / (d0 den)
+    a2 = mul2(swap2(sin_), fma2(d0, fma2(den, rest, num), den));
+    b2 = mul2(d0, den);
+    return near;
 }
 
 struct Target32 {
@@ -163,25 +194,11 @@ struct Target32 {
 // verdict from either side): its terms are then 0 here and come from the FP64 pass.
 __device__ __forceinline__ bool periodic_values32(const F32Geometry &f, const float4 t,
                                                   const float4 s, float &ku, float &kv) {
-    const float dx = (t.x - s.x) + (t.z - s.z);
-    const float dy = (t.y - s.y) + (t.w - s.w);
-    float rx, ry;
-    const float hx = half_angle_f32(f, dx, rx), hy = half_angle_f32(f, dy, ry);
-    const bool near = fmaf(rx, rx, ry * ry) < f.near2;
-    float shx, chx, snx, csx, shy, chy, sny, csy;
-    shcs_f32(hx, shx, chx, snx, csx);
-    shcs_f32(hy, shy, chy, sny, csy);
-    const float tshx = 2.0f * shx, tshy = 2.0f * shy, nsnx = -2.0f * snx, nsny = -2.0f * sny;
-    const float cosh_x = fmaf(tshx, shx, 1.0f), cosh_y = fmaf(tshy, shy, 1.0f);
-    const float cos_x = fmaf(nsnx, snx, 1.0f), cos_y = fmaf(nsny, sny, 1.0f);
-    const float sin_x = 2.0f * snx * csx, sin_y = 2.0f * sny * csy;
-    const float d0u = near ? 1.0f : fmaf(tshx, shx, -(nsny * sny)); // 2 (sh_x^2 + sn_y^2)
-    const float d0v = near ? 1.0f : fmaf(tshy, shy, -(nsnx * snx));
-    float nu, du, ru, nv, dv, rv;
-    image_sum_f32(f, cosh_x, cos_y, nu, du, ru);
-    image_sum_f32(f, cosh_y, cos_x, nv, dv, rv);
-    ku = near ? 0.0f : sin_y * fmaf(d0u, fmaf(du, ru, nu), du) * rcp_approx_f32(d0u * du);
-    kv = near ? 0.0f : sin_x * fmaf(d0v, fmaf(dv, rv, nv), dv) * rcp_approx_f32(d0v * dv);
+    float2 a2, b2;
+    const bool near = periodic_core_x2(f, make_float2(t.x, t.y), make_float2(t.z, t.w),
+                                       make_float2(s.x, s.y), make_float2(s.z, s.w), false, a2, b2);
+    ku = near ? 0.0f : a2.x * rcp_approx_f32(b2.x);
+    kv = near ? 0.0f : a2.y * rcp_approx_f32(b2.y);
     return near;
 }
 
@@ -231,28 +248,16 @@ __device__ __forceinline__ bool pair32(const F32Geometry &f, const Target32 &t, 
     const float dx = (t.xh - s.x) + (t.xl - s.z);
     const float dy = (t.yh - s.y) + (t.yl - s.w);
     if (GEO == GEO_PERIODIC) {
-        float rx, ry;
-        const float hx = half_angle_f32(f, dx, rx), hy = half_angle_f32(f, dy, ry);
-        const bool near = fmaf(rx, rx, ry * ry) < f.near2 && !(CHECK && self);
-        float shx, chx, snx, csx, shy, chy, sny, csy;
-        shcs_f32(hx, shx, chx, snx, csx);
-        shcs_f32(hy, shy, chy, sny, csy);
-        const float tshx = 2.0f * shx, tshy = 2.0f * shy, nsnx = -2.0f * snx, nsny = -2.0f * sny;
-        const float cosh_x = fmaf(tshx, shx, 1.0f), cosh_y = fmaf(tshy, shy, 1.0f);
-        const float cos_x = fmaf(nsnx, snx, 1.0f), cos_y = fmaf(nsny, sny, 1.0f);
-        const float sin_x = 2.0f * snx * csx, sin_y = 2.0f * sny * csy;
-        const bool skip = near || (CHECK && self);
-        const float d0u = skip ? 1.0f : fmaf(tshx, shx, -(nsny * sny)); // 2 (sh_x^2 + sn_y^2)
-        const float d0v = skip ? 1.0f : fmaf(tshy, shy, -(nsnx * snx));
-        float nu, du, ru, nv, dv, rv;
-        image_sum_f32(f, cosh_x, cos_y, nu, du, ru);
-        image_sum_f32(f, cosh_y, cos_x, nv, dv, rv);
-        const float numer_u = fmaf(d0u, fmaf(du, ru, nu), du);
-        const float numer_v = fmaf(d0v, fmaf(dv, rv, nv), dv);
-        const float cu = skip ? 0.0f : sgf * sin_y * numer_u;
-        const float cv = skip ? 0.0f : sgf * sin_x * numer_v;
-        u = fmaf(-cu, rcp_approx_f32(d0u * du), u);
-        v = fmaf(cv, rcp_approx_f32(d0v * dv), v);
+        float2 a2, b2;
+        const bool self_pair = CHECK && self;
+        const bool near = periodic_core_x2(f, make_float2(t.xh, t.yh), make_float2(t.xl, t.yl),
+                                           make_float2(s.x, s.y), make_float2(s.z, s.w), self_pair,
+                                           a2, b2);
+        const bool skip = near || self_pair;
+        const float cu = skip ? 0.0f : sgf * a2.x;
+        const float cv = skip ? 0.0f : sgf * a2.y;
+        u = fmaf(-cu, rcp_approx_f32(b2.x), u);
+        v = fmaf(cv, rcp_approx_f32(b2.y), v);
         near_pair = near;
         return near;
     }

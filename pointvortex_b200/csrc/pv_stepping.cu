@@ -67,13 +67,48 @@ __device__ void dopri_control(DeviceControl *ctl) {
 }
 } // namespace
 
+// What a target's finish reads besides its own velocity: the step-start position, the earlier
+// stage velocities k_j (j != s) that its combination uses, and for the DOPRI5 error the
+// fifth-order point. All of them were written by kernels that completed before this stage kernel
+// was launched (the earlier stage kernels; the velocity launch it waits for writes only partial
+// rows), so the stage kernel may load them before its wait on the velocity launch.
+struct FinishInputs {
+    double x0, y0, xt, yt;
+    double kx[7], ky[7];
+};
+
+template <int MODE>
+__device__ __forceinline__ void load_finish_inputs(const StageArgs &a, size_t i, FinishInputs &p) {
+    p.x0 = a.x0[i];
+    p.y0 = a.y0[i];
+    if (MODE == STAGE_DOPRI_ERROR) {
+        p.xt = a.xt[i];
+        p.yt = a.yt[i];
+    }
+#pragma unroll
+    for (int j = 0; j < 7; ++j) {
+        bool used = false;
+        if (MODE == STAGE_POSITION)
+            used = j < a.ncoef && a.coef[j] != 0.0;
+        else if (MODE == STAGE_DOPRI_ERROR)
+            used = a.w[j] != 0.0;
+        else if (MODE == STAGE_RK4_COMBINE)
+            used = j < 3;
+        if (used && j != a.s) {
+            p.kx[j] = a.kx[j][i];
+            p.ky[j] = a.ky[j][i];
+        }
+    }
+}
+
 // Everything a stage does for one target once its velocity (ku, kv) is summed: the slow path of
 // a non-finite sum, the stage velocity, and the stage position / RK4 combination / DOPRI5 error.
-// ex, ey: the positions the slow path recomputes from (a.ex, a.ey, or a copy of them).
+// ex, ey: the positions the slow path recomputes from (a.ex, a.ey, or a copy of them). p: the
+// target's FinishInputs.
 template <int MODE>
 __device__ __forceinline__ void finish_target(const StageArgs &a, size_t i, double ku, double kv,
                                               double dt, double &local_max, const double *ex,
-                                              const double *ey) {
+                                              const double *ey, const FinishInputs &p) {
     if (a.reduce) {
         if (!isfinite(ku) || !isfinite(kv)) {
             const int verdict =
@@ -87,30 +122,31 @@ __device__ __forceinline__ void finish_target(const StageArgs &a, size_t i, doub
     if (MODE == STAGE_POSITION) {
         // makeStage, src/timestep.cpp:19-30 (zero coefficients add an exact zero: skipped)
         double dx = 0.0, dy = 0.0;
-        for (int j = 0; j < a.ncoef; ++j) {
+#pragma unroll
+        for (int j = 0; j < 7; ++j) {  // unrolled: p's fields stay in registers
             const double c = a.coef[j];
-            if (c == 0.0)
+            if (j >= a.ncoef || c == 0.0)
                 continue;
-            const double kxj = j == a.s ? ku : a.kx[j][i];
-            const double kyj = j == a.s ? kv : a.ky[j][i];
+            const double kxj = j == a.s ? ku : p.kx[j];
+            const double kyj = j == a.s ? kv : p.ky[j];
             dx = __dadd_rn(dx, __dmul_rn(c, kxj));
             dy = __dadd_rn(dy, __dmul_rn(c, kyj));
         }
-        const double nx = __dadd_rn(a.x0[i], __dmul_rn(dt, dx));
-        const double ny = __dadd_rn(a.y0[i], __dmul_rn(dt, dy));
+        const double nx = __dadd_rn(p.x0, __dmul_rn(dt, dx));
+        const double ny = __dadd_rn(p.y0, __dmul_rn(dt, dy));
         a.xt[i] = nx;
         a.yt[i] = ny;
         validate_position(a, nx, ny);
     } else if (MODE == STAGE_RK4_COMBINE) {
         // src/timestep.cpp:52-57: x0 + dt * (k1 + 2 k2 + 2 k3 + k4) / 6
-        const double sx = __dadd_rn(__dadd_rn(__dadd_rn(a.kx[0][i], __dmul_rn(2.0, a.kx[1][i])),
-                                              __dmul_rn(2.0, a.kx[2][i])),
+        const double sx = __dadd_rn(__dadd_rn(__dadd_rn(p.kx[0], __dmul_rn(2.0, p.kx[1])),
+                                              __dmul_rn(2.0, p.kx[2])),
                                     ku);
-        const double sy = __dadd_rn(__dadd_rn(__dadd_rn(a.ky[0][i], __dmul_rn(2.0, a.ky[1][i])),
-                                              __dmul_rn(2.0, a.ky[2][i])),
+        const double sy = __dadd_rn(__dadd_rn(__dadd_rn(p.ky[0], __dmul_rn(2.0, p.ky[1])),
+                                              __dmul_rn(2.0, p.ky[2])),
                                     kv);
-        const double nx = __dadd_rn(a.x0[i], __ddiv_rn(__dmul_rn(dt, sx), 6.0));
-        const double ny = __dadd_rn(a.y0[i], __ddiv_rn(__dmul_rn(dt, sy), 6.0));
+        const double nx = __dadd_rn(p.x0, __ddiv_rn(__dmul_rn(dt, sx), 6.0));
+        const double ny = __dadd_rn(p.y0, __ddiv_rn(__dmul_rn(dt, sy), 6.0));
         a.xt[i] = nx;
         a.yt[i] = ny;
         if (!isfinite(nx) || !isfinite(ny))
@@ -118,23 +154,24 @@ __device__ __forceinline__ void finish_target(const StageArgs &a, size_t i, doub
     } else if (MODE == STAGE_DOPRI_ERROR) {
         // src/timestep.cpp:78-95: xt holds the fifth-order point y5 (stage 7's position).
         double xe = 0.0, ye = 0.0;
+#pragma unroll
         for (int j = 0; j < 7; ++j) {
             const double w = a.w[j];
             if (w == 0.0)
                 continue;
             const double h = __dmul_rn(dt, w);
-            const double kxj = j == a.s ? ku : a.kx[j][i];
-            const double kyj = j == a.s ? kv : a.ky[j][i];
+            const double kxj = j == a.s ? ku : p.kx[j];
+            const double kyj = j == a.s ? kv : p.ky[j];
             xe = __dadd_rn(xe, __dmul_rn(h, kxj));
             ye = __dadd_rn(ye, __dmul_rn(h, kyj));
         }
-        const double x5 = a.xt[i], y5 = a.yt[i];
+        const double x5 = p.xt, y5 = p.yt;
         const double xs = __dadd_rn(a.ctl->absolute_tolerance,
                                     __dmul_rn(a.ctl->relative_tolerance,
-                                              max_ref(fabs(a.x0[i]), fabs(x5))));
+                                              max_ref(fabs(p.x0), fabs(x5))));
         const double ys = __dadd_rn(a.ctl->absolute_tolerance,
                                     __dmul_rn(a.ctl->relative_tolerance,
-                                              max_ref(fabs(a.y0[i]), fabs(y5))));
+                                              max_ref(fabs(p.y0), fabs(y5))));
         if (!isfinite(xe) || !isfinite(ye) || !isfinite(xs) || !isfinite(ys) || !(xs > 0.0) ||
             !(ys > 0.0)) {
             set_status(&a.ctl->status, ST_DOPRI_NONFINITE);
@@ -158,8 +195,13 @@ __global__ void __launch_bounds__(256) stage_kernel(const StageArgs a) {
     __shared__ double s_max[8];
     __shared__ double s_u[WIDE ? kWideGroups : 1][kWideTargets],
         s_v[WIDE ? kWideGroups : 1][kWideTargets];
-    pdl_enter();
     const int tid = threadIdx.x;
+    // WIDE: the finishing threads load their first target's FinishInputs before the wait
+    FinishInputs early;
+    const size_t first = static_cast<size_t>(blockIdx.x) * kWideTargets + tid % kWideTargets;
+    if (WIDE && tid < kWideTargets && first < a.n && MODE != STAGE_REDUCE_ONLY)
+        load_finish_inputs<MODE>(a, first, early);
+    pdl_enter();
     if (tid == 0)
         s_status = *reinterpret_cast<volatile int *>(&a.ctl->status);
     __syncthreads();
@@ -212,7 +254,9 @@ __global__ void __launch_bounds__(256) stage_kernel(const StageArgs a) {
                     ku += s_u[g][lane];
                     kv += s_v[g][lane];
                 }
-                finish_target<MODE>(a, i, ku, kv, dt, local_max, a.ex, a.ey);
+                if (i != first && MODE != STAGE_REDUCE_ONLY)
+                    load_finish_inputs<MODE>(a, i, early);
+                finish_target<MODE>(a, i, ku, kv, dt, local_max, a.ex, a.ey, early);
             }
             __syncthreads();
         }
@@ -237,7 +281,10 @@ __global__ void __launch_bounds__(256) stage_kernel(const StageArgs a) {
                 ku = a.kx[a.s][i];
                 kv = a.ky[a.s][i];
             }
-            finish_target<MODE>(a, i, ku, kv, dt, local_max, a.ex, a.ey);
+            FinishInputs in;
+            if (MODE != STAGE_REDUCE_ONLY)
+                load_finish_inputs<MODE>(a, i, in);
+            finish_target<MODE>(a, i, ku, kv, dt, local_max, a.ex, a.ey, in);
         }
     }
 
@@ -438,10 +485,14 @@ __global__ void __launch_bounds__(256) rk4_steps_kernel(const Rk4Steps p) {
                     kv += qv[li * nc + c];
                 }
                 // the slow path recomputes from this phase's positions, held in shared memory
-                if (s < 3)
-                    finish_target<STAGE_POSITION>(a, i, ku, kv, a.dt, local_max, sx, sy);
-                else
-                    finish_target<STAGE_RK4_COMBINE>(a, i, ku, kv, a.dt, local_max, sx, sy);
+                FinishInputs in;
+                if (s < 3) {
+                    load_finish_inputs<STAGE_POSITION>(a, i, in);
+                    finish_target<STAGE_POSITION>(a, i, ku, kv, a.dt, local_max, sx, sy, in);
+                } else {
+                    load_finish_inputs<STAGE_RK4_COMBINE>(a, i, in);
+                    finish_target<STAGE_RK4_COMBINE>(a, i, ku, kv, a.dt, local_max, sx, sy, in);
+                }
             }
             open_at += gridDim.x;
             if (!grid_barrier(p.barrier, open_at, status, p.spin_limit))
