@@ -685,10 +685,15 @@ def run_serving(budget: int = 10, streams=SERVING_STREAMS) -> dict:
            "server": [], "one_request_per_launch_fp64": []}
     for rate, count in streams:
         reqs = poisson_stream(count, rate, seed=int(rate), max_steps=budget)
-        # split: cheap and expensive requests in two batches (16 and 2 attempts per call), each
-        # driven by its own host thread and stream; waiting requests admitted shortest work first
+        # split_context: cheap requests share batched launches (16 attempts per call), expensive
+        # ones run one at a time on single-simulation contexts (each fills the GPU alone and
+        # gets the fastest kernels, the periodic box once per unordered pair), the two lanes on
+        # their own host threads and streams; waiting requests are admitted shortest work first;
+        # a cheap request that finds its lane idle is solved at once on a context. Measured
+        # against policy "split" (the expensive requests batched too): higher throughput and
+        # lower p50 and p99 at every rate.
         server = Server(capacity_vortices=4_000_000, max_slots=1024, attempts_per_tick=2,
-                        policy="split", order="sjf")
+                        policy="split_context", order="sjf", solo_max_steps=64)
         summary = server.serve(reqs)
         server.close()
         summary["rate_per_s"] = rate

@@ -362,6 +362,17 @@ __device__ __forceinline__ void run_item32(const GeometryConsts &g, const double
         u[k] = v[k] = 0.0f;
         ud[k] = vd[k] = 0.0;
     }
+    // the disk's pairs in f32x2 lanes (direct term, wall image): f32::disk_pair_x2
+    f32::DiskTarget2 t2[GEO == GEO_DISK ? T : 1];
+    float2 u2[GEO == GEO_DISK ? T : 1], v2[GEO == GEO_DISK ? T : 1];
+    float2 *s_g2 = reinterpret_cast<float2 *>(s_gf);
+    if (GEO == GEO_DISK) {
+#pragma unroll
+        for (int k = 0; k < T; ++k) {
+            t2[k] = f32::disk_target2(tg[k]);
+            u2[k] = v2[k] = make_float2(0.0f, 0.0f);
+        }
+    }
     const int ntiles = src1 > src0 ? static_cast<int>((src1 - src0 + kTileB - 1) / kTileB) : 0;
     const uint32_t seq0 = seq;
     auto issue = [&](int t) {
@@ -404,10 +415,13 @@ __device__ __forceinline__ void run_item32(const GeometryConsts &g, const double
         const int cnt = static_cast<int>(min(static_cast<size_t>(kTileB), src1 - j0));
         for (int j = tid; j < cnt; j += kBlock) {
             const double xj = s_x[st][j], yj = s_y[st][j];
-            s_f[j] = f32::split_position(xj, yj);
-            if (GEO == GEO_DISK)
-                s_fi[j] = f32::image_position(g, xj, yj);
-            s_gf[j] = static_cast<float>(s_g[st][j]);
+            if (GEO == GEO_DISK) {
+                f32::disk_pack_source(f32::split_position(xj, yj), f32::image_position(g, xj, yj),
+                                      static_cast<float>(s_g[st][j]), s_f[j], s_fi[j], s_g2[j]);
+            } else {
+                s_f[j] = f32::split_position(xj, yj);
+                s_gf[j] = static_cast<float>(s_g[st][j]);
+            }
         }
         __syncthreads();
         const bool diagonal = j0 < blk1 && blk0 < j0 + cnt;
@@ -416,9 +430,14 @@ __device__ __forceinline__ void run_item32(const GeometryConsts &g, const double
             if (diagonal) {
 #pragma unroll 1
                 for (int j = jb; j < je; ++j) {
-                    const float4 sf = s_f[j];
-                    const float4 si = GEO == GEO_DISK ? s_fi[j] : sf;
-                    const float gf = s_gf[j];
+                    float4 sf = s_f[j], si = sf;
+                    float gf;
+                    if (GEO == GEO_DISK) {
+                        f32::disk_unpack_source(sf, s_fi[j], sf, si);
+                        gf = s_g2[j].x;
+                    } else {
+                        gf = s_gf[j];
+                    }
 #pragma unroll
                     for (int q = 0; q < T; ++q) {  // ensembles: no near field (nothing is listed)
                         bool np, nw;
@@ -426,16 +445,26 @@ __device__ __forceinline__ void run_item32(const GeometryConsts &g, const double
                                                nw);
                     }
                 }
+            } else if (GEO == GEO_DISK) {
+#pragma unroll 4
+                for (int j = jb; j < je; ++j) {
+                    const float4 px4 = s_f[j], py4 = s_fi[j];
+                    const float2 g2 = s_g2[j];
+#pragma unroll
+                    for (int q = 0; q < T; ++q) {
+                        float closest = 0.0f;  // no near field in ensembles: unused
+                        f32::disk_pair_x2(f, t2[q], px4, py4, g2, u2[q], v2[q], closest);
+                    }
+                }
             } else {
 #pragma unroll 2
                 for (int j = jb; j < je; ++j) {
                     const float4 sf = s_f[j];
-                    const float4 si = GEO == GEO_DISK ? s_fi[j] : sf;
                     const float gf = s_gf[j];
 #pragma unroll
                     for (int q = 0; q < T; ++q) {
                         bool np, nw;
-                        f32::pair32<GEO, false>(f, tg[q], sf, si, gf, false, u[q], v[q], np, nw);
+                        f32::pair32<GEO, false>(f, tg[q], sf, sf, gf, false, u[q], v[q], np, nw);
                     }
                 }
             }
@@ -444,6 +473,13 @@ __device__ __forceinline__ void run_item32(const GeometryConsts &g, const double
                 ud[q] += static_cast<double>(u[q]);
                 vd[q] += static_cast<double>(v[q]);
                 u[q] = v[q] = 0.0f;
+                if (GEO == GEO_DISK) { // the direct and the image lanes, in that order
+                    ud[q] += static_cast<double>(u2[q].x);
+                    ud[q] += static_cast<double>(u2[q].y);
+                    vd[q] += static_cast<double>(v2[q].x);
+                    vd[q] += static_cast<double>(v2[q].y);
+                    u2[q] = v2[q] = make_float2(0.0f, 0.0f);
+                }
             }
         }
         __syncthreads();
@@ -480,7 +516,7 @@ __global__ void __launch_bounds__(kBlock) batch_velocity_kernel(const VelocityBa
     __shared__ alignas(128) double s_g[2][kTileB];
     __shared__ alignas(16) float4 s_f[PREC == PV_PRECISION_FP32C ? kTileB : 1];
     __shared__ alignas(16) float4 s_fi[PREC == PV_PRECISION_FP32C ? kTileB : 1];  // disk images
-    __shared__ float s_gf[PREC == PV_PRECISION_FP32C ? kTileB : 1];
+    __shared__ alignas(8) float s_gf[PREC == PV_PRECISION_FP32C ? 2 * kTileB : 1];  // disk: (g, -g)
     __shared__ alignas(8) uint64_t bars[2];
     __shared__ GeometryConsts s_geo;
     __shared__ unsigned s_item;

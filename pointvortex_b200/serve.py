@@ -62,6 +62,7 @@ class Completion:
     x: Optional[np.ndarray] = None
     y: Optional[np.ndarray] = None
     pairs: float = 0.0            # pair interactions evaluated for this request
+    engine: str = "batch"         # batch: in a batched launch; context: alone on a context
 
 
 # Relative cost of one ordered pair by geometry, from the measured FP64 pair rates of the
@@ -95,13 +96,39 @@ def poisson_stream(n_requests: int, rate: float, seed: int, n_min: int = 32, n_m
 
 
 class _Lane:
-    """One batch with its own queue of arrived requests."""
+    """One batch with its own queue of arrived requests. solo_max_steps > 0: a request that finds
+    the lane idle and alone in its queue, with a step budget of at most solo_max_steps, is solved
+    at once on the lane's own single-simulation contexts instead (a batch of one pays the batched
+    attempt's fixed launches; a context runs the attempt as one graph)."""
 
-    def __init__(self, capacity_vortices: int, max_slots: int, device: int, attempts: int):
+    def __init__(self, capacity_vortices: int, max_slots: int, device: int, attempts: int,
+                 solo_max_steps: int = 0):
         self.batch = Batch(capacity_vortices, max_slots, device)
         self.attempts = attempts
         self.ready: list = []            # (arrival, rid, request), in admission order
         self.running: dict[int, tuple] = {}
+        self.solo_max_steps = solo_max_steps
+        self.kernels = _contexts(device) if solo_max_steps > 0 else None
+
+    def take_solo(self):
+        """The request to solve alone now, removed from the queue, or None."""
+        if (self.kernels is None or self.running or len(self.ready) != 1 or
+                not 0 < self.ready[0][2].max_steps <= self.solo_max_steps):
+            return None
+        return self.ready.pop(0)[2]
+
+    def run_solo(self, server: "Server", req: "Request", clock, start: float, want_states: bool):
+        """(completion, x, y): the request solved alone; x, y the final positions if wanted."""
+        solver = _Solver(self.kernels, req)
+        while not solver.step():
+            pass
+        x = y = None
+        if server.keep_states or want_states:
+            x, y = solver.positions()
+        c = Completion(req.rid, solver.state, clock() - start - req.arrival, solver.steps,
+                       solver.t, x if server.keep_states else None,
+                       y if server.keep_states else None, solver.pairs(), engine="context")
+        return c, x, y
 
     def admit(self, server: "Server", now: float) -> int:
         return server._admit_lane(self, now)
@@ -114,6 +141,8 @@ class _Lane:
 
     def close(self) -> None:
         self.batch.close()
+        for k in (self.kernels or {}).values():
+            k.close()
 
 
 class _Solver:
@@ -206,7 +235,7 @@ class _ContextLane:
             x, y = solver.positions()
         c = Completion(req.rid, solver.state, now - req.arrival, solver.steps, solver.t,
                        x if server.keep_states else None, y if server.keep_states else None,
-                       solver.pairs())
+                       solver.pairs(), engine="context")
         server.completions.append(c)
         if on_complete is not None:
             on_complete(c, x, y)
@@ -228,12 +257,15 @@ class Server:
     the pace of an expensive one and the two batches' kernels overlap. policy "split_context":
     the expensive requests are instead solved one at a time on single-simulation contexts.
     order: "sjf" admits a lane's waiting requests shortest estimated work first, "fifo" in
-    arrival order (a request that does not fit blocks the ones behind it)."""
+    arrival order (a request that does not fit blocks the ones behind it). solo_max_steps > 0
+    (policies split and split_context): a cheap request that finds its lane idle is solved at once
+    on single-simulation contexts (_Lane.take_solo), so a lightly loaded server answers as fast as
+    one request per launch."""
 
     def __init__(self, capacity_vortices: int, max_slots: int, attempts_per_tick: int = 4,
                  device: int = 0, keep_states: bool = False, policy: str = "fifo",
                  split_work: float = 2.0 ** 26, small_attempts: int = 16, order: str = "fifo",
-                 expensive_fraction: float = 0.75):
+                 expensive_fraction: float = 0.75, solo_max_steps: int = 0):
         if policy not in ("fifo", "split", "split_context"):
             raise ValueError("policy must be fifo, split or split_context")
         if order not in ("fifo", "sjf"):
@@ -249,10 +281,12 @@ class Server:
         elif policy == "split":
             # the arena (the HBM budget) is shared out: most room to the expensive requests
             big = int(capacity_vortices * expensive_fraction)
-            self.lanes = [_Lane(capacity_vortices - big, max_slots, device, small_attempts),
+            self.lanes = [_Lane(capacity_vortices - big, max_slots, device, small_attempts,
+                                solo_max_steps),
                           _Lane(big, max(max_slots // 4, 1), device, attempts_per_tick)]
         else:
-            self.lanes = [_Lane(capacity_vortices, max_slots, device, small_attempts),
+            self.lanes = [_Lane(capacity_vortices, max_slots, device, small_attempts,
+                                solo_max_steps),
                           _ContextLane(device, attempts_per_tick)]
 
     @property
@@ -362,10 +396,26 @@ class Server:
                 while not finished.is_set():
                     with lock:
                         self._route(clock() - start)
-                        lane.admit(self, clock() - start)
-                        idle = not lane.running
+                        solo = lane.take_solo() if isinstance(lane, _Lane) else None
+                        if solo is None:
+                            lane.admit(self, clock() - start)
+                        idle = not lane.running and solo is None
+                        # sleep until the next arrival, at most 0.5 ms (another lane's arrival
+                        # may be first)
+                        nap = 0.0005
+                        if self.arrivals:
+                            nap = min(nap, max(0.0, self.arrivals[0][0] - (clock() - start)))
+                    if solo is not None:
+                        c, x, y = lane.run_solo(self, solo, clock, start, on_complete is not None)
+                        with lock:
+                            self.completions.append(c)
+                            if on_complete is not None:
+                                on_complete(c, x, y)
+                            if len(self.completions) >= total:
+                                finished.set()
+                        continue
                     if idle:
-                        time.sleep(0.0005)
+                        time.sleep(nap)
                         continue
                     lane.advance()   # the GIL is released inside the library calls
                     with lock:
@@ -394,12 +444,16 @@ def summarize(completions: list[Completion], elapsed: float) -> dict:
     states = {}
     for c in completions:
         states[c.state] = states.get(c.state, 0) + 1
+    engines = {}
+    for c in completions:
+        engines[c.engine] = engines.get(c.engine, 0) + 1
     pairs = sum(c.pairs for c in completions)
     return {"requests": len(completions), "elapsed_s": elapsed,
             "solves_per_s": len(completions) / elapsed if elapsed > 0 else 0.0,
             "pair_interactions_per_s": pairs / elapsed if elapsed > 0 else 0.0,
             "p50_latency_s": float(np.percentile(lat, 50)),
-            "p99_latency_s": float(np.percentile(lat, 99)), "states": states}
+            "p99_latency_s": float(np.percentile(lat, 99)), "states": states,
+            "engines": engines}
 
 
 def one_at_a_time(requests: list[Request], device: int = 0, clock=time.perf_counter) -> dict:
@@ -416,7 +470,7 @@ def one_at_a_time(requests: list[Request], device: int = 0, clock=time.perf_coun
         while not solver.step():
             pass
         out.append(Completion(req.rid, solver.state, clock() - start - req.arrival, solver.steps,
-                              solver.t, pairs=solver.pairs()))
+                              solver.t, pairs=solver.pairs(), engine="context"))
     for k in kernels.values():
         k.close()
     return summarize(out, clock() - start)

@@ -107,3 +107,40 @@ def test_split_context_policy_results_equal_alone_results():
         assert np.array_equal(c.x, x) and np.array_equal(c.y, y), req
         assert c.pairs > 0
     assert 0 < on_contexts < len(reqs)
+
+
+def test_idle_cheap_requests_are_solved_alone_on_contexts():
+    """solo_max_steps: a cheap request that finds its lane idle and alone in its queue is solved at
+    once on single-simulation contexts (the same result as alone on a context); requests that
+    arrive together are batched (the same result as alone in a batch)."""
+    reqs = poisson_stream(10, rate=60.0, seed=13, n_min=32, n_max=800, t_end_range=(0.01, 0.02),
+                          rtols=(1e-6, 1e-9), max_steps=12)
+    # two requests at the same instant: they cannot both go solo
+    reqs[5].arrival = reqs[4].arrival
+    server = Server(capacity_vortices=20000, max_slots=8, attempts_per_tick=2, keep_states=True,
+                    policy="split", split_work=2.0 ** 30, small_attempts=4, order="sjf",
+                    solo_max_steps=16)
+    streamed = []
+    summary = server.serve(reqs, on_complete=lambda c, x, y: streamed.append((c.rid, x is not None)))
+    server.close()
+    assert summary["requests"] == len(reqs) == len(streamed)
+    assert all(has_state for _, has_state in streamed)
+    by_id = {c.rid: c for c in server.completions}
+    engines = set()
+    for req in reqs:
+        c = by_id[req.rid]
+        engines.add(c.engine)
+        if c.engine == "context":
+            state, steps, (x, y) = alone_on_a_context(req)
+            assert c.state == state and c.accepted_steps == steps, req
+        else:
+            info, (x, y) = alone(req)
+            assert c.state == info.state and c.accepted_steps == info.acceptedSteps, req
+        assert np.array_equal(c.x, x) and np.array_equal(c.y, y), req
+    assert "context" in engines
+    # a request with a budget above solo_max_steps never goes solo
+    big = poisson_stream(1, rate=10.0, seed=14, n_min=32, n_max=64, max_steps=40)
+    server = Server(capacity_vortices=20000, max_slots=8, policy="split", solo_max_steps=16)
+    server.serve(big)
+    server.close()
+    assert server.completions[0].engine == "batch"
