@@ -14,12 +14,16 @@
 //   d2 = dx*dx + dy*dy (two products, one sum, each rounded) < threshold*threshold;
 //   disk wall image: r2 = x*x + y*y > 0, image = (R*R - r2)/sqrt(r2), image*image < threshold^2.
 #include "pv_internal.h"
+#include "pv_pair32.cuh"
+
+#include <cmath>
+#include <limits>
 
 namespace pvb {
 
 namespace {
-constexpr int kDT = 128;  // targets per block
-constexpr int kDS = 32;   // sources per block
+constexpr int kDT = 128;  // targets per block (one per thread)
+constexpr int kDS = 128;  // sources per block
 
 __device__ __forceinline__ void push(DipoleCandidateDev *out, size_t capacity,
                                      unsigned long long *count, unsigned long long a,
@@ -32,25 +36,59 @@ __device__ __forceinline__ void push(DipoleCandidateDev *out, size_t capacity,
     }
 }
 
-// Block (source tile of kDS, target block of kDT): every unordered pair i < j once. Short source
-// tiles give many CTAs, so the scan hides its latency at small N too.
+// The exact test of one pair (i < j), bit for bit the reference's (see the file comment).
+__device__ __forceinline__ void exact_pair(const GeometryConsts &gc, double xi, double yi,
+                                           bool neg_i, size_t i, double xj, double yj, double gj,
+                                           size_t j, double thr2, DipoleCandidateDev *out,
+                                           size_t capacity, unsigned long long *count) {
+    double dx = xi - xj, dy = yi - yj;
+    if (gc.geometry == GEO_PERIODIC) {
+        dx = exact_remainder(dx, gc.lx, gc.inv_lx, gc.half_lx);
+        dy = exact_remainder(dy, gc.ly, gc.inv_ly, gc.half_ly);
+    }
+    const double d2 = __dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy));
+    if (d2 < thr2 && gj != 0.0 && neg_i != static_cast<bool>(signbit(gj)))
+        push(out, capacity, count, i, j, d2);
+}
+
+// Blocks cover the tiles (target block I, source block J >= I), b = J (J + 1) / 2 + I: every
+// unordered pair i < j once, and no block starts only to find its tile below the diagonal.
+//
+// Prefilter (prefilter != 0): the squared minimum-image distance in FP32 from double-float
+// coordinates (hi = fp32(x), lo = fp32(x - hi); the displacement (t_hi - s_hi) + (t_lo - s_lo)
+// and its remainder keep a few FP32 ulp of relative accuracy whatever the coordinates' size, as in
+// the FP32-compensated velocity) in f32x2 lanes (x, y). Only a pair whose FP32 distance is not
+// above thr2f = thr2 (1 + 2^-12) -- a margin far above those errors -- or is not finite takes the
+// exact FP64 test, so the candidates are exactly the reference's. The host turns the prefilter
+// off when the threshold is not small against the box (the FP32 remainder could then pick
+// another image than the exact one for a pair within reach).
 __global__ void __launch_bounds__(kDT)
     dipole_scan_kernel(const double *x, const double *y, const double *g, size_t n,
-                       GeometryConsts gc, double thr2, DipoleCandidateDev *out, size_t capacity,
-                       unsigned long long *count, const DeviceControl *gate) {
+                       GeometryConsts gc, double thr2, float thr2f, int prefilter,
+                       DipoleCandidateDev *out, size_t capacity, unsigned long long *count,
+                       const DeviceControl *gate) {
+    __shared__ alignas(16) float4 s_neg[kDS];  // (-x_hi, -y_hi, -x_lo, -y_lo) of the sources
+    __shared__ double sx[kDS], sy[kDS], sg[kDS];
     pdl_enter();
     if (gate && !gate->accepted)  // after a DOPRI5 attempt: only the accepted state is scanned
         return;
-    const size_t i0 = static_cast<size_t>(blockIdx.y) * kDT;
-    const size_t j0 = static_cast<size_t>(blockIdx.x) * kDS;
-    if (j0 + kDS <= i0 + 1)  // every source of the tile precedes every target of the block
-        return;
-    __shared__ double sx[kDS], sy[kDS], sg[kDS];
-    if (threadIdx.x < kDS) {
-        const size_t jl = j0 + threadIdx.x;
-        sx[threadIdx.x] = jl < n ? x[jl] : 0.0;
-        sy[threadIdx.x] = jl < n ? y[jl] : 0.0;
-        sg[threadIdx.x] = jl < n ? g[jl] : 0.0;
+    const unsigned b = blockIdx.x;
+    unsigned J = static_cast<unsigned>((sqrt(8.0 * b + 1.0) - 1.0) * 0.5);
+    while (static_cast<unsigned long long>(J + 1) * (J + 2) / 2 <= b)
+        ++J;
+    while (static_cast<unsigned long long>(J) * (J + 1) / 2 > b)
+        --J;
+    const unsigned I = b - J * (J + 1) / 2;
+    const size_t i0 = static_cast<size_t>(I) * kDT;
+    const size_t j0 = static_cast<size_t>(J) * kDS;
+    for (int t = threadIdx.x; t < kDS; t += kDT) {
+        const size_t jl = j0 + t;
+        const double xj = jl < n ? x[jl] : 0.0, yj = jl < n ? y[jl] : 0.0;
+        sx[t] = xj;
+        sy[t] = yj;
+        sg[t] = jl < n ? g[jl] : 0.0;
+        const float4 f = f32::split_position(xj, yj);
+        s_neg[t] = make_float4(-f.x, -f.y, -f.z, -f.w);
     }
     __syncthreads();
     const size_t i = i0 + threadIdx.x;
@@ -62,24 +100,36 @@ __global__ void __launch_bounds__(kDT)
     const bool periodic = gc.geometry == GEO_PERIODIC;
     const int jcount = static_cast<int>(min(static_cast<size_t>(kDS), n - j0));
     const bool neg_i = signbit(gi);
-    // every pair's distance first (no divergence); the order and sign conditions only for the
-    // rare pair closer than the threshold
+    if (prefilter) {
+        const float4 t = f32::split_position(xi, yi);
+        const float2 th = make_float2(t.x, t.y), tl = make_float2(t.z, t.w);
+        const float inv_l = static_cast<float>(gc.inv_lx);
+        const float l_hi = static_cast<float>(gc.lx);
+        const float l_lo = static_cast<float>(gc.lx - static_cast<double>(l_hi));
 #pragma unroll 4
-    for (int jj = 0; jj < jcount; ++jj) {
-        double dx = xi - sx[jj], dy = yi - sy[jj];
-        if (periodic) {
-            dx = exact_remainder(dx, gc.lx, gc.inv_lx, gc.half_lx);
-            dy = exact_remainder(dy, gc.ly, gc.inv_ly, gc.half_ly);
+        for (int jj = 0; jj < jcount; ++jj) {
+            const float4 s = s_neg[jj];
+            float2 r = f32::add2(f32::add2(th, make_float2(s.x, s.y)),
+                                 f32::add2(tl, make_float2(s.z, s.w)));
+            if (periodic) {
+                const float2 q = f32::mul2(r, f32::splat2(inv_l));
+                const float2 m = make_float2(rintf(q.x), rintf(q.y));
+                r = f32::fma2(m, f32::splat2(-l_lo), f32::fma2(m, f32::splat2(-l_hi), r));
+            }
+            const float d2f = fmaf(r.x, r.x, r.y * r.y);
+            if (!(d2f > thr2f) && j0 + jj > i)  // rare: the exact test
+                exact_pair(gc, xi, yi, neg_i, i, sx[jj], sy[jj], sg[jj], j0 + jj, thr2, out,
+                           capacity, count);
         }
-        const double d2 = __dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy));
-        if (d2 < thr2) {
-            const double gj = sg[jj];
-            if (j0 + jj > i && gj != 0.0 && neg_i != static_cast<bool>(signbit(gj)))
-                push(out, capacity, count, i, j0 + jj, d2);
-        }
+    } else {
+#pragma unroll 4
+        for (int jj = 0; jj < jcount; ++jj)
+            if (j0 + jj > i)
+                exact_pair(gc, xi, yi, neg_i, i, sx[jj], sy[jj], sg[jj], j0 + jj, thr2, out,
+                           capacity, count);
     }
-    // the wall image of each target once: in the block whose source tile starts at the target block
-    if (gc.geometry == GEO_DISK && j0 == i0) {
+    // the wall image of each target once: in the block of its own tile
+    if (gc.geometry == GEO_DISK && I == J) {
         const double r2 = __dadd_rn(__dmul_rn(xi, xi), __dmul_rn(yi, yi));
         if (r2 > 0.0) {
             const double image = __ddiv_rn(__dsub_rn(gc.radius2, r2), __dsqrt_rn(r2));
@@ -147,12 +197,23 @@ cudaError_t launch_dipole_scan(const double *x, const double *y, const double *g
     }
     if (n == 0)
         return cudaSuccess;
-    const size_t nt = (n + kDT - 1) / kDT, ns = (n + kDS - 1) / kDS;
-    if (nt > 65535)
+    const size_t nb = (n + kDT - 1) / kDT;  // kDT == kDS: target and source blocks alike
+    const size_t blocks = nb * (nb + 1) / 2;
+    if (blocks > 0x7fffffffu)
         return cudaErrorInvalidValue;
-    const dim3 grid(static_cast<unsigned>(ns), static_cast<unsigned>(nt));
-    return launch_pdl(dipole_scan_kernel, grid, dim3(kDT), 0, stream, x, y, gamma, n, g,
-                      threshold * threshold, out, capacity, count, gate);
+    const double thr2 = threshold * threshold;
+    // the FP32 prefilter needs a threshold well inside the FP32 range and, in the box, small
+    // against the box (so the FP32 minimum image is the exact one for every pair within reach)
+    const bool small = thr2 > 0.0 && thr2 < 1e30 &&
+                       (g.geometry != GEO_PERIODIC ||
+                        (threshold < 0.125 * g.lx && threshold < 0.125 * g.ly &&
+                         g.lx == g.ly));
+    const float thr2f = small ? std::nextafter(static_cast<float>(thr2 * (1.0 + 1.0 / 4096.0)),
+                                               std::numeric_limits<float>::infinity())
+                              : 0.0f;
+    return launch_pdl(dipole_scan_kernel, dim3(static_cast<unsigned>(blocks)), dim3(kDT), 0,
+                      stream, x, y, gamma, n, g, thr2, thr2f, small ? 1 : 0, out, capacity, count,
+                      gate);
 }
 
 namespace {
