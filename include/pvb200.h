@@ -377,7 +377,8 @@ pv_status pv_get_symmetric_tuning(int geometry, int precision, int log2_n, int *
 /* Near-field radius of the FP32-compensated form (precision PV_PRECISION_FP32C): periodic pairs
  * closer than it (minimum image), disk pairs closer than it and disk wall images closer than it to
  * their target are left out of the FP32 sums and evaluated in FP64. radius < 0 selects the default for the population (twice
- * the mean spacing of N uniform vortices), 0 turns the near field off. Applies to the device state
+ * the mean spacing of N uniform vortices in the periodic box, once in the disk), 0 turns the near
+ * field off. Applies to the device state
  * at once and to later evaluations; the plane and FP64 contexts ignore it. No reference
  * counterpart (the reference evaluates in FP64 only). */
 pv_status pv_set_near_field(pv_context *ctx, double radius);

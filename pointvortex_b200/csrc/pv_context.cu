@@ -124,6 +124,8 @@ struct pv_context {
     // FP32C near field (pv_set_near_field): the lists of pairs left to the FP64 pass, and the
     // radius (< 0: the default for the population, 0: none)
     DeviceArray near_count, near_slot;
+    // an evaluation's near-field pass, left to the stage launched after it (StageArgs::near)
+    NearPass pending_near{};
     double near_radius = -1.0;
 
     // polls of the bounded device waits (pv_set_wait_limits): tile copies, grid barrier
@@ -462,6 +464,11 @@ f32::NearLists near_lists(const pv_context *c) {
 
 // Velocity of the state positions (px, py) into k_s via partials + stage kernel.
 pv_status launch_eval(pv_context *c, const double *px, const double *py) {
+    if (c->pending_near.lists.count) {  // a near pass no stage took over: it still resets the lists
+        const NearPass stale = c->pending_near;
+        c->pending_near = NearPass{};
+        PV_CUDA(c, counted(c, PV_KERNEL_NEAR, 1, [&] { return launch_near_field(stale, c->stream); }));
+    }
     const bool near = near_field_used(c);
     const f32::NearLists lists = near ? near_lists(c) : f32::NearLists{nullptr, nullptr};
     NearPass np{};
@@ -486,8 +493,7 @@ pv_status launch_eval(pv_context *c, const double *px, const double *py) {
         if (near) {
             np.pr = reinterpret_cast<double2 *>(c->pu.p);
             np.rows = c->sym.blocks;
-            PV_CUDA(c, counted(c, PV_KERNEL_NEAR, 1,
-                               [&] { return launch_near_field(np, c->stream); }));
+            c->pending_near = np;  // the stage after this evaluation runs it
         }
         ++c->evaluations;
         return PV_OK;
@@ -519,10 +525,16 @@ pv_status launch_eval(pv_context *c, const double *px, const double *py) {
         np.pu = c->pu.p;
         np.pv = c->pv.p;
         np.rows = c->plan.num_chunks;
-        PV_CUDA(c, counted(c, PV_KERNEL_NEAR, 1, [&] { return launch_near_field(np, c->stream); }));
+        c->pending_near = np;  // the stage after this evaluation runs it
     }
     ++c->evaluations;
     return PV_OK;
+}
+
+// The stage launched after an evaluation takes over its near-field pass, if launch_eval left one.
+void attach_pending_near(pv_context *c, StageArgs &s) {
+    s.near = c->pending_near;
+    c->pending_near = NearPass{};
 }
 
 StageArgs stage_base(pv_context *c) {
@@ -711,7 +723,7 @@ pv_status evaluate_host(pv_context *c, const double *x, const double *y, const d
         np.stride = stride;
         np.rows = plan.num_chunks;
         np.g = a.g;
-        PV_CUDA(c, counted(c, PV_KERNEL_NEAR, 1, [&] { return launch_near_field(np, c->stream); }));
+        c->pending_near = np;  // the stage below runs it
     }
     StageArgs s{};
     s.n = nt;
@@ -732,6 +744,7 @@ pv_status evaluate_host(pv_context *c, const double *x, const double *y, const d
     s.nonfinite_ok = nonfinite_is_error ? 0 : 1;
     s.ctl = c->ctl;
     s.g = c->gc;
+    attach_pending_near(c, s);
     PV_CUDA(c, counted(c, PV_KERNEL_STAGE, 1, [&] { return launch_stage(s, c->stream, c->sm_count); }));
     PV_CUDA(c, cudaMemcpyAsync(u, c->eu.p, nt * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
     PV_CUDA(c, cudaMemcpyAsync(v, c->ev.p, nt * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
@@ -972,6 +985,7 @@ pv_status enqueue_state_velocity(pv_context *ctx) {
     s.ky[0] = ctx->p1y.p;
     s.ex = ctx->x.p;
     s.ey = ctx->y.p;
+    attach_pending_near(ctx, s);
     PV_CUDA(ctx, counted(ctx, PV_KERNEL_STAGE, 1,
                          [&] { return launch_stage(s, ctx->stream, ctx->sm_count); }));
     return PV_OK;
@@ -1059,7 +1073,8 @@ pv_status enqueue_rk4(pv_context *c, double dt) {
     for (int s = 0; s < 4; ++s) {
         if ((st = launch_eval(c, px, py)) != PV_OK)
             return st;
-        const StageArgs a = rk4_stage(c, dt, s);
+        StageArgs a = rk4_stage(c, dt, s);
+        attach_pending_near(c, a);
         PV_CUDA(c, counted(c, PV_KERNEL_STAGE, 1, [&] { return launch_stage(a, c->stream, c->sm_count); }));
         px = a.xt;
         py = a.yt;
@@ -1199,6 +1214,7 @@ pv_status enqueue_dopri_attempt(pv_context *ctx, bool need_k0) {
             for (int j = 0; j < 7; ++j)
                 a.w[j] = w[j];
         }
+        attach_pending_near(ctx, a);
         PV_CUDA(ctx, counted(ctx, PV_KERNEL_STAGE, 1,
                              [&] { return launch_stage(a, ctx->stream, ctx->sm_count); }));
         if (s < 6) {

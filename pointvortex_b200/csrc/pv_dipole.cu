@@ -22,8 +22,8 @@
 namespace pvb {
 
 namespace {
-constexpr int kDT = 128;  // targets per block (one per thread)
-constexpr int kDS = 128;  // sources per block
+constexpr int kDT = 64;  // targets per block (one per thread)
+constexpr int kDS = 64;  // sources per block
 
 __device__ __forceinline__ void push(DipoleCandidateDev *out, size_t capacity,
                                      unsigned long long *count, unsigned long long a,
@@ -55,20 +55,25 @@ __device__ __forceinline__ void exact_pair(const GeometryConsts &gc, double xi, 
 // unordered pair i < j once, and no block starts only to find its tile below the diagonal.
 //
 // Prefilter (prefilter != 0): the squared minimum-image distance in FP32 from double-float
-// coordinates (hi = fp32(x), lo = fp32(x - hi); the displacement (t_hi - s_hi) + (t_lo - s_lo)
-// and its remainder keep a few FP32 ulp of relative accuracy whatever the coordinates' size, as in
-// the FP32-compensated velocity) in f32x2 lanes (x, y). Only a pair whose FP32 distance is not
-// above thr2f = thr2 (1 + 2^-12) -- a margin far above those errors -- or is not finite takes the
-// exact FP64 test, so the candidates are exactly the reference's. The host turns the prefilter
-// off when the threshold is not small against the box (the FP32 remainder could then pick
-// another image than the exact one for a pair within reach).
+// coordinates (hi = fp32(x), lo = fp32(x - hi)): d = (t_hi - s_hi) + (t_lo - s_lo), then
+// r = d - m L with m = round(d / L) and L = l_hi + l_lo, in f32x2 lanes (x, y). Only a pair whose
+// FP32 distance is not above the target's bound thr2f, or is not finite, takes the exact FP64
+// test, so the candidates are exactly the reference's. The bound covers the FP32 errors: with M
+// the largest coordinate magnitude of the target and the block's sources, each component of d
+// is within 2^-22 * 2M of the exact difference (two roundings of differences of coordinates up
+// to M, the lo parts' own error below 2^-48 M), and r adds 2^-22 |r| (two roundings; a wrong m
+// is only possible for |r| near L/2, a pair out of reach); so a true candidate (|r| < thr) has
+// |r_fp32| < thr + e per component with e = 2^-21 M + 2^-22 thr, and its computed squared
+// distance is below thr2f = (thr + 2e)^2 (1 + 2^-20). The host turns the prefilter off when the
+// threshold is not small against the box (0.125 L).
 __global__ void __launch_bounds__(kDT)
     dipole_scan_kernel(const double *x, const double *y, const double *g, size_t n,
-                       GeometryConsts gc, double thr2, float thr2f, int prefilter,
+                       GeometryConsts gc, double thr2, int prefilter,
                        DipoleCandidateDev *out, size_t capacity, unsigned long long *count,
                        const DeviceControl *gate) {
     __shared__ alignas(16) float4 s_neg[kDS];  // (-x_hi, -y_hi, -x_lo, -y_lo) of the sources
     __shared__ double sx[kDS], sy[kDS], sg[kDS];
+    __shared__ unsigned s_mag;                  // bits of the sources' largest |coordinate|
     pdl_enter();
     if (gate && !gate->accepted)  // after a DOPRI5 attempt: only the accepted state is scanned
         return;
@@ -81,6 +86,9 @@ __global__ void __launch_bounds__(kDT)
     const unsigned I = b - J * (J + 1) / 2;
     const size_t i0 = static_cast<size_t>(I) * kDT;
     const size_t j0 = static_cast<size_t>(J) * kDS;
+    if (threadIdx.x == 0)
+        s_mag = 0u;
+    __syncthreads();
     for (int t = threadIdx.x; t < kDS; t += kDT) {
         const size_t jl = j0 + t;
         const double xj = jl < n ? x[jl] : 0.0, yj = jl < n ? y[jl] : 0.0;
@@ -89,6 +97,10 @@ __global__ void __launch_bounds__(kDT)
         sg[t] = jl < n ? g[jl] : 0.0;
         const float4 f = f32::split_position(xj, yj);
         s_neg[t] = make_float4(-f.x, -f.y, -f.z, -f.w);
+        // non-negative floats order as their bits; a NaN's bits exceed every finite one's
+        const float mag = fmaxf(fabsf(static_cast<float>(xj)), fabsf(static_cast<float>(yj)));
+        atomicMax(&s_mag, __float_as_uint(isnan(xj) || isnan(yj) ? __int_as_float(0x7fc00000)
+                                                                   : mag));
     }
     __syncthreads();
     const size_t i = i0 + threadIdx.x;
@@ -101,26 +113,50 @@ __global__ void __launch_bounds__(kDT)
     const int jcount = static_cast<int>(min(static_cast<size_t>(kDS), n - j0));
     const bool neg_i = signbit(gi);
     if (prefilter) {
+        // this target's bound (see above), rounded up to FP32; a NaN coordinate makes it NaN,
+        // and then every pair takes the exact test
+        const float smag = __uint_as_float(s_mag);
+        const double m = fmax(fmax(fabs(xi), fabs(yi)), static_cast<double>(smag));
+        const double thr = sqrt(thr2);
+        const double e = 0x1p-21 * m + 0x1p-22 * thr;
+        const double bound = (thr + 2.0 * e) * (thr + 2.0 * e) * (1.0 + 0x1p-20);
+        const float thr2f = isnan(smag) || isnan(xi) || isnan(yi) ? __int_as_float(0x7fc00000)
+                                                                  : __double2float_ru(bound);
         const float4 t = f32::split_position(xi, yi);
         const float2 th = make_float2(t.x, t.y), tl = make_float2(t.z, t.w);
         const float inv_l = static_cast<float>(gc.inv_lx);
         const float l_hi = static_cast<float>(gc.lx);
         const float l_lo = static_cast<float>(gc.lx - static_cast<double>(l_hi));
-#pragma unroll 4
-        for (int jj = 0; jj < jcount; ++jj) {
+        // the squared FP32 distance to source jj; rounding to an integer by adding and subtracting
+        // 1.5 * 2^23 (round to nearest even for |q| < 2^22, as rintf) keeps it on the FMA pipe
+        const auto dist2 = [&](int jj) {
             const float4 s = s_neg[jj];
             float2 r = f32::add2(f32::add2(th, make_float2(s.x, s.y)),
                                  f32::add2(tl, make_float2(s.z, s.w)));
             if (periodic) {
                 const float2 q = f32::mul2(r, f32::splat2(inv_l));
-                const float2 m = make_float2(rintf(q.x), rintf(q.y));
+                const float2 m = f32::add2(f32::add2(q, f32::splat2(12582912.0f)),
+                                           f32::splat2(-12582912.0f));
                 r = f32::fma2(m, f32::splat2(-l_lo), f32::fma2(m, f32::splat2(-l_hi), r));
             }
-            const float d2f = fmaf(r.x, r.x, r.y * r.y);
-            if (!(d2f > thr2f) && j0 + jj > i)  // rare: the exact test
-                exact_pair(gc, xi, yi, neg_i, i, sx[jj], sy[jj], sg[jj], j0 + jj, thr2, out,
-                           capacity, count);
+            return fmaf(r.x, r.x, r.y * r.y);
+        };
+        // no branch per pair: the smallest distance decides whether the exact tests run (rarely).
+        // In the diagonal tile only sources after the target count (the target itself is at 0).
+        float closest = __int_as_float(0x7f800000);
+        bool nonfinite = false;
+        const int first = I == J ? static_cast<int>(i - j0) + 1 : 0;
+#pragma unroll 4
+        for (int jj = first; jj < jcount; ++jj) {
+            const float d2f = dist2(jj);
+            closest = fminf(closest, d2f);
+            nonfinite |= !(d2f == d2f);
         }
+        if (!(closest > thr2f) || nonfinite)
+            for (int jj = first; jj < jcount; ++jj)
+                if (!(dist2(jj) > thr2f))
+                    exact_pair(gc, xi, yi, neg_i, i, sx[jj], sy[jj], sg[jj], j0 + jj, thr2, out,
+                               capacity, count);
     } else {
 #pragma unroll 4
         for (int jj = 0; jj < jcount; ++jj)
@@ -208,12 +244,8 @@ cudaError_t launch_dipole_scan(const double *x, const double *y, const double *g
                        (g.geometry != GEO_PERIODIC ||
                         (threshold < 0.125 * g.lx && threshold < 0.125 * g.ly &&
                          g.lx == g.ly));
-    const float thr2f = small ? std::nextafter(static_cast<float>(thr2 * (1.0 + 1.0 / 4096.0)),
-                                               std::numeric_limits<float>::infinity())
-                              : 0.0f;
     return launch_pdl(dipole_scan_kernel, dim3(static_cast<unsigned>(blocks)), dim3(kDT), 0,
-                      stream, x, y, gamma, n, g, thr2, thr2f, small ? 1 : 0, out, capacity, count,
-                      gate);
+                      stream, x, y, gamma, n, g, thr2, small ? 1 : 0, out, capacity, count, gate);
 }
 
 namespace {

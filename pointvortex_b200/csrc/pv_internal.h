@@ -158,6 +158,10 @@ struct StageArgs {
     double w[7];                    // DOPRI5: b5 - b4
     DeviceControl *ctl;
     GeometryConsts g;
+    // FP32C: the near-field pass of the evaluation whose partial rows this stage reduces, fused
+    // into it (near.lists.count == nullptr: none; reduce must be 1). The stage's target i is the
+    // lists' target near.t_begin + i.
+    NearPass near;
 };
 
 cudaError_t launch_stage(const StageArgs &a, cudaStream_t stream, int sm_count);

@@ -20,6 +20,7 @@
 #include "pv_internal.h"
 
 #include <algorithm>
+#include <type_traits>
 
 namespace pvb {
 
@@ -182,6 +183,88 @@ __device__ __forceinline__ void finish_target(const StageArgs &a, size_t i, doub
     }
 }
 
+// The near-field terms of the block's kWideTargets targets, fused into the wide stage (the work of
+// pv_near.cu's near_field_kernel): the kWideGroups threads of a target share its listed entries
+// (at most f32::kNearSlots), each computes its entries' FP64 terms (the plain kernels' pair
+// functions) and their rank in (source, image) order, and the target's first thread adds them in
+// that order, so the sum does not depend on the order of the listing. A target with more
+// entries than slots is evaluated whole in FP64 instead (the threads striding over the sources,
+// their sums added in thread order), replacing its partial rows. Every count is reset.
+// Returns, for the calling first thread (group 0) of target `lane`, the near sum (nu, nv) and
+// whether it replaces the rows.
+struct NearScratch {
+    unsigned key[16][f32::kNearSlots];
+    double tu[16][f32::kNearSlots], tv[16][f32::kNearSlots];
+    unsigned count[16];
+};
+
+__device__ __forceinline__ bool fused_near(const NearPass &np, size_t i, bool valid, int lane,
+                                           int group, int groups, NearScratch &sc, double &nu,
+                                           double &nv) {
+    const size_t gi = np.t_begin + i;
+    if (group == 0) {
+        unsigned c = 0;
+        if (valid) {
+            c = np.lists.count[gi];
+            if (c)
+                np.lists.count[gi] = 0u;
+        }
+        sc.count[lane] = c;
+    }
+    __syncthreads();
+    const unsigned count = sc.count[lane];
+    bool whole = false;
+    nu = nv = 0.0;
+    const double tx = valid && count ? np.x[gi] : 0.0, ty = valid && count ? np.y[gi] : 0.0;
+    if (count > static_cast<unsigned>(f32::kNearSlots)) {
+        // overflow: the whole target in FP64
+        double su = 0.0, sv = 0.0;
+        for (size_t j = group; j < np.n; j += groups) {
+            if (np.g.geometry == GEO_PERIODIC)
+                PeriodicPair::pair<true>(np.g, tx, ty, np.x[j], np.y[j], np.gs[j], j == gi, su,
+                                         sv);
+            else
+                DiskPair::pair<true>(np.g, tx, ty, np.x[j], np.y[j], np.gs[j], j == gi, su, sv);
+        }
+        sc.tu[lane][group] = su;
+        sc.tv[lane][group] = sv;
+        whole = true;
+    } else if (count) {
+        for (int e = group; e < static_cast<int>(count); e += groups) {
+            const unsigned v = np.lists.slot[gi * f32::kNearSlots + e];
+            sc.key[lane][e] = (v & ~f32::kNearImage) * 2u + (v >> 31);
+        }
+    }
+    __syncthreads();
+    if (!whole && count) {
+        for (int e = group; e < static_cast<int>(count); e += groups) {
+            const unsigned key = sc.key[lane][e];
+            int rank = 0;
+            for (int k = 0; k < static_cast<int>(count); ++k)
+                rank += sc.key[lane][k] < key ? 1 : 0;
+            double du = 0.0, dv = 0.0;
+            const size_t j = key >> 1;
+            if (key & 1u)
+                DiskPair::image(np.g, tx, ty, np.x[j], np.y[j], np.gs[j], du, dv);
+            else if (np.g.geometry == GEO_PERIODIC)
+                PeriodicPair::pair<false>(np.g, tx, ty, np.x[j], np.y[j], np.gs[j], false, du, dv);
+            else
+                DiskPair::direct(tx, ty, np.x[j], np.y[j], np.gs[j], du, dv);
+            sc.tu[lane][rank] = du;
+            sc.tv[lane][rank] = dv;
+        }
+    }
+    __syncthreads();
+    if (group == 0 && count) {
+        const int terms = whole ? groups : static_cast<int>(count);
+        for (int r = 0; r < terms; ++r) {
+            nu += sc.tu[lane][r];
+            nv += sc.tv[lane][r];
+        }
+    }
+    return whole;
+}
+
 // WIDE: many partial rows (the symmetric kernel's). A block then covers kWideTargets targets with
 // 256 / kWideTargets row groups: thread (group, t) sums rows group, group + groups, ...
 // (coalesced over the targets), and the threads of group 0 add the group sums in fixed order.
@@ -189,12 +272,13 @@ __device__ __forceinline__ void finish_target(const StageArgs &a, size_t i, doub
 constexpr int kWideTargets = 16;
 constexpr int kWideGroups = 256 / kWideTargets;
 
-template <int MODE, bool WIDE>
+template <int MODE, bool WIDE, bool NEAR = false>
 __global__ void __launch_bounds__(256) stage_kernel(const StageArgs a) {
     __shared__ int s_status;
     __shared__ double s_max[8];
     __shared__ double s_u[WIDE ? kWideGroups : 1][kWideTargets],
         s_v[WIDE ? kWideGroups : 1][kWideTargets];
+    __shared__ typename std::conditional<NEAR, NearScratch, char>::type s_near;
     const int tid = threadIdx.x;
     // WIDE: the finishing threads load their first target's FinishInputs before the wait
     FinishInputs early;
@@ -205,8 +289,14 @@ __global__ void __launch_bounds__(256) stage_kernel(const StageArgs a) {
     if (tid == 0)
         s_status = *reinterpret_cast<volatile int *>(&a.ctl->status);
     __syncthreads();
-    if (s_status != 0)
+    if (s_status != 0) {
+        if (NEAR)  // the next evaluation starts from empty lists
+            for (size_t i = static_cast<size_t>(blockIdx.x) * kWideTargets + tid; i < a.n;
+                 i += static_cast<size_t>(gridDim.x) * kWideTargets)
+                if (tid < kWideTargets)
+                    a.near.lists.count[a.near.t_begin + i] = 0u;
         return;
+    }
 
     const double dt = a.dt_from_control ? a.ctl->dt : a.dt;
     double local_max = 0.0;
@@ -247,12 +337,20 @@ __global__ void __launch_bounds__(256) stage_kernel(const StageArgs a) {
             }
             s_u[group][lane] = su;
             s_v[group][lane] = sv;
+            double nu = 0.0, nv = 0.0;
+            bool whole = false;
+            if constexpr (NEAR)  // its barriers also order the row sums above
+                whole = fused_near(a.near, i, i < a.n, lane, group, kWideGroups, s_near, nu, nv);
             __syncthreads();
             if (group == 0 && i < a.n) {
                 double ku = s_u[0][lane], kv = s_v[0][lane];
                 for (int g = 1; g < kWideGroups; ++g) {
                     ku += s_u[g][lane];
                     kv += s_v[g][lane];
+                }
+                if (NEAR) {  // the near terms after the rows, or instead of them
+                    ku = whole ? nu : ku + nu;
+                    kv = whole ? nv : kv + nv;
                 }
                 if (i != first && MODE != STAGE_REDUCE_ONLY)
                     load_finish_inputs<MODE>(a, i, early);
@@ -341,10 +439,17 @@ constexpr int kWideRows = 32;
 
 template <int MODE>
 cudaError_t launch_stage_mode(const StageArgs &a, cudaStream_t stream, int sm_count) {
-    if (a.reduce && a.num_chunks >= kWideRows) {
+    const bool near = a.near.lists.count != nullptr;
+    if (near && !a.reduce)
+        return cudaErrorInvalidValue;
+    // the near-field terms need the wide layout (a target's threads share its list), whatever
+    // the number of rows
+    if (a.reduce && (a.num_chunks >= kWideRows || near)) {
         const size_t blocks = (a.n + kWideTargets - 1) / kWideTargets;
         const size_t cap = static_cast<size_t>(sm_count > 0 ? sm_count : 148) * 8;
         const unsigned grid = static_cast<unsigned>(blocks < 1 ? 1 : (blocks < cap ? blocks : cap));
+        if (near)
+            return launch_pdl(stage_kernel<MODE, true, true>, dim3(grid), dim3(256), 0, stream, a);
         return launch_pdl(stage_kernel<MODE, true>, dim3(grid), dim3(256), 0, stream, a);
     }
     return launch_pdl(stage_kernel<MODE, false>, dim3(grid_for(a.n, sm_count)), dim3(256), 0,
