@@ -256,8 +256,9 @@ class Server:
     host threads drive the two batches on their own streams, so cheap requests are never held to
     the pace of an expensive one and the two batches' kernels overlap. policy "split_context":
     the expensive requests are instead solved one at a time on single-simulation contexts.
-    order: "sjf" admits a lane's waiting requests shortest estimated work first, "fifo" in
-    arrival order (a request that does not fit blocks the ones behind it). solo_max_steps > 0
+    order: "sjf" admits a batch lane's waiting requests shortest estimated work first, "fifo" in
+    arrival order (a request that does not fit blocks the ones behind it); the context lane of
+    split_context always takes its requests in arrival order. solo_max_steps > 0
     (policies split and split_context): a cheap request that finds its lane idle is solved at once
     on single-simulation contexts (_Lane.take_solo), so a lightly loaded server answers as fast as
     one request per launch."""
@@ -311,8 +312,10 @@ class Server:
             lane.ready.append(item)
             touched.add(id(lane))
         if self.order == "sjf":
+            # the context lane (split_context) keeps arrival order: it runs one request at a
+            # time, and shortest-first there would hold the largest requests back without bound
             for lane in self.lanes:
-                if id(lane) in touched:
+                if id(lane) in touched and not isinstance(lane, _ContextLane):
                     lane.ready.sort(key=lambda it: (work(it[2]), it[0], it[1]))
 
     def _admit_lane(self, lane: _Lane, now: float) -> int:
