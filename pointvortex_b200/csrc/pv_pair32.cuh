@@ -105,26 +105,27 @@ __device__ __forceinline__ float2 mul2(float2 a, float2 b) { return __fmul2_rn(a
 __device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
 __device__ __forceinline__ float2 swap2(float2 a) { return make_float2(a.y, a.x); }
 
-// sinh, sin and cos of t (|t| <= pi/2) for both lanes, the FP32 truncation of the shared series in
-// pv_common.cuh (first omitted term below 1e-8 relative; cosh t is not needed in FP32).
+// sinh, sin and cos of t (|t| <= pi/2) for both lanes, from the grouping of the shared series in
+// pv_common.cuh (sinh t = t (E1 + t^2 O1), sin t = t (E1 - t^2 O1), cos t = E0 - t^2 O0 in
+// w = t^4) at FP32 accuracy: E1, E0 and O0 are their degree-3 Taylor polynomials economized to
+// degree 2 over w in [0, (pi/2)^4] (Lanczos: the w^3 term traded for the shifted Chebyshev
+// polynomial of that degree), adding at most 1.1e-9, 1.5e-8 and 8e-11 to them; O1 keeps its three
+// Taylor terms (economizing it would add 3e-7 to sinh). cosh t is not needed in FP32. O0 is
+// evaluated negated, so that cos needs no negation.
 __device__ __forceinline__ void sh_sn_cs_x2(float2 t, float2 &sh, float2 &sn, float2 &cs) {
-    const float2 m1 = splat2(-1.0f);
     const float2 t2 = mul2(t, t), w = mul2(t2, t2);
-    float2 e1 = fma2(w, splat2(1.6059043836821613e-10f), splat2(2.7557319223985893e-06f)); // 1/13!, 1/9!
-    e1 = fma2(w, e1, splat2(8.333333333333333e-03f));
+    float2 e1 = fma2(w, splat2(2.7571984e-06f), splat2(8.33333e-03f));
     e1 = fma2(w, e1, splat2(1.0f));
     float2 o1 = fma2(w, splat2(2.505210838544172e-08f), splat2(1.984126984126984e-04f)); // 1/11!, 1/7!
     o1 = fma2(w, o1, splat2(1.6666666666666666e-01f));
-    float2 e0 = fma2(w, splat2(2.08767569878681e-09f), splat2(2.48015873015873e-05f)); // 1/12!, 1/8!
-    e0 = fma2(w, e0, splat2(4.1666666666666664e-02f));
+    float2 e0 = fma2(w, splat2(2.4820652e-05f), splat2(4.1666623e-02f));
     e0 = fma2(w, e0, splat2(1.0f));
-    float2 o0 = fma2(w, splat2(1.1470745597729725e-11f), splat2(2.755731922398589e-07f)); // 1/14!, 1/10!
-    o0 = fma2(w, o0, splat2(1.388888888888889e-03f));
-    o0 = fma2(w, o0, splat2(0.5f));
+    float2 o0n = fma2(w, splat2(-2.7567793e-07f), splat2(-1.3888887e-03f));
+    o0n = fma2(w, o0n, splat2(-0.5f));
     const float2 t3 = mul2(t, t2), te1 = mul2(t, e1);
     sh = fma2(t3, o1, te1);
-    sn = fma2(mul2(t3, m1), o1, te1);
-    cs = fma2(mul2(t2, m1), o0, e0);
+    sn = fma2(mul2(t3, splat2(-1.0f)), o1, te1);
+    cs = fma2(t2, o0n, e0);
 }
 
 // The periodic pair's core in FP32, both axes at once (lane 0: the target's u term, lane 1: its v
@@ -147,11 +148,12 @@ __device__ __forceinline__ bool periodic_core_x2(const F32Geometry &f, float2 th
     float2 shh, snh, csh;
     sh_sn_cs_x2(h, shh, snh, csh);
     const float2 tsh = mul2(splat2(2.0f), shh), tsn = mul2(splat2(2.0f), snh);
-    const float2 cosh_ = fma2(tsh, shh, splat2(1.0f));                  // cosh x^ = 1 + 2 sinh^2
-    const float2 cos_ = fma2(mul2(splat2(-2.0f), snh), snh, splat2(1.0f)); // cos x^ = 1 - 2 sin^2
-    const float2 sin_ = mul2(tsn, csh);                                  // sin x^ = 2 sin cos
+    const float2 sn2 = mul2(tsn, snh);                          // 2 sin^2
+    const float2 cosh_ = fma2(tsh, shh, splat2(1.0f));          // cosh x^ = 1 + 2 sinh^2
+    const float2 cos_ = fma2(sn2, splat2(-1.0f), splat2(1.0f)); // cos x^ = 1 - 2 sin^2
+    const float2 sin_ = mul2(tsn, csh);                         // sin x^ = 2 sin cos
     // d0 = (2 (sh_x^2 + sn_y^2), 2 (sh_y^2 + sn_x^2))
-    float2 d0 = fma2(tsh, shh, swap2(mul2(tsn, snh)));
+    float2 d0 = fma2(tsh, shh, swap2(sn2));
     if (near || self)
         d0 = splat2(1.0f);
     // the images m != 0 of each lane's axis, as PeriodicPair::image_sum; C = cosh of the lane's

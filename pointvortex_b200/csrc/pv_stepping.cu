@@ -195,24 +195,15 @@ __device__ __forceinline__ void finish_target(const StageArgs &a, size_t i, doub
 struct NearScratch {
     unsigned key[16][f32::kNearSlots];
     double tu[16][f32::kNearSlots], tv[16][f32::kNearSlots];
-    unsigned count[16];
 };
 
 __device__ __forceinline__ bool fused_near(const NearPass &np, size_t i, bool valid, int lane,
                                            int group, int groups, NearScratch &sc, double &nu,
                                            double &nv) {
     const size_t gi = np.t_begin + i;
-    if (group == 0) {
-        unsigned c = 0;
-        if (valid) {
-            c = np.lists.count[gi];
-            if (c)
-                np.lists.count[gi] = 0u;
-        }
-        sc.count[lane] = c;
-    }
-    __syncthreads();
-    const unsigned count = sc.count[lane];
+    // every thread of the target reads its count (the first one resets it after the barrier
+    // below, once all have read it)
+    const unsigned count = valid ? np.lists.count[gi] : 0u;
     bool whole = false;
     nu = nv = 0.0;
     const double tx = valid && count ? np.x[gi] : 0.0, ty = valid && count ? np.y[gi] : 0.0;
@@ -236,6 +227,8 @@ __device__ __forceinline__ bool fused_near(const NearPass &np, size_t i, bool va
         }
     }
     __syncthreads();
+    if (group == 0 && count)
+        np.lists.count[gi] = 0u;
     if (!whole && count) {
         for (int e = group; e < static_cast<int>(count); e += groups) {
             const unsigned key = sc.key[lane][e];

@@ -73,3 +73,38 @@ def test_economized_coefficients_stay_near_taylor():
         assert abs(low_first[0] - taylor[name][0]) <= 1e-14 * taylor[name][0], name
         for got, exact in zip(low_first, taylor[name]):
             assert abs(got - exact) <= 0.05 * exact, (name, got, exact)
+
+
+PAIR32 = pathlib.Path(__file__).resolve().parent.parent / "pointvortex_b200" / "csrc" / "pv_pair32.cuh"
+
+
+def _fp32_coefficients():
+    text = PAIR32.read_text()
+    body = text[text.index("void sh_sn_cs_x2"):]
+    body = body[: body.index("\n}\n")]
+    num = r"([-0-9.e+]+)f"
+    polys = {}
+    for name in ("e1", "o1", "e0", "o0n"):
+        first = re.search(rf"float2 {name} = fma2\(w, splat2\({num}\), splat2\({num}\)\);", body)
+        rest = re.findall(rf"\n\s*{name} = fma2\(w, {name}, splat2\({num}\)\);", body)
+        assert first, name
+        polys[name] = [float(first.group(1)), float(first.group(2))] + [float(c) for c in rest]
+    return {k: np.array(v, dtype=np.float32).astype(np.float64).tolist() for k, v in polys.items()}
+
+
+def test_fp32_series_is_accurate_to_fp32():
+    """The FP32 periodic pair's economized series (csrc/pv_pair32.cuh): sinh and sin within 1e-7
+    and cos within 2e-7 absolute of the functions over |t| <= pi/2, evaluated in float64 with
+    the FP32 coefficients (the coefficients' own rounding included)."""
+    p = _fp32_coefficients()
+    t = np.linspace(-np.pi / 2, np.pi / 2, 200001)
+    t2 = t * t
+    w = t2 * t2
+    e1, o1, e0, o0n = (_horner(p[k], w) for k in ("e1", "o1", "e0", "o0n"))
+    sh = t * e1 + t * t2 * o1
+    sn = t * e1 - t * t2 * o1
+    cs = e0 + t2 * o0n
+    nz = t != 0
+    assert np.max(np.abs((sh - np.sinh(t))[nz] / np.sinh(t)[nz])) <= 1e-7
+    assert np.max(np.abs((sn - np.sin(t))[nz] / np.sin(t)[nz])) <= 1e-7
+    assert np.max(np.abs(cs - np.cos(t))) <= 2e-7
