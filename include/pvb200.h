@@ -368,7 +368,8 @@ pv_status pv_get_tuning(int geometry, int precision, int log2_n, int *per_thread
 /* Autotuner table of the once-per-unordered-pair form (periodic box and plane), by geometry,
  * precision and floor(log2 N): mode 0 restores the built-in plan, 1 selects the ordered kernel,
  * 2 the symmetric form; min_ctas (periodic FP64: 7 or 8, else 0) selects the kernel built for that
- * many resident CTAs per SM; targets (plane: 4 or 8, else 0) the targets per lane. Process-wide;
+ * many resident CTAs per SM; targets (plane: 4 or 8; periodic FP64: 2, with min_ctas 0; else 0)
+ * the targets per lane off the diagonal. Process-wide;
  * read when a context plans its device state (pv_upload_state). No reference counterpart. */
 pv_status pv_set_symmetric_tuning(int geometry, int precision, int log2_n, int mode, int min_ctas,
                                   int targets);

@@ -327,7 +327,8 @@ enum SymKernel : int {
     SYM_PLANE32_WIDE = 5,
     SYM_PERIODIC_7 = 6,   // the periodic FP64 kernel built for 7 resident CTAs per SM
     SYM_PERIODIC_8 = 7,   // ... and for 8
-    SYM_KERNELS = 8
+    SYM_PERIODIC_T2 = 8,  // the periodic FP64 kernel with two targets per lane off the diagonal
+    SYM_KERNELS = 9
 };
 
 int kernel_of(const SymmetricPlan &p) {
@@ -338,6 +339,8 @@ int kernel_of(const SymmetricPlan &p) {
     }
     if (fp32c)
         return SYM_PERIODIC32;
+    if (p.targets == 2)
+        return SYM_PERIODIC_T2;
     return p.min_ctas == 8 ? SYM_PERIODIC_8 : (p.min_ctas == 7 ? SYM_PERIODIC_7 : SYM_PERIODIC);
 }
 
@@ -382,6 +385,9 @@ int resident_ctas(int a, int kernel) {
         case SYM_PERIODIC_8:
             blocks = occupancy(symmetric_kernel<sym::PeriodicSym, 1, 8>, smem);
             break;
+        case SYM_PERIODIC_T2:
+            blocks = occupancy(symmetric_kernel<sym::PeriodicSym, 2>, smem);
+            break;
         default:
             blocks = occupancy(symmetric_kernel<sym::PeriodicSym, 1>, smem);
             break;
@@ -413,7 +419,9 @@ bool symmetric_tuning_store(int geometry, int precision, int log2_n, int mode, i
                            (min_ctas == 7 || min_ctas == 8)))
         return false;
     if (targets != 0 && !(geometry == GEO_INFINITE && (targets == kPlaneTargets ||
-                                                      targets == kPlaneTargetsWide)))
+                                                      targets == kPlaneTargetsWide)) &&
+        !(geometry == GEO_PERIODIC && precision == PV_PRECISION_FP64 && targets == 2 &&
+          min_ctas == 0))
         return false;
     const int packed = mode == 0 ? 0 : (mode | (min_ctas << 4) | (targets << 8));
     g_sym_tuning[geometry == GEO_PERIODIC ? 1 : 0][precision][log2_n].store(
@@ -441,10 +449,11 @@ SymmetricPlan plan_symmetric(size_t n, int sm_count, int precision, int geometry
     // the smallest block that keeps the partial rows within kSymmetricPartialBytes, or the largest
     // block up to kSymmetricPartialBytesMax (N ~ 3.7e5); beyond that the ordered kernel runs. The
     // plane's blocks hold at least as many sub-blocks as a lane holds targets.
+    // the periodic FP64 kernel: two targets per lane only where the table asks for it
     const int targets =
         plane ? (tuned_targets ? tuned_targets
                                : (n >= kSymmetricPlaneWideN ? kPlaneTargetsWide : kPlaneTargets))
-              : 1;
+              : (precision == PV_PRECISION_FP64 && tuned_targets == 2 ? 2 : 1);
     p.min_ctas = tuned_ctas;
     const size_t np = (n + 255) & ~static_cast<size_t>(255);
     for (int a = targets; a <= 16; a *= 2) {
@@ -506,6 +515,9 @@ cudaError_t launch_symmetric(const double *x, const double *y, const double *gs,
                           gs, n, p.a, items, p.items, counter, rows, stride, g);
     case SYM_PERIODIC_8:
         return launch_pdl(symmetric_kernel<sym::PeriodicSym, 1, 8>, grid, block, smem, stream, x, y,
+                          gs, n, p.a, items, p.items, counter, rows, stride, g);
+    case SYM_PERIODIC_T2:
+        return launch_pdl(symmetric_kernel<sym::PeriodicSym, 2>, grid, block, smem, stream, x, y,
                           gs, n, p.a, items, p.items, counter, rows, stride, g);
     default:
         return launch_pdl(symmetric_kernel<sym::PeriodicSym, 1>, grid, block, smem, stream, x, y,

@@ -79,11 +79,15 @@ def test_symmetric_tuning_table_round_trip_and_validation():
         assert autotune.get_symmetric_entry(periodic, fp64, 12) == (2, 8, 0)
         autotune.set_symmetric_entry(plane, fp32c, 15, 2, 0, 8)
         assert autotune.get_symmetric_entry(plane, fp32c, 15) == (2, 0, 8)
+        autotune.set_symmetric_entry(periodic, fp64, 12, 2, 0, 2)
+        assert autotune.get_symmetric_entry(periodic, fp64, 12) == (2, 0, 2)
         autotune.set_symmetric_entry(periodic, fp64, 12, 1)
         assert autotune.get_symmetric_entry(periodic, fp64, 12) == (1, 0, 0)
         for bad in [(2, fp64, 12, 2, 0, 0),        # the disk has no symmetric form
                     (periodic, fp32c, 12, 2, 8, 0),  # occupancy variants: periodic FP64 only
                     (plane, fp64, 15, 2, 0, 3),      # plane targets: 4 or 8
+                    (periodic, fp64, 12, 2, 8, 2),   # periodic two targets: no occupancy variant
+                    (periodic, fp32c, 12, 2, 0, 2),  # ... and FP64 only
                     (periodic, fp64, 12, 3, 0, 0)]:  # modes 0..2
             with pytest.raises(ValueError):
                 autotune.set_symmetric_entry(*bad)

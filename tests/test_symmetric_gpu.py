@@ -238,15 +238,42 @@ def test_tuning_table_changes_the_plan_and_keeps_parity(port):
     seen = []
     saved = autotune.get_symmetric_entry(1, 0, 12)
     try:
-        for entry in [(1,), (2, 7), (2, 8), (0,)]:
+        for entry in [(1,), (2, 7), (2, 8), (2, 0, 2), (0,)]:
             autotune.set_symmetric_entry(1, 0, 12, *entry)
             k = pv.PeriodicBoxKernel(2.0, 2.0, 8)
             k.uploadDeviceState(pv.VortexSystem(x, y, g))
             plan = k.statePlan()
-            seen.append((plan["symmetric"], plan["symmetric_min_ctas"]))
+            seen.append((plan["symmetric"], plan["symmetric_min_ctas"],
+                         plan["symmetric_targets"] if plan["symmetric"] else 0))
             f = k.evaluateDeviceState()
             assert normalized_error(f.x, f.y, ur, vr).max() <= 1e-12, entry
             k.close()
     finally:
         autotune.set_symmetric_entry(1, 0, 12, *saved)
-    assert seen == [(False, 0), (True, 7), (True, 8), (True, 0)]
+    assert seen == [(False, 0, 0), (True, 7, 1), (True, 8, 1), (True, 0, 2), (True, 0, 1)]
+
+
+def test_periodic_two_targets_per_lane_ragged_against_ordered_and_oracle(port):
+    """The periodic kernel with two targets per lane (blocks of 64, table entry targets = 2) on a
+    population that ends inside a block: the same velocities as the oracle and the ordered
+    kernel, within the parity tolerance."""
+    from pointvortex_b200 import autotune
+    n = 4136
+    x, y, g = ics.periodic_box(n, 92, 2.0)
+    geo = Geometry("periodic", box_length_x=2.0, box_length_y=2.0)
+    saved = autotune.get_symmetric_entry(1, 0, 12)
+    try:
+        autotune.set_symmetric_entry(1, 0, 12, 2, 0, 2)
+        k = pv.PeriodicBoxKernel(2.0, 2.0, 8)
+        k.uploadDeviceState(pv.VortexSystem(x, y, g))
+        plan = k.statePlan()
+        assert plan["symmetric"] and plan["symmetric_targets"] == 2
+        f = k.evaluateDeviceState()
+        ordered = k.evaluate(x, y, g)
+        k.close()
+    finally:
+        autotune.set_symmetric_entry(1, 0, 12, *saved)
+    assert normalized_error(f.x, f.y, ordered.x, ordered.y).max() <= 1e-12
+    for t0, t1 in ((0, 64), (n - 72, n)):
+        u, v = port.evaluate_range(geo, x, y, g, t0, t1)
+        assert normalized_error(f.x[t0:t1], f.y[t0:t1], u, v).max() <= 1e-12
