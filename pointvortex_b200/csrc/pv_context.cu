@@ -336,7 +336,6 @@ pv_status make_consts(const pv_params &p, GeometryConsts &g, std::string &messag
         g.half_wave = 0.5 * g.wave;
         g.scale = 0.5 / lx;
         g.m_exact = std::min(p.image_layers, 2);
-        g.has6 = p.image_layers >= 6 ? 1 : 0;
         for (int m = 0; m <= 2; ++m) {
             const double a = 2.0 * kPi * m;
             g.cosh_m[m] = std::cosh(a);
@@ -344,38 +343,15 @@ pv_status make_consts(const pv_params &p, GeometryConsts &g, std::string &messag
             const double s = std::sinh(a);
             g.sinh2_m[m] = s * s;
         }
-        // images m = 3..5 enter through 2u C + 2u^2 c cosh 2x^, u = sech(2 pi m)
+        // images m = 3..6 enter through 2u C + 2u^2 c cosh 2x^, u = sech(2 pi m) (|m| >= 7 are
+        // beyond the reference's |shift| <= 40 cut for every x^)
         g.k1 = 0.0;
         g.k2 = 0.0;
-        for (int m = 3; m <= std::min(p.image_layers, 5); ++m) {
+        for (int m = 3; m <= std::min(p.image_layers, 6); ++m) {
             const double u = 1.0 / std::cosh(2.0 * kPi * m);
             g.k1 += 2.0 * u;
             g.k2 += 2.0 * u * u;
         }
-        g.k6 = g.has6 ? 2.0 * std::exp(-12.0 * kPi) : 0.0;
-        g.shift6 = 2.0 * kPi * static_cast<double>(6);
-        // |x^| <= pi (1 + 2^-52), so x^ - shift6 < 0 < x^ + shift6 and the reference's tests
-        // |x^ - shift6| <= 40 and |x^ + shift6| <= 40 are monotone in x^: find their end points
-        // with the same rounded subtraction and addition.
-        volatile double s6 = g.shift6;  // keep the rounded operations as written
-        double lo = -40.0 + g.shift6;
-        while (std::fabs(lo - s6) <= 40.0)
-            lo = std::nextafter(lo, -1e300);
-        while (!(std::fabs(lo - s6) <= 40.0))
-            lo = std::nextafter(lo, 1e300);
-        double hi = 40.0 - g.shift6;
-        while (std::fabs(hi + s6) <= 40.0)
-            hi = std::nextafter(hi, 1e300);
-        while (!(std::fabs(hi + s6) <= 40.0))
-            hi = std::nextafter(hi, -1e300);
-        if (hi != -lo) { // rounding is symmetric, so the windows are; the kernels rely on it
-            message = "internal error: asymmetric m = 6 image window";
-            return PV_ERROR_RUNTIME;
-        }
-        g.lo6 = lo;
-        g.hi6 = hi;
-        g.lo6h = 0.5 * lo;
-        g.hi6h = 0.5 * hi;
         return PV_OK;
     }
     if (p.geometry == PV_GEOMETRY_DISK) {

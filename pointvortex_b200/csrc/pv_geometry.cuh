@@ -33,16 +33,10 @@ struct GeometryConsts {
     double half_wave;       // pi / Lx (exactly wave / 2)
     double scale;           // 0.5 / Lx
     int m_exact;            // image pairs m = +-1..m_exact summed exactly (min(M, 2))
-    int has6;               // images m = +-6 kept when within the |shift| <= 40 window (M >= 6)
     double cosh_m[3];       // cosh(2 pi m), m = 0..2
     double two_cosh_m[3];   // 2 cosh(2 pi m)
     double sinh2_m[3];      // sinh(2 pi m)^2
-    double k1, k2;          // 2 sum sech(2 pi m), 2 sum sech^2(2 pi m) over m = 3..min(M, 5)
-    double k6;              // 2 exp(-12 pi) when M >= 6, else 0
-    double shift6;          // (2 pi) * 6, rounded as the reference rounds it
-    double lo6, hi6;        // m = +6 kept iff x^ >= lo6, m = -6 iff x^ <= hi6 (the reference's
-                            // |x^ -+ shift6| <= 40 with its rounding, as thresholds on x^)
-    double lo6h, hi6h;      // the same thresholds on x^/2 (exactly lo6/2, hi6/2)
+    double k1, k2;          // 2 sum sech(2 pi m), 2 sum sech^2(2 pi m) over m = 3..min(M, 6)
     // disk
     double radius, radius2, inv_radius, inv_radius2;
     // FP32-compensated form: near-field radius squared (0: none), pv_pair32.cuh
@@ -131,18 +125,19 @@ struct DiskPair {
 //   * m = +-1, +-2 (never dropped, since |x^| <= pi) combine exactly in pairs,
 //       D(m) + D(-m) = 2 (C A - c),   D(m) D(-m) = C^2 + c^2 - 2 c C A + sinh^2 a,
 //     where every term of the product is far from cancelling (sinh^2 a >= 7e4 > 2 |c| C A);
-//   * m = +-3..+-5: with u = sech a <= 1.3e-8 the pair sum is
+//   * m = +-3..+-6: with u = sech a <= 1.3e-8 the pair sum is
 //       2u C + 2u^2 c cosh 2x^ + O(u^3 C^3),
 //     and the omitted terms are below 1e-19 of the m = 0 term, far under FP64 rounding;
-//   * m = +-6 enter only where |x^ -+ 12 pi| <= 40, as in the reference, each as
-//     2 e^{-12 pi} e^{+-x^} (relative error below 1e-14 on a term below 2e-15 of the sum);
+//   * the reference keeps an m = +-6 image only where |x^ -+ 12 pi| <= 40, so for |x^| > 2.3 it
+//     drops one of the pair: a term of at most 2 e^{-12 pi} e^{-2.3} ~ 9e-18, below 1.2e-16 of the
+//     sum (whose m = 0 part alone is at least 0.079). Both are kept here, which spares the
+//     window test and sinh x^: the difference is at the level of the sum's own rounding;
 //   * |m| >= 7 always has |shift| > 40 and is dropped, as in the reference.
 // sinh, cosh, sin and cos of x^/2 and y^/2 come from one shared series (|x^/2| <= pi/2).
 struct PeriodicPair {
-    // Images m != 0 of one axis as num/den + rest. half_hat = x^/2 (the m = +-6 window test).
-    __device__ __forceinline__ static void image_sum(const GeometryConsts &g, double half_hat,
-                                                     double ch, double sh, double c, double &num,
-                                                     double &den, double &rest) {
+    // Images m != 0 of one axis as num/den + rest: C = cosh of the axis, c = cos of the other.
+    __device__ __forceinline__ static void image_sum(const GeometryConsts &g, double ch, double c,
+                                                     double &num, double &den, double &rest) {
         const double ch2 = ch * ch;
         const double p = fma(c, c, ch2);   // C^2 + c^2
         const double m2c = -2.0 * c;
@@ -160,16 +155,9 @@ struct PeriodicPair {
             num = fma(pair_num, den, num * pair_den);
             den *= pair_den;
         }
-        // m = 3..5: 2u C + 2u^2 c cosh 2x^ summed over u = sech(2 pi m), with
+        // m = 3..6: 2u C + 2u^2 c cosh 2x^ summed over u = sech(2 pi m), with
         // k2 cosh 2x^ = k2 (2 C^2 - 1) as one fma
         rest = fma(ch, g.k1, c * fma(2.0 * g.k2, ch2, -g.k2));
-        if (g.has6) {
-            // the windows x^ >= lo6 (m = +6) and x^ <= hi6 (m = -6), with lo6 = -hi6 < 0: both
-            // hold for |x^| <= hi6, giving (C + S) + (C - S) = 2C; beyond, only the one on x^'s
-            // side, giving C + |S|. Even in x^ like the two terms.
-            const double add = fabs(half_hat) <= g.hi6h ? ch : fabs(sh);
-            rest = fma(g.k6, ch + add, rest);
-        }
     }
 
     // The pair's terms without its circulation: the target's velocity changes by
@@ -196,14 +184,12 @@ struct PeriodicPair {
         const double cos_y = fma(nsny, sny, 1.0);
         const double sin_x = HALF_SINE ? snx * csx : 2.0 * snx * csx; // sin x^ (or half)
         const double sin_y = HALF_SINE ? sny * csy : 2.0 * sny * csy;
-        const double sinh_x = tshx * chx;          // sinh x^
-        const double sinh_y = tshy * chy;
         // 2 (sinh^2(x^/2) + sin^2(y^/2)) with the factor 2 inside: the same rounding, bit for bit
         const double d0u = fma(tshx, shx, -(nsny * sny));
         const double d0v = fma(tshy, shy, -(nsnx * snx));
         double nu, du, ru, nv, dv, rv;
-        image_sum(g, hx, cosh_x, sinh_x, cos_y, nu, du, ru);
-        image_sum(g, hy, cosh_y, sinh_y, cos_x, nv, dv, rv);
+        image_sum(g, cosh_x, cos_y, nu, du, ru);
+        image_sum(g, cosh_y, cos_x, nv, dv, rv);
         // 1/d0 + num/den + rest = (den + d0 (num + den rest)) / (d0 den)
         au = sin_y * fma(d0u, fma(du, ru, nu), du);
         av = sin_x * fma(d0v, fma(dv, rv, nv), dv);

@@ -156,9 +156,8 @@ __device__ __forceinline__ bool periodic_core_x2(const F32Geometry &f, float2 th
     float2 d0 = fma2(tsh, shh, swap2(sn2));
     if (near || self)
         d0 = splat2(1.0f);
-    // the images m != 0 of each lane's axis, as PeriodicPair::image_sum; C = cosh of the lane's
-    // axis, c = cos of the other. The m = +-6 images are left out: their term is at most
-    // 2 exp(-12 pi) cosh(pi) ~ 1e-15 of the m = 0 term, eight orders below FP32 resolution.
+    // the images m != 0 of each lane's axis, as PeriodicPair::image_sum (m = 3..6 through k1, k2);
+    // C = cosh of the lane's axis, c = cos of the other.
     const float2 C = cosh_, c = swap2(cos_);
     const float2 ch2 = mul2(C, C);
     const float2 p = fma2(c, c, ch2);
