@@ -54,10 +54,11 @@ FLOPS_PER_PAIR_PERIODIC = 240
 # 240 plus two more FMA updates (the source's reaction) per unordered pair.
 FLOPS_PER_UNORDERED_PAIR_SYMMETRIC = 244
 # The work these counts state is kept fixed, so that the roofline fraction stays comparable as the
-# kernel changes. What the kernel now executes per unordered pair is less: the half angles come
-# from one multiply by pi/L (2 flops fewer) and the four series polynomials are economized, one
-# FMA fewer each per half angle (16 flops fewer): 226.
-FLOPS_EXECUTED_PER_UNORDERED_PAIR_SYMMETRIC = 226
+# kernel changes. What the kernel now executes per unordered pair is less (economized series,
+# shared doubled values, the m = 1, 2 fraction started from m = 1, the m = +-6 images in the
+# m = 3..6 expansion): 189, counted by ncu as 2 x DFMA + DMUL + DADD per unordered pair (72.5,
+# 36.3 and 8.1 FP64 instructions) at N = 4096.
+FLOPS_EXECUTED_PER_UNORDERED_PAIR_SYMMETRIC = 189
 # The plane in the same count: an ordered pair is 11 (displacement 2, r^2 3, reciprocal 1, scale
 # 1, two FMA updates 4); the symmetric form spends 16 per unordered pair (the shared displacement,
 # r^2 and reciprocal, the two kernel values 2, four FMA updates 8).
