@@ -134,7 +134,7 @@ __device__ __forceinline__ void sh_sn_cs_x2(float2 t, float2 &sh, float2 &sn, fl
 
 // The periodic pair's core in FP32, both axes at once (lane 0: the target's u term, lane 1: its v
 // term). th/tl and sh/sl are the (x, y) hi and lo parts of target and source. Returns the near
-// verdict (minimum-image distance below the near-field radius); a2 = (sin y^ N_u, sin x^ N_v)
+// decision (minimum-image distance below the near-field radius); a2 = (sin y^ N_u, sin x^ N_v)
 // and b2 = (d0_u den_u, d0_v den_v): the terms are a2 / b2. skip (near or the self pair) sets
 // d0 = 1 so that b2 stays finite; the caller discards those terms.
 __device__ __forceinline__ bool periodic_core_x2(const F32Geometry &f, float2 th, float2 tl,
@@ -191,7 +191,7 @@ struct Target32 {
 // negates the displacement exactly, and every quantity below is an exactly odd or even function
 // of it, so ku and kv are exactly odd: the symmetric kernels use one evaluation for both.
 // Returns true for a near pair (minimum-image distance below the near-field radius, the same
-// verdict from either side): its terms are then 0 here and come from the FP64 pass.
+// decision from either side): its terms are then 0 here and come from the FP64 pass.
 __device__ __forceinline__ bool periodic_values32(const F32Geometry &f, const float4 t,
                                                   const float4 s, float &ku, float &kv) {
     float2 a2, b2;
@@ -344,7 +344,7 @@ __device__ __forceinline__ void disk_pair_x2(const F32Geometry &f, const DiskTar
 // Lists the near terms that disk_pair_x2 left out among the staged sources [jb, je) (source
 // index j0 + j), for every lane whose `flagged` is set, the whole warp at a time: the flagged
 // target is broadcast and each lane recomputes the squared distances (the same operations, so
-// the same verdicts) of every 32nd source. Near terms are rare (a dozen per target at the default
+// the same decisions) of every 32nd source. Near terms are rare (a dozen per target at the default
 // radius), so this runs for few blocks; all 32 lanes must be present.
 __device__ __forceinline__ void disk_list_near_x2(const F32Geometry &f, const NearLists &lists,
                                                   const DiskTarget2 &t, size_t ti, bool flagged,
