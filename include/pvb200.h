@@ -223,6 +223,7 @@ typedef struct pv_plan_info {
     int chunk;              /* ordered kernel: sources per work item */
     int symmetric_min_ctas; /* symmetric form: the kernel built for this many CTAs per SM (0: default) */
     int symmetric_targets;  /* symmetric form: targets per lane off the diagonal */
+    int symmetric_grid_ctas; /* symmetric form: persistent CTAs per SM of its grid */
 } pv_plan_info;
 pv_status pv_state_plan(const pv_context *ctx, pv_plan_info *info);
 
@@ -375,6 +376,13 @@ pv_status pv_set_symmetric_tuning(int geometry, int precision, int log2_n, int m
                                   int targets);
 pv_status pv_get_symmetric_tuning(int geometry, int precision, int log2_n, int *mode,
                                   int *min_ctas, int *targets);
+/* Autotuner table of the symmetric form's persistent grid: CTAs per SM for a geometry (0 plane,
+ * 1 periodic), a precision and populations N with floor(log2 N) == log2_n (0 restores as many as
+ * fit, the default; a value above what fits is clamped to it). Fewer CTAs than fit can finish
+ * sooner: the work queue's last round of items is then fuller. Process-wide; read when a context
+ * plans its device state (pv_upload_state). No reference counterpart. */
+pv_status pv_set_symmetric_grid(int geometry, int precision, int log2_n, int ctas_per_sm);
+pv_status pv_get_symmetric_grid(int geometry, int precision, int log2_n, int *ctas_per_sm);
 /* Near-field radius of the FP32-compensated form (precision PV_PRECISION_FP32C): periodic pairs
  * closer than it (minimum image), disk pairs closer than it and disk wall images closer than it to
  * their target are left out of the FP32 sums and evaluated in FP64. radius < 0 selects the default for the population (twice

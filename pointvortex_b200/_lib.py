@@ -68,7 +68,8 @@ REINJECTION = {"none": 0, "independent": 1, "paired": 2}
 class PvPlanInfo(ctypes.Structure):
     _fields_ = [("symmetric", ctypes.c_int), ("rows", ctypes.c_int),
                 ("targets_per_thread", ctypes.c_int), ("chunk", ctypes.c_int),
-                ("symmetric_min_ctas", ctypes.c_int), ("symmetric_targets", ctypes.c_int)]
+                ("symmetric_min_ctas", ctypes.c_int), ("symmetric_targets", ctypes.c_int),
+                ("symmetric_grid_ctas", ctypes.c_int)]
 
 
 TRAJECTORY_ROW_MAX = 192   # PV_TRAJECTORY_ROW_MAX
@@ -177,6 +178,8 @@ SIGNATURES = {
     "pv_set_symmetric_tuning": (_ST, [ctypes.c_int] * 6),
     "pv_get_symmetric_tuning": (_ST, [ctypes.c_int, ctypes.c_int, ctypes.c_int] +
                                 [ctypes.POINTER(ctypes.c_int)] * 3),
+    "pv_set_symmetric_grid": (_ST, [ctypes.c_int] * 4),
+    "pv_get_symmetric_grid": (_ST, [ctypes.c_int] * 3 + [ctypes.POINTER(ctypes.c_int)]),
     "pv_set_profiling": (_ST, [_CTX, ctypes.c_int]),
     "pv_set_wait_limits": (_ST, [_CTX, ctypes.c_int64, ctypes.c_int64]),
     "pv_set_near_field": (_ST, [_CTX, ctypes.c_double]),

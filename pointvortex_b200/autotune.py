@@ -6,7 +6,9 @@ seeded state of that size, keeping the fastest in the library's tables:
   the ordered kernel or the symmetric form, and for the symmetric form the occupancy it is built
   for (periodic FP64: the default, 7 or 8 CTAs per SM) or the targets per lane (plane: 4 or 8).
   A candidate is timed as a whole evaluation of the device state: velocity launches and the
-  reduction of their partial rows.
+  reduction of their partial rows;
+* for the chosen symmetric form, the persistent grid's CTAs per SM (pv_set_symmetric_grid): as
+  many as fit, or down to three fewer (a fuller last round of the work queue can finish sooner).
 
 Results are cached as JSON; the package loads `tuning.json` next to this file when it exists.
 
@@ -53,6 +55,18 @@ def get_symmetric_entry(geometry: int, precision: int, log2_n: int) -> tuple:
     return m.value, c.value, t.value
 
 
+def set_symmetric_grid(geometry: int, precision: int, log2_n: int, ctas_per_sm: int) -> None:
+    rc = lib.pv_set_symmetric_grid(geometry, precision, log2_n, ctas_per_sm)
+    if rc != _lib.PV_OK:
+        raise ValueError(lib.pv_last_error(None).decode())
+
+
+def get_symmetric_grid(geometry: int, precision: int, log2_n: int) -> int:
+    out = ctypes.c_int(0)
+    lib.pv_get_symmetric_grid(geometry, precision, log2_n, ctypes.byref(out))
+    return out.value
+
+
 def load(path: str = DEFAULT_PATH) -> int:
     """Applies a cached table; returns the number of entries."""
     if not os.path.exists(path):
@@ -64,6 +78,8 @@ def load(path: str = DEFAULT_PATH) -> int:
     for e in table.get("symmetric", []):
         set_symmetric_entry(GEOMETRIES[e["geometry"]], PRECISIONS[e["precision"]], e["log2_n"],
                             e["mode"], e.get("min_ctas", 0), e.get("targets", 0))
+        set_symmetric_grid(GEOMETRIES[e["geometry"]], PRECISIONS[e["precision"]], e["log2_n"],
+                           e.get("grid_ctas", 0))
     return len(table.get("entries", [])) + len(table.get("symmetric", []))
 
 
@@ -130,10 +146,37 @@ def tune_symmetric(log2_range=range(11, 17), evals: int = 3) -> list:
                 times[cand] = _time_evaluation(geo, PRECISIONS[prec], n, evals)
             best = min(times, key=times.get)
             set_symmetric_entry(GEOMETRIES[geo], PRECISIONS[prec], b, *best)
+            grid, grid_ms = 0, {}
+            if best[0] == 2:
+                set_symmetric_grid(GEOMETRIES[geo], PRECISIONS[prec], b, 0)
+                fit = _grid_ctas(geo, PRECISIONS[prec], n)
+                grid_ms[fit] = times[best]
+                for c in range(fit - 1, max(fit - 4, 1), -1):
+                    set_symmetric_grid(GEOMETRIES[geo], PRECISIONS[prec], b, c)
+                    grid_ms[c] = _time_evaluation(geo, PRECISIONS[prec], n, evals)
+                best_c = min(grid_ms, key=grid_ms.get)
+                grid = 0 if best_c == fit else best_c
+            set_symmetric_grid(GEOMETRIES[geo], PRECISIONS[prec], b, grid)
             entries.append({"geometry": geo, "precision": prec, "log2_n": b, "mode": best[0],
-                            "min_ctas": best[1], "targets": best[2],
-                            "ms": {"/".join(map(str, c)): v for c, v in times.items()}})
+                            "min_ctas": best[1], "targets": best[2], "grid_ctas": grid,
+                            "ms": {"/".join(map(str, c)): v for c, v in times.items()},
+                            "grid_ms": {str(c): v for c, v in grid_ms.items()}})
     return entries
+
+
+def _grid_ctas(geometry: str, precision: int, n: int) -> int:
+    """CTAs per SM of the symmetric form's grid as the current tables plan it."""
+    from .kernel import InfinitePlaneKernel, PeriodicBoxKernel, VortexSystem
+    if geometry == "infinite":
+        k = InfinitePlaneKernel(0.0, precision=precision)
+        x, y, g = ics.infinite_plane(n, 1)
+    else:
+        k = PeriodicBoxKernel(6.283185307179586, 6.283185307179586, 8, precision=precision)
+        x, y, g = ics.periodic_box(n + n % 2, 1)
+    k.uploadDeviceState(VortexSystem(x, y, g))
+    c = k.statePlan()["symmetric_grid_ctas"]
+    k.close()
+    return c
 
 
 def tune(geometries=("infinite", "periodic", "disk"), precisions=("fp64", "fp32c"),

@@ -1805,6 +1805,7 @@ pv_status pv_state_plan(const pv_context *ctx, pv_plan_info *info) {
     info->chunk = ctx->plan.chunk;
     info->symmetric_min_ctas = ctx->sym.enabled() ? ctx->sym.min_ctas : 0;
     info->symmetric_targets = ctx->sym.enabled() ? ctx->sym.targets : 0;
+    info->symmetric_grid_ctas = ctx->sym.enabled() ? ctx->sym.grid_ctas : 0;
     return PV_OK;
 }
 
@@ -1847,6 +1848,21 @@ pv_status pv_get_symmetric_tuning(int geometry, int precision, int log2_n, int *
     *mode = packed & 15;
     *min_ctas = (packed >> 4) & 15;
     *targets = (packed >> 8) & 15;
+    return PV_OK;
+}
+
+pv_status pv_set_symmetric_grid(int geometry, int precision, int log2_n, int ctas_per_sm) {
+    if (!symmetric_grid_store(geometry, precision, log2_n, ctas_per_sm)) {
+        g_create_error = "invalid symmetric grid entry";
+        return PV_ERROR_INVALID_ARGUMENT;
+    }
+    return PV_OK;
+}
+
+pv_status pv_get_symmetric_grid(int geometry, int precision, int log2_n, int *ctas_per_sm) {
+    if (!ctas_per_sm || log2_n < 0 || log2_n >= 40)
+        return PV_ERROR_INVALID_ARGUMENT;
+    *ctas_per_sm = symmetric_grid_lookup(geometry, precision, size_t(1) << log2_n);
     return PV_OK;
 }
 

@@ -83,6 +83,7 @@ struct SymmetricPlan {
     int geometry = 0;    // GEO_PERIODIC or GEO_INFINITE
     int targets = 1;     // targets per lane off the diagonal (the plane: 4 or 8)
     int min_ctas = 0;    // periodic FP64: the kernel built for 7 or 8 CTAs per SM (0: default)
+    int grid_ctas = 0;   // persistent CTAs per SM (grid / SMs)
     bool enabled() const { return a > 0; }
 };
 constexpr size_t kSymmetricMinN = 2048;       // periodic box below: the ordered kernel
@@ -94,6 +95,10 @@ constexpr size_t kSymmetricPartialBytesMax = static_cast<size_t>(4) << 30;  // b
 SymmetricPlan plan_symmetric(size_t n, int sm_count, int precision, int geometry);
 // The autotuner's table of the symmetric form (pv_set_symmetric_tuning); 0 = the built-in plan.
 int symmetric_tuning_lookup(int geometry, int precision, size_t n);
+// Autotuner table of the symmetric form's persistent grid: CTAs per SM (0: as many as fit), by
+// geometry, precision and floor(log2 N) (pv_set_symmetric_grid).
+int symmetric_grid_lookup(int geometry, int precision, size_t n);
+bool symmetric_grid_store(int geometry, int precision, int log2_n, int ctas_per_sm);
 bool symmetric_tuning_store(int geometry, int precision, int log2_n, int mode, int min_ctas,
                             int targets);
 // p.items packed (I << 16) | J: the diagonal items first, then I < J row by row.

@@ -410,6 +410,30 @@ int symmetric_tuning_lookup(int geometry, int precision, size_t n) {
         std::memory_order_relaxed);
 }
 
+// Persistent CTAs per SM of the symmetric form's grid (0: as many as fit). Fewer CTAs than fit
+// can be faster: the work queue's last round of items is fuller.
+std::atomic<int> g_sym_grid[2][2][40] = {};
+
+int symmetric_grid_lookup(int geometry, int precision, size_t n) {
+    if ((geometry != GEO_INFINITE && geometry != GEO_PERIODIC) || precision < 0 || precision > 1 ||
+        n == 0)
+        return 0;
+    int bucket = 0;
+    while ((size_t(2) << bucket) <= n && bucket < 39)
+        ++bucket;
+    return g_sym_grid[geometry == GEO_PERIODIC ? 1 : 0][precision][bucket].load(
+        std::memory_order_relaxed);
+}
+
+bool symmetric_grid_store(int geometry, int precision, int log2_n, int ctas_per_sm) {
+    if ((geometry != GEO_INFINITE && geometry != GEO_PERIODIC) || precision < 0 || precision > 1 ||
+        log2_n < 0 || log2_n >= 40 || ctas_per_sm < 0 || ctas_per_sm > 16)
+        return false;
+    g_sym_grid[geometry == GEO_PERIODIC ? 1 : 0][precision][log2_n].store(
+        ctas_per_sm, std::memory_order_relaxed);
+    return true;
+}
+
 bool symmetric_tuning_store(int geometry, int precision, int log2_n, int mode, int min_ctas,
                             int targets) {
     if ((geometry != GEO_INFINITE && geometry != GEO_PERIODIC) || precision < 0 || precision > 1 ||
@@ -469,7 +493,10 @@ SymmetricPlan plan_symmetric(size_t n, int sm_count, int precision, int geometry
             p.precision = precision;
             p.geometry = geometry;
             p.targets = targets;
-            p.grid = std::max(sm_count, 1) * resident_ctas(a, kernel_of(p));
+            const int fit = resident_ctas(a, kernel_of(p));
+            const int want = symmetric_grid_lookup(geometry, precision, n);
+            p.grid_ctas = want > 0 && want < fit ? want : fit;
+            p.grid = std::max(sm_count, 1) * p.grid_ctas;
             return p;
         }
     }

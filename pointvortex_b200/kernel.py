@@ -332,7 +332,8 @@ class VelocityKernel:
         return {"symmetric": bool(info.symmetric), "rows": info.rows,
                 "targets_per_thread": info.targets_per_thread, "chunk": info.chunk,
                 "symmetric_min_ctas": info.symmetric_min_ctas,
-                "symmetric_targets": info.symmetric_targets}
+                "symmetric_targets": info.symmetric_targets,
+                "symmetric_grid_ctas": info.symmetric_grid_ctas}
 
     @property
     def evaluationCount(self) -> int:

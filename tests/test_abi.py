@@ -98,6 +98,23 @@ def test_symmetric_tuning_table_round_trip_and_validation():
         autotune.set_symmetric_entry(plane, fp32c, 15, *saved[1])
 
 
+def test_symmetric_grid_table_round_trip_and_validation():
+    """The symmetric form's grid table (pv_set_symmetric_grid): CTAs per SM per geometry,
+    precision and N bucket, 0 for as many as fit; out-of-range entries are rejected. Host-only."""
+    from pointvortex_b200 import autotune
+    saved = autotune.get_symmetric_grid(1, 0, 12)
+    try:
+        autotune.set_symmetric_grid(1, 0, 12, 5)
+        assert autotune.get_symmetric_grid(1, 0, 12) == 5
+        for bad in [(2, 0, 12, 5), (1, 2, 12, 5), (1, 0, 40, 5), (1, 0, 12, -1), (1, 0, 12, 17)]:
+            with pytest.raises(ValueError):
+                autotune.set_symmetric_grid(*bad)
+        autotune.set_symmetric_grid(1, 0, 12, 0)
+        assert autotune.get_symmetric_grid(1, 0, 12) == 0
+    finally:
+        autotune.set_symmetric_grid(1, 0, 12, saved)
+
+
 def test_kernel_stats_struct_matches_the_header():
     """The ctypes mirror of pv_kernel_stats holds PV_KERNEL_KINDS entries per array."""
     from pointvortex_b200 import _lib

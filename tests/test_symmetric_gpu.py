@@ -260,6 +260,34 @@ def test_tuning_table_changes_the_plan_and_keeps_parity(port):
     assert seen == [(False, 0, 0), (True, 7, 1), (True, 8, 1), (True, 0, 2), (True, 0, 1)]
 
 
+def test_grid_table_changes_the_grid_and_keeps_the_result(port):
+    """An entry of the grid table (pv_set_symmetric_grid) changes the persistent grid's CTAs per
+    SM (pv_state_plan), clamped to what fits; the velocities are bit for bit the same, since
+    every (row, vortex) entry is written by one item whichever warp takes it."""
+    from pointvortex_b200 import autotune
+    x, y, g = ics.periodic_box(4096, 93, 2.0)
+    saved = autotune.get_symmetric_entry(1, 0, 12), autotune.get_symmetric_grid(1, 0, 12)
+    out = []
+    try:
+        autotune.set_symmetric_entry(1, 0, 12, 2)
+        for ctas in (0, 3, 16):
+            autotune.set_symmetric_grid(1, 0, 12, ctas)
+            k = pv.PeriodicBoxKernel(2.0, 2.0, 8)
+            k.uploadDeviceState(pv.VortexSystem(x, y, g))
+            out.append((k.statePlan()["symmetric_grid_ctas"], k.evaluateDeviceState()))
+            k.close()
+    finally:
+        autotune.set_symmetric_entry(1, 0, 12, *saved[0])
+        autotune.set_symmetric_grid(1, 0, 12, saved[1])
+    fit = out[0][0]
+    assert fit >= 4 and out[1][0] == 3 and out[2][0] == fit
+    for _, f in out[1:]:
+        assert np.array_equal(f.x, out[0][1].x) and np.array_equal(f.y, out[0][1].y)
+    geo = Geometry("periodic", box_length_x=2.0, box_length_y=2.0)
+    u, v = port.evaluate_range(geo, x, y, g, 0, 64)
+    assert normalized_error(out[1][1].x[:64], out[1][1].y[:64], u, v).max() <= 1e-12
+
+
 def test_periodic_two_targets_per_lane_ragged_against_ordered_and_oracle(port):
     """The periodic kernel with two targets per lane (blocks of 64, table entry targets = 2) on a
     population that ends inside a block: the same velocities as the oracle and the ordered
