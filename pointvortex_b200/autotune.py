@@ -5,8 +5,8 @@ seeded state of that size, keeping the fastest in the library's tables:
 * the once-per-unordered-pair form of the periodic box and the plane (pv_set_symmetric_tuning):
   the ordered kernel or the symmetric form, and for the symmetric form the occupancy it is built
   for (periodic FP64: the default, 7 or 8 CTAs per SM) or the targets per lane (plane: 4 or 8).
-  A candidate is timed as a whole evaluation of the device state: velocity launches and the
-  reduction of their partial rows;
+  A candidate is timed per evaluation inside DOPRI5 steps of the device state (velocity launches,
+  stage kernels, the captured attempt), the way the steppers use it;
 * for the chosen symmetric form, the persistent grid's CTAs per SM (pv_set_symmetric_grid): as
   many as fit, or down to three fewer (a fuller last round of the work queue can finish sooner).
 
@@ -106,8 +106,12 @@ def _time_plan(geometry: str, precision: int, n: int, per_thread: int, evals: in
     return ms / max(timed, 1)
 
 
-def _time_evaluation(geometry: str, precision: int, n: int, evals: int) -> float:
-    """ms per evaluation of the device state (velocity launches + reduction), current tables."""
+def _time_steps(geometry: str, precision: int, n: int, steps: int) -> float:
+    """ms per evaluation inside DOPRI5 steps of the device state (the captured attempt with its
+    stage kernels and programmatic launches, as the steppers run it), current tables. An
+    evaluation timed alone can rank plans differently: a grid that leaves SM room lets the next
+    kernels of a step start early beside it."""
+    import time
     from .kernel import InfinitePlaneKernel, PeriodicBoxKernel, VortexSystem
     if geometry == "infinite":
         k = InfinitePlaneKernel(0.0, precision=precision)
@@ -116,14 +120,17 @@ def _time_evaluation(geometry: str, precision: int, n: int, evals: int) -> float
         k = PeriodicBoxKernel(6.283185307179586, 6.283185307179586, 8, precision=precision)
         x, y, g = ics.periodic_box(n + n % 2, 1)
     k.uploadDeviceState(VortexSystem(x, y, g))
-    k.evaluateDeviceState()
-    k.setProfiling(True)
-    k.resetKernelStats()
-    for _ in range(evals):
-        k.evaluateDeviceState()
-    st = k.kernelStats()
+    dt = 1e-3
+    for _ in range(3):
+        dt = k.deviceDopri5Step(dt, 1e-12, 1e-9, 1e-12, 0.1).suggestedTimeStep
+    e0 = k.evaluationCount
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        dt = k.deviceDopri5Step(dt, 1e-12, 1e-9, 1e-12, 0.1).suggestedTimeStep
+    t1 = time.perf_counter()
+    evals = k.evaluationCount - e0
     k.close()
-    return (st["velocity"][2] + st["near"][2] + st["stage"][2]) / max(st["stage"][1], 1)
+    return (t1 - t0) * 1e3 / max(evals, 1)
 
 
 # candidates of the symmetric-form table: (mode, min_ctas, targets)
@@ -136,14 +143,16 @@ SYMMETRIC_CANDIDATES = {
 
 
 def tune_symmetric(log2_range=range(11, 17), evals: int = 3) -> list:
+    """Each candidate timed per evaluation inside DOPRI5 steps (_time_steps), 3 + evals steps."""
     entries = []
+    steps = max(evals, 3)
     for (geo, prec), cands in SYMMETRIC_CANDIDATES.items():
         for b in log2_range:
             n = 1 << b
             times = {}
             for cand in cands:
                 set_symmetric_entry(GEOMETRIES[geo], PRECISIONS[prec], b, *cand)
-                times[cand] = _time_evaluation(geo, PRECISIONS[prec], n, evals)
+                times[cand] = _time_steps(geo, PRECISIONS[prec], n, steps)
             best = min(times, key=times.get)
             set_symmetric_entry(GEOMETRIES[geo], PRECISIONS[prec], b, *best)
             grid, grid_ms = 0, {}
@@ -153,7 +162,7 @@ def tune_symmetric(log2_range=range(11, 17), evals: int = 3) -> list:
                 grid_ms[fit] = times[best]
                 for c in range(fit - 1, max(fit - 4, 1), -1):
                     set_symmetric_grid(GEOMETRIES[geo], PRECISIONS[prec], b, c)
-                    grid_ms[c] = _time_evaluation(geo, PRECISIONS[prec], n, evals)
+                    grid_ms[c] = _time_steps(geo, PRECISIONS[prec], n, steps)
                 best_c = min(grid_ms, key=grid_ms.get)
                 grid = 0 if best_c == fit else best_c
             set_symmetric_grid(GEOMETRIES[geo], PRECISIONS[prec], b, grid)
