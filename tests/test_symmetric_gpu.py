@@ -134,11 +134,13 @@ def plane_kernel_with(x, y, g, core=0.0):
 
 @pytest.mark.parametrize("n,core", [(16384, 0.0), (16400, 0.0), (20000, 0.05)])
 def test_plane_symmetric_matches_oracle(reference, n, core):
-    """16400 and 20000 end in a ragged block (128-vortex blocks); 0.05 is a core radius."""
+    """16400 and 20000 end in a ragged block (blocks of 32 vortices per target of a lane, 128 or
+    256 as the tables choose); 0.05 is a core radius."""
     x, y, g = ics.infinite_plane(n, 70 + n)
     k = plane_kernel_with(x, y, g, core)
     plan = k.statePlan()
-    assert plan["symmetric"] and plan["rows"] == (n + 127) // 128
+    block = 32 * plan["symmetric_targets"]  # 4 or 8 targets per lane, as the tables choose
+    assert plan["symmetric"] and plan["rows"] == (n + block - 1) // block
     vel = k.evaluateDeviceState()
     u, v = reference.evaluate(Geometry("infinite", core_radius=core), x, y, g)
     assert normalized_error(vel.x, vel.y, u, v).max() <= 1e-12
@@ -151,7 +153,8 @@ def test_plane_symmetric_wide_against_ordered_and_oracle(port, n):
     x, y, g = ics.infinite_plane(n, 17)
     k = plane_kernel_with(x, y, g)
     plan = k.statePlan()
-    assert plan["symmetric"] and plan["rows"] == (n + 255) // 256
+    block = 32 * plan["symmetric_targets"]
+    assert plan["symmetric"] and plan["rows"] == (n + block - 1) // block
     vel = k.evaluateDeviceState()
     ordered = k.evaluate(x, y, g)
     assert normalized_error(vel.x, vel.y, ordered.x, ordered.y).max() <= 1e-12
@@ -209,8 +212,8 @@ def test_plane_fp32c_symmetric_against_the_fp64_oracle(port, n):
     k = pv.InfinitePlaneKernel(0.0, precision=_lib.PRECISION_FP32C)
     k.uploadDeviceState(pv.VortexSystem(x, y, g))
     plan = k.statePlan()
-    assert plan["symmetric"] and plan["rows"] == (n + (255 if n >= 32768 else 127)) // (
-        256 if n >= 32768 else 128)
+    block = 32 * plan["symmetric_targets"]
+    assert plan["symmetric"] and plan["rows"] == (n + block - 1) // block
     vel = k.evaluateDeviceState()
     ref = pv.InfinitePlaneKernel(0.0).evaluate(x, y, g)
     err = normalized_error(vel.x, vel.y, ref.x, ref.y)
