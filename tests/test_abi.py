@@ -122,3 +122,23 @@ def test_kernel_stats_struct_matches_the_header():
     kinds = int(re.search(r"#define PV_KERNEL_KINDS (\d+)", text).group(1))
     assert len(_lib.KERNEL_KINDS) == kinds
     assert ctypes.sizeof(_lib.PvKernelStats) == kinds * 3 * 8
+
+
+def test_committed_tuning_table_loads_every_field():
+    """The package's tuning.json (the autotuner's output) applies each of its entries: targets per
+    thread, the symmetric form's choice and its grid size. Host-only."""
+    import json
+
+    from pointvortex_b200 import autotune
+    with open(autotune.DEFAULT_PATH) as f:
+        table = json.load(f)
+    assert autotune.load() == len(table["entries"]) + len(table["symmetric"])
+    for e in table["entries"]:
+        got = autotune.get_entry(autotune.GEOMETRIES[e["geometry"]],
+                                 autotune.PRECISIONS[e["precision"]], e["log2_n"])
+        assert got == e["per_thread"], e
+    for e in table["symmetric"]:
+        geo, prec = autotune.GEOMETRIES[e["geometry"]], autotune.PRECISIONS[e["precision"]]
+        assert autotune.get_symmetric_entry(geo, prec, e["log2_n"]) == (
+            e["mode"], e.get("min_ctas", 0), e.get("targets", 0)), e
+        assert autotune.get_symmetric_grid(geo, prec, e["log2_n"]) == e.get("grid_ctas", 0), e
