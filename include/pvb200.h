@@ -289,6 +289,8 @@ typedef struct pv_batch_sim_info {
     uint64_t rejected_steps;
     uint32_t population;
     int failure;                /* PV_FAILURE_* when status is the integrator's failure */
+    int targets_per_thread;     /* of its ordered work items (pv_set_batch_tuning); 0 when it takes
+                                   the once-per-unordered-pair items */
 } pv_batch_sim_info;
 
 typedef struct pv_batch_totals {
@@ -317,6 +319,13 @@ pv_status pv_batch_result(pv_batch *batch, uint32_t id, double *x, double *y, si
 pv_status pv_batch_release(pv_batch *batch, uint32_t id);
 pv_status pv_batch_status(pv_batch *batch, pv_batch_totals *totals);
 pv_status pv_batch_stream(const pv_batch *batch, void **stream);
+/* Autotuner table of the batch's ordered work items: targets per thread (1, 2 or 4; 4 not for the
+ * periodic box; 0 restores the default of 4 for the plane, 1 for the box and 2 for the disk) for a
+ * geometry, a precision and populations with floor(log2 N) == log2_n. Process-wide; read when a
+ * simulation is admitted (pv_batch_add), so a simulation's work items, like its results, depend
+ * only on its own geometry, precision and N. pv_get_batch_tuning returns the value in effect. */
+pv_status pv_set_batch_tuning(int geometry, int precision, int log2_n, int per_thread);
+pv_status pv_get_batch_tuning(int geometry, int precision, int log2_n, int *per_thread);
 
 /* ---- allocation-free evaluation (no counterpart in the reference) ------------------------ */
 

@@ -96,7 +96,7 @@ class PvBatchSimInfo(ctypes.Structure):
     _fields_ = [("state", ctypes.c_int), ("status", ctypes.c_int), ("time", ctypes.c_double),
                 ("suggested_time_step", ctypes.c_double), ("accepted_steps", ctypes.c_uint64),
                 ("rejected_steps", ctypes.c_uint64), ("population", ctypes.c_uint32),
-                ("failure", ctypes.c_int)]
+                ("failure", ctypes.c_int), ("targets_per_thread", ctypes.c_int)]
 
 
 class PvBatchTotals(ctypes.Structure):
@@ -180,6 +180,8 @@ SIGNATURES = {
                                 [ctypes.POINTER(ctypes.c_int)] * 3),
     "pv_set_symmetric_grid": (_ST, [ctypes.c_int] * 4),
     "pv_get_symmetric_grid": (_ST, [ctypes.c_int] * 3 + [ctypes.POINTER(ctypes.c_int)]),
+    "pv_set_batch_tuning": (_ST, [ctypes.c_int] * 4),
+    "pv_get_batch_tuning": (_ST, [ctypes.c_int] * 3 + [ctypes.POINTER(ctypes.c_int)]),
     "pv_set_profiling": (_ST, [_CTX, ctypes.c_int]),
     "pv_set_wait_limits": (_ST, [_CTX, ctypes.c_int64, ctypes.c_int64]),
     "pv_set_near_field": (_ST, [_CTX, ctypes.c_double]),

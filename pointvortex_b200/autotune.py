@@ -8,11 +8,15 @@ seeded state of that size, keeping the fastest in the library's tables:
   A candidate is timed per evaluation inside DOPRI5 steps of the device state (velocity launches,
   stage kernels, the captured attempt), the way the steppers use it;
 * for the chosen symmetric form, the persistent grid's CTAs per SM (pv_set_symmetric_grid): as
-  many as fit, or down to three fewer (a fuller last round of the work queue can finish sooner).
+  many as fit, or down to three fewer (a fuller last round of the work queue can finish sooner);
+* the batch engine's ordered work items: 1, 2 or 4 targets per thread (pv_set_batch_tuning),
+  timed per DOPRI5 attempt of a batch of simulations of that size (as many as make about 2^26
+  pair interactions per evaluation, at most 512), so the choice is made where the grid is full.
 
 Results are cached as JSON; the package loads `tuning.json` next to this file when it exists.
 
     python -m pointvortex_b200.autotune [--out path] [--min-log2 6] [--max-log2 16]
+    python -m pointvortex_b200.autotune --only batch [--out path]   # replace the batch part only
 """
 from __future__ import annotations
 
@@ -67,6 +71,18 @@ def get_symmetric_grid(geometry: int, precision: int, log2_n: int) -> int:
     return out.value
 
 
+def set_batch_entry(geometry: int, precision: int, log2_n: int, per_thread: int) -> None:
+    rc = lib.pv_set_batch_tuning(geometry, precision, log2_n, per_thread)
+    if rc != _lib.PV_OK:
+        raise ValueError("invalid batch tuning entry")
+
+
+def get_batch_entry(geometry: int, precision: int, log2_n: int) -> int:
+    out = ctypes.c_int(0)
+    lib.pv_get_batch_tuning(geometry, precision, log2_n, ctypes.byref(out))
+    return out.value
+
+
 def load(path: str = DEFAULT_PATH) -> int:
     """Applies a cached table; returns the number of entries."""
     if not os.path.exists(path):
@@ -80,7 +96,10 @@ def load(path: str = DEFAULT_PATH) -> int:
                             e["mode"], e.get("min_ctas", 0), e.get("targets", 0))
         set_symmetric_grid(GEOMETRIES[e["geometry"]], PRECISIONS[e["precision"]], e["log2_n"],
                            e.get("grid_ctas", 0))
-    return len(table.get("entries", [])) + len(table.get("symmetric", []))
+    for e in table.get("batch", []):
+        set_batch_entry(GEOMETRIES[e["geometry"]], PRECISIONS[e["precision"]], e["log2_n"],
+                        e["per_thread"])
+    return sum(len(table.get(k, [])) for k in ("entries", "symmetric", "batch"))
 
 
 def _time_plan(geometry: str, precision: int, n: int, per_thread: int, evals: int) -> float:
@@ -188,6 +207,61 @@ def _grid_ctas(geometry: str, precision: int, n: int) -> int:
     return c
 
 
+# targets per thread of the batch's ordered items, by geometry (pv_set_batch_tuning allows these)
+BATCH_CANDIDATES = {"infinite": (1, 2, 4), "periodic": (1, 2), "disk": (1, 2, 4)}
+
+
+def _time_batch(geometry: str, precision: str, n: int, attempts: int) -> float | None:
+    """ms per DOPRI5 attempt of a batch of equal simulations of population n under the current
+    batch table, or None where the simulations take the once-per-unordered-pair items (the table
+    does not apply). Two untimed attempts first; the simulations run far from their end time."""
+    import time
+    from .batch import Batch, geometry_params
+    sims = max(1, min(512, (1 << 26) // (n * n)))
+    b = Batch(sims * (n + 256) + 256, sims, max_steps=1 << 30)
+    try:
+        for s in range(sims):
+            if geometry == "periodic":
+                st = ics.periodic_box(n + n % 2, 100 + s)
+            elif geometry == "disk":
+                st = ics.disk(n, 100 + s, 1.0, 0.95, gaussian=False)
+            else:
+                st = ics.infinite_plane(n, 100 + s)
+            sid = b.add(geometry_params(geometry, precision=precision), *st, 1e6, dt=1e-4,
+                        atol=1e-10, rtol=1e-8)
+            if b.info(sid).targetsPerThread == 0:
+                return None
+        b.advance(2)
+        t0 = time.perf_counter()
+        b.advance(attempts)
+        return (time.perf_counter() - t0) * 1e3 / attempts
+    finally:
+        b.close()
+
+
+def tune_batch(log2_range=range(5, 16), attempts: int = 6) -> list:
+    """Each candidate of BATCH_CANDIDATES timed per attempt (_time_batch); the fastest is kept."""
+    entries = []
+    for geo, cands in BATCH_CANDIDATES.items():
+        for prec in PRECISIONS:
+            for b in log2_range:
+                times = {}
+                for t in cands:
+                    set_batch_entry(GEOMETRIES[geo], PRECISIONS[prec], b, t)
+                    ms = _time_batch(geo, prec, 1 << b, attempts)
+                    if ms is None:
+                        break
+                    times[t] = ms
+                if not times:
+                    set_batch_entry(GEOMETRIES[geo], PRECISIONS[prec], b, 0)
+                    continue
+                best = min(times, key=times.get)
+                set_batch_entry(GEOMETRIES[geo], PRECISIONS[prec], b, best)
+                entries.append({"geometry": geo, "precision": prec, "log2_n": b, "per_thread": best,
+                                "ms": {str(k): v for k, v in times.items()}})
+    return entries
+
+
 def tune(geometries=("infinite", "periodic", "disk"), precisions=("fp64", "fp32c"),
          log2_range=range(6, 17), evals: int = 3) -> dict:
     entries = []
@@ -201,7 +275,8 @@ def tune(geometries=("infinite", "periodic", "disk"), precisions=("fp64", "fp32c
                 entries.append({"geometry": geo, "precision": prec, "log2_n": b, "per_thread": best,
                                 "ms": {str(k): v for k, v in times.items()}})
     symmetric = tune_symmetric(range(max(11, log2_range.start), log2_range.stop), evals)
-    return {"entries": entries, "symmetric": symmetric}
+    batch = tune_batch(range(max(5, log2_range.start - 1), min(16, log2_range.stop)))
+    return {"entries": entries, "symmetric": symmetric, "batch": batch}
 
 
 def main(argv=None) -> int:
@@ -210,11 +285,22 @@ def main(argv=None) -> int:
     ap.add_argument("--min-log2", type=int, default=6)
     ap.add_argument("--max-log2", type=int, default=16)
     ap.add_argument("--evals", type=int, default=3)
+    ap.add_argument("--only", choices=["batch"], default=None,
+                    help="tune only the batch table, keeping the rest of the table at --out")
     args = ap.parse_args(argv)
-    table = tune(log2_range=range(args.min_log2, args.max_log2 + 1), evals=args.evals)
+    if args.only == "batch":
+        table = {}
+        if os.path.exists(args.out):
+            with open(args.out) as f:
+                table = json.load(f)
+        load(args.out)
+        table["batch"] = tune_batch()
+    else:
+        table = tune(log2_range=range(args.min_log2, args.max_log2 + 1), evals=args.evals)
     with open(args.out, "w") as f:
         json.dump(table, f, indent=1)
-    print(f"wrote {len(table['entries'])} entries to {args.out}")
+    print(f"wrote {sum(len(table.get(k, [])) for k in ('entries', 'symmetric', 'batch'))} "
+          f"entries to {args.out}")
     return 0
 
 

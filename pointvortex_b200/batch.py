@@ -40,6 +40,7 @@ class SimInfo:
     rejectedSteps: int
     population: int
     failure: int = 0
+    targetsPerThread: int = 0  # of the ordered work items; 0: once-per-unordered-pair items
 
     @property
     def reason(self) -> str:
@@ -126,7 +127,7 @@ class Batch:
         self._check(lib.pv_batch_info(self._b, sid, ctypes.byref(i)))
         return SimInfo(STATES.get(i.state, "free"), i.status, i.time, i.suggested_time_step,
                        int(i.accepted_steps), int(i.rejected_steps), int(i.population),
-                       int(i.failure))
+                       int(i.failure), int(i.targets_per_thread))
 
     def result(self, sid: int):
         n = self.info(sid).population

@@ -29,10 +29,12 @@
 #include "pv_symmetric.cuh"
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstring>
 #include <map>
 #include <string>
+#include <type_traits>
 #include <vector>
 
 using namespace pvb;
@@ -44,10 +46,28 @@ constexpr int kTileB = 256;          // sources per shared-memory stage
 constexpr size_t kAlign = 256;       // arena granularity (elements)
 constexpr int kCounters = 16;        // work-queue counters: two launches per velocity stage
 
-// Targets per thread by geometry (as the single-simulation plan uses them): the plane's cheap
-// pairs share each staged source among 4 targets, the disk's among 2.
-__host__ __device__ constexpr int targets_per_thread(int geometry) {
+// Default targets per thread of the ordered items by geometry: the plane's cheap pairs share
+// each staged source among 4 targets, the disk's among 2. The autotuner's batch table
+// (pv_set_batch_tuning) overrides it per geometry, precision and floor(log2 N).
+constexpr int default_targets_per_thread(int geometry) {
     return geometry == GEO_INFINITE ? 4 : (geometry == GEO_DISK ? 2 : 1);
+}
+// Targets per thread the ordered items may hold, by geometry: 1, 2 or 4; the periodic pair's
+// registers allow 1 or 2 beside the other forms in the one persistent kernel.
+constexpr bool batch_targets_allowed(int geometry, int per_thread) {
+    return per_thread == 1 || per_thread == 2 || (per_thread == 4 && geometry != GEO_PERIODIC);
+}
+
+// The batch table: targets per thread by (geometry, precision, floor(log2 N)); 0 = the default.
+// Atomic entries: a table update may run beside admissions on other host threads.
+std::atomic<int> g_batch_tuning[3][2][40] = {};
+
+int batch_targets_for(int geometry, int precision, size_t n) {
+    int bucket = 0;
+    while ((size_t(2) << bucket) <= n && bucket < 39)
+        ++bucket;
+    const int t = g_batch_tuning[geometry][precision][bucket].load(std::memory_order_relaxed);
+    return t ? t : default_targets_per_thread(geometry);
 }
 // Sources per work item, a function of the population only (so a simulation's summation order
 // never depends on its batch): 512 up to N = 16384, then N/32 rounded up to 512.
@@ -65,6 +85,7 @@ struct SimDesc {
     unsigned chunk;
     int precision;                // PV_PRECISION_*
     int symmetric;                // periodic, evaluated once per unordered pair (either form)
+    int per_thread;               // targets per thread of the ordered items (1, 2 or 4)
 };
 
 struct SimControl {
@@ -570,43 +591,38 @@ __global__ void __launch_bounds__(kBlock, 5) batch_velocity_kernel(const Velocit
         }
         const size_t src0 = static_cast<size_t>(it.chunk) * d.chunk;
         const size_t src1 = min(src0 + d.chunk, static_cast<size_t>(d.n));
-        const size_t per_block = static_cast<size_t>(kBlock) * targets_per_thread(s_geo.geometry);
+        const size_t per_block = static_cast<size_t>(kBlock) * d.per_thread;
         const size_t blk0 = static_cast<size_t>(it.tb) * per_block;
         const size_t blk1 = min(blk0 + per_block, static_cast<size_t>(d.n));
         const size_t out0 = static_cast<size_t>(it.chunk) * d.pad_n;
-        if (PREC == PV_PRECISION_FP32C) {
-            switch (s_geo.geometry) {
-            case GEO_INFINITE:
-                run_item32<GEO_INFINITE, 4>(s_geo, px, py, sgs, src0, src1, blk0, blk1, pu, pv,
-                                            out0, s_x, s_y, s_g, s_f, s_fi, s_gf, bars, seq,
-                                            a.timeout_status, timed_out);
-                break;
-            case GEO_PERIODIC:
-                run_item32<GEO_PERIODIC, 1>(s_geo, px, py, sgs, src0, src1, blk0, blk1, pu, pv,
-                                            out0, s_x, s_y, s_g, s_f, s_fi, s_gf, bars, seq,
-                                            a.timeout_status, timed_out);
-                break;
-            default:
-                run_item32<GEO_DISK, 2>(s_geo, px, py, sgs, src0, src1, blk0, blk1, pu, pv, out0,
-                                        s_x, s_y, s_g, s_f, s_fi, s_gf, bars, seq, a.timeout_status,
-                                        timed_out);
-                break;
+        // one instantiation per (geometry, targets per thread) the batch table allows
+        auto ordered = [&](auto geo, auto per_thread) {
+            constexpr int G = decltype(geo)::value, T = decltype(per_thread)::value;
+            if constexpr (PREC == PV_PRECISION_FP32C) {
+                run_item32<G, T>(s_geo, px, py, sgs, src0, src1, blk0, blk1, pu, pv, out0, s_x, s_y,
+                                 s_g, s_f, s_fi, s_gf, bars, seq, a.timeout_status, timed_out);
+            } else {
+                using Pair = std::conditional_t<G == GEO_INFINITE, InfinitePair,
+                             std::conditional_t<G == GEO_PERIODIC, PeriodicPair, DiskPair>>;
+                run_item<Pair, T>(s_geo, px, py, sgs, src0, src1, blk0, blk1, pu, pv, out0, s_x,
+                                  s_y, s_g, bars, seq, a.timeout_status, timed_out);
             }
-        } else {
-            switch (s_geo.geometry) {
-            case GEO_INFINITE:
-                run_item<InfinitePair, 4>(s_geo, px, py, sgs, src0, src1, blk0, blk1, pu, pv, out0,
-                                          s_x, s_y, s_g, bars, seq, a.timeout_status, timed_out);
-                break;
-            case GEO_PERIODIC:
-                run_item<PeriodicPair, 1>(s_geo, px, py, sgs, src0, src1, blk0, blk1, pu, pv, out0,
-                                          s_x, s_y, s_g, bars, seq, a.timeout_status, timed_out);
-                break;
-            default:
-                run_item<DiskPair, 2>(s_geo, px, py, sgs, src0, src1, blk0, blk1, pu, pv, out0,
-                                      s_x, s_y, s_g, bars, seq, a.timeout_status, timed_out);
-                break;
-            }
+        };
+        using I0 = std::integral_constant<int, GEO_INFINITE>;
+        using I1 = std::integral_constant<int, GEO_PERIODIC>;
+        using I2 = std::integral_constant<int, GEO_DISK>;
+        using T1 = std::integral_constant<int, 1>;
+        using T2 = std::integral_constant<int, 2>;
+        using T4 = std::integral_constant<int, 4>;
+        switch (s_geo.geometry * 8 + d.per_thread) {
+        case GEO_INFINITE * 8 + 1: ordered(I0{}, T1{}); break;
+        case GEO_INFINITE * 8 + 2: ordered(I0{}, T2{}); break;
+        case GEO_INFINITE * 8 + 4: ordered(I0{}, T4{}); break;
+        case GEO_PERIODIC * 8 + 1: ordered(I1{}, T1{}); break;
+        case GEO_PERIODIC * 8 + 2: ordered(I1{}, T2{}); break;
+        case GEO_DISK * 8 + 1: ordered(I2{}, T1{}); break;
+        case GEO_DISK * 8 + 2: ordered(I2{}, T2{}); break;
+        default: ordered(I2{}, T4{}); break;  // admission allows no other combination
         }
         if (timed_out)
             return;
@@ -955,7 +971,7 @@ pv_status rebuild_tables(pv_batch *b) {
                     cost[q].push_back(w * ni * nj);
                 }
         } else {
-            const unsigned per_block = kBlock * targets_per_thread(d.g.geometry);
+            const unsigned per_block = kBlock * d.per_thread;
             const unsigned tbs = (d.n + per_block - 1) / per_block;
             for (unsigned tb = 0; tb < tbs; ++tb)
                 for (unsigned ch = 0; ch < d.num_chunks; ++ch) {
@@ -1277,6 +1293,7 @@ pv_status pv_batch_add(pv_batch *b, const pv_params *params, const double *x, co
     d.chunk = static_cast<unsigned>(chunk);
     d.precision = params->precision;
     d.symmetric = symmetric ? 1 : 0;
+    d.per_thread = batch_targets_for(g.geometry, params->precision, n);
     b->descs[slot] = d;
     b->sim_ranges[slot] = {off, pad};
     b->part_ranges[slot] = {poff, pad * chunks};
@@ -1373,6 +1390,23 @@ pv_status pv_batch_info(pv_batch *b, uint32_t id, pv_batch_sim_info *info) {
     info->rejected_steps = c.rejections_total;
     info->population = b->descs[id].n;
     info->failure = c.status == ST_DOPRI_FAILED ? c.failure : PV_FAILURE_NONE;
+    info->targets_per_thread = b->descs[id].symmetric ? 0 : b->descs[id].per_thread;
+    return PV_OK;
+}
+
+pv_status pv_set_batch_tuning(int geometry, int precision, int log2_n, int per_thread) {
+    if (geometry < 0 || geometry > 2 || precision < 0 || precision > 1 || log2_n < 0 ||
+        log2_n >= 40 || (per_thread != 0 && !batch_targets_allowed(geometry, per_thread)))
+        return PV_ERROR_INVALID_ARGUMENT;
+    g_batch_tuning[geometry][precision][log2_n].store(per_thread, std::memory_order_relaxed);
+    return PV_OK;
+}
+
+pv_status pv_get_batch_tuning(int geometry, int precision, int log2_n, int *per_thread) {
+    if (!per_thread || geometry < 0 || geometry > 2 || precision < 0 || precision > 1 ||
+        log2_n < 0 || log2_n >= 40)
+        return PV_ERROR_INVALID_ARGUMENT;
+    *per_thread = batch_targets_for(geometry, precision, size_t(1) << log2_n);
     return PV_OK;
 }
 

@@ -115,6 +115,29 @@ def test_symmetric_grid_table_round_trip_and_validation():
         autotune.set_symmetric_grid(1, 0, 12, saved)
 
 
+def test_batch_tuning_table_round_trip_and_validation():
+    """The batch table (pv_set_batch_tuning): targets per thread of the ordered work items per
+    geometry, precision and N bucket; 0 restores the default (plane 4, box 1, disk 2), and the
+    box takes no 4. pv_get_batch_tuning returns the value in effect. Host-only."""
+    from pointvortex_b200 import autotune
+    keys = [(0, 0, 10), (1, 1, 9), (2, 0, 12)]
+    saved = [autotune.get_batch_entry(*k) for k in keys]
+    try:
+        for k, default in zip(keys, (4, 1, 2)):
+            autotune.set_batch_entry(*k, 0)
+            assert autotune.get_batch_entry(*k) == default
+        for k, t in zip(keys, (1, 2, 4)):
+            autotune.set_batch_entry(*k, t)
+            assert autotune.get_batch_entry(*k) == t
+        for bad in [(1, 0, 10, 4), (0, 0, 10, 3), (3, 0, 10, 1), (0, 2, 10, 1), (0, 0, 40, 1),
+                    (0, 0, -1, 1)]:
+            with pytest.raises(ValueError):
+                autotune.set_batch_entry(*bad)
+    finally:
+        for k, t in zip(keys, saved):
+            autotune.set_batch_entry(*k, t)
+
+
 def test_kernel_stats_struct_matches_the_header():
     """The ctypes mirror of pv_kernel_stats holds PV_KERNEL_KINDS entries per array."""
     from pointvortex_b200 import _lib
@@ -132,7 +155,7 @@ def test_committed_tuning_table_loads_every_field():
     from pointvortex_b200 import autotune
     with open(autotune.DEFAULT_PATH) as f:
         table = json.load(f)
-    assert autotune.load() == len(table["entries"]) + len(table["symmetric"])
+    assert autotune.load() == sum(len(table.get(k, [])) for k in ("entries", "symmetric", "batch"))
     for e in table["entries"]:
         got = autotune.get_entry(autotune.GEOMETRIES[e["geometry"]],
                                  autotune.PRECISIONS[e["precision"]], e["log2_n"])
@@ -142,3 +165,6 @@ def test_committed_tuning_table_loads_every_field():
         assert autotune.get_symmetric_entry(geo, prec, e["log2_n"]) == (
             e["mode"], e.get("min_ctas", 0), e.get("targets", 0)), e
         assert autotune.get_symmetric_grid(geo, prec, e["log2_n"]) == e.get("grid_ctas", 0), e
+    for e in table.get("batch", []):
+        geo, prec = autotune.GEOMETRIES[e["geometry"]], autotune.PRECISIONS[e["precision"]]
+        assert autotune.get_batch_entry(geo, prec, e["log2_n"]) == e["per_thread"], e

@@ -173,3 +173,55 @@ def test_fp32c_batch_tracks_fp64():
     for spec, (i32, (x32, y32)), (i64, (x64, y64)) in zip(forms, fp32, fp64):
         assert i32.state == i64.state == "done", spec
         assert np.max(np.hypot(x32 - x64, y32 - y64)) < 1e-6, spec
+
+
+@pytest.fixture
+def batch_table():
+    """Sets batch table entries (pv_set_batch_tuning) and restores the values in effect before."""
+    from pointvortex_b200 import autotune
+    saved = {}
+
+    def set_entry(boundary, precision, n, per_thread):
+        key = (autotune.GEOMETRIES[boundary], autotune.PRECISIONS[precision], n.bit_length() - 1)
+        saved.setdefault(key, autotune.get_batch_entry(*key))
+        autotune.set_batch_entry(*key, per_thread)
+
+    yield set_entry
+    for key, value in saved.items():
+        autotune.set_batch_entry(*key, value)
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32c"])
+def test_batch_table_sets_targets_per_thread(batch_table, precision):
+    """An entry of the batch table changes the simulation's work items (targets per thread of its
+    ordered items) and, where every tile runs the same pair arithmetic, nothing of its result: a
+    target's sum over a chunk runs over the same sources in the same order for any T. The FP32C
+    disk's tiles that hold the target block itself take the scalar pair form, so its result moves
+    within the compensated form's own error when the block size changes: the bound is the one
+    test_fp32c_batch_tracks_fp64 holds it to against FP64 (a vortex near the wall moved 1.1e-7
+    between 2 and 4 targets per thread, the others 1e-10)."""
+    cases = [("infinite", 1000, 4, 0.002, (1, 2, 4)), ("periodic", 700, 5, 0.002, (1, 2)),
+             ("disk", 600, 15, 0.002, (1, 2, 4))]
+    for boundary, n, seed, t_end, cands in cases:
+        runs = {}
+        for t in cands:
+            batch_table(boundary, precision, n, t)
+            (info, (x, y)), = run_batch([(boundary, n, seed, t_end, precision)])
+            assert info.state == "done" and info.targetsPerThread == t, (boundary, t, info)
+            runs[t] = (info.acceptedSteps, x, y)
+        steps0, x0, y0 = runs[cands[0]]
+        for t in cands[1:]:
+            steps, x, y = runs[t]
+            if precision == "fp32c" and boundary == "disk":
+                assert np.max(np.hypot(x - x0, y - y0)) < 1e-6, (boundary, t)
+            else:
+                assert steps == steps0 and np.array_equal(x, x0) and np.array_equal(y, y0), \
+                    (boundary, precision, t)
+
+
+def test_batch_table_skips_the_symmetric_items(batch_table):
+    """Periodic FP64 simulations from N = 2048 take the once-per-unordered-pair items, which hold
+    no targets per thread: their info reports 0 whatever the table says."""
+    batch_table("periodic", "fp64", 2100, 2)
+    (info, _), = run_batch([("periodic", 2100, 7, 0.0004)], capacity=40000)
+    assert info.state == "done" and info.targetsPerThread == 0
