@@ -211,14 +211,23 @@ def _grid_ctas(geometry: str, precision: int, n: int) -> int:
 BATCH_CANDIDATES = {"infinite": (1, 2, 4), "periodic": (1, 2), "disk": (1, 2, 4)}
 
 
+def batch_room(n: int) -> tuple:
+    """(simulations, arena vortices, partial chunks per vortex slot) of the tuner's batch of
+    population n: as many simulations as make about 2^26 pair interactions per evaluation (at
+    most 512), each with room for the most partial rows a simulation of that size can take: one
+    per 128-block in the once-per-unordered-pair form, else one per source chunk (at most 33)."""
+    sims = max(1, min(512, (1 << 26) // (n * n)))
+    return sims, sims * (n + 256) + 256, max(-(-n // 128), 64) + 1
+
+
 def _time_batch(geometry: str, precision: str, n: int, attempts: int) -> float | None:
     """ms per DOPRI5 attempt of a batch of equal simulations of population n under the current
     batch table, or None where the simulations take the once-per-unordered-pair items (the table
     does not apply). Two untimed attempts first; the simulations run far from their end time."""
     import time
     from .batch import Batch, geometry_params
-    sims = max(1, min(512, (1 << 26) // (n * n)))
-    b = Batch(sims * (n + 256) + 256, sims, max_steps=1 << 30)
+    sims, vortices, chunks = batch_room(n)
+    b = Batch(vortices, sims, max_steps=1 << 30, partial_factor=chunks)
     try:
         for s in range(sims):
             if geometry == "periodic":

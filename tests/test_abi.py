@@ -138,6 +138,23 @@ def test_batch_tuning_table_round_trip_and_validation():
             autotune.set_batch_entry(*k, t)
 
 
+def test_batch_tuner_sizes_its_batches():
+    """The batch tuner's batches admit their simulations: per simulation pad(N) = N rounded up
+    to 256 arena elements and pad(N) x rows partial elements, rows = ceil(N/128) for the
+    once-per-unordered-pair items or ceil(N/chunk) for ordered ones (chunk 512 up to N = 16384,
+    then N/32 rounded up to 512), against the arena and the partial buffer (arena x chunks)."""
+    from pointvortex_b200 import autotune
+    for log2_n in range(5, 17):
+        for n in (1 << log2_n, (1 << log2_n) + 77):
+            sims, vortices, chunks = autotune.batch_room(n)
+            pad = -(-n // 256) * 256
+            chunk = 512 if n <= 16384 else -(-(n // 32) // 512) * 512
+            rows = max(-(-n // 128), -(-n // chunk))
+            assert sims * pad <= vortices
+            assert sims * pad * rows <= vortices * chunks
+            assert sims * n * n <= max(1 << 26, n * n)
+
+
 def test_kernel_stats_struct_matches_the_header():
     """The ctypes mirror of pv_kernel_stats holds PV_KERNEL_KINDS entries per array."""
     from pointvortex_b200 import _lib
