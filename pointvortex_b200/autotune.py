@@ -74,7 +74,7 @@ def get_symmetric_grid(geometry: int, precision: int, log2_n: int) -> int:
 def set_batch_entry(geometry: int, precision: int, log2_n: int, per_thread: int) -> None:
     rc = lib.pv_set_batch_tuning(geometry, precision, log2_n, per_thread)
     if rc != _lib.PV_OK:
-        raise ValueError("invalid batch tuning entry")
+        raise ValueError(lib.pv_last_error(None).decode())
 
 
 def get_batch_entry(geometry: int, precision: int, log2_n: int) -> int:

@@ -1396,8 +1396,10 @@ pv_status pv_batch_info(pv_batch *b, uint32_t id, pv_batch_sim_info *info) {
 
 pv_status pv_set_batch_tuning(int geometry, int precision, int log2_n, int per_thread) {
     if (geometry < 0 || geometry > 2 || precision < 0 || precision > 1 || log2_n < 0 ||
-        log2_n >= 40 || (per_thread != 0 && !batch_targets_allowed(geometry, per_thread)))
+        log2_n >= 40 || (per_thread != 0 && !batch_targets_allowed(geometry, per_thread))) {
+        set_thread_error("invalid batch tuning entry");
         return PV_ERROR_INVALID_ARGUMENT;
+    }
     g_batch_tuning[geometry][precision][log2_n].store(per_thread, std::memory_order_relaxed);
     return PV_OK;
 }
