@@ -608,10 +608,12 @@ def run_ensemble(n_sims: int = 512, budget: int = 10, seed: int = 7,
     workloads are chaotic, so unbudgeted work per simulation is unbounded)."""
     specs = ensemble_specs(n_sims, seed)
     results, attempts, elapsed = solve_batch(specs, budget, precision)
-    finished, reasons = {}, {}
+    finished, reasons, per_thread = {}, {}, {}
     projected = {}
     for (info, _), (geo, n, _) in zip(results, specs):
         finished[info.state] = finished.get(info.state, 0) + 1
+        kind = f"{geo}:{info.targetsPerThread}"  # 0: once-per-unordered-pair items
+        per_thread[kind] = per_thread.get(kind, 0) + 1
         key = f"{geo}:{info.reason}"
         reasons[key] = reasons.get(key, 0) + 1
         if info.state == "budget" and info.time > 0:
@@ -622,6 +624,7 @@ def run_ensemble(n_sims: int = 512, budget: int = 10, seed: int = 7,
             "attempts": attempts, "seconds": elapsed, "budgeted_solves_per_s": n_sims / elapsed,
             "pair_interactions_per_s": pairs / elapsed, "states": finished,
             "stop_reasons": dict(sorted(reasons.items())),
+            "targets_per_thread": dict(sorted(per_thread.items())),
             "projected_steps_to_t_end_median": {g: float(np.median(v)) for g, v in projected.items()},
             "dtype": "f64" if precision == "fp64" else "f32 compensated (f64 state and control)",
             "note": "one arena, lock-step DOPRI5 attempts, CUDA-graph replay per attempt; a "
