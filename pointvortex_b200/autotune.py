@@ -249,7 +249,11 @@ def _time_batch(geometry: str, precision: str, n: int, attempts: int) -> float |
 
 
 def tune_batch(log2_range=range(5, 16), attempts: int = 6) -> list:
-    """Each candidate of BATCH_CANDIDATES timed per attempt (_time_batch); the fastest is kept."""
+    """Each candidate of BATCH_CANDIDATES timed per attempt (_time_batch); the fastest is kept.
+    A size whose batch cannot be admitted (CapacityError: the device's memory) keeps the default
+    and is reported on stderr; the other sizes are still tuned."""
+    import sys
+    from .batch import CapacityError
     entries = []
     for geo, cands in BATCH_CANDIDATES.items():
         for prec in PRECISIONS:
@@ -257,7 +261,13 @@ def tune_batch(log2_range=range(5, 16), attempts: int = 6) -> list:
                 times = {}
                 for t in cands:
                     set_batch_entry(GEOMETRIES[geo], PRECISIONS[prec], b, t)
-                    ms = _time_batch(geo, prec, 1 << b, attempts)
+                    try:
+                        ms = _time_batch(geo, prec, 1 << b, attempts)
+                    except CapacityError as exc:
+                        print(f"batch tuning: {geo} {prec} N = 2^{b} skipped: {exc}",
+                              file=sys.stderr)
+                        times = {}
+                        break
                     if ms is None:
                         break
                     times[t] = ms

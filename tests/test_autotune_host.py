@@ -57,6 +57,24 @@ def test_tune_batch_keeps_the_fastest(monkeypatch, restore_batch_table):
     assert all(t in autotune.BATCH_CANDIDATES[g] for g, _, _, t in calls)
 
 
+def test_tune_batch_skips_a_size_it_cannot_admit(monkeypatch, restore_batch_table, capsys):
+    from pointvortex_b200.batch import CapacityError
+    _fake_timings(monkeypatch)
+    timed = autotune._time_batch
+
+    def fake(geometry, precision, n, attempts):
+        if geometry == "disk" and n == 4096:
+            raise CapacityError("the batch arena has no room for this population")
+        return timed(geometry, precision, n, attempts)
+
+    monkeypatch.setattr(autotune, "_time_batch", fake)
+    entries = autotune.tune_batch(range(11, 13), attempts=2)
+    keys = {(e["geometry"], e["log2_n"]) for e in entries}
+    assert ("disk", 12) not in keys and ("disk", 11) in keys and ("infinite", 12) in keys
+    assert autotune.get_batch_entry(2, 0, 12) == 2  # the default
+    assert "disk fp64 N = 2^12 skipped" in capsys.readouterr().err
+
+
 def test_only_batch_replaces_the_batch_part(monkeypatch, tmp_path, restore_batch_table):
     _fake_timings(monkeypatch)
     monkeypatch.setattr(autotune, "tune_batch",
